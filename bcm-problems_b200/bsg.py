@@ -1,0 +1,280 @@
+"""Python binding of libbsg.so, the B200 solver library (C ABI in include/bslib_gpu.h).
+
+This module is a thin ctypes layer: PyTorch provides device buffers and the
+CUDA stream, every computation runs in the library's own sm_100a kernels.
+There is no CPU fallback -- if the library or a GPU is missing, the calls
+raise.
+
+Naming follows Bslib: ``Matrix`` is a device CSMatrixR / CSMatrixRS,
+``Factor`` an IC2 / ILU2 factor, ``Param`` the CSlvParam fields of the path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_SO = os.path.join(HERE, "libbsg.so")
+
+OK = 0
+ERR_ARG, ERR_PIVOT, ERR_WORKSPACE, ERR_BREAKDOWN, ERR_CUDA, ERR_TIMEOUT, ERR_NOCONV, ERR_UNSUPPORTED, ERR_NOMEM = \
+    -1, -2, -3, -4, -5, -6, -7, -8, -9
+
+
+class BsgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Param(C.Structure):
+    """Mirror of ``bsg_param`` (CSlvParam fields of the path + GPU extensions)."""
+    _fields_ = [
+        ("msglev", C.c_int), ("fcttyp", C.c_int), ("ordtype", C.c_int), ("memory", C.c_double),
+        ("tau1", C.c_double), ("tau2", C.c_double), ("theta", C.c_double), ("sclmin", C.c_double),
+        ("pivmin", C.c_double), ("ittype", C.c_int), ("sttype", C.c_int), ("niter", C.c_int),
+        ("eps", C.c_double), ("ichk", C.c_int), ("nitperf", C.c_int), ("resfin", C.c_double),
+        ("density", C.c_double), ("density2", C.c_double), ("timefct", C.c_double), ("timeitr", C.c_double),
+        ("precision", C.c_int), ("trisolve", C.c_int), ("nsweeps", C.c_int), ("krylov", C.c_int),
+        ("restart", C.c_int), ("true_residual", C.c_int), ("learned", C.c_void_p), ("resrec", C.c_double),
+        ("pad", C.c_int * 4),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbsg.so (raises when it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_SO):
+        raise RuntimeError(f"{LIB_SO} is not built; run __graft_entry__.build()")
+    L = C.CDLL(LIB_SO)
+    vp, ip, dp, i_ = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int
+    pp = C.POINTER(C.c_void_p)
+    sig = {
+        "bsg_param_default": (None, [C.POINTER(Param)]),
+        "bsg_last_error": (C.c_char_p, []),
+        "bsg_version": (C.c_char_p, []),
+        "bsg_create": (i_, [pp, i_, vp]),
+        "bsg_destroy": (i_, [vp]),
+        "bsg_sync": (i_, [vp]),
+        "bsg_mat_csr": (i_, [vp, i_, ip, ip, dp, i_, pp]),
+        "bsg_mat_csr_dev": (i_, [vp, i_, vp, vp, vp, i_, pp]),
+        "bsg_mat_bsr": (i_, [vp, i_, i_, ip, ip, dp, i_, pp]),
+        "bsg_mat_free": (i_, [vp]),
+        "bsg_mat_info": (i_, [vp, ip, ip, ip]),
+        "bsg_mvm_dev": (i_, [vp, vp, vp, vp]),
+        "bsg_mvm": (i_, [vp, vp, dp, dp]),
+        "bsg_mvm_multi_dev": (i_, [vp, vp, i_, vp, vp]),
+        "bsg_fct_ich2": (i_, [vp, vp, C.POINTER(Param), pp]),
+        "bsg_fct_ilu2": (i_, [vp, vp, C.POINTER(Param), pp]),
+        "bsg_fct_to_fp32": (i_, [vp]),
+        "bsg_fct_export": (i_, [vp, ip, ip, ip, dp, dp]),
+        "bsg_fct_info": (i_, [vp, ip, ip, ip, ip, dp, dp]),
+        "bsg_fct_free": (i_, [vp]),
+        "bsg_solve_l_dev": (i_, [vp, vp, i_, i_, vp, vp]),
+        "bsg_solve_u_dev": (i_, [vp, vp, i_, i_, vp, vp]),
+        "bsg_pcg_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
+        "bsg_gmres_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
+        "bsg_solve_symm_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
+        "bsg_solver_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
+    }
+    for name, (rt, at) in sig.items():
+        f = getattr(L, name)
+        f.restype = rt
+        f.argtypes = at
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != OK:
+        raise BsgError(rc, lib().bsg_last_error().decode(errors="replace"))
+
+
+def _ip(a):
+    return np.ascontiguousarray(a, dtype=np.int32).ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _dp(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.POINTER(C.c_double))
+
+
+def default_param(**kw):
+    p = Param()
+    lib().bsg_param_default(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(t):
+    """Device pointer of a contiguous CUDA tensor."""
+    import torch
+    assert isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """A device + stream.  By default it runs on PyTorch's current stream, so
+    library kernels are ordered with the tensors the caller hands in."""
+
+    def __init__(self, device=0, stream=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("bsg needs a CUDA device (no CPU fallback)")
+        torch.cuda.set_device(device)
+        if stream is None:
+            stream = torch.cuda.current_stream(device).cuda_stream
+        self.h = C.c_void_p()
+        _check(lib().bsg_create(C.byref(self.h), device, C.c_void_p(stream)))
+        self.device = device
+
+    def sync(self):
+        _check(lib().bsg_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().bsg_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Matrix:
+    """Device copy of a CSMatrixR (bs == 1) or 3x3 CSMatrixRS (bs == 3)."""
+
+    def __init__(self, ctx, n, ia, ja, a, bs=1, symm_upper=False):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        self.n, self.bs = n, bs
+        self._keep = (np.ascontiguousarray(ia, np.int32), np.ascontiguousarray(ja, np.int32),
+                      np.ascontiguousarray(a, np.float64))
+        ia_, ja_, a_ = self._keep
+        if bs == 1:
+            _check(lib().bsg_mat_csr(ctx.h, n, _ip(ia_), _ip(ja_), _dp(a_), int(symm_upper), C.byref(self.h)))
+        else:
+            _check(lib().bsg_mat_bsr(ctx.h, n, bs, _ip(ia_), _ip(ja_), _dp(a_), int(symm_upper), C.byref(self.h)))
+        self._keep = None
+
+    @classmethod
+    def from_system(cls, ctx, sysm, symm_upper=False):
+        s = sysm.upper() if symm_upper else sysm
+        return cls(ctx, s.n, s.ia, s.ja, s.a, s.bs, symm_upper)
+
+    def info(self):
+        n, bs, nnz = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().bsg_mat_info(self.h, C.byref(n), C.byref(bs), C.byref(nnz)))
+        return n.value, bs.value, nnz.value
+
+    def mvm(self, x, y):
+        """y = A x, both CUDA float64 tensors of length n*bs."""
+        _check(lib().bsg_mvm_dev(self.ctx.h, self.h, _ptr(x), _ptr(y)))
+
+    def mvm_multi(self, X, Y):
+        """Y = A X for X of shape (nrhs, n*bs)."""
+        _check(lib().bsg_mvm_multi_dev(self.ctx.h, self.h, X.shape[0], _ptr(X), _ptr(Y)))
+
+    def mvm_host(self, x):
+        y = np.zeros(self.n * self.bs)
+        _check(lib().bsg_mvm(self.ctx.h, self.h, _dp(x), _dp(y)))
+        return y
+
+    def free(self):
+        if self.h:
+            lib().bsg_mat_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Factor:
+    """IC2 (kind 'ich2') or ILU2 (kind 'ilu2') factor of a Matrix, on the device."""
+
+    def __init__(self, ctx, mat, kind="ich2", param=None):
+        self.ctx = ctx
+        self.param = param if param is not None else default_param(ordtype=0, fcttyp=2)
+        self.h = C.c_void_p()
+        f = lib().bsg_fct_ich2 if kind == "ich2" else lib().bsg_fct_ilu2
+        _check(f(ctx.h, mat.h, C.byref(self.param), C.byref(self.h)))
+        self.kind = kind
+
+    def info(self):
+        n, nnz, ll, lu = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        d1, d2 = C.c_double(), C.c_double()
+        _check(lib().bsg_fct_info(self.h, C.byref(n), C.byref(nnz), C.byref(ll), C.byref(lu), C.byref(d1),
+                                  C.byref(d2)))
+        return dict(n=n.value, nnz=nnz.value, levels_l=ll.value, levels_u=lu.value, density=d1.value,
+                    density2=d2.value)
+
+    def export(self):
+        """Factor in the reference layout: (iu, ju, l, u), inverse pivots first."""
+        info = self.info()
+        n, nnz = info["n"], info["nnz"]
+        iu = np.zeros(n + 1, np.int32)
+        ju = np.zeros(nnz, np.int32)
+        l = np.zeros(nnz)
+        u = np.zeros(nnz)
+        _check(lib().bsg_fct_export(self.h, None, iu.ctypes.data_as(C.POINTER(C.c_int)),
+                                    ju.ctypes.data_as(C.POINTER(C.c_int)), l.ctypes.data_as(C.POINTER(C.c_double)),
+                                    u.ctypes.data_as(C.POINTER(C.c_double))))
+        return iu, ju, l, u
+
+    def to_fp32(self):
+        _check(lib().bsg_fct_to_fp32(self.h))
+
+    def solve_l(self, x, y, mode=0, nsweeps=3):
+        _check(lib().bsg_solve_l_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))
+
+    def solve_u(self, x, y, mode=0, nsweeps=3):
+        _check(lib().bsg_solve_u_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))
+
+    def free(self):
+        if self.h:
+            lib().bsg_fct_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def pcg(ctx, mat, fct, b, x, param):
+    """PCG on device tensors (x holds the initial guess, overwritten)."""
+    _check(lib().bsg_pcg_dev(ctx.h, mat.h, fct.h, _ptr(b), _ptr(x), C.byref(param)))
+    return param
+
+
+def gmres(ctx, mat, fct, b, x, param):
+    """GMRES(restart) / FGMRES(restart) (param.krylov == 2) on device tensors."""
+    _check(lib().bsg_gmres_dev(ctx.h, mat.h, fct.h, _ptr(b), _ptr(x), C.byref(param)))
+    return param
+
+
+def solve_symm(ctx, n, ia, ja, a, b, param):
+    """CSVector::SolveSymm(CSMatrixR&) counterpart: upper-stored SPD CSR, host buffers."""
+    x = np.zeros(n)
+    _check(lib().bsg_solve_symm_csr(ctx.h, n, _ip(ia), _ip(ja), _dp(a), _dp(b), _dp(x), C.byref(param)))
+    return x
+
+
+def solver(ctx, n, ia, ja, a, b, param):
+    """CSVector::Solver(CSMatrixR&) counterpart: full CSR, ILU2 + GMRES, host buffers."""
+    x = np.zeros(n)
+    _check(lib().bsg_solver_csr(ctx.h, n, _ip(ia), _ip(ja), _dp(a), _dp(b), _dp(x), C.byref(param)))
+    return x

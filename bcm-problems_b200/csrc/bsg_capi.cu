@@ -1,0 +1,505 @@
+// C ABI of libbsg.so (declared in include/bslib_gpu.h): contexts, device
+// matrices and factors, and the host-buffer drivers that stand in for
+// CSVector::SolveSymm / CSVector::Solver.
+#include "bsg_internal.cuh"
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <new>
+#include <vector>
+
+int bsg_expand_symmetric(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz_up, int **ia_o,
+                         int **ja_o, double **a_o, int *nnz_o);
+int bsg_combine_lu(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz, int **iu_o,
+                   int **ju_o, double **al_o, double **au_o, int *nnz_o);
+int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nnz, int **it_o, int **jt_o,
+                         int **perm_o, int *nnz_o);
+int bsg_choose_group(double mean_row);
+int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
+int bsg_fct_make_fp32(bsg_fct *f);
+
+static thread_local char g_err[512] = "";
+
+int bsg_set_error(int code, const char *msg) {
+	std::snprintf(g_err, sizeof(g_err), "%s", msg ? msg : "");
+	return code;
+}
+int bsg_set_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+	std::snprintf(g_err, sizeof(g_err), "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
+	              cudaGetErrorString(e), what, file, line);
+	if (e == cudaErrorMemoryAllocation) return BSG_ERR_NOMEM;
+	return BSG_ERR_CUDA;
+}
+
+extern "C" const char *bsg_last_error(void) { return g_err; }
+extern "C" const char *bsg_version(void) { return "bsg 0.1 sm_100a"; }
+
+// Reads the device status word after the work queued so far.
+int bsg_check_devstat(bsg_ctx *c) {
+	bsg_devstat h;
+	cudaError_t e = cudaMemcpyAsync(&h, c->d_stat, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+	if (e != cudaSuccess) return bsg_set_cuda_error(e, "device status", __FILE__, __LINE__);
+	if (h.code == 0) return BSG_OK;
+	char msg[160];
+	switch (h.code) {
+	case BSG_ERR_PIVOT: std::snprintf(msg, sizeof msg, " Ich2: Diagonal pivot is nonpositive (row %d)", h.where); break;
+	case BSG_ERR_WORKSPACE: std::snprintf(msg, sizeof msg, " Insufficient workspace in Ich2/Ilu2 (row %d)", h.where); break;
+	case BSG_ERR_TIMEOUT: std::snprintf(msg, sizeof msg, "device wait limit reached (index %d)", h.where); break;
+	case BSG_ERR_ARG: std::snprintf(msg, sizeof msg, "malformed matrix: missing or misplaced diagonal (row %d)", h.where); break;
+	default: std::snprintf(msg, sizeof msg, "device error %d at %d", h.code, h.where);
+	}
+	cudaMemsetAsync(c->d_stat, 0, sizeof(bsg_devstat), c->stream);
+	return bsg_set_error(h.code, msg);
+}
+
+extern "C" void bsg_param_default(bsg_param *p) {
+	std::memset(p, 0, sizeof(*p));
+	// CSlvParam() (Bslib/slvparam.h:121-214)
+	p->msglev = 0;
+	p->fcttyp = 1;
+	p->ordtype = 1;
+	p->memory = 1.0;
+	p->tau1 = 1.0e-2;
+	p->tau2 = 1.0e-4;
+	p->theta = 1.0e-1;
+	p->sclmin = 1.0e-8;
+	p->pivmin = 1.0e-8;
+	p->ittype = 2;
+	p->sttype = 2;
+	p->niter = 1000;
+	p->eps = 1.0e-9;
+	p->ichk = 5;
+	p->resfin = 1.0e10;
+	// GPU-path defaults
+	p->precision = 0;
+	p->trisolve = 0;
+	p->nsweeps = 3;
+	p->krylov = 0;
+	p->restart = 50;
+	p->true_residual = 1;
+	p->learned = nullptr;
+}
+
+extern "C" int bsg_create(bsg_ctx **out, int device, void *stream) {
+	if (!out) return bsg_set_error(BSG_ERR_ARG, "bsg_create: null output");
+	*out = nullptr;
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || ndev == 0) return bsg_set_error(BSG_ERR_CUDA, "no CUDA device");
+	if (device < 0 || device >= ndev) return bsg_set_error(BSG_ERR_ARG, "bsg_create: bad device");
+	BSG_CUDA(cudaSetDevice(device));
+	bsg_ctx *c = new (std::nothrow) bsg_ctx();
+	if (!c) return bsg_set_error(BSG_ERR_NOMEM, "bsg_create");
+	c->device = device;
+	if (stream) {
+		c->stream = (cudaStream_t)stream;
+		c->own_stream = false;
+	} else {
+		BSG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+		c->own_stream = true;
+	}
+	c->n_partials = 8192;
+	BSG_CUDA(cudaMalloc(&c->d_stat, sizeof(bsg_devstat)));
+	BSG_CUDA(cudaMalloc(&c->d_scalars, 64 * sizeof(double)));
+	BSG_CUDA(cudaMalloc(&c->d_partials, c->n_partials * sizeof(double)));
+	BSG_CUDA(cudaMalloc(&c->d_counters, 16 * sizeof(unsigned)));
+	BSG_CUDA(cudaMemset(c->d_stat, 0, sizeof(bsg_devstat)));
+	BSG_CUDA(cudaMemset(c->d_scalars, 0, 64 * sizeof(double)));
+	BSG_CUDA(cudaMemset(c->d_counters, 0, 16 * sizeof(unsigned)));
+	BSG_CUDA(cudaMallocHost(&c->h_pinned, 64 * sizeof(double)));
+	BSG_CUDA(cudaEventCreate(&c->ev0));
+	BSG_CUDA(cudaEventCreate(&c->ev1));
+	c->spmv_group = 0;
+	*out = c;
+	return BSG_OK;
+}
+
+extern "C" int bsg_destroy(bsg_ctx *c) {
+	if (!c) return BSG_OK;
+	cudaSetDevice(c->device);
+	cudaStreamSynchronize(c->stream);
+	cudaFree(c->d_stat);
+	cudaFree(c->d_scalars);
+	cudaFree(c->d_partials);
+	cudaFree(c->d_counters);
+	cudaFreeHost(c->h_pinned);
+	cudaEventDestroy(c->ev0);
+	cudaEventDestroy(c->ev1);
+	if (c->own_stream) cudaStreamDestroy(c->stream);
+	delete c;
+	return BSG_OK;
+}
+
+extern "C" int bsg_sync(bsg_ctx *c) {
+	if (!c) return bsg_set_error(BSG_ERR_ARG, "bsg_sync: null context");
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	return bsg_check_devstat(c);
+}
+
+// ---- matrices -------------------------------------------------------------
+
+static int check_csr_host(int n, const int *ia, const int *ja, int bs) {
+	if (n < 0 || !ia) return bsg_set_error(BSG_ERR_ARG, "bad CSR: n < 0 or ia == NULL");
+	if (ia[0] != 0) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia[0] != 0");
+	for (int i = 0; i < n; i++) {
+		if (ia[i + 1] < ia[i]) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia not monotone");
+	}
+	int nz = ia[n];
+	if (nz > 0 && !ja) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ja == NULL");
+	for (int k = 0; k < nz; k++)
+		if (ja[k] < 0 || ja[k] >= n) return bsg_set_error(BSG_ERR_ARG, "bad CSR: column index out of range");
+	(void)bs;
+	return BSG_OK;
+}
+
+// Symmetric input must hold the upper triangle only, diagonal first.
+static int check_upper_host(int n, const int *ia, const int *ja) {
+	for (int i = 0; i < n; i++) {
+		if (ia[i + 1] == ia[i] || ja[ia[i]] != i)
+			return bsg_set_error(BSG_ERR_ARG, "symmetric input: every row must start with its diagonal");
+		for (int k = ia[i]; k < ia[i + 1]; k++)
+			if (ja[k] < i) return bsg_set_error(BSG_ERR_ARG, "symmetric input: entry below the diagonal");
+	}
+	return BSG_OK;
+}
+
+// Finish a point matrix whose device full storage is set: upper split,
+// static contributor lists, SpMV group size.
+static int mat_finish_point(bsg_mat *m, const int *d_up_ia, const int *d_up_ja, const double *d_up_a, int nnz_up,
+                            bool from_upper) {
+	bsg_ctx *c = m->ctx;
+	int rc;
+	if (from_upper) {
+		// the upper input already is the split pattern (al == au)
+		BSG_CUDA(cudaMallocAsync(&m->d_iu, sizeof(int) * (m->n + 1), c->stream));
+		BSG_CUDA(cudaMallocAsync(&m->d_ju, sizeof(int) * (nnz_up > 0 ? nnz_up : 1), c->stream));
+		BSG_CUDA(cudaMallocAsync(&m->d_al, sizeof(double) * (nnz_up > 0 ? nnz_up : 1), c->stream));
+		BSG_CUDA(cudaMemcpyAsync(m->d_iu, d_up_ia, sizeof(int) * (m->n + 1), cudaMemcpyDeviceToDevice, c->stream));
+		BSG_CUDA(cudaMemcpyAsync(m->d_ju, d_up_ja, sizeof(int) * nnz_up, cudaMemcpyDeviceToDevice, c->stream));
+		BSG_CUDA(cudaMemcpyAsync(m->d_al, d_up_a, sizeof(double) * nnz_up, cudaMemcpyDeviceToDevice, c->stream));
+		m->d_au = m->d_al;
+		m->nnz_up = nnz_up;
+	} else {
+		rc = bsg_combine_lu(c, m->n, m->d_ia, m->d_ja, m->d_a, m->nnz, &m->d_iu, &m->d_ju, &m->d_al, &m->d_au,
+		                    &m->nnz_up);
+		if (rc) return rc;
+	}
+	int nt = 0;
+	rc = bsg_strict_transpose(c, m->n, m->d_iu, m->d_ju, m->nnz_up, &m->d_it, &m->d_jt, nullptr, &nt);
+	if (rc) return rc;
+	m->group = bsg_choose_group(m->n > 0 ? (double)m->nnz / m->n : 1.0);
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	return BSG_OK;
+}
+
+static int mat_csr_common(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int symm_upper,
+                          bool host, bsg_mat **out) {
+	if (!c || !out) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_csr: null argument");
+	*out = nullptr;
+	int nz = 0;
+	if (host) {
+		int rc = check_csr_host(n, ia, ja, 1);
+		if (!rc && symm_upper) rc = check_upper_host(n, ia, ja);
+		if (rc) return rc;
+		nz = ia[n];
+	} else {
+		BSG_CUDA(cudaMemcpy(&nz, ia + n, sizeof(int), cudaMemcpyDeviceToHost));
+	}
+	BSG_CUDA(cudaSetDevice(c->device));
+	bsg_mat *m = new (std::nothrow) bsg_mat();
+	if (!m) return bsg_set_error(BSG_ERR_NOMEM, "bsg_mat_csr");
+	m->ctx = c;
+	m->n = n;
+	m->bs = 1;
+	m->symm = symm_upper ? 1 : 0;
+	cudaStream_t s = c->stream;
+	cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+	int *d_ia, *d_ja;
+	double *d_a;
+	BSG_CUDA(cudaMallocAsync(&d_ia, sizeof(int) * (n + 1), s));
+	BSG_CUDA(cudaMallocAsync(&d_ja, sizeof(int) * (nz > 0 ? nz : 1), s));
+	BSG_CUDA(cudaMallocAsync(&d_a, sizeof(double) * (nz > 0 ? nz : 1), s));
+	BSG_CUDA(cudaMemcpyAsync(d_ia, ia, sizeof(int) * (n + 1), kind, s));
+	if (nz > 0) {
+		BSG_CUDA(cudaMemcpyAsync(d_ja, ja, sizeof(int) * nz, kind, s));
+		BSG_CUDA(cudaMemcpyAsync(d_a, a, sizeof(double) * nz, kind, s));
+	}
+	int rc;
+	if (symm_upper) {
+		rc = bsg_expand_symmetric(c, n, d_ia, d_ja, d_a, nz, &m->d_ia, &m->d_ja, &m->d_a, &m->nnz);
+		if (!rc) rc = mat_finish_point(m, d_ia, d_ja, d_a, nz, true);
+		cudaFreeAsync(d_ia, s);
+		cudaFreeAsync(d_ja, s);
+		cudaFreeAsync(d_a, s);
+	} else {
+		m->d_ia = d_ia;
+		m->d_ja = d_ja;
+		m->d_a = d_a;
+		m->nnz = nz;
+		rc = mat_finish_point(m, nullptr, nullptr, nullptr, 0, false);
+	}
+	if (rc) {
+		bsg_mat_free(m);
+		return rc;
+	}
+	*out = m;
+	return BSG_OK;
+}
+
+extern "C" int bsg_mat_csr(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int symm_upper,
+                           bsg_mat **out) {
+	return mat_csr_common(c, n, ia, ja, a, symm_upper, true, out);
+}
+extern "C" int bsg_mat_csr_dev(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int symm_upper,
+                               bsg_mat **out) {
+	return mat_csr_common(c, n, ia, ja, a, symm_upper, false, out);
+}
+
+extern "C" int bsg_mat_bsr(bsg_ctx *c, int nsup, int bs, const int *ia, const int *ja, const double *a,
+                           int symm_upper, bsg_mat **out) {
+	if (!c || !out) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_bsr: null argument");
+	if (bs == 1) return bsg_mat_csr(c, nsup, ia, ja, a, symm_upper, out);
+	if (bs != 3) return bsg_set_error(BSG_ERR_UNSUPPORTED, "bsg_mat_bsr: block size must be 1 or 3");
+	int rc = check_csr_host(nsup, ia, ja, bs);
+	if (!rc && symm_upper) rc = check_upper_host(nsup, ia, ja);
+	if (rc) return rc;
+	const int nz = ia[nsup];
+	// host: expand symmetric blocks (A(j,i) = A(i,j)^T) and go row-major
+	std::vector<int> fia, fja;
+	std::vector<double> fa;
+	if (symm_upper) {
+		std::vector<int> cnt(nsup + 1, 0);
+		for (int i = 0; i < nsup; i++)
+			for (int k = ia[i]; k < ia[i + 1]; k++) {
+				cnt[i + 1]++;
+				if (ja[k] != i) cnt[ja[k] + 1]++;
+			}
+		for (int i = 0; i < nsup; i++) cnt[i + 1] += cnt[i];
+		fia = cnt;
+		fja.resize(cnt[nsup]);
+		fa.resize((size_t)cnt[nsup] * 9);
+		std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+		for (int i = 0; i < nsup; i++)
+			for (int k = ia[i]; k < ia[i + 1]; k++) {
+				int j = ja[k];
+				const double *blk = a + (size_t)k * 9; // column-major (r,c) at 3c+r
+				int p = pos[i]++;
+				fja[p] = j;
+				for (int r = 0; r < 3; r++)
+					for (int cc = 0; cc < 3; cc++) fa[(size_t)p * 9 + 3 * r + cc] = blk[3 * cc + r];
+				if (j != i) {
+					int q = pos[j]++;
+					fja[q] = i;
+					for (int r = 0; r < 3; r++)
+						for (int cc = 0; cc < 3; cc++) fa[(size_t)q * 9 + 3 * r + cc] = blk[3 * r + cc];
+				}
+			}
+	} else {
+		fia.assign(ia, ia + nsup + 1);
+		fja.assign(ja, ja + nz);
+		fa.resize((size_t)nz * 9);
+		for (int k = 0; k < nz; k++)
+			for (int r = 0; r < 3; r++)
+				for (int cc = 0; cc < 3; cc++) fa[(size_t)k * 9 + 3 * r + cc] = a[(size_t)k * 9 + 3 * cc + r];
+	}
+	bsg_mat *m = new (std::nothrow) bsg_mat();
+	if (!m) return bsg_set_error(BSG_ERR_NOMEM, "bsg_mat_bsr");
+	m->ctx = c;
+	m->n = nsup;
+	m->bs = 3;
+	m->symm = symm_upper ? 1 : 0;
+	m->nnz = (int)fja.size();
+	cudaStream_t s = c->stream;
+	BSG_CUDA(cudaMallocAsync(&m->d_ia, sizeof(int) * (nsup + 1), s));
+	BSG_CUDA(cudaMallocAsync(&m->d_ja, sizeof(int) * (m->nnz > 0 ? m->nnz : 1), s));
+	BSG_CUDA(cudaMallocAsync(&m->d_a, sizeof(double) * 9 * (m->nnz > 0 ? m->nnz : 1), s));
+	BSG_CUDA(cudaMemcpyAsync(m->d_ia, fia.data(), sizeof(int) * (nsup + 1), cudaMemcpyHostToDevice, s));
+	BSG_CUDA(cudaMemcpyAsync(m->d_ja, fja.data(), sizeof(int) * m->nnz, cudaMemcpyHostToDevice, s));
+	BSG_CUDA(cudaMemcpyAsync(m->d_a, fa.data(), sizeof(double) * 9 * m->nnz, cudaMemcpyHostToDevice, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	m->group = 32;
+	*out = m;
+	return BSG_OK;
+}
+
+extern "C" int bsg_mat_free(bsg_mat *m) {
+	if (!m) return BSG_OK;
+	cudaStream_t s = m->ctx->stream;
+	if (m->d_au && m->d_au != m->d_al) cudaFreeAsync(m->d_au, s);
+	for (void *p : {(void *)m->d_ia, (void *)m->d_ja, (void *)m->d_a, (void *)m->d_iu, (void *)m->d_ju,
+	                (void *)m->d_al, (void *)m->d_it, (void *)m->d_jt})
+		if (p) cudaFreeAsync(p, s);
+	cudaStreamSynchronize(s);
+	delete m;
+	return BSG_OK;
+}
+
+extern "C" int bsg_mat_info(const bsg_mat *m, int *n, int *bs, int *nnz) {
+	if (!m) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_info: null matrix");
+	if (n) *n = m->n;
+	if (bs) *bs = m->bs;
+	if (nnz) *nnz = m->nnz;
+	return BSG_OK;
+}
+
+extern "C" int bsg_mvm_dev(bsg_ctx *c, const bsg_mat *m, const double *x, double *y) {
+	if (!c || !m || !x || !y) return bsg_set_error(BSG_ERR_ARG, "bsg_mvm_dev: null argument");
+	int rc = bsg_spmm_launch(m, 1, x, y, (long long)m->n * m->bs, c->stream);
+	return rc ? bsg_set_error(rc, "SpMV launch failed") : BSG_OK;
+}
+
+extern "C" int bsg_mvm_multi_dev(bsg_ctx *c, const bsg_mat *m, int nrhs, const double *X, double *Y) {
+	if (!c || !m || !X || !Y || nrhs < 1) return bsg_set_error(BSG_ERR_ARG, "bsg_mvm_multi_dev: bad argument");
+	int rc = bsg_spmm_launch(m, nrhs, X, Y, (long long)m->n * m->bs, c->stream);
+	return rc ? bsg_set_error(rc, "SpMM launch failed") : BSG_OK;
+}
+
+extern "C" int bsg_mvm(bsg_ctx *c, const bsg_mat *m, const double *x, double *y) {
+	if (!c || !m || !x || !y) return bsg_set_error(BSG_ERR_ARG, "bsg_mvm: null argument");
+	const size_t N = (size_t)m->n * m->bs;
+	double *dx, *dy;
+	BSG_CUDA(cudaMallocAsync(&dx, sizeof(double) * N, c->stream));
+	BSG_CUDA(cudaMallocAsync(&dy, sizeof(double) * N, c->stream));
+	BSG_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+	int rc = bsg_mvm_dev(c, m, dx, dy);
+	if (!rc) {
+		BSG_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+		BSG_CUDA(cudaStreamSynchronize(c->stream));
+	}
+	cudaFreeAsync(dx, c->stream);
+	cudaFreeAsync(dy, c->stream);
+	return rc;
+}
+
+// ---- factors --------------------------------------------------------------
+
+static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **out) {
+	if (!c || !m || !p || !out) return bsg_set_error(BSG_ERR_ARG, "factorisation: null argument");
+	*out = nullptr;
+	if (m->bs != 1) return bsg_set_error(BSG_ERR_UNSUPPORTED, "block factorisation is not available on this path");
+	if (p->ordtype != 0) return bsg_set_error(BSG_ERR_UNSUPPORTED, "only natural ordering (ordtype = 0) runs on the GPU");
+	if (kind == 0 && p->fcttyp == 1)
+		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) is not on the GPU path; use fcttyp = 2");
+	bsg_fct *f = nullptr;
+	int rc = bsg_fact_run(c, m, kind, p, &f);
+	if (rc) return rc;
+	float ms = 0;
+	cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+	p->timefct = ms * 1e-3;
+	p->density = f->density;
+	p->density2 = f->density2;
+	if (p->precision == 1) {
+		rc = bsg_fct_make_fp32(f);
+		if (rc) { bsg_fct_free(f); return rc; }
+	}
+	*out = f;
+	return BSG_OK;
+}
+
+extern "C" int bsg_fct_ich2(bsg_ctx *c, bsg_mat *m, bsg_param *p, bsg_fct **out) { return fct_common(c, m, p, 0, out); }
+extern "C" int bsg_fct_ilu2(bsg_ctx *c, bsg_mat *m, bsg_param *p, bsg_fct **out) { return fct_common(c, m, p, 1, out); }
+extern "C" int bsg_fct_to_fp32(bsg_fct *f) {
+	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_to_fp32: null factor");
+	return bsg_fct_make_fp32(f);
+}
+
+extern "C" int bsg_fct_export(const bsg_fct *f, int *nnz, int *iu, int *ju, double *l, double *u) {
+	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_export: null factor");
+	if (nnz) *nnz = f->nnz;
+	cudaStream_t s = f->ctx->stream;
+	if (iu) BSG_CUDA(cudaMemcpyAsync(iu, f->d_iu, sizeof(int) * (f->n + 1), cudaMemcpyDeviceToHost, s));
+	if (ju) BSG_CUDA(cudaMemcpyAsync(ju, f->d_ju, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, s));
+	if (l) BSG_CUDA(cudaMemcpyAsync(l, f->d_l, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, s));
+	if (u) BSG_CUDA(cudaMemcpyAsync(u, f->d_u, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	return BSG_OK;
+}
+
+extern "C" int bsg_fct_info(const bsg_fct *f, int *n, int *nnz, int *levels_l, int *levels_u, double *density,
+                            double *density2) {
+	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_info: null factor");
+	if (n) *n = f->n;
+	if (nnz) *nnz = f->nnz;
+	if (levels_l) *levels_l = f->levels_l;
+	if (levels_u) *levels_u = f->levels_u;
+	if (density) *density = f->density;
+	if (density2) *density2 = f->density2;
+	return BSG_OK;
+}
+
+extern "C" int bsg_fct_free(bsg_fct *f) {
+	if (!f) return BSG_OK;
+	cudaStream_t s = f->ctx->stream;
+	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);
+	for (void *p : {(void *)f->d_iu, (void *)f->d_ju, (void *)f->d_u, (void *)f->d_dinv_l, (void *)f->d_dinv_u,
+	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f})
+		if (p) cudaFreeAsync(p, s);
+	cudaStreamSynchronize(s);
+	delete f;
+	return BSG_OK;
+}
+
+extern "C" int bsg_solve_l_dev(bsg_ctx *c, const bsg_fct *f, int mode, int nsweeps, const double *x, double *y) {
+	if (!c || !f || !x || !y || x == y) return bsg_set_error(BSG_ERR_ARG, "bsg_solve_l_dev: bad argument");
+	double *work = nullptr;
+	if (mode == 1 && nsweeps > 1) BSG_CUDA(cudaMallocAsync(&work, sizeof(double) * f->n, c->stream));
+	int rc = bsg_trisolve_launch(c, f, 1, mode, nsweeps, x, y, work);
+	if (work) cudaFreeAsync(work, c->stream);
+	if (!rc) rc = bsg_check_devstat(c);
+	return rc;
+}
+extern "C" int bsg_solve_u_dev(bsg_ctx *c, const bsg_fct *f, int mode, int nsweeps, const double *x, double *y) {
+	if (!c || !f || !x || !y || x == y) return bsg_set_error(BSG_ERR_ARG, "bsg_solve_u_dev: bad argument");
+	double *work = nullptr;
+	if (mode == 1 && nsweeps > 1) BSG_CUDA(cudaMallocAsync(&work, sizeof(double) * f->n, c->stream));
+	int rc = bsg_trisolve_launch(c, f, 0, mode, nsweeps, x, y, work);
+	if (work) cudaFreeAsync(work, c->stream);
+	if (!rc) rc = bsg_check_devstat(c);
+	return rc;
+}
+
+// ---- learned stage hook (implemented in unet.cu) ---------------------------
+__attribute__((weak)) int bsg_unet_apply(void *, bsg_ctx *, const double *, double *, double *) {
+	return bsg_set_error(BSG_ERR_UNSUPPORTED, "learned preconditioner not built");
+}
+
+// ---- host-buffer drivers ----------------------------------------------------
+
+static int drive(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
+                 bsg_param *p, int symm) {
+	if (!c || !p || !b || !x) return bsg_set_error(BSG_ERR_ARG, "driver: null argument");
+	bsg_mat *m = nullptr;
+	bsg_fct *f = nullptr;
+	int rc = bsg_mat_csr(c, n, ia, ja, a, symm, &m);
+	if (rc) return rc;
+	rc = symm ? bsg_fct_ich2(c, m, p, &f) : bsg_fct_ilu2(c, m, p, &f);
+	if (rc) { bsg_mat_free(m); return rc; }
+	double *db = nullptr, *dx = nullptr;
+	cudaStream_t s = c->stream;
+	if (cudaMallocAsync(&db, sizeof(double) * n, s) != cudaSuccess || cudaMallocAsync(&dx, sizeof(double) * n, s) != cudaSuccess) {
+		bsg_fct_free(f); bsg_mat_free(m);
+		return bsg_set_error(BSG_ERR_NOMEM, "driver vectors");
+	}
+	cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+	cudaMemsetAsync(dx, 0, sizeof(double) * n, s);
+	bool pcg = symm && p->krylov == 0;
+	rc = pcg ? bsg_pcg_dev(c, m, f, db, dx, p) : bsg_gmres_dev(c, m, f, db, dx, p);
+	int rc2 = (int)cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+	cudaStreamSynchronize(s);
+	cudaFreeAsync(db, s);
+	cudaFreeAsync(dx, s);
+	bsg_fct_free(f);
+	bsg_mat_free(m);
+	if (!rc && rc2) rc = bsg_set_error(BSG_ERR_CUDA, "copy of the solution failed");
+	return rc;
+}
+
+extern "C" int bsg_solve_symm_csr(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, const double *b,
+                                  double *x, bsg_param *p) {
+	return drive(c, n, ia, ja, a, b, x, p, 1);
+}
+extern "C" int bsg_solver_csr(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, const double *b,
+                              double *x, bsg_param *p) {
+	return drive(c, n, ia, ja, a, b, x, p, 0);
+}

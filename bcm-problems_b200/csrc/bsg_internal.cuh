@@ -1,0 +1,137 @@
+// Internal declarations of the B200 solver library (libbsg.so).
+// Everything here is sm_100a device code or host glue around it; the public
+// C ABI lives in include/bslib_gpu.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include "../../include/bslib_gpu.h"
+
+#define BSG_WARP 32
+#define BSG_SMS 148
+
+// ---- error handling -------------------------------------------------------
+#define BSG_CUDA(call)                                                        \
+	do {                                                                      \
+		cudaError_t e_ = (call);                                              \
+		if (e_ != cudaSuccess) return bsg_set_cuda_error(e_, #call, __FILE__, __LINE__); \
+	} while (0)
+
+int bsg_set_cuda_error(cudaError_t e, const char *what, const char *file, int line);
+int bsg_set_error(int code, const char *msg);
+
+// Device-side status word written by kernels that can fail (pivot, workspace,
+// spin-wait limit).  The first failure wins (atomicCAS from 0).
+struct bsg_devstat {
+	int code;  // 0 = ok, else a BSG_ERR_* value
+	int where; // row / index that failed
+	int pad[2];
+};
+
+// ---- device helpers -------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+	return v;
+}
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+	for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+	return v;
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+	int v;
+	asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+	asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const void *p) {
+	unsigned long long v;
+	asm volatile("ld.volatile.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
+	return v;
+}
+__device__ __forceinline__ void st_volatile_f64(double *p, double v) {
+	asm volatile("st.volatile.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+__device__ __forceinline__ void devstat_fail(bsg_devstat *st, int code, int where) {
+	if (atomicCAS(&st->code, 0, code) == 0) st->where = where;
+}
+
+// Bit pattern that no arithmetic result carries (a signalling NaN payload);
+// marks "not yet solved" entries in the sync-free triangular solves.
+#define BSG_PENDING 0x7FF4DEADBEEF0001ull
+
+// Spin-wait bound: every device wait on another warp's result gives up after
+// this many nanoseconds of globaltimer time, reports BSG_ERR_TIMEOUT and
+// returns.  Two seconds is far above any legitimate wait.
+#define BSG_SPIN_LIMIT_NS 2000000000ull
+
+// ---- device-resident objects ---------------------------------------------
+struct bsg_ctx {
+	int device;
+	cudaStream_t stream;
+	bool own_stream;
+	bsg_devstat *d_stat;     // device status word
+	double *d_scalars;       // small device scratch for reductions / Krylov scalars
+	double *d_partials;      // block partial sums
+	unsigned int *d_counters;
+	double *h_pinned;        // pinned host mirror of a few scalars
+	int n_partials;
+	cudaEvent_t ev0, ev1;
+	int spmv_group;          // autotuned sub-warp size for CSR SpMV (0 = choose per matrix)
+};
+
+struct bsg_mat {
+	bsg_ctx *ctx;
+	int n;        // rows (point) or block rows
+	int bs;       // block size
+	int nnz;      // stored entries / blocks in the full (both triangles) matrix
+	int symm;     // 1 if created from an upper-triangle symmetric input
+	int *d_ia, *d_ja;
+	double *d_a;  // point values, or bs*bs row-major blocks for bs > 1
+	// upper pattern with diagonal first (factorisation input) and its
+	// transpose (the static contributor lists of each row)
+	int nnz_up;
+	int *d_iu, *d_ju;
+	double *d_al, *d_au;  // ILU2 split values (al == au for symmetric input)
+	int *d_it, *d_jt;     // transpose of the strict upper pattern: rows k < i with (k,i) stored
+	int group;            // CSR SpMV sub-warp size
+};
+
+struct bsg_fct {
+	bsg_ctx *ctx;
+	int n, bs;
+	int kind;      // 0 IC2, 1 ILU2
+	int nnz;       // entries of U including the diagonal
+	int fp32;      // 1 if off-diagonal values are stored in FP32
+	// U by rows (reference layout, diagonal = inverse pivot first), FP64
+	int *d_iu, *d_ju;
+	double *d_u;   // U values
+	double *d_l;   // L values by columns (== d_u for IC2)
+	// solve-ready forms: strict parts + inverse pivots
+	double *d_dinv_l, *d_dinv_u;  // inverse pivots (FP64)
+	int *d_ur_i, *d_ur_j;         // strict U rows
+	int *d_lr_i, *d_lr_j;         // strict L rows (transpose of the column storage)
+	double *d_ur_v, *d_lr_v;      // FP64 strict values
+	float *d_ur_f, *d_lr_f;       // FP32 strict values
+	int nnz_strict;
+	int levels_l, levels_u;       // dependency depth (diagnostic)
+	double density, density2;
+};
+
+// ---- internal entry points shared between translation units --------------
+int bsg_prepare_upper(bsg_mat *m);                       // builds d_iu/d_ju/d_al/d_au/d_it/d_jt
+int bsg_spmv_launch(const bsg_mat *m, const double *x, double *y, cudaStream_t s);
+int bsg_dot_launch(bsg_ctx *c, int n, const double *x, const double *y, double *d_out);
+int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct **out);
+int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
+                        double *work);
+int bsg_check_devstat(bsg_ctx *c);

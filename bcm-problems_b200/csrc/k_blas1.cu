@@ -1,0 +1,181 @@
+// Fused FP64 vector kernels of the Krylov loops (the reference's
+// ScProdSVect / DaxpySVect / ScaleSVect, Bslib/svector.cpp:321-390, and the
+// inline loops of Bslib/cg.cpp:247-285, Bslib/lanczos.cpp:684-697).
+//
+// Reductions are deterministic: a fixed grid of RED_BLOCKS blocks writes one
+// partial per block and the last block to finish (ticket counter) sums the
+// partials in block order, so results do not depend on scheduling.  Scalars
+// stay on the device (d_s[]) so a loop needs no host round trip per kernel.
+// Each reduction reads its vectors once: 16 B per element for a dot.
+#include "bsg_internal.cuh"
+
+#define RED_BLOCKS (2 * BSG_SMS)
+#define RED_THREADS 256
+
+namespace {
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+	v = warp_sum(v);
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+	__syncthreads();
+	if (l == 0) sh[w] = v;
+	__syncthreads();
+	double t = 0.0;
+	if (threadIdx.x < 32) {
+		t = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+		t = warp_sum(t);
+	}
+	return t; // valid in thread 0
+}
+
+// Finish a Q-way reduction: partials[q*gridDim.x + b].  Returns true in the
+// last block, which leaves the totals in out[q].
+template <int Q>
+__device__ bool finish_reduction(const double *vals, double *partials, unsigned int *counter, double *out,
+                                 double *sh) {
+	__shared__ bool last;
+	for (int q = 0; q < Q; q++) {
+		double t = block_sum(vals[q], sh);
+		if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = t;
+	}
+	__threadfence();
+	__syncthreads();
+	if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+	__syncthreads();
+	if (!last) return false;
+	__threadfence();
+	for (int q = 0; q < Q; q++) {
+		double v = 0.0;
+		for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) v += __ldcg(partials + q * gridDim.x + b);
+		double t = block_sum(v, sh);
+		if (threadIdx.x == 0) out[q] = t;
+	}
+	if (threadIdx.x == 0) *counter = 0;
+	return true;
+}
+
+// out[q] = x_q . y_q for Q pairs.
+template <int Q>
+__global__ void __launch_bounds__(RED_THREADS) k_dots(int n, const double *x0, const double *y0, const double *x1,
+                                                      const double *y1, const double *x2, const double *y2,
+                                                      double *partials, unsigned int *counter, double *out) {
+	__shared__ double sh[32];
+	double v[3] = {0.0, 0.0, 0.0};
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		v[0] = fma(x0[i], y0[i], v[0]);
+		if (Q > 1) v[1] = fma(x1[i], y1[i], v[1]);
+		if (Q > 2) v[2] = fma(x2[i], y2[i], v[2]);
+	}
+	finish_reduction<Q>(v, partials, counter, out, sh);
+}
+
+// out[j] = V_j . w, j < k (k <= 8), V column-major with leading dim ld.
+template <int K>
+__global__ void __launch_bounds__(RED_THREADS) k_mdot(int n, const double *V, long long ld, const double *w,
+                                                      double *partials, unsigned int *counter, double *out) {
+	__shared__ double sh[32];
+	double v[K];
+#pragma unroll
+	for (int j = 0; j < K; j++) v[j] = 0.0;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		double wi = w[i];
+#pragma unroll
+		for (int j = 0; j < K; j++) v[j] = fma(V[j * ld + i], wi, v[j]);
+	}
+	finish_reduction<K>(v, partials, counter, out, sh);
+}
+
+// w -= V h  (h on the device, k vectors)
+__global__ void k_gemv_sub(int n, const double *V, long long ld, int k, const double *h, double *w) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		double s = w[i];
+		for (int j = 0; j < k; j++) s = fma(-h[j], V[j * ld + i], s);
+		w[i] = s;
+	}
+}
+
+// x += V y (y on device)
+__global__ void k_gemv_add(int n, const double *V, long long ld, int k, const double *y, double *x) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		double s = x[i];
+		for (int j = 0; j < k; j++) s = fma(y[j], V[j * ld + i], s);
+		x[i] = s;
+	}
+}
+
+// y = x * scale, scale = num / den with num/den on the device (den <= 0 -> 0)
+__global__ void k_scale_by(int n, const double *x, double *y, const double *num, const double *den, int sqrt_den) {
+	double d = *den;
+	if (sqrt_den) d = sqrt(d);
+	double f = (d > 0.0) ? ((num ? *num : 1.0) / d) : 0.0;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] * f;
+}
+
+// r = b - r
+__global__ void k_residual(int n, const double *b, double *r) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r[i] = b[i] - r[i];
+}
+
+__global__ void k_fill(int n, double *x, double v) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+
+} // namespace
+
+static inline int ew_grid(long long n) {
+	long long b = (n + 255) / 256;
+	long long cap = (long long)BSG_SMS * 8;
+	return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+int bsg_dots_launch(bsg_ctx *c, int q, int n, const double *x0, const double *y0, const double *x1,
+                    const double *y1, const double *x2, const double *y2, double *d_out) {
+	if (q == 1)
+		k_dots<1><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, x0, y0, x1, y1, x2, y2, c->d_partials, c->d_counters, d_out);
+	else if (q == 2)
+		k_dots<2><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, x0, y0, x1, y1, x2, y2, c->d_partials, c->d_counters, d_out);
+	else
+		k_dots<3><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, x0, y0, x1, y1, x2, y2, c->d_partials, c->d_counters, d_out);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
+int bsg_dot_launch(bsg_ctx *c, int n, const double *x, const double *y, double *d_out) {
+	return bsg_dots_launch(c, 1, n, x, y, nullptr, nullptr, nullptr, nullptr, d_out);
+}
+
+// d_out[j] = V_j . w for j < k
+int bsg_mdot_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *w, double *d_out) {
+	for (int j0 = 0; j0 < k; j0 += 8) {
+		int kk = k - j0 < 8 ? k - j0 : 8;
+		const double *Vj = V + j0 * ld;
+		double *o = d_out + j0;
+		switch (kk) {
+#define BSG_MDOT(K) case K: k_mdot<K><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, Vj, ld, w, c->d_partials, c->d_counters, o); break;
+			BSG_MDOT(1) BSG_MDOT(2) BSG_MDOT(3) BSG_MDOT(4) BSG_MDOT(5) BSG_MDOT(6) BSG_MDOT(7) BSG_MDOT(8)
+#undef BSG_MDOT
+		}
+	}
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
+int bsg_gemv_sub_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *h, double *w) {
+	k_gemv_sub<<<ew_grid(n), 256, 0, c->stream>>>(n, V, ld, k, h, w);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+int bsg_gemv_add_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *y, double *x) {
+	k_gemv_add<<<ew_grid(n), 256, 0, c->stream>>>(n, V, ld, k, y, x);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+int bsg_scale_by_launch(bsg_ctx *c, int n, const double *x, double *y, const double *num, const double *den,
+                        int sqrt_den) {
+	k_scale_by<<<ew_grid(n), 256, 0, c->stream>>>(n, x, y, num, den, sqrt_den);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+int bsg_residual_launch(bsg_ctx *c, int n, const double *b, double *r) {
+	k_residual<<<ew_grid(n), 256, 0, c->stream>>>(n, b, r);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v) {
+	k_fill<<<ew_grid(n), 256, 0, s>>>((int)n, x, v);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}

@@ -1,0 +1,250 @@
+// Device-side storage transforms for the solver path:
+//   * symmetric expansion of an upper-stored matrix to both triangles (the
+//     gather form of MvmASymm, Bslib/mvm.cpp:2637-2652);
+//   * the CombineLU split (Bslib/smatrixr.cpp:1142-1258): the union upper
+//     pattern with diagonal first plus the two value arrays al = A(j,i),
+//     au = A(i,j);
+//   * pattern transposes (static contributor lists for the factorisation,
+//     row form of L for the forward solve).
+// All transforms sort 64-bit (row << 32 | col) keys with CUB radix sort, then
+// rebuild row pointers by binary search, so they are deterministic.
+#include "bsg_internal.cuh"
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+namespace {
+
+__global__ void k_expand_keys(int n, const int *ia, const int *ja, unsigned long long *keys, int *vals, int *count) {
+	// For each stored (i,j): emit (i,j); if j != i also emit (j,i).  Slots
+	// are taken by an atomic counter; the sort restores a fixed order.
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	for (int k = ia[i]; k < ia[i + 1]; k++) {
+		int j = ja[k];
+		int s = atomicAdd(count, j != i ? 2 : 1);
+		keys[s] = ((unsigned long long)(unsigned)i << 32) | (unsigned)j;
+		vals[s] = k;
+		if (j != i) {
+			keys[s + 1] = ((unsigned long long)(unsigned)j << 32) | (unsigned)i;
+			vals[s + 1] = k;
+		}
+	}
+}
+
+__global__ void k_split_keys(int n, const int *ia, const int *ja, unsigned long long *keys, int *vals) {
+	// CombineLU: entry (i,j) goes to upper row min(i,j); vals carries the
+	// source index and, in bit 31, whether it came from the lower triangle.
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	for (int k = ia[i]; k < ia[i + 1]; k++) {
+		int j = ja[k];
+		int r = j < i ? j : i, c = j < i ? i : j;
+		keys[k] = ((unsigned long long)(unsigned)r << 32) | (unsigned)c;
+		vals[k] = k | (j < i ? (int)0x80000000 : 0);
+	}
+}
+
+__global__ void k_row_ptr(int n, int nk, const unsigned long long *keys, int *ia) {
+	// ia[r] = first position with key row >= r (lower bound), r in [0, n].
+	int r = blockIdx.x * blockDim.x + threadIdx.x;
+	if (r > n) return;
+	int lo = 0, hi = nk;
+	while (lo < hi) {
+		int mid = (lo + hi) >> 1;
+		if ((int)(keys[mid] >> 32) < r) lo = mid + 1; else hi = mid;
+	}
+	ia[r] = lo;
+}
+
+__global__ void k_unique_flags(int nk, const unsigned long long *keys, int *flag) {
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= nk) return;
+	flag[k] = (k == 0 || keys[k] != keys[k - 1]) ? 1 : 0;
+}
+
+__global__ void k_split_scatter(int nk, const unsigned long long *keys, const int *vals, const int *pos,
+                                const double *a, int *ja_out, double *al, double *au, unsigned long long *ukeys) {
+	// pos[k] = inclusive scan of unique flags; slot = pos[k]-1.
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= nk) return;
+	int s = pos[k] - 1;
+	unsigned long long key = keys[k];
+	int r = (int)(key >> 32), c = (int)(key & 0xffffffffu);
+	int v = vals[k];
+	bool lower = v < 0;
+	int src = v & 0x7fffffff;
+	if (k == 0 || keys[k - 1] != key) {
+		ja_out[s] = c;
+		ukeys[s] = key;
+	}
+	// at most one lower and one upper (or one diagonal) source per key;
+	// write without races by ownership: the diagonal writes both.
+	if (r == c) {
+		al[s] = a[src];
+		au[s] = a[src];
+	} else if (lower) {
+		al[s] = a[src];
+	} else {
+		au[s] = a[src];
+	}
+}
+
+__global__ void k_gather_vals(int nk, const int *vals, const double *a, double *out) {
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < nk) out[k] = a[vals[k]];
+}
+
+__global__ void k_cols_from_keys(int nk, const unsigned long long *keys, int *ja) {
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < nk) ja[k] = (int)(keys[k] & 0xffffffffu);
+}
+
+__global__ void k_strict_transpose_keys(int n, const int *ia, const int *ja, unsigned long long *keys, int *vals,
+                                        int *count) {
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	for (int k = ia[i]; k < ia[i + 1]; k++) {
+		int j = ja[k];
+		if (j == i) continue;
+		int s = atomicAdd(count, 1);
+		keys[s] = ((unsigned long long)(unsigned)j << 32) | (unsigned)i;
+		vals[s] = k;
+	}
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+} // namespace
+
+// Sort (keys, vals) pairs on the context stream.  Keys < 2^63.
+int bsg_sort_pairs(bsg_ctx *c, unsigned long long *keys, int *vals, int nk, int nbits_row) {
+	if (nk <= 1) return BSG_OK;
+	unsigned long long *k2;
+	int *v2;
+	BSG_CUDA(cudaMallocAsync(&k2, sizeof(unsigned long long) * nk, c->stream));
+	BSG_CUDA(cudaMallocAsync(&v2, sizeof(int) * nk, c->stream));
+	cub::DoubleBuffer<unsigned long long> dk(keys, k2);
+	cub::DoubleBuffer<int> dv(vals, v2);
+	size_t tmp = 0;
+	int end_bit = 32 + nbits_row;
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, dk, dv, nk, 0, end_bit, c->stream));
+	void *d_tmp;
+	BSG_CUDA(cudaMallocAsync(&d_tmp, tmp > 0 ? tmp : 1, c->stream));
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp, dk, dv, nk, 0, end_bit, c->stream));
+	if (dk.Current() != keys) {
+		BSG_CUDA(cudaMemcpyAsync(keys, dk.Current(), sizeof(unsigned long long) * nk, cudaMemcpyDeviceToDevice, c->stream));
+		BSG_CUDA(cudaMemcpyAsync(vals, dv.Current(), sizeof(int) * nk, cudaMemcpyDeviceToDevice, c->stream));
+	}
+	BSG_CUDA(cudaFreeAsync(d_tmp, c->stream));
+	BSG_CUDA(cudaFreeAsync(k2, c->stream));
+	BSG_CUDA(cudaFreeAsync(v2, c->stream));
+	return BSG_OK;
+}
+
+static int bits_for(int n) {
+	int b = 1;
+	while ((1ll << b) <= (long long)n) b++;
+	return b;
+}
+
+// Expand an upper-stored symmetric CSR (device arrays) to both triangles,
+// columns ascending in every row.  Allocates *ia_o, *ja_o, *a_o.
+int bsg_expand_symmetric(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz_up, int **ia_o,
+                         int **ja_o, double **a_o, int *nnz_o) {
+	int ndiag_max = nnz_up * 2;
+	unsigned long long *keys;
+	int *vals, *cnt;
+	BSG_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * ndiag_max, c->stream));
+	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * ndiag_max, c->stream));
+	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int), c->stream));
+	BSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), c->stream));
+	k_expand_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals, cnt);
+	int nk = 0;
+	BSG_CUDA(cudaMemcpyAsync(&nk, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	int rc = bsg_sort_pairs(c, keys, vals, nk, bits_for(n));
+	if (rc) return rc;
+	BSG_CUDA(cudaMallocAsync(ia_o, sizeof(int) * (n + 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(ja_o, sizeof(int) * (nk > 0 ? nk : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(a_o, sizeof(double) * (nk > 0 ? nk : 1), c->stream));
+	k_row_ptr<<<nblk(n + 1, 256), 256, 0, c->stream>>>(n, nk, keys, *ia_o);
+	k_cols_from_keys<<<nblk(nk, 256), 256, 0, c->stream>>>(nk, keys, *ja_o);
+	k_gather_vals<<<nblk(nk, 256), 256, 0, c->stream>>>(nk, vals, a, *a_o);
+	BSG_CUDA(cudaGetLastError());
+	BSG_CUDA(cudaFreeAsync(keys, c->stream));
+	BSG_CUDA(cudaFreeAsync(vals, c->stream));
+	BSG_CUDA(cudaFreeAsync(cnt, c->stream));
+	*nnz_o = nk;
+	return BSG_OK;
+}
+
+// CombineLU on the device: union upper pattern (diagonal first because it is
+// the smallest column >= row), al/au values.  Returns BSG_ERR_ARG when a
+// diagonal entry is structurally missing.
+int bsg_combine_lu(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz, int **iu_o,
+                   int **ju_o, double **al_o, double **au_o, int *nnz_o) {
+	unsigned long long *keys, *ukeys;
+	int *vals, *flag, *pos;
+	BSG_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * nnz, c->stream));
+	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * nnz, c->stream));
+	k_split_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals);
+	int rc = bsg_sort_pairs(c, keys, vals, nnz, bits_for(n));
+	if (rc) return rc;
+	BSG_CUDA(cudaMallocAsync(&flag, sizeof(int) * nnz, c->stream));
+	BSG_CUDA(cudaMallocAsync(&pos, sizeof(int) * nnz, c->stream));
+	k_unique_flags<<<nblk(nnz, 256), 256, 0, c->stream>>>(nnz, keys, flag);
+	size_t tmp = 0;
+	BSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, flag, pos, nnz, c->stream));
+	void *d_tmp;
+	BSG_CUDA(cudaMallocAsync(&d_tmp, tmp > 0 ? tmp : 1, c->stream));
+	BSG_CUDA(cub::DeviceScan::InclusiveSum(d_tmp, tmp, flag, pos, nnz, c->stream));
+	int nu = 0;
+	BSG_CUDA(cudaMemcpyAsync(&nu, pos + nnz - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	BSG_CUDA(cudaMallocAsync(iu_o, sizeof(int) * (n + 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(ju_o, sizeof(int) * nu, c->stream));
+	BSG_CUDA(cudaMallocAsync(al_o, sizeof(double) * nu, c->stream));
+	BSG_CUDA(cudaMallocAsync(au_o, sizeof(double) * nu, c->stream));
+	BSG_CUDA(cudaMallocAsync(&ukeys, sizeof(unsigned long long) * nu, c->stream));
+	BSG_CUDA(cudaMemsetAsync(*al_o, 0, sizeof(double) * nu, c->stream));
+	BSG_CUDA(cudaMemsetAsync(*au_o, 0, sizeof(double) * nu, c->stream));
+	k_split_scatter<<<nblk(nnz, 256), 256, 0, c->stream>>>(nnz, keys, vals, pos, a, *ju_o, *al_o, *au_o, ukeys);
+	k_row_ptr<<<nblk(n + 1, 256), 256, 0, c->stream>>>(n, nu, ukeys, *iu_o);
+	BSG_CUDA(cudaGetLastError());
+	BSG_CUDA(cudaFreeAsync(keys, c->stream));
+	BSG_CUDA(cudaFreeAsync(vals, c->stream));
+	BSG_CUDA(cudaFreeAsync(flag, c->stream));
+	BSG_CUDA(cudaFreeAsync(pos, c->stream));
+	BSG_CUDA(cudaFreeAsync(d_tmp, c->stream));
+	BSG_CUDA(cudaFreeAsync(ukeys, c->stream));
+	*nnz_o = nu;
+	return BSG_OK;
+}
+
+// Transpose of the strict part of a CSR pattern: row j lists the rows i < j
+// with (i,j) stored, ascending.  perm[k] = source position of entry k.
+int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nnz, int **it_o, int **jt_o,
+                         int **perm_o, int *nnz_o) {
+	unsigned long long *keys;
+	int *vals, *cnt;
+	BSG_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int), c->stream));
+	BSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), c->stream));
+	k_strict_transpose_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals, cnt);
+	int nk = 0;
+	BSG_CUDA(cudaMemcpyAsync(&nk, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	int rc = bsg_sort_pairs(c, keys, vals, nk, bits_for(n));
+	if (rc) return rc;
+	BSG_CUDA(cudaMallocAsync(it_o, sizeof(int) * (n + 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(jt_o, sizeof(int) * (nk > 0 ? nk : 1), c->stream));
+	k_row_ptr<<<nblk(n + 1, 256), 256, 0, c->stream>>>(n, nk, keys, *it_o);
+	k_cols_from_keys<<<nblk(nk, 256), 256, 0, c->stream>>>(nk, keys, *jt_o);
+	BSG_CUDA(cudaGetLastError());
+	BSG_CUDA(cudaFreeAsync(keys, c->stream));
+	BSG_CUDA(cudaFreeAsync(cnt, c->stream));
+	if (perm_o) *perm_o = vals; else BSG_CUDA(cudaFreeAsync(vals, c->stream));
+	*nnz_o = nk;
+	return BSG_OK;
+}

@@ -1,0 +1,203 @@
+// Triangular solves with an IC2 / ILU2 factor (CSMatrixR::SolveL,
+// Bslib/mvm.cpp:3042 -- L by columns, inverse pivot first; SolveU, :3343 --
+// U by rows, inverse pivot first).
+//
+// The column-stored L is turned into rows (gather form) once per factor, so
+// both solves read their factor rows contiguously:
+//   forward  y_i = dinv_l[i] * (x_i - sum_{k<i} L(i,k) y_k)
+//   backward y_i = dinv_u[i] * (x_i - sum_{k>i} U(i,k) y_k)
+//
+// mode 0 -- exact, sync-free: a warp solves one row; warps claim rows in
+//   dependency order (ascending for L, descending for U) from an atomic
+//   counter, and each lane waits on the entry it needs.  "Solved" is encoded
+//   in the value itself: y is pre-filled with a NaN bit pattern no arithmetic
+//   produces, and a 64-bit store publishes the result in one transaction.
+//   Every wait is bounded by globaltimer (BSG_ERR_TIMEOUT).
+// mode 1 -- Jacobi sweeps: y <- D^{-1}(x - N y) repeated nsweeps times from
+//   y = D^{-1} x; every sweep is a fully parallel pass over the factor (HBM
+//   bound: 4 B value (FP32) or 8 B (FP64) + 4 B column per entry).  It applies
+//   a fixed polynomial in the factor, so it is a valid flexible (FGMRES)
+//   preconditioner and, applied symmetrically, a valid PCG preconditioner.
+#include "bsg_internal.cuh"
+
+namespace {
+
+template <typename VT>
+__global__ void __launch_bounds__(256) k_trsv_syncfree(int n, int lower, const int *__restrict__ rp,
+                                                       const int *__restrict__ ci, const VT *__restrict__ v,
+                                                       int skip_first, const double *__restrict__ dinv,
+                                                       const double *__restrict__ x, double *y, unsigned *claim,
+                                                       bsg_devstat *st) {
+	const int lane = threadIdx.x & 31;
+	for (;;) {
+		int t = 0;
+		if (lane == 0) t = (int)atomicAdd(claim, 1u);
+		t = __shfl_sync(0xffffffffu, t, 0);
+		if (t >= n) return;
+		const int row = lower ? t : n - 1 - t;
+		const int b = rp[row] + skip_first, e = rp[row + 1];
+		double s = 0.0;
+		for (int k = b + lane; k < e; k += 32) {
+			const int c = ci[k];
+			unsigned long long raw = ld_volatile_u64(y + c);
+			if (raw == BSG_PENDING) {
+				unsigned long long t0 = globaltimer_ns();
+				for (unsigned it = 1;; it++) {
+					__nanosleep(32);
+					raw = ld_volatile_u64(y + c);
+					if (raw != BSG_PENDING) break;
+					if ((it & 127) == 0) {
+						if (*(volatile int *)&st->code != 0) { raw = 0; break; }
+						if (globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) {
+							devstat_fail(st, BSG_ERR_TIMEOUT, row);
+							raw = 0;
+							break;
+						}
+					}
+				}
+			}
+			s = fma((double)v[k], __longlong_as_double((long long)raw), s);
+		}
+		s = warp_sum(s);
+		if (lane == 0) st_volatile_f64(y + row, (x[row] - s) * dinv[row]);
+	}
+}
+
+template <int G, typename VT>
+__global__ void __launch_bounds__(256) k_trsv_jacobi(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                                     const VT *__restrict__ v, int skip_first,
+                                                     const double *__restrict__ dinv, const double *__restrict__ x,
+                                                     const double *__restrict__ yin, double *__restrict__ yout) {
+	const int lane32 = threadIdx.x & 31;
+	const int lane = lane32 & (G - 1);
+	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	constexpr int RPW = 32 / G;
+	for (int r0 = warp * RPW; r0 < n; r0 += nwarps * RPW) {
+		int row = r0 + lane32 / G;
+		double s = 0.0;
+		if (row < n && yin) {
+			int b = rp[row] + skip_first, e = rp[row + 1];
+			for (int k = b + lane; k < e; k += G) s = fma((double)__ldcs(v + k), __ldg(yin + __ldcs(ci + k)), s);
+		}
+		s = group_sum<G>(s);
+		if (row < n && lane == 0) yout[row] = (x[row] - s) * dinv[row];
+	}
+}
+
+__global__ void k_fill_u64(long long n, unsigned long long *p, unsigned long long v) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		p[i] = v;
+}
+
+__global__ void k_diag_inv(int n, const int *iu, const double *l, const double *u, double *dl, double *du) {
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) {
+		dl[i] = l[iu[i]];
+		du[i] = u[iu[i]];
+	}
+}
+
+__global__ void k_permute(int nk, const int *perm, const double *src, double *dst) {
+	int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < nk) dst[k] = src[perm[k]];
+}
+
+__global__ void k_to_f32(long long nk, const double *src, float *dst) {
+	for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nk; k += (long long)gridDim.x * blockDim.x)
+		dst[k] = (float)src[k];
+}
+
+inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
+
+} // namespace
+
+int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nnz, int **it_o, int **jt_o,
+                         int **perm_o, int *nnz_o);
+int bsg_choose_group(double mean_row);
+
+// Build the gather forms of a freshly compacted factor.
+int bsg_fct_finish(bsg_ctx *c, bsg_fct *f) {
+	cudaStream_t s = c->stream;
+	const int n = f->n;
+	BSG_CUDA(cudaMallocAsync(&f->d_dinv_l, sizeof(double) * n, s));
+	BSG_CUDA(cudaMallocAsync(&f->d_dinv_u, sizeof(double) * n, s));
+	k_diag_inv<<<nb(n, 256), 256, 0, s>>>(n, f->d_iu, f->d_l, f->d_u, f->d_dinv_l, f->d_dinv_u);
+	int *perm = nullptr, nk = 0;
+	int rc = bsg_strict_transpose(c, n, f->d_iu, f->d_ju, f->nnz, &f->d_lr_i, &f->d_lr_j, &perm, &nk);
+	if (rc) return rc;
+	f->nnz_strict = nk;
+	BSG_CUDA(cudaMallocAsync(&f->d_lr_v, sizeof(double) * (nk > 0 ? nk : 1), s));
+	k_permute<<<nb(nk, 256), 256, 0, s>>>(nk, perm, f->d_l, f->d_lr_v);
+	BSG_CUDA(cudaFreeAsync(perm, s));
+	// strict U rows are the factor rows minus their first (diagonal) entry
+	f->d_ur_i = f->d_iu;
+	f->d_ur_j = f->d_ju;
+	f->d_ur_v = f->d_u;
+	f->levels_l = f->levels_u = -1;
+	BSG_CUDA(cudaGetLastError());
+	BSG_CUDA(cudaStreamSynchronize(s));
+	return BSG_OK;
+}
+
+int bsg_fct_make_fp32(bsg_fct *f) {
+	if (f->fp32) return BSG_OK;
+	cudaStream_t s = f->ctx->stream;
+	BSG_CUDA(cudaMallocAsync(&f->d_ur_f, sizeof(float) * (f->nnz > 0 ? f->nnz : 1), s));
+	BSG_CUDA(cudaMallocAsync(&f->d_lr_f, sizeof(float) * (f->nnz_strict > 0 ? f->nnz_strict : 1), s));
+	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz, f->d_u, f->d_ur_f);
+	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz_strict, f->d_lr_v, f->d_lr_f);
+	BSG_CUDA(cudaGetLastError());
+	f->fp32 = 1;
+	return BSG_OK;
+}
+
+int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
+
+// Solve with L (lower != 0) or U.  x and y must not alias.  `work` (n
+// doubles) is needed for mode 1 with nsweeps > 1.
+int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
+                        double *work) {
+	cudaStream_t s = c->stream;
+	const int n = f->n;
+	const int *rp = lower ? f->d_lr_i : f->d_ur_i;
+	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
+	const int skip = lower ? 0 : 1;
+	const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
+	const double *vd = lower ? f->d_lr_v : f->d_ur_v;
+	const float *vf = lower ? f->d_lr_f : f->d_ur_f;
+	const bool use32 = f->fp32 != 0;
+	if (mode == 0) {
+		k_fill_u64<<<BSG_SMS * 4, 256, 0, s>>>(n, (unsigned long long *)y, BSG_PENDING);
+		unsigned *claim = c->d_counters + 1;
+		BSG_CUDA(cudaMemsetAsync(claim, 0, sizeof(unsigned), s));
+		int grid = BSG_SMS * 8;
+		int need = (n + 7) / 8;
+		if (grid > need) grid = need > 0 ? need : 1;
+		if (use32)
+			k_trsv_syncfree<float><<<grid, 256, 0, s>>>(n, lower, rp, ci, vf, skip, dinv, x, y, claim, c->d_stat);
+		else
+			k_trsv_syncfree<double><<<grid, 256, 0, s>>>(n, lower, rp, ci, vd, skip, dinv, x, y, claim, c->d_stat);
+		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	}
+	if (nsweeps < 1) nsweeps = 1;
+	if (nsweeps > 1 && !work) return BSG_ERR_ARG;
+	const int G = 16;
+	int grid = ((n + 1) / 2 + 7) / 8;
+	if (grid > BSG_SMS * 8) grid = BSG_SMS * 8;
+	if (grid < 1) grid = 1;
+	// ping-pong so that the last sweep lands in y
+	double *bufs[2] = {y, work};
+	int cur = (nsweeps % 2 == 1) ? 0 : 1;
+	const double *yin = nullptr;
+	for (int sw = 0; sw < nsweeps; sw++) {
+		double *out = bufs[cur];
+		if (use32)
+			k_trsv_jacobi<G, float><<<grid, 256, 0, s>>>(n, rp, ci, vf, skip, dinv, x, yin, out);
+		else
+			k_trsv_jacobi<G, double><<<grid, 256, 0, s>>>(n, rp, ci, vd, skip, dinv, x, yin, out);
+		yin = out;
+		cur ^= 1;
+	}
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}

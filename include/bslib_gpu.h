@@ -1,0 +1,168 @@
+/* bslib_gpu.h -- C ABI of the B200 (sm_100a) solver library libbsg.so.
+ *
+ * A drop-in replacement, on one GPU, for Bslib's preconditioned Krylov path:
+ * point/block CSR SpMV, the second-order threshold IC2/ILU2 numeric
+ * factorisation, the forward/backward triangular solves, and the PCG /
+ * GMRES(m) / FGMRES(m) loops.  Matrices cross the boundary in the reference
+ * storage (CSMatrixR: 0-based CSR, diagonal first in every row; CSMatrixRS:
+ * block CSR with column-major blocks); solver settings in bsg_param, a plain-C
+ * mirror of the CSlvParam fields the path reads and writes.
+ *
+ * Every function returns an int status: BSG_OK (0) or a negative BSG_ERR_*
+ * code, mirroring the integer convention of the reference's C API
+ * (Bslib/parfbss.cpp:37,74); bsg_last_error() gives the message, using the
+ * reference's own exception strings where one exists.
+ *
+ * Threading: one context = one CUDA stream; a context and the objects made
+ * from it are not thread-safe.  Separate contexts are independent.
+ * Host pointers are borrowed for the duration of a call only.  Functions
+ * named *_dev take device pointers and never copy between host and device.
+ */
+#ifndef BSLIB_GPU_H
+#define BSLIB_GPU_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define BSG_OK 0
+#define BSG_ERR_ARG (-1)         /* invalid argument or malformed CSR/BSR       */
+#define BSG_ERR_PIVOT (-2)       /* " Ich2: Diagonal pivot is nonpositive"       */
+#define BSG_ERR_WORKSPACE (-3)   /* " Insufficient workspace in Ich2/Ilu2"       */
+#define BSG_ERR_BREAKDOWN (-4)   /* Krylov breakdown (CG: matrix not SPD)       */
+#define BSG_ERR_CUDA (-5)        /* CUDA runtime error                          */
+#define BSG_ERR_TIMEOUT (-6)     /* a device spin-wait reached its time limit   */
+#define BSG_ERR_NOCONV (-7)      /* iteration limit reached before tolerance    */
+#define BSG_ERR_UNSUPPORTED (-8) /* option not implemented on the GPU path      */
+#define BSG_ERR_NOMEM (-9)       /* device allocation failed                    */
+
+/* ---- solver parameters ---------------------------------------------------- */
+/* Fields up to `timeitr` carry the meaning of the CSlvParam member of the same
+ * name (Bslib/slvparam.h:19-120, defaults :121-214).  The fields after it are
+ * extensions of the GPU path that the reference does not have. */
+typedef struct bsg_param {
+	int msglev;       /* output level (0 quiet)                                   */
+	int fcttyp;       /* 1: IC(0)-like first order (not on GPU), else second order */
+	int ordtype;      /* ordering; only 0 (natural) is accepted on the GPU        */
+	double memory;    /* factor workspace, multiples of nnz(A) (|memory| used)    */
+	double tau1;      /* first-order threshold: |v| >= tau1 kept in U            */
+	double tau2;      /* second-order threshold: tau2 <= |v| < tau1 kept in R    */
+	double theta;     /* diagonal compensation factor for dropped entries        */
+	double sclmin;    /* minimal scaling value (ILU2)                            */
+	double pivmin;    /* minimal pivot (ILU2)                                    */
+	int ittype;       /* CG stop rule: 0 relative, 1 absolute (recursive resid.) */
+	int sttype;       /* GMRES stop rule: 0 absolute, else relative              */
+	int niter;        /* maximal number of iterations                            */
+	double eps;       /* stopping tolerance                                      */
+	int ichk;         /* iterations between convergence checks                   */
+	/* outputs, as filled by the reference */
+	int nitperf;      /* iterations performed                                    */
+	double resfin;    /* final relative FP64 true residual ||b-Ax||/||b||        */
+	double density;   /* nnz(U) / nnz(A)                                         */
+	double density2;  /* nnz(R) / nnz(A)                                         */
+	double timefct;   /* factorisation time, seconds (device events)            */
+	double timeitr;   /* iteration time, seconds (device events)                */
+	/* GPU-path extensions */
+	int precision;    /* 0: FP64 factor values; 1: FP32 factor values, FP64 pivots */
+	int trisolve;     /* 0: exact sync-free level solve; 1: Jacobi sweeps         */
+	int nsweeps;      /* Jacobi sweeps per triangular solve when trisolve == 1   */
+	int krylov;       /* 0: method of the driver (PCG symm / GMRES nonsymm),
+	                     1: GMRES(restart), 2: FGMRES(restart)                   */
+	int restart;      /* GMRES/FGMRES restart length m                           */
+	int true_residual;/* 1: recompute r = b - Ax in FP64 at every restart/stop   */
+	void *learned;    /* optional learned preconditioner stage (bsg_unet*) for FGMRES */
+	double resrec;    /* output: last recursive residual estimate (relative)     */
+	int pad[4];
+} bsg_param;
+
+/* CSlvParam's constructor defaults (Bslib/slvparam.h:121-214) plus the
+ * GPU-path defaults (FP64, exact solves, restart 50). */
+void bsg_param_default(bsg_param *p);
+
+const char *bsg_last_error(void);
+const char *bsg_version(void);
+
+/* ---- context -------------------------------------------------------------- */
+typedef struct bsg_ctx bsg_ctx;
+typedef struct bsg_mat bsg_mat;
+typedef struct bsg_fct bsg_fct;
+
+/* Create a context on `device` with its own stream (stream == NULL) or on the
+ * caller's cudaStream_t. */
+int bsg_create(bsg_ctx **ctx, int device, void *stream);
+int bsg_destroy(bsg_ctx *ctx);
+int bsg_sync(bsg_ctx *ctx);
+
+/* ---- matrices (CSMatrixR / CSMatrixRS, Bslib/smatrix.h:540-546, :1040-1048) */
+/* Point CSR from host arrays.  symm_upper = 1: only the upper triangle is
+ * given (the input of SolveSymm / MvmASymm, Bslib/mvm.cpp:2637); the device
+ * copy is expanded to both triangles for gather SpMV. */
+int bsg_mat_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, int symm_upper,
+                bsg_mat **out);
+/* Same from device arrays (copied device-to-device). */
+int bsg_mat_csr_dev(bsg_ctx *ctx, int n, const int *d_ia, const int *d_ja, const double *d_a, int symm_upper,
+                    bsg_mat **out);
+/* Block CSR with uniform block size bs (1..4), blocks column-major as in
+ * CSMatrixRS (a[9*j + 3*c + r] for bs == 3). */
+int bsg_mat_bsr(bsg_ctx *ctx, int nsup, int bs, const int *ia, const int *ja, const double *a, int symm_upper,
+                bsg_mat **out);
+int bsg_mat_free(bsg_mat *m);
+int bsg_mat_info(const bsg_mat *m, int *n, int *bs, int *nnz);
+
+/* y = A x (CSMatrixR::MvmA Bslib/mvm.cpp:2489, MvmASymm :2637;
+ * CSMatrixRS::MvmA :2530, MvmASymm :3008).  FP64. */
+int bsg_mvm_dev(bsg_ctx *ctx, const bsg_mat *m, const double *d_x, double *d_y);
+int bsg_mvm(bsg_ctx *ctx, const bsg_mat *m, const double *x, double *y); /* host buffers */
+/* Y = A X for nrhs column vectors stored one after another (leading dim n*bs):
+ * the matrix is read once for all right-hand sides (CSMatrixRS::MvmA loops
+ * irhs outside the sweep, Bslib/mvm.cpp:2545). */
+int bsg_mvm_multi_dev(bsg_ctx *ctx, const bsg_mat *m, int nrhs, const double *d_X, double *d_Y);
+
+/* ---- factorisation (CSMatrixR::Ich2 Bslib/ich2r.cpp:956; CSMatrixR::Ilu2
+ * Bslib/ilu2r.cpp:1122; CSMatrixRS::Ich2 Bslib/ich2rs.cpp:1075;
+ * CSMatrixRS::Ilu2 Bslib/ilu2rs.cpp:1458) ---------------------------------- */
+/* IC2 of a symmetric matrix (created with symm_upper = 1 or symmetric full). */
+int bsg_fct_ich2(bsg_ctx *ctx, bsg_mat *m, bsg_param *p, bsg_fct **out);
+/* ILU2 of a general matrix (the CombineLU split, Bslib/smatrixr.cpp:1142,
+ * is done on the device). */
+int bsg_fct_ilu2(bsg_ctx *ctx, bsg_mat *m, bsg_param *p, bsg_fct **out);
+/* Convert the factor values to FP32 (pivots stay FP64) for the mixed path. */
+int bsg_fct_to_fp32(bsg_fct *f);
+/* Copy the factor to host in the reference layout: iu[n+1], ju[nnz],
+ * l[nnz] (L by columns) and u[nnz] (U by rows), inverse pivots first.  Call
+ * with NULL arrays to get nnz only. */
+int bsg_fct_export(const bsg_fct *f, int *nnz, int *iu, int *ju, double *l, double *u);
+int bsg_fct_info(const bsg_fct *f, int *n, int *nnz, int *levels_l, int *levels_u, double *density,
+                 double *density2);
+int bsg_fct_free(bsg_fct *f);
+
+/* ---- triangular solves (CSMatrixR::SolveL Bslib/mvm.cpp:3042 / SolveU :3343;
+ * CSMatrixRS::SolveL :3140 / SolveU :3410) -------------------------------- */
+/* mode 0: exact (sync-free, dependency-ordered); mode 1: nsweeps Jacobi
+ * sweeps (approximate, fully parallel).  `work` may be NULL for mode 0. */
+int bsg_solve_l_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
+int bsg_solve_u_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
+
+/* ---- Krylov loops --------------------------------------------------------- */
+/* PCG (CSVector::Cg, Bslib/cg.cpp:31) with A symmetric and an IC2 factor;
+ * x0 = d_x on entry. */
+int bsg_pcg_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x, bsg_param *p);
+/* Right-preconditioned GMRES(restart) / FGMRES(restart) (the restarted FP64
+ * counterpart of CSVector::BlockGMRES, Bslib/gmres.cpp:337). */
+int bsg_gmres_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x,
+                  bsg_param *p);
+
+/* ---- whole drivers with host buffers ------------------------------------- */
+/* CSVector::SolveSymm(CSMatrixR&) (Bslib/solvers.cpp:4615): upper-stored SPD
+ * CSR in, IC2 + PCG (or GMRES/FGMRES per p->krylov), solution out. */
+int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b,
+                       double *x, bsg_param *p);
+/* CSVector::Solver(CSMatrixR&) (Bslib/solvers.cpp:1339): full CSR in,
+ * CombineLU + ILU2 + GMRES(restart), solution out. */
+int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
+                   bsg_param *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

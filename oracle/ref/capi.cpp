@@ -1,0 +1,221 @@
+// Oracle build support (test infrastructure, not shipped): plain C entry
+// points over the reference Bslib classes, so the parity tests can drive the
+// reference's own code on identical inputs through ctypes.
+//
+// Matrices cross this boundary as 0-based CSR arrays (ia[n+1], ja[nz], a[nz]),
+// each row's diagonal entry first, which is the layout CSMatrixR keeps
+// (Bslib/smatrix.h:540-546).  Factor results are returned in malloc'ed arrays
+// that the caller releases with ref_free().
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <chrono>
+#include "smatrix.h"
+#include "slvparam.h"
+#include "svector.h"
+
+namespace {
+
+CSMatrixR make_csr(int n, const int *ia, const int *ja, const double *a) {
+	int nz = ia[n];
+	CSMatrixR m(n, nz);
+	std::memcpy(m.GetIa(), ia, sizeof(int) * (n + 1));
+	std::memcpy(m.GetJa(), ja, sizeof(int) * nz);
+	std::memcpy(m.GetA(), a, sizeof(double) * nz);
+	m.SetNza(nz);
+	m.SetNzatot(nz);
+	return m;
+}
+
+void export_csr(const CSMatrixR &m, int **ia, int **ja, double **a) {
+	int n = m.GetNlist();
+	int nz = m.GetIa()[n];
+	*ia = (int *)std::malloc(sizeof(int) * (n + 1));
+	*ja = (int *)std::malloc(sizeof(int) * (nz > 0 ? nz : 1));
+	*a = (double *)std::malloc(sizeof(double) * (nz > 0 ? nz : 1));
+	std::memcpy(*ia, m.GetIa(), sizeof(int) * (n + 1));
+	std::memcpy(*ja, m.GetJa(), sizeof(int) * nz);
+	std::memcpy(*a, m.GetA(), sizeof(double) * nz);
+}
+
+CSVector make_vec(int n, const double *x) {
+	CSVector v(n);
+	if (x) std::memcpy(v.GetVect(), x, sizeof(double) * n);
+	return v;
+}
+
+double now_s() {
+	using namespace std::chrono;
+	return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// Error convention: the reference throws const char*; map it to a negative code
+// and keep the message for ref_last_error().
+thread_local char g_err[256];
+int fail(const char *msg) {
+	std::strncpy(g_err, msg ? msg : "unknown", sizeof(g_err) - 1);
+	return -1;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *ref_last_error() { return g_err; }
+void ref_free(void *p) { std::free(p); }
+
+// y = A x with A stored in full (MvmA, Bslib/mvm.cpp:2489) or symmetric
+// upper-only (MvmASymm, Bslib/mvm.cpp:2637) form.
+int ref_mvm(int n, const int *ia, const int *ja, const double *a, const double *x, double *y, int symm_upper) {
+	CSMatrixR m = make_csr(n, ia, ja, a);
+	CSVector vx = make_vec(n, x), vy(n);
+	if (symm_upper) m.MvmASymm(vx, vy); else m.MvmA(vx, vy);
+	std::memcpy(y, vy.GetVect(), sizeof(double) * n);
+	return 0;
+}
+
+// Triangular solves with a factor in the reference layout
+// (SolveL: L by columns, Bslib/mvm.cpp:3042; SolveU: U by rows, :3343).
+int ref_solve_l(int n, const int *ia, const int *ja, const double *a, const double *x, double *y) {
+	CSMatrixR m = make_csr(n, ia, ja, a);
+	CSVector vx = make_vec(n, x), vy(n);
+	m.SolveL(vx, vy);
+	std::memcpy(y, vy.GetVect(), sizeof(double) * n);
+	return 0;
+}
+int ref_solve_u(int n, const int *ia, const int *ja, const double *a, const double *x, double *y) {
+	CSMatrixR m = make_csr(n, ia, ja, a);
+	CSVector vx = make_vec(n, x), vy(n);
+	m.SolveU(vx, vy);
+	std::memcpy(y, vy.GetVect(), sizeof(double) * n);
+	return 0;
+}
+
+// IC2 of an upper-stored SPD matrix (CSMatrixR::Ich2, Bslib/ich2r.cpp:956).
+// stats[0]=density, stats[1]=density2, stats[2]=factor seconds.
+int ref_ich2(int n, const int *ia, const int *ja, const double *a, double tau1, double tau2, double theta,
+             double memory, int **ia_u, int **ja_u, double **a_u, double *stats) {
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		double t0 = now_s();
+		CSMatrixR u = m.Ich2(p);
+		double t1 = now_s();
+		export_csr(u, ia_u, ja_u, a_u);
+		if (stats) { stats[0] = p.density; stats[1] = p.density2; stats[2] = t1 - t0; }
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// CombineLU + ILU2 of a full-stored matrix (Bslib/smatrixr.cpp:1142,
+// Bslib/ilu2r.cpp:1122).  L comes back by columns, U by rows, same pattern.
+int ref_ilu2(int n, const int *ia, const int *ja, const double *a, double tau1, double tau2, double theta,
+             double memory, double sclmin, double pivmin,
+             int **ia_l, int **ja_l, double **a_l, int **ia_u, int **ja_u, double **a_u, double *stats) {
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		p.sclmin = sclmin; p.pivmin = pivmin;
+		CSMatrixR al, au, l, u, dummy;
+		m.CombineLU(al, au);
+		std::ofstream fout("/dev/null");
+		double t0 = now_s();
+		dummy.Ilu2(fout, p, al, au, l, u);
+		double t1 = now_s();
+		export_csr(l, ia_l, ja_l, a_l);
+		export_csr(u, ia_u, ja_u, a_u);
+		if (stats) { stats[0] = p.density; stats[1] = p.density2; stats[2] = t1 - t0; }
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// Whole symmetric driver CSVector::SolveSymm(CSMatrixR&) (Bslib/solvers.cpp:4615)
+// with natural ordering: IC2 (fcttyp != 1) or IC(0) (fcttyp == 1), then PCG
+// (Bslib/cg.cpp:31).  stats: [0]=iterations, [1]=resfin, [2]=factor s,
+// [3]=iteration s, [4]=density, [5]=density2, [6]=total wall s.
+int ref_solve_symm(int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
+                   int fcttyp, double tau1, double tau2, double theta, double memory,
+                   int ittype, double eps, int niter, int ichk, double *stats) {
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.fcttyp = fcttyp; p.ordtype = 0;
+		p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = ichk;
+		CSVector vb = make_vec(n, b), norm(n), sol(n);
+		norm.SetSVect(1.0);
+		std::ofstream fout("/dev/null");
+		double t0 = now_s();
+		sol.SolveSymm(fout, m, vb, p, norm);
+		double t1 = now_s();
+		std::memcpy(x, sol.GetVect(), sizeof(double) * n);
+		if (stats) {
+			stats[0] = p.nitperf; stats[1] = p.resfin; stats[2] = p.timefct; stats[3] = p.timeitr;
+			stats[4] = p.density; stats[5] = p.density2; stats[6] = t1 - t0;
+		}
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// PCG alone (Bslib/cg.cpp:31) with a given upper-stored A and IC factor U.
+int ref_cg(int n, const int *ia, const int *ja, const double *a,
+           const int *iu, const int *ju, const double *u, const double *b, double *x,
+           int ittype, double eps, int niter, int ichk, double *stats) {
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSMatrixR f = make_csr(n, iu, ju, u);
+		CSlvParam p;
+		p.msglev = 0; p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = ichk;
+		CSVector vb = make_vec(n, b), x0(n), norm(n), sol(n);
+		norm.SetSVect(1.0);
+		std::ofstream fout("/dev/null");
+		double t0 = now_s();
+		sol.Cg(fout, &m, 0, nullptr, &f, x0, vb, p, norm);
+		double t1 = now_s();
+		std::memcpy(x, sol.GetVect(), sizeof(double) * n);
+		if (stats) { stats[0] = p.nitperf; stats[1] = p.resfin; stats[2] = t1 - t0; }
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// Whole nonsymmetric driver CSVector::Solver(CSMatrixR&) (Bslib/solvers.cpp:1339):
+// CombineLU + ILU2 + preconditioned Lanczos (Bslib/lanczos.cpp:34), natural
+// ordering.  stats as ref_solve_symm.
+int ref_solver(int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
+               double tau1, double tau2, double theta, double memory, double sclmin, double pivmin,
+               int sttype, double eps, int niter, int ichk, double *stats) {
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.ordtype = 0; p.ittype = 1;
+		p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		p.sclmin = sclmin; p.pivmin = pivmin;
+		p.sttype = sttype; p.eps = eps; p.niter = niter; p.ichk = ichk;
+		CSVector vb = make_vec(n, b), norm(n), sol(n);
+		norm.SetSVect(1.0);
+		std::ofstream fout("/dev/null");
+		double t0 = now_s();
+		sol.Solver(fout, m, vb, p, norm);
+		double t1 = now_s();
+		std::memcpy(x, sol.GetVect(), sizeof(double) * n);
+		if (stats) {
+			stats[0] = p.nitperf; stats[1] = p.resfin; stats[2] = p.timefct; stats[3] = p.timeitr;
+			stats[4] = p.density; stats[5] = p.density2; stats[6] = t1 - t0;
+		}
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+} // extern "C"

@@ -1,0 +1,212 @@
+"""ctypes access to the two CPU checkers (test infrastructure only).
+
+* ``Oracle`` -- the C restatement in ``oracle/bsl_oracle.c`` (``oracle/_build``).
+* ``RefLib`` -- the reference Bslib compiled from its own sources into
+  ``oracle/_ref/libbslib_ref.so`` by ``oracle/Makefile``.
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+use this module; the product never imports it.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libbslib_ref.so")
+
+_ip = C.POINTER(C.c_int)
+_dp = C.POINTER(C.c_double)
+
+
+def _i(x):
+    return np.ascontiguousarray(x, dtype=np.int32).ctypes.data_as(_ip)
+
+
+def _d(x):
+    return np.ascontiguousarray(x, dtype=np.float64).ctypes.data_as(_dp)
+
+
+def _take_csr(lib, n, pia, pja, pa, pb=None):
+    ia = np.ctypeslib.as_array(pia, (n + 1,)).copy()
+    nz = int(ia[-1])
+    ja = np.ctypeslib.as_array(pja, (max(nz, 1),))[:nz].copy()
+    a = np.ctypeslib.as_array(pa, (max(nz, 1),))[:nz].copy()
+    b = None
+    if pb is not None:
+        b = np.ctypeslib.as_array(pb, (max(nz, 1),))[:nz].copy()
+    return ia, ja, a, b
+
+
+class Oracle:
+    def __init__(self, path=ORACLE_SO):
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.orc_fact.restype = C.c_int
+        L.orc_combine_lu.restype = C.c_int
+        L.orc_pcg.restype = C.c_int
+        L.orc_gmres.restype = C.c_int
+
+    def mvm(self, ia, ja, a, x, symm=False):
+        n = len(ia) - 1
+        y = np.zeros(n)
+        f = self.lib.orc_mvm_symm if symm else self.lib.orc_mvm
+        f(n, _i(ia), _i(ja), _d(a), _d(x), _d(y))
+        return y
+
+    def bsr_mvm(self, ia, ja, a, x, bs):
+        nb = len(ia) - 1
+        y = np.zeros(nb * bs)
+        self.lib.orc_bsr_mvm(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y))
+        return y
+
+    def solve_l(self, iu, ju, u, x):
+        n = len(iu) - 1
+        y = np.zeros(n)
+        self.lib.orc_solve_l(n, _i(iu), _i(ju), _d(u), _d(x), _d(y))
+        return y
+
+    def solve_u(self, iu, ju, u, x):
+        n = len(iu) - 1
+        y = np.zeros(n)
+        self.lib.orc_solve_u(n, _i(iu), _i(ju), _d(u), _d(x), _d(y))
+        return y
+
+    def combine_lu(self, ia, ja, a):
+        n = len(ia) - 1
+        pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
+        ia, ja, a = [np.ascontiguousarray(v) for v in (ia, ja, a)]
+        rc = self.lib.orc_combine_lu(n, _i(ia), _i(ja), _d(a), C.byref(pia), C.byref(pja), C.byref(pl), C.byref(pu))
+        if rc < 0:
+            raise ValueError("combine_lu failed")
+        sia, sja, al, au = _take_csr(self.lib, n, pia, pja, pl, pu)
+        for p in (pia, pja, pl, pu):
+            self.lib.orc_free(p)
+        return sia, sja, al, au
+
+    def fact(self, kind, ia, ja, al, au=None, tau1=1e-3, tau2=1e-3, theta=0.1, sclmin=1e-8, pivmin=1e-8):
+        n = len(ia) - 1
+        if au is None:
+            au = al
+        piu, pju, pl, pu = _ip(), _ip(), _dp(), _dp()
+        st = (C.c_double * 4)()
+        keep = [np.ascontiguousarray(v) for v in (ia, ja, al, au)]
+        rc = self.lib.orc_fact(kind, n, _i(keep[0]), _i(keep[1]), _d(keep[2]), _d(keep[3]), C.c_double(tau1),
+                               C.c_double(tau2), C.c_double(theta), C.c_double(sclmin), C.c_double(pivmin),
+                               C.byref(piu), C.byref(pju), C.byref(pl), C.byref(pu), st)
+        if rc == -2:
+            raise ArithmeticError(f"Ich2: Diagonal pivot is nonpositive (row {int(st[2])})")
+        if rc != 0:
+            raise RuntimeError(f"orc_fact failed rc={rc}")
+        iu, ju, lv, uv = _take_csr(self.lib, n, piu, pju, pl, pu if kind == 1 else None)
+        self.lib.orc_free(piu)
+        self.lib.orc_free(pju)
+        self.lib.orc_free(pl)
+        if kind == 1:
+            self.lib.orc_free(pu)
+        else:
+            uv = lv
+        return iu, ju, lv, uv, (st[0], st[1])
+
+    def pcg(self, ia, ja, a, iu, ju, u, b, ittype=0, eps=1e-10, niter=1000):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        res = C.c_double()
+        it = self.lib.orc_pcg(n, _i(ia), _i(ja), _d(a), _i(iu), _i(ju), _d(u), _d(b), _d(x), ittype,
+                              C.c_double(eps), niter, C.byref(res))
+        return x, it, res.value
+
+    def gmres(self, ia, ja, a, iu, ju, l, u, b, m=50, eps=1e-8, sttype=1, niter=2000):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        res = C.c_double()
+        it = self.lib.orc_gmres(n, _i(ia), _i(ja), _d(a), _i(iu), _i(ju), _d(l), _d(u), _d(b), _d(x), m,
+                                C.c_double(eps), sttype, niter, C.byref(res))
+        return x, it, res.value
+
+
+class RefLib:
+    """The reference Bslib, compiled here from its sources (oracle/Makefile)."""
+
+    def __init__(self, path=REF_SO):
+        self.lib = C.CDLL(path)
+        self.lib.ref_last_error.restype = C.c_char_p
+
+    def _err(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def mvm(self, ia, ja, a, x, symm=False):
+        n = len(ia) - 1
+        y = np.zeros(n)
+        self._err(self.lib.ref_mvm(n, _i(ia), _i(ja), _d(a), _d(x), _d(y), int(symm)))
+        return y
+
+    def solve_l(self, iu, ju, u, x):
+        n = len(iu) - 1
+        y = np.zeros(n)
+        self._err(self.lib.ref_solve_l(n, _i(iu), _i(ju), _d(u), _d(x), _d(y)))
+        return y
+
+    def solve_u(self, iu, ju, u, x):
+        n = len(iu) - 1
+        y = np.zeros(n)
+        self._err(self.lib.ref_solve_u(n, _i(iu), _i(ju), _d(u), _d(x), _d(y)))
+        return y
+
+    def ich2(self, ia, ja, a, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0):
+        n = len(ia) - 1
+        piu, pju, pu = _ip(), _ip(), _dp()
+        st = (C.c_double * 3)()
+        self._err(self.lib.ref_ich2(n, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+                                    C.c_double(theta), C.c_double(memory), C.byref(piu), C.byref(pju),
+                                    C.byref(pu), st))
+        iu, ju, u, _ = _take_csr(self.lib, n, piu, pju, pu)
+        for p in (piu, pju, pu):
+            self.lib.ref_free(p)
+        return iu, ju, u, (st[0], st[1], st[2])
+
+    def ilu2(self, ia, ja, a, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, sclmin=1e-8, pivmin=1e-8):
+        n = len(ia) - 1
+        pil, pjl, pl, piu, pju, pu = _ip(), _ip(), _dp(), _ip(), _ip(), _dp()
+        st = (C.c_double * 3)()
+        self._err(self.lib.ref_ilu2(n, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+                                    C.c_double(theta), C.c_double(memory), C.c_double(sclmin), C.c_double(pivmin),
+                                    C.byref(pil), C.byref(pjl), C.byref(pl), C.byref(piu), C.byref(pju),
+                                    C.byref(pu), st))
+        il, jl, lv, _ = _take_csr(self.lib, n, pil, pjl, pl)
+        iu, ju, uv, _ = _take_csr(self.lib, n, piu, pju, pu)
+        for p in (pil, pjl, pl, piu, pju, pu):
+            self.lib.ref_free(p)
+        return (il, jl, lv), (iu, ju, uv), (st[0], st[1], st[2])
+
+    def solve_symm(self, ia, ja, a, b, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, ittype=0,
+                   eps=1e-10, niter=1000, ichk=1):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        st = (C.c_double * 8)()
+        self._err(self.lib.ref_solve_symm(n, _i(ia), _i(ja), _d(a), _d(b), _d(x), fcttyp, C.c_double(tau1),
+                                          C.c_double(tau2), C.c_double(theta), C.c_double(memory), ittype,
+                                          C.c_double(eps), niter, ichk, st))
+        return x, dict(iters=int(st[0]), resfin=st[1], tfct=st[2], titr=st[3], density=st[4], density2=st[5],
+                       wall=st[6])
+
+    def cg(self, ia, ja, a, iu, ju, u, b, ittype=0, eps=1e-10, niter=1000, ichk=1):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        st = (C.c_double * 3)()
+        self._err(self.lib.ref_cg(n, _i(ia), _i(ja), _d(a), _i(iu), _i(ju), _d(u), _d(b), _d(x), ittype,
+                                  C.c_double(eps), niter, ichk, st))
+        return x, dict(iters=int(st[0]), resfin=st[1], wall=st[2])
+
+    def solver(self, ia, ja, a, b, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, sclmin=1e-8, pivmin=1e-8,
+               sttype=1, eps=1e-8, niter=1000, ichk=1):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        st = (C.c_double * 8)()
+        self._err(self.lib.ref_solver(n, _i(ia), _i(ja), _d(a), _d(b), _d(x), C.c_double(tau1), C.c_double(tau2),
+                                      C.c_double(theta), C.c_double(memory), C.c_double(sclmin),
+                                      C.c_double(pivmin), sttype, C.c_double(eps), niter, ichk, st))
+        return x, dict(iters=int(st[0]), resfin=st[1], tfct=st[2], titr=st[3], density=st[4], density2=st[5],
+                       wall=st[6])

@@ -1,0 +1,232 @@
+"""GPU parity of the solver path against the CPU oracle (oracle/bsl_oracle.c).
+
+Inputs are the seeded generators at sizes the oracle finishes in seconds.
+Tolerances: integer/pattern work is compared exactly; the factorisation is
+compared entry by entry (same arithmetic order and fma, so bit-exact unless a
+product lands within rounding of a threshold); products and solves that sum
+in a different order than the CPU loop are held to 1e-13 relative; Krylov
+solutions to their stopping tolerance.
+"""
+import numpy as np
+import pytest
+
+import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=torch.float64, device="cuda")
+
+
+def _nonsymmetric(s, skew=0.3):
+    """Convection-like perturbation of a heat matrix: off-diagonal (i,j) scaled
+    by 1 + skew*sign(j - i); stays diagonally dominant, loses symmetry."""
+    a = s.a.copy()
+    rows = np.repeat(np.arange(s.n), np.diff(s.ia))
+    off = s.ja != rows
+    a[off] *= 1.0 + skew * np.sign(s.ja[off] - rows[off])
+    return P.System(s.n, s.bs, s.ia, s.ja, a, s.rhs, s.parts)
+
+
+@pytest.fixture(scope="module")
+def heat():
+    return P.heat3d(14, 12, 10, sigma=1.0, seed=11)
+
+
+def test_spmv_csr_full_and_symmetric(ctx, oracle, heat):
+    import bsg
+    import torch
+    s = heat
+    u = s.upper()
+    x = np.random.default_rng(1).standard_normal(s.n)
+    ref = oracle.mvm(s.ia, s.ja, s.a, x)
+    ref_s = oracle.mvm(u.ia, u.ja, u.a, x, symm=True)
+    for sysm, symm, r in ((s, False, ref), (s, True, ref_s)):
+        m = bsg.Matrix.from_system(ctx, sysm, symm_upper=symm)
+        y = torch.empty(s.n, dtype=torch.float64, device="cuda")
+        m.mvm(_t(x), y)
+        got = y.cpu().numpy()
+        assert np.abs(got - r).max() <= 1e-13 * np.abs(r).max()
+        # host-buffer entry point
+        assert np.abs(m.mvm_host(x) - r).max() <= 1e-13 * np.abs(r).max()
+
+
+def test_spmm_multi_rhs(ctx, oracle, heat):
+    import bsg
+    import torch
+    s = heat
+    X = np.random.default_rng(2).standard_normal((5, s.n))
+    m = bsg.Matrix.from_system(ctx, s)
+    Y = torch.empty((5, s.n), dtype=torch.float64, device="cuda")
+    m.mvm_multi(_t(X), Y)
+    for r in range(5):
+        ref = oracle.mvm(s.ia, s.ja, s.a, X[r])
+        assert np.abs(Y[r].cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_spmv_bsr3(ctx, oracle):
+    import bsg
+    import torch
+    s = P.lame3d(6, 0.3, 1.0, 5)
+    x = np.random.default_rng(3).standard_normal(s.n * 3)
+    ref = oracle.bsr_mvm(s.ia, s.ja, s.a, x, 3)
+    m = bsg.Matrix.from_system(ctx, s)
+    y = torch.empty(s.n * 3, dtype=torch.float64, device="cuda")
+    m.mvm(_t(x), y)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    # symmetric (upper block triangle) input
+    u = s.upper()
+    ms = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+    ms.mvm(_t(x), y)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    del u
+
+
+def _factor_match(gpu, ora):
+    giu, gju, gl, gu = gpu
+    oiu, oju, ol, ou = ora[:4]
+    assert np.array_equal(giu, oiu), "row pointers differ"
+    assert np.array_equal(gju, oju), "column pattern differs"
+    scale = np.abs(ol).max()
+    assert np.abs(gl - ol).max() <= 1e-14 * scale
+    assert np.abs(gu - ou).max() <= 1e-14 * np.abs(ou).max()
+
+
+@pytest.mark.parametrize("tau1,tau2", [(1e-3, 1e-3), (1e-2, 1e-4)])
+def test_ich2_matches_oracle(ctx, oracle, heat, tau1, tau2):
+    import bsg
+    u = heat.upper()
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=tau1, tau2=tau2, theta=0.1, memory=20.0)
+    m = bsg.Matrix.from_system(ctx, heat, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    ora = oracle.fact(0, u.ia, u.ja, u.a, tau1=tau1, tau2=tau2, theta=0.1)
+    _factor_match(f.export(), ora)
+    assert abs(p.density - ora[4][0]) < 1e-12 and abs(p.density2 - ora[4][1]) < 1e-12
+
+
+@pytest.mark.parametrize("tau1,tau2", [(1e-3, 1e-3), (1e-2, 1e-4)])
+def test_ilu2_matches_oracle(ctx, oracle, heat, tau1, tau2):
+    import bsg
+    s = _nonsymmetric(heat)
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=tau1, tau2=tau2, theta=0.1, memory=20.0)
+    m = bsg.Matrix.from_system(ctx, s)
+    f = bsg.Factor(ctx, m, "ilu2", p)
+    sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, s.a)
+    ora = oracle.fact(1, sia, sja, al, au, tau1=tau1, tau2=tau2, theta=0.1)
+    _factor_match(f.export(), ora)
+
+
+def test_trisolve_exact_matches_oracle(ctx, oracle, heat):
+    import bsg
+    import torch
+    u = heat.upper()
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0)
+    m = bsg.Matrix.from_system(ctx, heat, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    iu, ju, l, uu = f.export()
+    x = np.random.default_rng(4).standard_normal(heat.n)
+    y = torch.empty(heat.n, dtype=torch.float64, device="cuda")
+    f.solve_l(_t(x), y, mode=0)
+    ref = oracle.solve_l(iu, ju, l, x)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+    f.solve_u(_t(x), y, mode=0)
+    ref = oracle.solve_u(iu, ju, uu, x)
+    assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_trisolve_jacobi_converges(ctx, oracle, heat):
+    import bsg
+    import torch
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-2, tau2=1e-4, memory=20.0)
+    m = bsg.Matrix.from_system(ctx, heat, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    iu, ju, l, uu = f.export()
+    x = np.random.default_rng(5).standard_normal(heat.n)
+    ref = oracle.solve_u(iu, ju, uu, x)
+    y = torch.empty(heat.n, dtype=torch.float64, device="cuda")
+    errs = []
+    for sw in (1, 4, 40):
+        f.solve_u(_t(x), y, mode=1, nsweeps=sw)
+        errs.append(np.linalg.norm(y.cpu().numpy() - ref) / np.linalg.norm(ref))
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-10
+
+
+def test_pcg_matches_oracle(ctx, oracle, heat):
+    import bsg
+    import torch
+    u = heat.upper()
+    b = heat.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, ittype=0, eps=1e-10)
+    m = bsg.Matrix.from_system(ctx, heat, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    x = torch.zeros(heat.n, dtype=torch.float64, device="cuda")
+    bsg.pcg(ctx, m, f, _t(b), x, p)
+    iu, ju, _, uu = f.export()
+    xo, it, _ = oracle.pcg(u.ia, u.ja, u.a, iu, ju, uu, b, ittype=0, eps=1e-10)
+    assert abs(p.nitperf - it) <= 1
+    xg = x.cpu().numpy()
+    assert np.linalg.norm(xg - xo) / np.linalg.norm(xo) < 1e-8
+    assert p.resfin < 1e-9
+
+
+@pytest.mark.parametrize("precision,trisolve", [(0, 0), (1, 0), (1, 1)])
+def test_gmres_nonsymmetric(ctx, oracle, heat, precision, trisolve):
+    import bsg
+    import torch
+    s = _nonsymmetric(heat)
+    b = s.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, sttype=1, eps=1e-8,
+                          restart=30, precision=precision, trisolve=trisolve, nsweeps=4, krylov=1)
+    m = bsg.Matrix.from_system(ctx, s)
+    f = bsg.Factor(ctx, m, "ilu2", p)
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    bsg.gmres(ctx, m, f, _t(b), x, p)
+    assert p.resfin <= 1e-8
+    sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, s.a)
+    oiu, oju, ol, ou, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    xo, it, _ = oracle.gmres(s.ia, s.ja, s.a, oiu, oju, ol, ou, b, m=30, eps=1e-10)
+    assert np.linalg.norm(x.cpu().numpy() - xo) / np.linalg.norm(xo) < 1e-6
+    if precision == 0 and trisolve == 0:
+        xg, itg, _ = oracle.gmres(s.ia, s.ja, s.a, oiu, oju, ol, ou, b, m=30, eps=1e-8)
+        assert abs(p.nitperf - itg) <= 1
+
+
+def test_solve_symm_host_driver(ctx, oracle, heat):
+    import bsg
+    u = heat.upper()
+    b = heat.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, ittype=0, eps=1e-10)
+    x = bsg.solve_symm(ctx, u.n, u.ia, u.ja, u.a, b, p)
+    oiu, oju, ou, _, _ = oracle.fact(0, u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3)
+    xo, it, _ = oracle.pcg(u.ia, u.ja, u.a, oiu, oju, ou, b, ittype=0, eps=1e-10)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+    assert p.resfin < 1e-9 and p.timefct > 0 and p.timeitr > 0
+
+
+def test_nonpositive_pivot_reports_reference_error(ctx):
+    import bsg
+    # 3x3 symmetric indefinite matrix, upper storage
+    ia = np.array([0, 2, 4, 5], np.int32)
+    ja = np.array([0, 1, 1, 2, 2], np.int32)
+    a = np.array([1.0, 2.0, 1.0, 0.5, 1.0])
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0)
+    m = bsg.Matrix(ctx, 3, ia, ja, a, symm_upper=True)
+    with pytest.raises(bsg.BsgError) as e:
+        bsg.Factor(ctx, m, "ich2", p)
+    assert e.value.code == bsg.ERR_PIVOT and "Diagonal pivot is nonpositive" in str(e.value)
+    # the context stays usable after the reported error
+    m2 = bsg.Matrix(ctx, 3, np.array([0, 1, 2, 3], np.int32), np.array([0, 1, 2], np.int32), np.ones(3),
+                    symm_upper=True)
+    bsg.Factor(ctx, m2, "ich2", p)
+
+
+def test_bad_csr_rejected(ctx):
+    import bsg
+    with pytest.raises(bsg.BsgError) as e:
+        bsg.Matrix(ctx, 2, np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32), np.ones(2))
+    assert e.value.code == bsg.ERR_ARG
+    with pytest.raises(bsg.BsgError) as e:
+        bsg.Matrix(ctx, 2, np.array([0, 1, 2], np.int32), np.array([0, 5], np.int32), np.ones(2))
+    assert e.value.code == bsg.ERR_ARG
