@@ -10,6 +10,7 @@ Naming follows Bslib: ``Matrix`` is a device CSMatrixR / CSMatrixRS,
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -134,12 +135,19 @@ class Context:
         self.h = C.c_void_p()
         _check(lib().bsg_create(C.byref(self.h), device, C.c_void_p(stream)))
         self.device = device
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, obj):
+        self._children.add(obj)
 
     def sync(self):
         _check(lib().bsg_sync(self.h))
 
     def close(self):
+        """Free every matrix / factor still alive on this context, then the context."""
         if self.h:
+            for obj in list(self._children):
+                obj.free()
             lib().bsg_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -165,6 +173,7 @@ class Matrix:
         else:
             _check(lib().bsg_mat_bsr(ctx.h, n, bs, _ip(ia_), _ip(ja_), _dp(a_), int(symm_upper), C.byref(self.h)))
         self._keep = None
+        ctx._adopt(self)
 
     @classmethod
     def from_system(cls, ctx, sysm, symm_upper=False):
@@ -211,6 +220,7 @@ class Factor:
         f = lib().bsg_fct_ich2 if kind == "ich2" else lib().bsg_fct_ilu2
         _check(f(ctx.h, mat.h, C.byref(self.param), C.byref(self.h)))
         self.kind = kind
+        ctx._adopt(self)
 
     def info(self):
         n, nnz, ll, lu = C.c_int(), C.c_int(), C.c_int(), C.c_int()

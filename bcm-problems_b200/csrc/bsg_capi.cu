@@ -17,8 +17,50 @@ int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nn
 int bsg_choose_group(double mean_row);
 int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
 int bsg_fct_make_fp32(bsg_fct *f);
+int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
 
 static thread_local char g_err[512] = "";
+unsigned long long g_bsg_launches = 0;
+
+extern "C" unsigned long long bsg_launch_count(void) { return g_bsg_launches; }
+
+// Average device time of `reps` back-to-back launches of one kernel, timed
+// with CUDA events on the context stream (kind 0: SpMV y = A x; kind 1 / 2:
+// forward / backward triangular solve in `mode` with `nsweeps`).  The
+// buffers are internal, so the call measures the kernel alone.
+extern "C" int bsg_time_kernel(bsg_ctx *c, int kind, const bsg_mat *m, const bsg_fct *f, int mode, int nsweeps,
+                               int reps, double *ms_per_launch) {
+	if (!c || reps < 1 || !ms_per_launch) return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: bad argument");
+	if ((kind == 0 && !m) || (kind != 0 && !f)) return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: missing object");
+	const size_t N = kind == 0 ? (size_t)m->n * m->bs : (size_t)f->n;
+	double *x, *y, *w;
+	BSG_CUDA(cudaMallocAsync(&x, sizeof(double) * N, c->stream));
+	BSG_CUDA(cudaMallocAsync(&y, sizeof(double) * N, c->stream));
+	BSG_CUDA(cudaMallocAsync(&w, sizeof(double) * N, c->stream));
+	int rc = bsg_fill_launch(c->stream, (long long)N, x, 1.0);
+	auto launch = [&]() {
+		if (kind == 0) return bsg_spmm_launch(m, 1, x, y, (long long)N, c->stream);
+		return bsg_trisolve_launch(c, f, kind == 1, mode, nsweeps, x, y, w);
+	};
+	for (int r = 0; r < 3 && !rc; r++) rc = launch(); // warm-up
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	cudaEventRecord(e0, c->stream);
+	for (int r = 0; r < reps && !rc; r++) rc = launch();
+	cudaEventRecord(e1, c->stream);
+	cudaEventSynchronize(e1);
+	float ms = 0;
+	cudaEventElapsedTime(&ms, e0, e1);
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaFreeAsync(x, c->stream);
+	cudaFreeAsync(y, c->stream);
+	cudaFreeAsync(w, c->stream);
+	if (!rc) rc = bsg_check_devstat(c);
+	*ms_per_launch = ms / reps;
+	return rc;
+}
 
 int bsg_set_error(int code, const char *msg) {
 	std::snprintf(g_err, sizeof(g_err), "%s", msg ? msg : "");
@@ -44,7 +86,9 @@ int bsg_check_devstat(bsg_ctx *c) {
 	char msg[160];
 	switch (h.code) {
 	case BSG_ERR_PIVOT: std::snprintf(msg, sizeof msg, " Ich2: Diagonal pivot is nonpositive (row %d)", h.where); break;
-	case BSG_ERR_WORKSPACE: std::snprintf(msg, sizeof msg, " Insufficient workspace in Ich2/Ilu2 (row %d)", h.where); break;
+	case BSG_ERR_WORKSPACE:
+		std::snprintf(msg, sizeof msg, " Insufficient workspace in Ich2/Ilu2 (row %d, check %d)", h.where, h.pad[0]);
+		break;
 	case BSG_ERR_TIMEOUT: std::snprintf(msg, sizeof msg, "device wait limit reached (index %d)", h.where); break;
 	case BSG_ERR_ARG: std::snprintf(msg, sizeof msg, "malformed matrix: missing or misplaced diagonal (row %d)", h.where); break;
 	default: std::snprintf(msg, sizeof msg, "device error %d at %d", h.code, h.where);
@@ -92,12 +136,12 @@ extern "C" int bsg_create(bsg_ctx **out, int device, void *stream) {
 	bsg_ctx *c = new (std::nothrow) bsg_ctx();
 	if (!c) return bsg_set_error(BSG_ERR_NOMEM, "bsg_create");
 	c->device = device;
-	if (stream) {
-		c->stream = (cudaStream_t)stream;
-		c->own_stream = false;
-	} else {
+	if (stream == BSG_OWN_STREAM) {
 		BSG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
 		c->own_stream = true;
+	} else {
+		c->stream = (cudaStream_t)stream; // NULL is the device's default stream
+		c->own_stream = false;
 	}
 	c->n_partials = 8192;
 	BSG_CUDA(cudaMalloc(&c->d_stat, sizeof(bsg_devstat)));
@@ -433,7 +477,8 @@ extern "C" int bsg_fct_free(bsg_fct *f) {
 	cudaStream_t s = f->ctx->stream;
 	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);
 	for (void *p : {(void *)f->d_iu, (void *)f->d_ju, (void *)f->d_u, (void *)f->d_dinv_l, (void *)f->d_dinv_u,
-	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f})
+	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f,
+	                (void *)f->d_perm})
 		if (p) cudaFreeAsync(p, s);
 	cudaStreamSynchronize(s);
 	delete f;

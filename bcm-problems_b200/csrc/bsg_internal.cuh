@@ -48,6 +48,14 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 __device__ __forceinline__ void st_release(int *p, int v) {
 	asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+	unsigned long long v;
+	asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+	asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const void *p) {
 	unsigned long long v;
 	asm volatile("ld.volatile.global.b64 %0, [%1];" : "=l"(v) : "l"(p));
@@ -61,8 +69,11 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
 	return t;
 }
-__device__ __forceinline__ void devstat_fail(bsg_devstat *st, int code, int where) {
-	if (atomicCAS(&st->code, 0, code) == 0) st->where = where;
+__device__ __forceinline__ void devstat_fail(bsg_devstat *st, int code, int where, int site = 0) {
+	if (atomicCAS(&st->code, 0, code) == 0) {
+		st->where = where;
+		st->pad[0] = site;
+	}
 }
 
 // Bit pattern that no arithmetic result carries (a signalling NaN payload);
@@ -123,9 +134,17 @@ struct bsg_fct {
 	double *d_ur_v, *d_lr_v;      // FP64 strict values
 	float *d_ur_f, *d_lr_f;       // FP32 strict values
 	int nnz_strict;
-	int levels_l, levels_u;       // dependency depth (diagnostic)
+	int *d_perm;                  // rows by (forward-solve level, index): claim order of the solves
+	int levels_l, levels_u;       // dependency depth
 	double density, density2;
 };
+
+// ---- launch accounting ------------------------------------------------------
+// Every kernel launch of the library adds to this process-wide counter
+// (bsg_launch_count() in the C ABI), so a benchmark can state how many of
+// its own kernels ran in a timed region.
+extern unsigned long long g_bsg_launches;
+#define BSG_COUNT(k) (g_bsg_launches += (unsigned long long)(k))
 
 // ---- internal entry points shared between translation units --------------
 int bsg_prepare_upper(bsg_mat *m);                       // builds d_iu/d_ju/d_al/d_au/d_it/d_jt

@@ -130,6 +130,7 @@ static inline int ew_grid(long long n) {
 
 int bsg_dots_launch(bsg_ctx *c, int q, int n, const double *x0, const double *y0, const double *x1,
                     const double *y1, const double *x2, const double *y2, double *d_out) {
+	BSG_COUNT(1);
 	if (q == 1)
 		k_dots<1><<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, x0, y0, x1, y1, x2, y2, c->d_partials, c->d_counters, d_out);
 	else if (q == 2)
@@ -146,6 +147,7 @@ int bsg_dot_launch(bsg_ctx *c, int n, const double *x, const double *y, double *
 // d_out[j] = V_j . w for j < k
 int bsg_mdot_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *w, double *d_out) {
 	for (int j0 = 0; j0 < k; j0 += 8) {
+		BSG_COUNT(1);
 		int kk = k - j0 < 8 ? k - j0 : 8;
 		const double *Vj = V + j0 * ld;
 		double *o = d_out + j0;
@@ -159,23 +161,28 @@ int bsg_mdot_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, con
 }
 
 int bsg_gemv_sub_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *h, double *w) {
+	BSG_COUNT(1);
 	k_gemv_sub<<<ew_grid(n), 256, 0, c->stream>>>(n, V, ld, k, h, w);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 int bsg_gemv_add_launch(bsg_ctx *c, int n, const double *V, long long ld, int k, const double *y, double *x) {
+	BSG_COUNT(1);
 	k_gemv_add<<<ew_grid(n), 256, 0, c->stream>>>(n, V, ld, k, y, x);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 int bsg_scale_by_launch(bsg_ctx *c, int n, const double *x, double *y, const double *num, const double *den,
                         int sqrt_den) {
+	BSG_COUNT(1);
 	k_scale_by<<<ew_grid(n), 256, 0, c->stream>>>(n, x, y, num, den, sqrt_den);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 int bsg_residual_launch(bsg_ctx *c, int n, const double *b, double *r) {
+	BSG_COUNT(1);
 	k_residual<<<ew_grid(n), 256, 0, c->stream>>>(n, b, r);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v) {
+	BSG_COUNT(1);
 	k_fill<<<ew_grid(n), 256, 0, s>>>((int)n, x, v);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }

@@ -112,7 +112,7 @@ __global__ void k_strict_transpose_keys(int n, const int *ia, const int *ja, uns
 	}
 }
 
-inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+inline int nblk(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
 
 } // namespace
 
@@ -158,6 +158,7 @@ int bsg_expand_symmetric(bsg_ctx *c, int n, const int *ia, const int *ja, const 
 	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * ndiag_max, c->stream));
 	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int), c->stream));
 	BSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), c->stream));
+	BSG_COUNT(4);
 	k_expand_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals, cnt);
 	int nk = 0;
 	BSG_CUDA(cudaMemcpyAsync(&nk, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -187,6 +188,7 @@ int bsg_combine_lu(bsg_ctx *c, int n, const int *ia, const int *ja, const double
 	int *vals, *flag, *pos;
 	BSG_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * nnz, c->stream));
 	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * nnz, c->stream));
+	BSG_COUNT(4);
 	k_split_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals);
 	int rc = bsg_sort_pairs(c, keys, vals, nnz, bits_for(n));
 	if (rc) return rc;
@@ -231,6 +233,7 @@ int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nn
 	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * (nnz > 0 ? nnz : 1), c->stream));
 	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int), c->stream));
 	BSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), c->stream));
+	BSG_COUNT(3);
 	k_strict_transpose_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals, cnt);
 	int nk = 0;
 	BSG_CUDA(cudaMemcpyAsync(&nk, cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

@@ -136,6 +136,7 @@ int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long
 	if (m->bs == 3) {
 		int g = grid_for(m->n);
 		for (int r0 = 0; r0 < nrhs;) {
+			BSG_COUNT(1);
 			int k = nrhs - r0;
 			const double *Xr = X + r0 * ld;
 			double *Yr = Y + r0 * ld;
@@ -150,6 +151,7 @@ int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long
 	const int rows_per_warp = 32 / G;
 	int g = grid_for((m->n + rows_per_warp - 1) / rows_per_warp);
 	for (int r0 = 0; r0 < nrhs;) {
+		BSG_COUNT(1);
 		int k = nrhs - r0;
 		const double *Xr = X + r0 * ld;
 		double *Yr = Y + r0 * ld;

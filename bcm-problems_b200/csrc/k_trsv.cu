@@ -22,19 +22,22 @@
 
 namespace {
 
+// Rows are claimed in the order of `perm` (ascending forward-solve level;
+// read backwards for U), a topological order of both dependency graphs that
+// keeps the rows in flight on the current wavefront.
 template <typename VT>
-__global__ void __launch_bounds__(256) k_trsv_syncfree(int n, int lower, const int *__restrict__ rp,
-                                                       const int *__restrict__ ci, const VT *__restrict__ v,
-                                                       int skip_first, const double *__restrict__ dinv,
-                                                       const double *__restrict__ x, double *y, unsigned *claim,
-                                                       bsg_devstat *st) {
+__global__ void __launch_bounds__(256) k_trsv_syncfree(int n, int lower, const int *__restrict__ perm,
+                                                       const int *__restrict__ rp, const int *__restrict__ ci,
+                                                       const VT *__restrict__ v, int skip_first,
+                                                       const double *__restrict__ dinv, const double *__restrict__ x,
+                                                       double *y, unsigned *claim, bsg_devstat *st) {
 	const int lane = threadIdx.x & 31;
 	for (;;) {
 		int t = 0;
 		if (lane == 0) t = (int)atomicAdd(claim, 1u);
 		t = __shfl_sync(0xffffffffu, t, 0);
 		if (t >= n) return;
-		const int row = lower ? t : n - 1 - t;
+		const int row = perm[lower ? t : n - 1 - t];
 		const int b = rp[row] + skip_first, e = rp[row + 1];
 		double s = 0.0;
 		for (int k = b + lane; k < e; k += 32) {
@@ -108,7 +111,7 @@ __global__ void k_to_f32(long long nk, const double *src, float *dst) {
 		dst[k] = (float)src[k];
 }
 
-inline int nb(long long n, int t) { return (int)((n + t - 1) / t); }
+inline int nb(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
 
 } // namespace
 
@@ -122,6 +125,7 @@ int bsg_fct_finish(bsg_ctx *c, bsg_fct *f) {
 	const int n = f->n;
 	BSG_CUDA(cudaMallocAsync(&f->d_dinv_l, sizeof(double) * n, s));
 	BSG_CUDA(cudaMallocAsync(&f->d_dinv_u, sizeof(double) * n, s));
+	BSG_COUNT(2); // diagonal inverse + value permutation
 	k_diag_inv<<<nb(n, 256), 256, 0, s>>>(n, f->d_iu, f->d_l, f->d_u, f->d_dinv_l, f->d_dinv_u);
 	int *perm = nullptr, nk = 0;
 	int rc = bsg_strict_transpose(c, n, f->d_iu, f->d_ju, f->nnz, &f->d_lr_i, &f->d_lr_j, &perm, &nk);
@@ -134,7 +138,6 @@ int bsg_fct_finish(bsg_ctx *c, bsg_fct *f) {
 	f->d_ur_i = f->d_iu;
 	f->d_ur_j = f->d_ju;
 	f->d_ur_v = f->d_u;
-	f->levels_l = f->levels_u = -1;
 	BSG_CUDA(cudaGetLastError());
 	BSG_CUDA(cudaStreamSynchronize(s));
 	return BSG_OK;
@@ -145,6 +148,7 @@ int bsg_fct_make_fp32(bsg_fct *f) {
 	cudaStream_t s = f->ctx->stream;
 	BSG_CUDA(cudaMallocAsync(&f->d_ur_f, sizeof(float) * (f->nnz > 0 ? f->nnz : 1), s));
 	BSG_CUDA(cudaMallocAsync(&f->d_lr_f, sizeof(float) * (f->nnz_strict > 0 ? f->nnz_strict : 1), s));
+	BSG_COUNT(2);
 	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz, f->d_u, f->d_ur_f);
 	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz_strict, f->d_lr_v, f->d_lr_f);
 	BSG_CUDA(cudaGetLastError());
@@ -168,6 +172,7 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 	const float *vf = lower ? f->d_lr_f : f->d_ur_f;
 	const bool use32 = f->fp32 != 0;
 	if (mode == 0) {
+		BSG_COUNT(2); // fill + solve
 		k_fill_u64<<<BSG_SMS * 4, 256, 0, s>>>(n, (unsigned long long *)y, BSG_PENDING);
 		unsigned *claim = c->d_counters + 1;
 		BSG_CUDA(cudaMemsetAsync(claim, 0, sizeof(unsigned), s));
@@ -175,9 +180,9 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 		int need = (n + 7) / 8;
 		if (grid > need) grid = need > 0 ? need : 1;
 		if (use32)
-			k_trsv_syncfree<float><<<grid, 256, 0, s>>>(n, lower, rp, ci, vf, skip, dinv, x, y, claim, c->d_stat);
+			k_trsv_syncfree<float><<<grid, 256, 0, s>>>(n, lower, f->d_perm, rp, ci, vf, skip, dinv, x, y, claim, c->d_stat);
 		else
-			k_trsv_syncfree<double><<<grid, 256, 0, s>>>(n, lower, rp, ci, vd, skip, dinv, x, y, claim, c->d_stat);
+			k_trsv_syncfree<double><<<grid, 256, 0, s>>>(n, lower, f->d_perm, rp, ci, vd, skip, dinv, x, y, claim, c->d_stat);
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}
 	if (nsweeps < 1) nsweeps = 1;
@@ -191,6 +196,7 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 	int cur = (nsweeps % 2 == 1) ? 0 : 1;
 	const double *yin = nullptr;
 	for (int sw = 0; sw < nsweeps; sw++) {
+		BSG_COUNT(1);
 		double *out = bufs[cur];
 		if (use32)
 			k_trsv_jacobi<G, float><<<grid, 256, 0, s>>>(n, rp, ci, vf, skip, dinv, x, yin, out);

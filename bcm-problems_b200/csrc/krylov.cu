@@ -136,6 +136,7 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 		if (c->h_pinned[S_BREAK] != 0.0) { status = BSG_ERR_BREAKDOWN; break; }
 		if (p->ittype == 0 && enrsq <= p->eps * p->eps * enrsq0) break;
 		if (p->ittype == 1 && enrsq <= p->eps * p->eps) break;
+		BSG_COUNT(3); // k_pcg_p, k_pcg_xr, k_copy_scalar
 		k_pcg_p<<<g, 256, 0, s>>>(N, z.p, pp.p, c->d_scalars, k == 1);
 		rc = bsg_spmm_launch(m, 1, pp.p, q.p, N, s);
 		if (rc) return rc;

@@ -87,8 +87,10 @@ typedef struct bsg_ctx bsg_ctx;
 typedef struct bsg_mat bsg_mat;
 typedef struct bsg_fct bsg_fct;
 
-/* Create a context on `device` with its own stream (stream == NULL) or on the
- * caller's cudaStream_t. */
+/* Create a context on `device` that runs on the caller's cudaStream_t
+ * (NULL: the device's default stream), or on a private non-blocking stream
+ * when stream == BSG_OWN_STREAM. */
+#define BSG_OWN_STREAM ((void *)-1)
 int bsg_create(bsg_ctx **ctx, int device, void *stream);
 int bsg_destroy(bsg_ctx *ctx);
 int bsg_sync(bsg_ctx *ctx);
@@ -161,6 +163,16 @@ int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const 
  * CombineLU + ILU2 + GMRES(restart), solution out. */
 int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
                    bsg_param *p);
+
+/* ---- measurement (no counterpart in the reference; it times with clock())  */
+/* Number of kernels this library has launched in the process so far. */
+unsigned long long bsg_launch_count(void);
+/* Average device time of `reps` launches of one kernel (kind 0: SpMV of m;
+ * 1 / 2: forward / backward solve with f in `mode`/`nsweeps`), CUDA events. */
+int bsg_time_kernel(bsg_ctx *ctx, int kind, const bsg_mat *m, const bsg_fct *f, int mode, int nsweeps, int reps,
+                    double *ms_per_launch);
+/* Scheduler counters of the last factorisation (see k_fact.cu). */
+int bsg_fact_stats(unsigned long long *out, int nout);
 
 #ifdef __cplusplus
 }

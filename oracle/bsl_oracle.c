@@ -125,6 +125,26 @@ int orc_combine_lu(int n, const int *ia, const int *ja, const double *a, int **i
 	return out;
 }
 
+/* Optional dependency-depth outputs of orc_fact (see orc_fact_levels). */
+static int *g_lev_fact, *g_lev_solve, *g_dropdep, *g_nmember, *g_nmask;
+
+/* Theta compensations received by a row are summed in 128-bit fixed point
+ * (value * 2^96, truncated per term): integer addition makes the sum
+ * independent of the order of the terms, which is what lets the GPU collect
+ * them from rows that finish in any order.  acc[2j] is the low word,
+ * acc[2j+1] the high word. */
+static void acc_push(unsigned long long *acc, int j, double comp) {
+	const double x = comp * 0x1p96;
+	const unsigned long long hi = (unsigned long long)(x * 0x1p-64);
+	const unsigned long long lo = (unsigned long long)(x - (double)hi * 0x1p64);
+	const unsigned long long old = acc[2 * j];
+	acc[2 * j] = old + lo;
+	acc[2 * j + 1] += hi + ((old + lo < lo) ? 1ull : 0ull);
+}
+static double acc_value(const unsigned long long *acc, int j) {
+	return ((double)acc[2 * j + 1] * 0x1p64 + (double)acc[2 * j]) * 0x1p-96;
+}
+
 /* Growable arrays for the stored rows of the working factor. */
 typedef struct { int *col; signed char *flag; double *gl, *gu; size_t len, cap; } pool_t;
 
@@ -186,10 +206,11 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 	int *madj = (int *)malloc(sizeof(int) * (size_t)n);
 	int *iv = (int *)malloc(sizeof(int) * (size_t)n);
 	int *contrib = (int *)malloc(sizeof(int) * (size_t)n);
+	unsigned long long *acc = (unsigned long long *)calloc(2 * (size_t)n, sizeof(unsigned long long));
 	pool_t P = {0};
 	int rc = 0;
 	if (!scll || !sclu || !diagg || !fl || !fu || !imask || !lst || !keep || !rowbeg || !ibegm || !madj || !iv ||
-	    !contrib) { rc = -1; goto done; }
+	    !contrib || !acc) { rc = -1; goto done; }
 
 	for (int i = 0; i < n; i++) {
 		double d = al[ia[i]];
@@ -213,7 +234,8 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 		int nl = 0;
 		/* init (Ich2InitRow / Ilu2InitRow) */
 		lst[nl++] = i; imask[i] = i;
-		fl[i] = diagg[i]; fu[i] = diagg[i];
+		fl[i] = diagg[i] + acc_value(acc, i);
+		fu[i] = fl[i];
 		for (int k = ia[i] + 1; k < ia[i + 1]; k++) {
 			int j = ja[k];
 			lst[nl++] = j; imask[j] = i;
@@ -225,6 +247,18 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 		int nc = 0;
 		for (int r = ibegm[i]; r != -1; r = madj[r]) contrib[nc++] = r;
 		qsort(contrib, (size_t)nc, sizeof(int), cmp_int);
+		if (g_lev_fact) {
+			/* dependency depth: 1 + deepest row that updated or compensated i */
+			int lf = g_dropdep ? g_dropdep[i] : 0, ls = 0;
+			for (int t = 0; t < nc; t++) {
+				int k = contrib[t];
+				if (g_lev_fact[k] + 1 > lf) lf = g_lev_fact[k] + 1;
+				if (P.flag[iv[k]] == 0 && g_lev_solve[k] + 1 > ls) ls = g_lev_solve[k] + 1;
+			}
+			g_lev_fact[i] = lf;
+			g_lev_solve[i] = ls;
+			if (g_nmember) g_nmember[i] += nc; /* plus the droppers counted in the filter */
+		}
 		for (int t = 0; t < nc; t++) {
 			int k = contrib[t];
 			size_t e0 = (size_t)iv[k];
@@ -261,6 +295,7 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 		if (!ilu) for (int s = 0; s < nl; s++) fu[lst[s]] = fl[lst[s]];
 		/* filter in ascending column order (Ich2FiltrRow / Ilu2FiltrRow) */
 		qsort(lst + 1, (size_t)(nl - 1), sizeof(int), cmp_int);
+		if (g_nmask) g_nmask[i] = nl - 1;
 		int nk = 0;
 		for (int s = 1; s < nl; s++) {
 			int j = lst[s];
@@ -272,7 +307,9 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 				v *= theta;
 				fl[i] += v;
 				fu[i] += v;
-				diagg[j] += v;
+				acc_push(acc, j, v);
+				if (g_dropdep && g_lev_fact[i] + 1 > g_dropdep[j]) g_dropdep[j] = g_lev_fact[i] + 1;
+				if (g_nmember) g_nmember[j]++;
 			}
 		}
 		/* pivot and scale */
@@ -353,7 +390,7 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 	}
 done:
 	free(scll); free(sclu); free(diagg); free(fl); free(fu); free(imask); free(lst); free(keep); free(rowbeg);
-	free(ibegm); free(madj); free(iv); free(contrib);
+	free(ibegm); free(madj); free(iv); free(contrib); free(acc);
 	free(P.col); free(P.flag); free(P.gl); free(P.gu);
 	return rc;
 }
@@ -477,4 +514,31 @@ int orc_gmres(int n, const int *ia, const int *ja, const double *a, const int *i
 	if (resfin) *resfin = bnorm > 0 ? beta / bnorm : 0.0;
 	free(V); free(Z); free(H); free(cs); free(sn); free(g); free(y); free(w); free(t);
 	return it;
+}
+
+/* orc_fact plus, per row, the depth of the row in the factorisation's
+ * dependency graph (lev_fact: longest chain of updating / compensating rows)
+ * and in the forward-solve graph (lev_solve: longest chain through U
+ * entries), and optionally the size of C(i) (rows that update or
+ * compensate row i) and of row i's mask before filtering.  Used to size and
+ * check the GPU schedule. */
+int orc_fact_levels(int kind, int n, const int *ia, const int *ja, const double *al, const double *au, double tau1,
+                    double tau2, double theta, double sclmin, double pivmin, int *lev_fact, int *lev_solve,
+                    int *nmember, int *nmask) {
+	int *iu, *ju;
+	double *lv, *uv;
+	g_lev_fact = lev_fact;
+	g_lev_solve = lev_solve;
+	g_nmember = nmember;
+	g_nmask = nmask;
+	if (nmember) memset(nmember, 0, sizeof(int) * (size_t)n);
+	g_dropdep = (int *)calloc((size_t)n, sizeof(int));
+	int rc = orc_fact(kind, n, ia, ja, al, au, tau1, tau2, theta, sclmin, pivmin, &iu, &ju, &lv, &uv, NULL);
+	free(g_dropdep);
+	g_lev_fact = g_lev_solve = g_dropdep = g_nmember = g_nmask = NULL;
+	if (rc == 0) {
+		free(iu); free(ju); free(lv);
+		if (uv != lv) free(uv);
+	}
+	return rc;
 }
