@@ -18,11 +18,23 @@ int bsg_choose_group(double mean_row);
 int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
 int bsg_fct_make_fp32(bsg_fct *f);
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
+int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const double *x, const double *yin,
+                              double *yout);
 
 static thread_local char g_err[512] = "";
 unsigned long long g_bsg_launches = 0;
 
 extern "C" unsigned long long bsg_launch_count(void) { return g_bsg_launches; }
+
+// Stored entries (padding included) of the SELL copies: [0] the matrix,
+// [1] strict L rows, [2] strict U rows of the factor (0 where absent).
+extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out) {
+	if (!out) return bsg_set_error(BSG_ERR_ARG, "bsg_sell_stats: null output");
+	out[0] = m ? m->sell.entries : 0;
+	out[1] = f ? f->sl.entries : 0;
+	out[2] = f ? f->su.entries : 0;
+	return BSG_OK;
+}
 
 // Average device time of `reps` back-to-back launches of one kernel, timed
 // with CUDA events on the context stream (kind 0: SpMV y = A x; kind 1 / 2:
@@ -38,8 +50,10 @@ extern "C" int bsg_time_kernel(bsg_ctx *c, int kind, const bsg_mat *m, const bsg
 	BSG_CUDA(cudaMallocAsync(&y, sizeof(double) * N, c->stream));
 	BSG_CUDA(cudaMallocAsync(&w, sizeof(double) * N, c->stream));
 	int rc = bsg_fill_launch(c->stream, (long long)N, x, 1.0);
+	if (!rc) rc = bsg_fill_launch(c->stream, (long long)N, w, 0.5);
 	auto launch = [&]() {
 		if (kind == 0) return bsg_spmm_launch(m, 1, x, y, (long long)N, c->stream);
+		if (mode == 1) return bsg_trisolve_sweep_launch(c, f, kind == 1, x, w, y); // one full sweep
 		return bsg_trisolve_launch(c, f, kind == 1, mode, nsweeps, x, y, w);
 	};
 	for (int r = 0; r < 3 && !rc; r++) rc = launch(); // warm-up
@@ -144,6 +158,16 @@ extern "C" int bsg_create(bsg_ctx **out, int device, void *stream) {
 		c->own_stream = false;
 	}
 	c->n_partials = 8192;
+	// Keep freed device memory in the stream-ordered pool: factor pools and
+	// Krylov bases are reallocated on every solve, and returning them to the
+	// driver at each synchronisation would re-map gigabytes per solve.
+	{
+		cudaMemPool_t pool;
+		if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+			unsigned long long keep = ~0ull;
+			cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+		}
+	}
 	BSG_CUDA(cudaMalloc(&c->d_stat, sizeof(bsg_devstat)));
 	BSG_CUDA(cudaMalloc(&c->d_scalars, 64 * sizeof(double)));
 	BSG_CUDA(cudaMalloc(&c->d_partials, c->n_partials * sizeof(double)));
@@ -231,6 +255,8 @@ static int mat_finish_point(bsg_mat *m, const int *d_up_ia, const int *d_up_ja, 
 	}
 	int nt = 0;
 	rc = bsg_strict_transpose(c, m->n, m->d_iu, m->d_ju, m->nnz_up, &m->d_it, &m->d_jt, nullptr, &nt);
+	if (rc) return rc;
+	rc = bsg_sell_build(c, m->n, m->d_ia, m->d_ja, m->d_a, 0, 0, &m->sell);
 	if (rc) return rc;
 	m->group = bsg_choose_group(m->n > 0 ? (double)m->nnz / m->n : 1.0);
 	BSG_CUDA(cudaStreamSynchronize(c->stream));
@@ -370,6 +396,7 @@ extern "C" int bsg_mat_bsr(bsg_ctx *c, int nsup, int bs, const int *ia, const in
 extern "C" int bsg_mat_free(bsg_mat *m) {
 	if (!m) return BSG_OK;
 	cudaStream_t s = m->ctx->stream;
+	bsg_sell_free(&m->sell, s);
 	if (m->d_au && m->d_au != m->d_al) cudaFreeAsync(m->d_au, s);
 	for (void *p : {(void *)m->d_ia, (void *)m->d_ja, (void *)m->d_a, (void *)m->d_iu, (void *)m->d_ju,
 	                (void *)m->d_al, (void *)m->d_it, (void *)m->d_jt})
@@ -475,6 +502,8 @@ extern "C" int bsg_fct_info(const bsg_fct *f, int *n, int *nnz, int *levels_l, i
 extern "C" int bsg_fct_free(bsg_fct *f) {
 	if (!f) return BSG_OK;
 	cudaStream_t s = f->ctx->stream;
+	bsg_sell_free(&f->sl, s);
+	bsg_sell_free(&f->su, s);
 	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);
 	for (void *p : {(void *)f->d_iu, (void *)f->d_ju, (void *)f->d_u, (void *)f->d_dinv_l, (void *)f->d_dinv_u,
 	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f,

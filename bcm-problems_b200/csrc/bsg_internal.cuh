@@ -100,6 +100,24 @@ struct bsg_ctx {
 	int spmv_group;          // autotuned sub-warp size for CSR SpMV (0 = choose per matrix)
 };
 
+// SELL-32: slices of 32 rows, entries column-major inside a slice (k_sell.cu).
+struct bsg_sell {
+	int n = 0;
+	int fp32 = 0;
+	long long entries = 0;   // stored entries including padding
+	long long *off = nullptr; // slice offsets [nslices + 1]
+	int *col = nullptr;
+	void *val = nullptr;      // float or double
+	int *perm = nullptr;      // slot -> row when rows are sorted by length in windows (SELL-C-sigma)
+};
+// sigma > 0: sort rows by length inside windows of sigma rows first
+int bsg_sell_build(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, int fp32,
+                   bsg_sell *out, int sigma = 0);
+void bsg_sell_free(bsg_sell *m, cudaStream_t s);
+int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y);
+int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const double *yin,
+                   int scaled_in, double *yout);
+
 struct bsg_mat {
 	bsg_ctx *ctx;
 	int n;        // rows (point) or block rows
@@ -115,6 +133,7 @@ struct bsg_mat {
 	double *d_al, *d_au;  // ILU2 split values (al == au for symmetric input)
 	int *d_it, *d_jt;     // transpose of the strict upper pattern: rows k < i with (k,i) stored
 	int group;            // CSR SpMV sub-warp size
+	bsg_sell sell;        // SELL-32 copy of a point matrix (single-vector SpMV)
 };
 
 struct bsg_fct {
@@ -135,6 +154,7 @@ struct bsg_fct {
 	float *d_ur_f, *d_lr_f;       // FP32 strict values
 	int nnz_strict;
 	int *d_perm;                  // rows by (forward-solve level, index): claim order of the solves
+	bsg_sell sl, su;              // SELL-32 strict L / U rows (Jacobi sweeps), FP64 or FP32
 	int levels_l, levels_u;       // dependency depth
 	double density, density2;
 };

@@ -77,7 +77,8 @@ struct FactArgs {
 	long long pool_cap;
 	unsigned long long *pool_len;
 	unsigned long long *rec;     // per-row record (see REC_*)
-	unsigned long long *acc;     // per-row fixed-point compensation: [2i] low, [2i+1] high word
+	unsigned long long *acc;     // per-row fixed-point compensation sum
+	double acc_scale, acc_inv_scale;
 	int *lev;
 	int *nstat, *whead, *wnext;
 	int *queue;
@@ -90,7 +91,7 @@ struct FactArgs {
 
 // Scheduler / phase counters summed over all warps of the last factorisation.
 enum { FS_TRY = 0, FS_PARK, FS_CYC_POP, FS_CYC_CLOSE, FS_CYC_BLOCKED, FS_CYC_PREF, FS_CYC_UPD, FS_CYC_FIN,
-       FS_CONTRIB, FS_MASK, FACT_NSTAT = 16 };
+       FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FACT_NSTAT = 16 };
 struct PhaseClock {
 	unsigned long long v[FACT_NSTAT];
 };
@@ -137,31 +138,32 @@ __device__ int hfind_insert(WarpShared &s, int c) {
 }
 
 // Insert row k into the member set; 1 if new, 0 if present, -1 if full.
+// Most candidates are already members: probe with plain reads, CAS only
+// into an empty slot.
 __device__ int wset_insert(WarpShared &s, int k) {
 	unsigned h = hash_u(k) & (2 * CMAX - 1);
 	for (int probe = 0; probe < 2 * CMAX; probe++) {
-		int old = atomicCAS(&s.wset[h], -1, k);
-		if (old == -1) return 1;
-		if (old == k) return 0;
+		int cur = s.wset[h];
+		if (cur == k) return 0;
+		if (cur == -1) {
+			int old = atomicCAS(&s.wset[h], -1, k);
+			if (old == -1) return 1;
+			if (old == k) return 0;
+		}
 		h = (h + 1) & (2 * CMAX - 1);
 	}
 	return -1;
 }
 
-// Add a nonnegative compensation to row j's 128-bit fixed-point accumulator
-// (value * 2^96, truncated); the carry is resolved per addition, so the sum
-// is exact integer arithmetic and independent of the order of the adds.
-__device__ void acc_push(unsigned long long *acc, int j, double comp) {
-	const double x = comp * 0x1p96;
-	const unsigned long long hi = (unsigned long long)(x * 0x1p-64);
-	const unsigned long long lo = (unsigned long long)(x - (double)hi * 0x1p64);
-	const unsigned long long old = atomicAdd(acc + 2 * j, lo);
-	const unsigned long long carry = (old + lo < lo) ? 1ull : 0ull;
-	if (hi + carry) atomicAdd(acc + 2 * j + 1, hi + carry);
+// Add a nonnegative compensation to row j's 64-bit fixed-point accumulator
+// (value * 2^scale_bits, truncated): integer addition makes the sum exact and
+// independent of the order of the adds, and a reduction without return value
+// costs no round trip.  scale_bits leaves room for 2^12 maximal terms.
+__device__ void acc_push(unsigned long long *acc, int j, double comp, double scale) {
+	atomicAdd(acc + j, (unsigned long long)(comp * scale));
 }
-__device__ double acc_value(const unsigned long long *acc, int j) {
-	const unsigned long long lo = __ldcg(acc + 2 * j), hi = __ldcg(acc + 2 * j + 1);
-	return __dmul_rn(__dadd_rn(__dmul_rn((double)hi, 0x1p64), (double)lo), 0x1p-96);
+__device__ double acc_value(const unsigned long long *acc, int j, double inv_scale) {
+	return __dmul_rn((double)__ldcg(acc + j), inv_scale);
 }
 
 __device__ void q_push(const FactArgs &A, int row) {
@@ -325,6 +327,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 	// ---- close C(i): rounds over the newest members, one member per lane
 	int err = 0, levmax = 0;
 	for (int lo = 0; lo < s.nW && !err;) {
+		pc.v[FS_ROUNDS]++;
 		const int hi = min(s.nW, CMAX);
 		for (int base = lo; base < hi; base += 32) {
 			const int t = base + lane;
@@ -377,7 +380,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		}
 		s.Wb[nW] = b;
 	}
-	const double comp = acc_value(A.acc, i);
+	const double comp = acc_value(A.acc, i, A.acc_inv_scale);
 	__syncwarp();
 	const long long c2 = clock64();
 	pc.v[FS_CYC_PREF] += c2 - c1;
@@ -420,6 +423,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 			return -2;
 		}
 		const int gb = s.Wb[t0], npf = s.Wb[t1] - gb;
+		long long g0 = clock64();
 		// prefetch: 4 independent loads per lane in flight
 		for (int f0 = 0; f0 < npf; f0 += 128) {
 			unsigned c4[4];
@@ -445,6 +449,8 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 			}
 		}
 		__syncwarp();
+		long long g1 = clock64();
+		pc.v[FS_CYC_PF] += g1 - g0;
 		// phase A: accumulator slot of every entry, in parallel (R x R gets none)
 		for (int f = lane; f < npf; f += 32) {
 			int lo = t0, hi = t1 - 1;
@@ -459,6 +465,8 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		}
 		err = __reduce_min_sync(0xffffffffu, err);
 		__syncwarp();
+		long long g2 = clock64();
+		pc.v[FS_CYC_PA] += g2 - g1;
 		// phase B: ascending members, fma(-l, g, f) per column
 		for (int t = t0; t < t1 && !err; t++) {
 			if (s.Wfs[t] == F_D) continue;
@@ -479,6 +487,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 			}
 			__syncwarp();
 		}
+		pc.v[FS_CYC_PB] += clock64() - g2;
 		t0 = t1;
 		__syncwarp();
 	}
@@ -583,7 +592,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		const int h = s.lsts[t];
 		double v = fabs(s.hl[h]);
 		if (ilu) v = fmax(v, fabs(s.hu[h]));
-		if (!(v >= A.tau2)) acc_push(A.acc, s.hkey[h], __dmul_rn(v, A.theta));
+		if (!(v >= A.tau2)) acc_push(A.acc, s.hkey[h], __dmul_rn(v, A.theta), A.acc_scale);
 	}
 	if (lane == 0) A.lev[i] = levmax;
 	__threadfence();
@@ -653,8 +662,7 @@ __global__ void k_fact_init(int n, const int *it, int *nstat, int *whead, unsign
 	nstat[i] = it[i + 1] - it[i];
 	whead[i] = W_EMPTY;
 	rec[i] = 0;
-	acc[2 * i] = 0;
-	acc[2 * i + 1] = 0;
+	acc[i] = 0;
 	lev[i] = 0;
 }
 // Initial queue: the rows with no static contributor.
@@ -745,6 +753,19 @@ inline int nb(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
 
 int bsg_fct_finish(bsg_ctx *c, bsg_fct *f);
 
+// Scale of the fixed-point compensation sums: a compensation is below
+// tau2 * theta < 2^e, so 2^(51 - e) leaves room for 2^12 maximal terms in 63
+// bits; the rule is exact (frexp) so the oracle derives the same scale.
+void bsg_comp_scale(double tau2, double theta, double *scale, double *inv_scale) {
+	int e = -13;
+	double maxterm = tau2 * theta;
+	if (maxterm > 0.0) frexp(maxterm, &e);
+	int bits = 51 - e;
+	if (bits > 1000) bits = 1000;
+	*scale = ldexp(1.0, bits);
+	*inv_scale = ldexp(1.0, -bits);
+}
+
 static unsigned long long g_fact_stats[FACT_NSTAT];
 
 // Counters of the last factorisation in this process: [0] row tries,
@@ -780,7 +801,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	if (kind == 1 && cudaMallocAsync(&pu, sizeof(double) * cap, st) != cudaSuccess)
 		return bsg_set_error(BSG_ERR_NOMEM, "factor pool");
 	BSG_CUDA(cudaMallocAsync(&rec, sizeof(unsigned long long) * n, st));
-	BSG_CUDA(cudaMallocAsync(&acc, sizeof(unsigned long long) * 2 * n, st));
+	BSG_CUDA(cudaMallocAsync(&acc, sizeof(unsigned long long) * n, st));
 	BSG_CUDA(cudaMallocAsync(&lev, sizeof(int) * n, st));
 	BSG_CUDA(cudaMallocAsync(&nstat, sizeof(int) * n, st));
 	BSG_CUDA(cudaMallocAsync(&whead, sizeof(int) * n, st));
@@ -810,6 +831,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	A.tau1 = p->tau1; A.tau2 = p->tau2; A.theta = p->theta; A.pivmin = p->pivmin;
 	A.pool_cf = cf; A.pool_l = pl; A.pool_u = pu; A.pool_cap = cap; A.pool_len = pool_len;
 	A.rec = rec; A.acc = acc; A.lev = lev;
+	bsg_comp_scale(p->tau2, p->theta, &A.acc_scale, &A.acc_inv_scale);
 	A.nstat = nstat; A.whead = whead; A.wnext = wnext; A.queue = queue; A.qcap = qcap;
 	A.qhead = qhead; A.qtail = qtail; A.done_count = done_count; A.st = c->d_stat;
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));

@@ -15,8 +15,17 @@
 //   * multi-RHS: the same sweeps carry K right-hand sides so the matrix is
 //     read once for all of them.
 #include "bsg_internal.cuh"
+#include "k_stream.cuh"
 
 namespace {
+
+// Point CSR, one right-hand side: row-chunk streaming (k_stream.cuh).
+__global__ void __launch_bounds__(256) k_spmv_stream(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                                                     const double *__restrict__ a, const double *__restrict__ x,
+                                                     double *__restrict__ y) {
+	__shared__ double prod[8][STREAM_CAP];
+	stream_rows<double, IN_VEC, OUT_SUM>(n, ia, ja, a, 0, x, nullptr, nullptr, nullptr, y, prod[threadIdx.x >> 5]);
+}
 
 __device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
 __device__ __forceinline__ int ld_stream(const int *p) { return __ldcs(p); }
@@ -147,6 +156,13 @@ int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}
 	if (m->bs != 1) return BSG_ERR_UNSUPPORTED;
+	if (nrhs == 1) {
+		if (m->sell.off) return bsg_sell_spmv(s, &m->sell, X, Y);
+		BSG_COUNT(1);
+		int warps = (m->n + STREAM_ROWS - 1) / STREAM_ROWS;
+		k_spmv_stream<<<grid_for(warps), 256, 0, s>>>(m->n, m->d_ia, m->d_ja, m->d_a, X, Y);
+		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	}
 	const int G = m->group;
 	const int rows_per_warp = 32 / G;
 	int g = grid_for((m->n + rows_per_warp - 1) / rows_per_warp);

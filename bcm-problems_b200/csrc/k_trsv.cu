@@ -19,8 +19,28 @@
 //   a fixed polynomial in the factor, so it is a valid flexible (FGMRES)
 //   preconditioner and, applied symmetrically, a valid PCG preconditioner.
 #include "bsg_internal.cuh"
+#include "k_stream.cuh"
+
+#define SELL_SIGMA 128 // rows per length-sorting window of the factor's sliced copies
 
 namespace {
+
+// One Jacobi sweep y_out = D^{-1}(x - N y_in) by row-chunk streaming; with
+// IN == IN_SCALED the input is the first iterate D^{-1} x, formed on the fly
+// (the first two sweeps in one pass).
+template <typename VT, int IN>
+__global__ void __launch_bounds__(256) k_trsv_sweep(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                                    const VT *__restrict__ v, int skip,
+                                                    const double *__restrict__ dinv, const double *__restrict__ x,
+                                                    const double *__restrict__ yin, double *__restrict__ yout) {
+	__shared__ double prod[8][STREAM_CAP];
+	stream_rows<VT, IN, OUT_SWEEP>(n, rp, ci, v, skip, IN == IN_VEC ? yin : x, dinv, x, dinv, yout,
+	                               prod[threadIdx.x >> 5]);
+}
+
+__global__ void k_scale_vec(int n, const double *x, const double *d, double *y) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[i] * d[i];
+}
 
 // Rows are claimed in the order of `perm` (ascending forward-solve level;
 // read backwards for U), a topological order of both dependency graphs that
@@ -138,6 +158,11 @@ int bsg_fct_finish(bsg_ctx *c, bsg_fct *f) {
 	f->d_ur_i = f->d_iu;
 	f->d_ur_j = f->d_ju;
 	f->d_ur_v = f->d_u;
+	// factor rows vary in length from row to row (thresholds): sort them by
+	// length inside windows of SELL_SIGMA rows so the slices need little padding
+	rc = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 0, &f->sl, SELL_SIGMA);
+	if (!rc) rc = bsg_sell_build(c, n, f->d_iu, f->d_ju, f->d_u, 1, 0, &f->su, SELL_SIGMA);
+	if (rc) return rc;
 	BSG_CUDA(cudaGetLastError());
 	BSG_CUDA(cudaStreamSynchronize(s));
 	return BSG_OK;
@@ -152,11 +177,29 @@ int bsg_fct_make_fp32(bsg_fct *f) {
 	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz, f->d_u, f->d_ur_f);
 	k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz_strict, f->d_lr_v, f->d_lr_f);
 	BSG_CUDA(cudaGetLastError());
+	// the sweeps read the SELL copies: rebuild them with FP32 values
+	bsg_sell_free(&f->sl, s);
+	bsg_sell_free(&f->su, s);
+	int rc = bsg_sell_build(f->ctx, f->n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 1, &f->sl, SELL_SIGMA);
+	if (!rc) rc = bsg_sell_build(f->ctx, f->n, f->d_iu, f->d_ju, f->d_u, 1, 1, &f->su, SELL_SIGMA);
+	if (rc) return rc;
 	f->fp32 = 1;
 	return BSG_OK;
 }
 
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
+
+// One full Jacobi sweep y_out = D^{-1}(x - N y_in) (reads the whole factor);
+// used to time the sweep kernel on its own.
+int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const double *x, const double *yin,
+                              double *yout) {
+	const int n = f->n;
+	const int *rp = lower ? f->d_lr_i : f->d_ur_i;
+	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
+	const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
+	(void)n; (void)rp; (void)ci;
+	return bsg_sell_sweep(c->stream, lower ? &f->sl : &f->su, x, dinv, yin, 0, yout);
+}
 
 // Solve with L (lower != 0) or U.  x and y must not alias.  `work` (n
 // doubles) is needed for mode 1 with nsweeps > 1.
@@ -186,24 +229,29 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}
 	if (nsweeps < 1) nsweeps = 1;
-	if (nsweeps > 1 && !work) return BSG_ERR_ARG;
-	const int G = 16;
-	int grid = ((n + 1) / 2 + 7) / 8;
+	if (nsweeps > 2 && !work) return BSG_ERR_ARG;
+	if (nsweeps == 1) { // the first iterate only: y = D^{-1} x
+		BSG_COUNT(1);
+		k_scale_vec<<<BSG_SMS * 8, 256, 0, s>>>(n, x, dinv, y);
+		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	}
+	int grid = ((n + STREAM_ROWS - 1) / STREAM_ROWS + 7) / 8;
 	if (grid > BSG_SMS * 8) grid = BSG_SMS * 8;
 	if (grid < 1) grid = 1;
-	// ping-pong so that the last sweep lands in y
+	// nsweeps - 1 passes (the first two iterates share one), ping-pong so
+	// that the last pass lands in y
+	const int passes = nsweeps - 1;
 	double *bufs[2] = {y, work};
-	int cur = (nsweeps % 2 == 1) ? 0 : 1;
+	int cur = (passes + 1) % 2;
 	const double *yin = nullptr;
-	for (int sw = 0; sw < nsweeps; sw++) {
-		BSG_COUNT(1);
+	const bsg_sell *sm = lower ? &f->sl : &f->su;
+	(void)grid; (void)rp; (void)ci; (void)vf; (void)vd; (void)skip;
+	for (int p = 0; p < passes; p++) {
 		double *out = bufs[cur];
-		if (use32)
-			k_trsv_jacobi<G, float><<<grid, 256, 0, s>>>(n, rp, ci, vf, skip, dinv, x, yin, out);
-		else
-			k_trsv_jacobi<G, double><<<grid, 256, 0, s>>>(n, rp, ci, vd, skip, dinv, x, yin, out);
+		int rc = bsg_sell_sweep(s, sm, x, dinv, yin, p == 0, out);
+		if (rc) return rc;
 		yin = out;
 		cur ^= 1;
 	}
-	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	return BSG_OK;
 }

@@ -119,7 +119,7 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 	if (!rc) rc = bsg_residual_launch(c, N, d_b, r.p);
 	if (rc) return rc;
 	double enrsq0 = 0.0, enrsq = 0.0;
-	int k, nit = 0, status = BSG_OK;
+	int k, nit = 0, status = BSG_OK, replacements = 0;
 	const int g = ew_grid(N);
 	for (k = 1; k < p->niter; k++) {
 		rc = bsg_precond_apply(c, f, p, r.p, z.p, t.p, w.p);
@@ -134,8 +134,25 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 		if (k == 1) enrsq0 = enrsq;
 		nit = k;
 		if (c->h_pinned[S_BREAK] != 0.0) { status = BSG_ERR_BREAKDOWN; break; }
-		if (p->ittype == 0 && enrsq <= p->eps * p->eps * enrsq0) break;
-		if (p->ittype == 1 && enrsq <= p->eps * p->eps) break;
+		const double goal = p->ittype == 0 ? p->eps * p->eps * enrsq0 : p->eps * p->eps;
+		if ((p->ittype == 0 || p->ittype == 1) && enrsq <= goal) {
+			if (!p->true_residual || replacements >= 5) break;
+			// the recursive residual says converged: confirm with the FP64
+			// true residual; if it drifted (FP32 preconditioner), continue
+			// from the true residual
+			rc = bsg_spmm_launch(m, 1, d_x, t.p, N, s);
+			if (!rc) rc = bsg_residual_launch(c, N, d_b, t.p);
+			if (!rc) rc = bsg_dots_launch(c, 1, N, t.p, t.p, nullptr, nullptr, nullptr, nullptr, c->d_scalars + S_TMP);
+			if (rc) return rc;
+			BSG_CUDA(cudaMemcpyAsync(c->h_pinned + 8, c->d_scalars + S_TMP, sizeof(double), cudaMemcpyDeviceToHost, s));
+			BSG_CUDA(cudaStreamSynchronize(s));
+			if (c->h_pinned[8] <= goal) break;
+			replacements++;
+			BSG_CUDA(cudaMemcpyAsync(r.p, t.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+			rc = bsg_precond_apply(c, f, p, r.p, z.p, t.p, w.p);
+			if (!rc) rc = bsg_dots_launch(c, 2, N, r.p, r.p, r.p, z.p, nullptr, nullptr, c->d_scalars + S_ENRSQ);
+			if (rc) return rc;
+		}
 		BSG_COUNT(3); // k_pcg_p, k_pcg_xr, k_copy_scalar
 		k_pcg_p<<<g, 256, 0, s>>>(N, z.p, pp.p, c->d_scalars, k == 1);
 		rc = bsg_spmm_launch(m, 1, pp.p, q.p, N, s);

@@ -173,6 +173,9 @@ int bsg_time_kernel(bsg_ctx *ctx, int kind, const bsg_mat *m, const bsg_fct *f, 
                     double *ms_per_launch);
 /* Scheduler counters of the last factorisation (see k_fact.cu). */
 int bsg_fact_stats(unsigned long long *out, int nout);
+/* Stored entries, padding included, of the sliced copies the bandwidth-bound
+ * products read: out[0] matrix, out[1] strict L, out[2] strict U. */
+int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out);
 
 #ifdef __cplusplus
 }

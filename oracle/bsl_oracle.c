@@ -128,22 +128,26 @@ int orc_combine_lu(int n, const int *ia, const int *ja, const double *a, int **i
 /* Optional dependency-depth outputs of orc_fact (see orc_fact_levels). */
 static int *g_lev_fact, *g_lev_solve, *g_dropdep, *g_nmember, *g_nmask;
 
-/* Theta compensations received by a row are summed in 128-bit fixed point
- * (value * 2^96, truncated per term): integer addition makes the sum
+/* Theta compensations received by a row are summed in 64-bit fixed point
+ * (value * 2^bits, truncated per term): integer addition makes the sum
  * independent of the order of the terms, which is what lets the GPU collect
- * them from rows that finish in any order.  acc[2j] is the low word,
- * acc[2j+1] the high word. */
+ * them from rows that finish in any order.  A compensation is below
+ * tau2 * theta < 2^e (frexp), and bits = 51 - e leaves room for 2^12 maximal
+ * terms in 63 bits. */
+static double g_acc_scale = 0x1p64, g_acc_inv = 0x1p-64;
+static void acc_setup(double tau2, double theta) {
+	int e = -13;
+	double maxterm = tau2 * theta;
+	if (maxterm > 0.0) frexp(maxterm, &e);
+	int bits = 51 - e;
+	if (bits > 1000) bits = 1000;
+	g_acc_scale = ldexp(1.0, bits);
+	g_acc_inv = ldexp(1.0, -bits);
+}
 static void acc_push(unsigned long long *acc, int j, double comp) {
-	const double x = comp * 0x1p96;
-	const unsigned long long hi = (unsigned long long)(x * 0x1p-64);
-	const unsigned long long lo = (unsigned long long)(x - (double)hi * 0x1p64);
-	const unsigned long long old = acc[2 * j];
-	acc[2 * j] = old + lo;
-	acc[2 * j + 1] += hi + ((old + lo < lo) ? 1ull : 0ull);
+	acc[j] += (unsigned long long)(comp * g_acc_scale);
 }
-static double acc_value(const unsigned long long *acc, int j) {
-	return ((double)acc[2 * j + 1] * 0x1p64 + (double)acc[2 * j]) * 0x1p-96;
-}
+static double acc_value(const unsigned long long *acc, int j) { return (double)acc[j] * g_acc_inv; }
 
 /* Growable arrays for the stored rows of the working factor. */
 typedef struct { int *col; signed char *flag; double *gl, *gu; size_t len, cap; } pool_t;
@@ -206,7 +210,8 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 	int *madj = (int *)malloc(sizeof(int) * (size_t)n);
 	int *iv = (int *)malloc(sizeof(int) * (size_t)n);
 	int *contrib = (int *)malloc(sizeof(int) * (size_t)n);
-	unsigned long long *acc = (unsigned long long *)calloc(2 * (size_t)n, sizeof(unsigned long long));
+	unsigned long long *acc = (unsigned long long *)calloc((size_t)n, sizeof(unsigned long long));
+	acc_setup(tau2, theta);
 	pool_t P = {0};
 	int rc = 0;
 	if (!scll || !sclu || !diagg || !fl || !fu || !imask || !lst || !keep || !rowbeg || !ibegm || !madj || !iv ||

@@ -1,0 +1,70 @@
+"""Generate tests/golden/*.npz from the reference Bslib itself.
+
+The reference ships no golden vectors or known-answer tests, so its own
+solver, compiled from its sources into oracle/_ref/libbslib_ref.so
+(``make -C oracle ref``), is run here on small seeded systems and the outputs
+are stored as fixtures.  The GPU box has no reference sources; the fixtures
+let every machine check the oracle against the reference.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "bcm-problems_b200"), os.path.join(ROOT, "tests")]
+
+import problems as P  # noqa: E402
+from oracle_ffi import RefLib  # noqa: E402
+
+
+def nonsymmetric(s, skew=0.3):
+    a = s.a.copy()
+    rows = np.repeat(np.arange(s.n), np.diff(s.ia))
+    off = s.ja != rows
+    a[off] *= 1.0 + skew * np.sign(s.ja[off] - rows[off])
+    return a
+
+
+def main():
+    ref = RefLib()
+    out = {}
+    s = P.heat3d(8, 8, 6, sigma=1.0, seed=21)
+    u = s.upper()
+    x = np.random.default_rng(22).standard_normal(s.n)
+    out["n"] = s.n
+    out["ia"], out["ja"], out["a"] = s.ia, s.ja, s.a
+    out["ua_ia"], out["ua_ja"], out["ua_a"] = u.ia, u.ja, u.a
+    out["b"] = s.rhs[0]
+    out["x"] = x
+    out["mvm"] = ref.mvm(s.ia, s.ja, s.a, x)
+    out["mvm_symm"] = ref.mvm(u.ia, u.ja, u.a, x, symm=True)
+    for tag, t1, t2 in (("ic2_a", 1e-3, 1e-3), ("ic2_b", 1e-2, 1e-4)):
+        iu, ju, uu, st = ref.ich2(u.ia, u.ja, u.a, tau1=t1, tau2=t2, theta=0.1)
+        out[f"{tag}_iu"], out[f"{tag}_ju"], out[f"{tag}_u"] = iu, ju, uu
+        out[f"{tag}_density"] = np.array(st[:2])
+        out[f"{tag}_solve_l"] = ref.solve_l(iu, ju, uu, x)
+        out[f"{tag}_solve_u"] = ref.solve_u(iu, ju, uu, x)
+    an = nonsymmetric(s)
+    out["ns_a"] = an
+    for tag, t1, t2 in (("ilu2_a", 1e-3, 1e-3), ("ilu2_b", 1e-2, 1e-4)):
+        (il, jl, lv), (iu, ju, uv), st = ref.ilu2(s.ia, s.ja, an, tau1=t1, tau2=t2, theta=0.1)
+        out[f"{tag}_iu"], out[f"{tag}_ju"], out[f"{tag}_l"], out[f"{tag}_u"] = iu, ju, lv, uv
+        out[f"{tag}_density"] = np.array(st[:2])
+    xs, info = ref.solve_symm(u.ia, u.ja, u.a, s.rhs[0], fcttyp=2, tau1=1e-3, tau2=1e-3, memory=-1.0, ittype=0,
+                              eps=1e-10)
+    out["symm_x"] = xs
+    out["symm_iters"] = np.array(info["iters"])
+    xn, info = ref.solver(s.ia, s.ja, an, s.rhs[0], tau1=1e-3, tau2=1e-3, sttype=1, eps=1e-10)
+    out["nonsymm_x"] = xn
+    out["nonsymm_iters"] = np.array(info["iters"])
+    path = os.path.join(HERE, "heat_8x8x6.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

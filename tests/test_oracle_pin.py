@@ -1,0 +1,97 @@
+"""The CPU oracle against the reference Bslib (CPU only).
+
+* against tests/golden/heat_8x8x6.npz -- outputs of the reference itself,
+  made by tests/golden/make_golden.py (runs everywhere);
+* against the live reference library oracle/_ref (runs where it was built).
+
+The oracle applies factorisation updates in ascending row order and sums the
+theta compensations in fixed point, the reference in its linked-list order:
+the factors agree in pattern exactly and in value to rounding (1e-13
+relative here); products and solves agree to 1e-14.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import problems as P
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "heat_8x8x6.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def test_mvm_matches_reference(oracle, gold):
+    g = gold
+    assert rel(oracle.mvm(g["ia"], g["ja"], g["a"], g["x"]), g["mvm"]) < 1e-15
+    assert rel(oracle.mvm(g["ua_ia"], g["ua_ja"], g["ua_a"], g["x"], symm=True), g["mvm_symm"]) < 1e-15
+
+
+@pytest.mark.parametrize("tag,t1,t2", [("ic2_a", 1e-3, 1e-3), ("ic2_b", 1e-2, 1e-4)])
+def test_ich2_matches_reference(oracle, gold, tag, t1, t2):
+    g = gold
+    iu, ju, uu, _, st = oracle.fact(0, g["ua_ia"], g["ua_ja"], g["ua_a"], tau1=t1, tau2=t2, theta=0.1)
+    assert np.array_equal(iu, g[f"{tag}_iu"]) and np.array_equal(ju, g[f"{tag}_ju"])
+    assert rel(uu, g[f"{tag}_u"]) < 1e-13
+    assert np.allclose(st, g[f"{tag}_density"], rtol=0, atol=1e-12)
+    # triangular solves with the reference's own factor
+    assert rel(oracle.solve_l(g[f"{tag}_iu"], g[f"{tag}_ju"], g[f"{tag}_u"], g["x"]), g[f"{tag}_solve_l"]) < 1e-14
+    assert rel(oracle.solve_u(g[f"{tag}_iu"], g[f"{tag}_ju"], g[f"{tag}_u"], g["x"]), g[f"{tag}_solve_u"]) < 1e-14
+
+
+@pytest.mark.parametrize("tag,t1,t2", [("ilu2_a", 1e-3, 1e-3), ("ilu2_b", 1e-2, 1e-4)])
+def test_ilu2_matches_reference(oracle, gold, tag, t1, t2):
+    g = gold
+    sia, sja, al, au = oracle.combine_lu(g["ia"], g["ja"], g["ns_a"])
+    iu, ju, lv, uv, st = oracle.fact(1, sia, sja, al, au, tau1=t1, tau2=t2, theta=0.1)
+    assert np.array_equal(iu, g[f"{tag}_iu"]) and np.array_equal(ju, g[f"{tag}_ju"])
+    assert rel(lv, g[f"{tag}_l"]) < 1e-13
+    assert rel(uv, g[f"{tag}_u"]) < 1e-13
+    assert np.allclose(st, g[f"{tag}_density"], rtol=0, atol=1e-12)
+
+
+def test_pcg_solution_matches_reference(oracle, gold):
+    g = gold
+    iu, ju, uu, _, _ = oracle.fact(0, g["ua_ia"], g["ua_ja"], g["ua_a"], tau1=1e-3, tau2=1e-3)
+    x, it, _ = oracle.pcg(g["ua_ia"], g["ua_ja"], g["ua_a"], iu, ju, uu, g["b"], ittype=0, eps=1e-10)
+    assert abs(it - int(g["symm_iters"])) <= 1
+    assert rel(x, g["symm_x"]) < 1e-9
+
+
+def test_gmres_solution_matches_reference_solver(oracle, gold):
+    """The reference's nonsymmetric driver runs Lanczos, the GPU path GMRES:
+    only the converged solutions are compared."""
+    g = gold
+    sia, sja, al, au = oracle.combine_lu(g["ia"], g["ja"], g["ns_a"])
+    iu, ju, lv, uv, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    x, it, res = oracle.gmres(g["ia"], g["ja"], g["ns_a"], iu, ju, lv, uv, g["b"], m=30, eps=1e-11)
+    assert res < 1e-11
+    assert rel(x, g["nonsymm_x"]) < 1e-8
+
+
+def test_compensation_sum_is_order_independent(oracle):
+    """Factors of a symmetric-permutation-free problem do not depend on how
+    many rows drop into the same diagonal: rerunning gives identical bits."""
+    s = P.heat3d(9, 7, 5, sigma=1.2, seed=5).upper()
+    a = oracle.fact(0, s.ia, s.ja, s.a, tau1=1e-2, tau2=1e-4)
+    b = oracle.fact(0, s.ia, s.ja, s.a, tau1=1e-2, tau2=1e-4)
+    assert all(np.array_equal(x, y) for x, y in zip(a[:4], b[:4]))
+
+
+def test_live_reference_larger_case(oracle, reflib):
+    s = P.heat3d(12, 11, 10, sigma=1.0, seed=23)
+    u = s.upper()
+    iu, ju, uu, _ = reflib.ich2(u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3)
+    oiu, oju, ouu, _, _ = oracle.fact(0, u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3)
+    assert np.array_equal(iu, oiu) and np.array_equal(ju, oju)
+    assert rel(ouu, uu) < 1e-13
+    x, info = reflib.solve_symm(u.ia, u.ja, u.a, s.rhs[0], memory=-1.0, eps=1e-10)
+    xo, it, _ = oracle.pcg(u.ia, u.ja, u.a, oiu, oju, ouu, s.rhs[0], eps=1e-10)
+    assert abs(it - info["iters"]) <= 1 and rel(xo, x) < 1e-9
