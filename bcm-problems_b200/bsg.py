@@ -82,6 +82,8 @@ def lib():
         "bsg_gmres_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
         "bsg_solve_symm_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
         "bsg_solver_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
+        "bsg_fact_stats": (i_, [C.POINTER(C.c_ulonglong), i_]),
+        "bsg_launch_count": (C.c_ulonglong, []),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -262,6 +264,17 @@ class Factor:
             self.free()
         except Exception:
             pass
+
+
+FACT_STAT_NAMES = ("tries", "parks", "cyc_pop", "cyc_close", "cyc_blocked", "cyc_pref", "cyc_upd", "cyc_fin",
+                   "members", "mask", "rounds", "cyc_pf", "cyc_pa", "cyc_pb", "big_rows", "warps")
+
+
+def fact_stats():
+    """Scheduler counters of the last factorisation in this process."""
+    out = (C.c_ulonglong * 16)()
+    _check(lib().bsg_fact_stats(out, 16))
+    return dict(zip(FACT_STAT_NAMES, list(out)))
 
 
 def pcg(ctx, mat, fct, b, x, param):

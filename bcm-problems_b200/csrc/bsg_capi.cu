@@ -14,6 +14,8 @@ int bsg_combine_lu(bsg_ctx *c, int n, const int *ia, const int *ja, const double
                    int **ju_o, double **al_o, double **au_o, int *nnz_o);
 int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nnz, int **it_o, int **jt_o,
                          int **perm_o, int *nnz_o);
+int bsg_bsr_to_point(bsg_ctx *c, int nsup, int bs, const int *ia, const int *ja, const double *a, int nnzb, int **pia_o,
+                     int **pja_o, double **pa_o);
 int bsg_choose_group(double mean_row);
 int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
 int bsg_fct_make_fp32(bsg_fct *f);
@@ -387,8 +389,30 @@ extern "C" int bsg_mat_bsr(bsg_ctx *c, int nsup, int bs, const int *ia, const in
 	BSG_CUDA(cudaMemcpyAsync(m->d_ia, fia.data(), sizeof(int) * (nsup + 1), cudaMemcpyHostToDevice, s));
 	BSG_CUDA(cudaMemcpyAsync(m->d_ja, fja.data(), sizeof(int) * m->nnz, cudaMemcpyHostToDevice, s));
 	BSG_CUDA(cudaMemcpyAsync(m->d_a, fa.data(), sizeof(double) * 9 * m->nnz, cudaMemcpyHostToDevice, s));
-	BSG_CUDA(cudaStreamSynchronize(s));
 	m->group = 32;
+	// the factorisations of a block matrix work on its point expansion: keep
+	// the point CombineLU split and its static contributor lists
+	int *pia = nullptr, *pja = nullptr;
+	double *pa = nullptr;
+	rc = bsg_bsr_to_point(c, nsup, 3, m->d_ia, m->d_ja, m->d_a, m->nnz, &pia, &pja, &pa);
+	if (!rc)
+		rc = bsg_combine_lu(c, nsup * 3, pia, pja, pa, m->nnz * 9, &m->d_iu, &m->d_ju, &m->d_al, &m->d_au,
+		                    &m->nnz_up);
+	for (void *q : {(void *)pia, (void *)pja, (void *)pa})
+		if (q) cudaFreeAsync(q, s);
+	if (!rc && symm_upper) {
+		// IC2 reads the upper values as given (au = A(i,j), j >= i), not
+		// the mirrored lower copies of the diagonal blocks
+		cudaFreeAsync(m->d_al, s);
+		m->d_al = m->d_au;
+	}
+	int nt = 0;
+	if (!rc) rc = bsg_strict_transpose(c, nsup * 3, m->d_iu, m->d_ju, m->nnz_up, &m->d_it, &m->d_jt, nullptr, &nt);
+	if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = bsg_set_error(BSG_ERR_CUDA, "bsg_mat_bsr");
+	if (rc) {
+		bsg_mat_free(m);
+		return rc;
+	}
 	*out = m;
 	return BSG_OK;
 }
@@ -448,7 +472,6 @@ extern "C" int bsg_mvm(bsg_ctx *c, const bsg_mat *m, const double *x, double *y)
 static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **out) {
 	if (!c || !m || !p || !out) return bsg_set_error(BSG_ERR_ARG, "factorisation: null argument");
 	*out = nullptr;
-	if (m->bs != 1) return bsg_set_error(BSG_ERR_UNSUPPORTED, "block factorisation is not available on this path");
 	if (p->ordtype != 0) return bsg_set_error(BSG_ERR_UNSUPPORTED, "only natural ordering (ordtype = 0) runs on the GPU");
 	if (kind == 0 && p->fcttyp == 1)
 		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) is not on the GPU path; use fcttyp = 2");

@@ -27,9 +27,9 @@
 // Storage.  A finished row keeps only its stored part: the diagonal (inverse
 // pivot) and the U / R entries sorted by column, in a pool, published by one
 // 64-bit release store of (done | offset | length).  Dropped entries are not
-// kept: their theta compensations are pushed at once into a per-row 128-bit
-// fixed-point accumulator (scale 2^96), whose integer sum does not depend on
-// the order of the pushes.
+// kept: their theta compensations are pushed at once into a per-row 64-bit
+// fixed-point accumulator (scale set by tau2 * theta, bsg_comp_scale), whose
+// integer sum does not depend on the order of the pushes.
 //
 // Arithmetic order (deterministic, identical to oracle/bsl_oracle.c):
 // diagonal = scaled a_ii + (fixed-point sum of compensations received);
@@ -55,6 +55,11 @@
 #define CMAX 256   // members of C(i)
 #define HCAP 512   // distinct mask columns per row (power of two)
 #define PFCAP 1024 // prefetched contributor entries per row
+// capacities of the global-memory workspace that takes the rows that do not
+// fit the shared one (about 0.7 MB per warp)
+#define CMAX_BIG 8192
+#define HCAP_BIG 8192
+#define PFCAP_BIG 8192
 #define W_EMPTY (-1)
 #define W_CLOSED (-2)
 
@@ -87,16 +92,24 @@ struct FactArgs {
 	int *done_count;
 	bsg_devstat *st;
 	unsigned long long *stats; // FACT_NSTAT counters (see bsg_fact_stats)
+	unsigned char *big_ws;     // GlobWS::bytes per warp of the launch
 };
 
 // Scheduler / phase counters summed over all warps of the last factorisation.
 enum { FS_TRY = 0, FS_PARK, FS_CYC_POP, FS_CYC_CLOSE, FS_CYC_BLOCKED, FS_CYC_PREF, FS_CYC_UPD, FS_CYC_FIN,
-       FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FACT_NSTAT = 16 };
+       FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FS_BIG, FACT_NSTAT = 16 };
 struct PhaseClock {
 	unsigned long long v[FACT_NSTAT];
 };
 
-struct WarpShared {
+// Per-warp workspace of one row.  Rows first run in shared memory (SmemWS);
+// a row whose member set, mask or a contributor segment does not fit is
+// tried again by the same warp in a larger workspace in global memory
+// (GlobWS), so any row up to the big capacities factors.  Both expose the
+// same members; sc[] = {members, mask columns, kept columns, blocking row}.
+struct SmemWS {
+	static constexpr bool big = false;
+	static constexpr int cmax = CMAX, hcap = HCAP, pfcap = PFCAP;
 	int W[CMAX];           // members (discovery order, then sorted)
 	int Wp[CMAX];          // pool index of column i in that row (stored members)
 	int We[CMAX];          // pool end of that row
@@ -112,15 +125,42 @@ struct WarpShared {
 	unsigned pf_cf[PFCAP]; // prefetched contributor segments
 	short pf_slot[PFCAP];
 	double pf_l[PFCAP], pf_u[PFCAP];
-	int nW, nl, nk, blocked;
+	int sc[4];
+};
+
+struct GlobWS {
+	static constexpr bool big = true;
+	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG;
+	static constexpr size_t bytes = 8 * (2 * (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
+	                                4 * (6 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
+	                                     3 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
+	                                2 * (size_t)PFCAP_BIG + 2 * (size_t)CMAX_BIG;
+	double *hl, *hu, *pf_l, *pf_u;
+	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wb, *wset, *hkey, *lst, *lsts, *sc;
+	unsigned *pf_cf;
+	short *pf_slot;
+	unsigned char *Wf, *Wfs;
+	__device__ explicit GlobWS(unsigned char *p) {
+		hl = reinterpret_cast<double *>(p); hu = hl + HCAP_BIG;
+		pf_l = hu + HCAP_BIG; pf_u = pf_l + PFCAP_BIG;
+		W = reinterpret_cast<int *>(pf_u + PFCAP_BIG);
+		Wp = W + CMAX_BIG; We = Wp + CMAX_BIG; Ws = We + CMAX_BIG; Wps = Ws + CMAX_BIG; Wes = Wps + CMAX_BIG;
+		Wb = Wes + CMAX_BIG; wset = Wb + CMAX_BIG + 4;
+		hkey = wset + 2 * CMAX_BIG; lst = hkey + HCAP_BIG; lsts = lst + HCAP_BIG;
+		pf_cf = reinterpret_cast<unsigned *>(lsts + HCAP_BIG);
+		sc = reinterpret_cast<int *>(pf_cf + PFCAP_BIG);
+		pf_slot = reinterpret_cast<short *>(sc + 4);
+		Wf = reinterpret_cast<unsigned char *>(pf_slot + PFCAP_BIG); Wfs = Wf + CMAX_BIG;
+	}
 };
 
 __device__ __forceinline__ unsigned hash_u(int k) { return (unsigned)k * 2654435761u; }
 
 // Find or insert column c; returns slot or -1 if full.
-__device__ int hfind_insert(WarpShared &s, int c) {
-	unsigned h = hash_u(c) & (HCAP - 1);
-	for (int probe = 0; probe < HCAP; probe++) {
+template <class WS>
+__device__ int hfind_insert(WS &s, int c) {
+	unsigned h = hash_u(c) & (s.hcap - 1);
+	for (int probe = 0; probe < s.hcap; probe++) {
 		int k = s.hkey[h];
 		if (k == c) return (int)h;
 		if (k == -1) {
@@ -132,7 +172,7 @@ __device__ int hfind_insert(WarpShared &s, int c) {
 			}
 			if (old == c) return (int)h;
 		}
-		h = (h + 1) & (HCAP - 1);
+		h = (h + 1) & (s.hcap - 1);
 	}
 	return -1;
 }
@@ -140,9 +180,10 @@ __device__ int hfind_insert(WarpShared &s, int c) {
 // Insert row k into the member set; 1 if new, 0 if present, -1 if full.
 // Most candidates are already members: probe with plain reads, CAS only
 // into an empty slot.
-__device__ int wset_insert(WarpShared &s, int k) {
-	unsigned h = hash_u(k) & (2 * CMAX - 1);
-	for (int probe = 0; probe < 2 * CMAX; probe++) {
+template <class WS>
+__device__ int wset_insert(WS &s, int k) {
+	unsigned h = hash_u(k) & (2 * s.cmax - 1);
+	for (int probe = 0; probe < 2 * s.cmax; probe++) {
 		int cur = s.wset[h];
 		if (cur == k) return 0;
 		if (cur == -1) {
@@ -150,7 +191,7 @@ __device__ int wset_insert(WarpShared &s, int k) {
 			if (old == -1) return 1;
 			if (old == k) return 0;
 		}
-		h = (h + 1) & (2 * CMAX - 1);
+		h = (h + 1) & (2 * s.cmax - 1);
 	}
 	return -1;
 }
@@ -210,7 +251,8 @@ __device__ void park(const FactArgs &A, int i, int m) {
 
 // Examine member m of C(i) (one lane): classify it and add its candidates.
 // Returns 0, or a BSG_ERR_* code.
-__device__ int close_member(const FactArgs &A, WarpShared &s, int i, int t, int m, unsigned long long rec,
+template <class WS>
+__device__ int close_member(const FactArgs &A, WS &s, int i, int t, int m, unsigned long long rec,
                            int &levmax) {
 	const long long off = REC_OFF(rec);
 	const int len = REC_LEN(rec);
@@ -281,8 +323,8 @@ __device__ int close_member(const FactArgs &A, WarpShared &s, int i, int t, int 
 			const int isnew = wset_insert(s, c);
 			if (isnew < 0) { err = BSG_ERR_WORKSPACE; continue; }
 			if (isnew == 1) {
-				int slot = atomicAdd(&s.nW, 1);
-				if (slot < CMAX) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
+				int slot = atomicAdd(&s.sc[0], 1);
+				if (slot < s.cmax) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
 			}
 		}
 	}
@@ -293,26 +335,30 @@ __device__ int close_member(const FactArgs &A, WarpShared &s, int i, int t, int 
 		const int isnew = wset_insert(s, c);
 		if (isnew < 0) { err = BSG_ERR_WORKSPACE; continue; }
 		if (isnew == 1) {
-			int slot = atomicAdd(&s.nW, 1);
-			if (slot < CMAX) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
+			int slot = atomicAdd(&s.sc[0], 1);
+			if (slot < s.cmax) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
 		}
 	}
 	return err;
 }
 
 // Factor row i.  Returns -1 when done, the unfinished row it waits for
-// (>= 0), or -2 on error (reported through the status word).
-__device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseClock &pc) {
+// (>= 0), -2 on error (reported through the status word), or -3 when the
+// row does not fit a shared-memory workspace (nothing was published yet, so
+// the caller retries it in the global one).
+template <class WS>
+__device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc) {
 	const bool ilu = A.kind == 1;
 	const long long c0 = clock64();
-	for (int t = lane; t < 2 * CMAX; t += 32) s.wset[t] = -1;
-	for (int t = lane; t < HCAP; t += 32) s.hkey[t] = -1;
-	if (lane == 0) { s.blocked = -1; s.nW = 0; }
+	for (int t = lane; t < 2 * s.cmax; t += 32) s.wset[t] = -1;
+	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
+	if (lane == 0) { s.sc[3] = -1; s.sc[0] = 0; }
 	__syncwarp();
 
 	// ---- seed with A's column i (all finished: the row was queued)
 	const int tb = A.it[i], te = A.it[i + 1];
-	if (te - tb > CMAX) {
+	if (te - tb > s.cmax) {
+		if (!WS::big) return -3;
 		if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 2);
 		return -2;
 	}
@@ -321,14 +367,14 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		s.W[t - tb] = k;
 		wset_insert(s, k);
 	}
-	if (lane == 0) s.nW = te - tb;
+	if (lane == 0) s.sc[0] = te - tb;
 	__syncwarp();
 
 	// ---- close C(i): rounds over the newest members, one member per lane
 	int err = 0, levmax = 0;
-	for (int lo = 0; lo < s.nW && !err;) {
+	for (int lo = 0; lo < s.sc[0] && !err;) {
 		pc.v[FS_ROUNDS]++;
-		const int hi = min(s.nW, CMAX);
+		const int hi = min(s.sc[0], s.cmax);
 		for (int base = lo; base < hi; base += 32) {
 			const int t = base + lane;
 			int m = -1;
@@ -336,12 +382,12 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 			if (t < hi) {
 				m = s.W[t];
 				rec = ld_acquire_u64(A.rec + m);
-				if (!(rec & REC_DONE)) { atomicCAS(&s.blocked, -1, m); m = -1; }
+				if (!(rec & REC_DONE)) { atomicCAS(&s.sc[3], -1, m); m = -1; }
 			}
 			__syncwarp();
-			if (s.blocked >= 0) {
+			if (s.sc[3] >= 0) {
 				pc.v[FS_CYC_BLOCKED] += clock64() - c0;
-				return s.blocked;
+				return s.sc[3];
 			}
 			if (m >= 0) {
 				int e2 = close_member(A, s, i, t, m, rec, levmax);
@@ -354,11 +400,12 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		__syncwarp();
 	}
 	if (err) {
+		if (!WS::big) return -3;
 		if (lane == 0) devstat_fail(A.st, err, i, 3);
 		return -2;
 	}
 	levmax = __reduce_max_sync(0xffffffffu, levmax);
-	const int nW = s.nW;
+	const int nW = s.sc[0];
 	const long long c1 = clock64();
 	pc.v[FS_CYC_CLOSE] += c1 - c0;
 	pc.v[FS_CONTRIB] += nW;
@@ -410,6 +457,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 				s.hu[sl] = v;
 			}
 		}
+		err = __reduce_min_sync(0xffffffffu, err);
 		__syncwarp();
 	}
 
@@ -417,8 +465,9 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 	//      consecutive members whose segments fit the shared prefetch buffer
 	for (int t0 = 0; t0 < nW && !err;) {
 		int t1 = t0;
-		while (t1 < nW && s.Wb[t1 + 1] - s.Wb[t0] <= PFCAP) t1++;
+		while (t1 < nW && s.Wb[t1 + 1] - s.Wb[t0] <= s.pfcap) t1++;
 		if (t1 == t0) { // one segment longer than the buffer
+			if (!WS::big) return -3;
 			if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 5);
 			return -2;
 		}
@@ -493,6 +542,7 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 	}
 	err = __reduce_min_sync(0xffffffffu, err);
 	if (err) {
+		if (!WS::big) return -3;
 		if (lane == 0) devstat_fail(A.st, err, i, 4);
 		return -2;
 	}
@@ -500,19 +550,19 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 	pc.v[FS_CYC_UPD] += c3 - c2;
 
 	// ---- extract the off-diagonal mask columns and sort them ascending
-	if (lane == 0) s.nl = 0;
+	if (lane == 0) s.sc[1] = 0;
 	__syncwarp();
-	for (int h = lane; h < HCAP; h += 32) {
+	for (int h = lane; h < s.hcap; h += 32) {
 		int c = s.hkey[h];
 		bool take = c >= 0 && c != i;
 		unsigned b = __ballot_sync(0xffffffffu, take);
-		int base = s.nl;
+		int base = s.sc[1];
 		if (take) s.lst[base + __popc(b & ((1u << lane) - 1))] = h;
 		__syncwarp();
-		if (lane == 0) s.nl = base + __popc(b);
+		if (lane == 0) s.sc[1] = base + __popc(b);
 		__syncwarp();
 	}
-	const int nl = s.nl;
+	const int nl = s.sc[1];
 	for (int t = lane; t < nl; t += 32) {
 		int c = s.hkey[s.lst[t]], r = 0;
 		for (int u = 0; u < nl; u++) r += s.hkey[s.lst[u]] < c;
@@ -540,10 +590,10 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 		}
 		s.hl[di] = dl;
 		s.hu[di] = du;
-		s.nk = nk;
+		s.sc[2] = nk;
 	}
 	__syncwarp();
-	const int nk = s.nk;
+	const int nk = s.sc[2];
 
 	// ---- pivot (Ich2PivScaleRow / Ilu2PivScaleRow)
 	const double fd = s.hl[di];
@@ -626,7 +676,9 @@ __device__ int try_row(const FactArgs &A, WarpShared &s, int i, int lane, PhaseC
 
 __global__ void __launch_bounds__(FACT_WARPS * 32) k_fact_rows(FactArgs A) {
 	extern __shared__ unsigned char smem_raw[];
-	WarpShared &s = reinterpret_cast<WarpShared *>(smem_raw)[threadIdx.x >> 5];
+	const int warp = threadIdx.x >> 5;
+	SmemWS &s = reinterpret_cast<SmemWS *>(smem_raw)[warp];
+	GlobWS g(A.big_ws + (size_t)(blockIdx.x * FACT_WARPS + warp) * GlobWS::bytes);
 	const int lane = threadIdx.x & 31;
 	PhaseClock pc;
 #pragma unroll
@@ -640,6 +692,11 @@ __global__ void __launch_bounds__(FACT_WARPS * 32) k_fact_rows(FactArgs A) {
 		if (i < 0) break;
 		pc.v[FS_TRY]++;
 		int r = try_row(A, s, i, lane, pc);
+		if (r == -3) {
+			pc.v[FS_BIG]++;
+			__syncwarp();
+			r = try_row(A, g, i, lane, pc);
+		}
 		if (r == -2) break;
 		if (r >= 0) {
 			pc.v[FS_PARK]++;
@@ -771,7 +828,9 @@ static unsigned long long g_fact_stats[FACT_NSTAT];
 // Counters of the last factorisation in this process: [0] row tries,
 // [1] parks, [2..7] SM cycles summed over warps in queue wait, closure,
 // blocked closures, prefetch, updates, finish; [8] members of C(i),
-// [9] mask columns, [15] warps launched.
+// [9] mask columns, [10] closure rounds, [11..13] SM cycles in prefetch,
+// slot resolution and fma phases, [14] rows retried in the global-memory
+// workspace, [15] warps launched.
 extern "C" int bsg_fact_stats(unsigned long long *out, int nout) {
 	for (int k = 0; k < nout && k < FACT_NSTAT; k++) out[k] = g_fact_stats[k];
 	return BSG_OK;
@@ -780,7 +839,7 @@ extern "C" int bsg_fact_stats(unsigned long long *out, int nout) {
 // Runs the factorisation of m (whose upper split d_iu/d_ju/d_al/d_au and
 // static contributor lists d_it/d_jt are prepared) and builds the factor.
 int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct **out) {
-	const int n = m->n;
+	const int n = m->n * m->bs; // point rows (block matrices factor their point expansion)
 	cudaStream_t st = c->stream;
 	double mem = p->memory < 0 ? -p->memory : p->memory;
 	if (mem < 8.0) mem = 8.0;
@@ -837,7 +896,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
 	BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
 	k_fact_seed<<<nb(n, 256), 256, 0, st>>>(A);
-	size_t smem = sizeof(WarpShared) * FACT_WARPS;
+	size_t smem = sizeof(SmemWS) * FACT_WARPS;
 	BSG_CUDA(cudaFuncSetAttribute(k_fact_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	int per_sm = 0;
 	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fact_rows, FACT_WARPS * 32, smem));
@@ -846,6 +905,8 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	int need = (n + FACT_WARPS - 1) / FACT_WARPS;
 	if (grid > need) grid = need;
 	if (grid < 1) grid = 1;
+	if (cudaMallocAsync(&A.big_ws, GlobWS::bytes * (size_t)grid * FACT_WARPS, st) != cudaSuccess)
+		return bsg_set_error(BSG_ERR_NOMEM, "factor row workspace");
 	k_fact_rows<<<grid, FACT_WARPS * 32, smem, st>>>(A);
 	BSG_CUDA(cudaGetLastError());
 	int rc = bsg_check_devstat(c);
@@ -853,6 +914,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	cudaStreamSynchronize(st);
 	g_fact_stats[FACT_NSTAT - 1] = (unsigned long long)grid * FACT_WARPS; // warps launched
 	cudaFreeAsync(A.stats, st);
+	cudaFreeAsync(A.big_ws, st);
 	int ndone = 0;
 	if (!rc) {
 		BSG_CUDA(cudaMemcpy(&ndone, done_count, sizeof(int), cudaMemcpyDeviceToHost));

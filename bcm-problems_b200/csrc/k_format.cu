@@ -251,3 +251,41 @@ int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nn
 	*nnz_o = nk;
 	return BSG_OK;
 }
+
+namespace {
+// Point row 3i+r of a block-CSR matrix with row-major bs x bs blocks: for
+// every block k of block row i, columns bs*ja[k] + c with values
+// a[bs*bs*k + bs*r + c].  Block columns ascending give point columns
+// ascending.
+__global__ void k_bsr_point_rows(int nsup, int bs, const int *ia, const int *ja, const double *a, int *pia, int *pja,
+                                 double *pa) {
+	const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (p >= (long long)nsup * bs) return;
+	const int i = (int)(p / bs), r = (int)(p % bs);
+	const int kb = ia[i], ke = ia[i + 1];
+	int z = bs * bs * kb + r * bs * (ke - kb);
+	pia[p] = z;
+	if (p == (long long)nsup * bs - 1) pia[p + 1] = bs * bs * ke;
+	for (int k = kb; k < ke; k++)
+		for (int c = 0; c < bs; c++, z++) {
+			pja[z] = bs * ja[k] + c;
+			pa[z] = a[(size_t)bs * bs * k + bs * r + c];
+		}
+}
+} // namespace
+
+// Point CSR copy of a block-CSR matrix (row-major blocks): the operator the
+// point factorisation of a block matrix works on.
+int bsg_bsr_to_point(bsg_ctx *c, int nsup, int bs, const int *ia, const int *ja, const double *a, int nnzb, int **pia_o,
+                     int **pja_o, double **pa_o) {
+	const long long np = (long long)nsup * bs, nz = (long long)nnzb * bs * bs;
+	if (nz > 0x7fffffffLL) return bsg_set_error(BSG_ERR_UNSUPPORTED, "point expansion exceeds 2^31 entries");
+	BSG_CUDA(cudaMallocAsync(pia_o, sizeof(int) * (np + 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(pja_o, sizeof(int) * (nz > 0 ? nz : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(pa_o, sizeof(double) * (nz > 0 ? nz : 1), c->stream));
+	if (np == 0) BSG_CUDA(cudaMemsetAsync(*pia_o, 0, sizeof(int), c->stream));
+	BSG_COUNT(1);
+	k_bsr_point_rows<<<nblk(np, 256), 256, 0, c->stream>>>(nsup, bs, ia, ja, a, *pia_o, *pja_o, *pa_o);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}

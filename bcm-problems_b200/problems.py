@@ -72,6 +72,31 @@ class System:
         a = self.a.reshape(-1, bs2)[keep].reshape(-1)
         return System(self.n, self.bs, ia, self.ja[keep].copy(), a.copy(), self.rhs, self.parts, self.info)
 
+    def to_point(self):
+        """The same matrix as a point (bs == 1) CSR system: every entry of every
+        block is kept (zeros included); point row bs*i + r holds columns
+        bs*j + c of the blocks of block row i, sorted ascending."""
+        if self.bs == 1:
+            return self
+        bs, n = self.bs, self.n
+        nb = np.diff(self.ia).astype(np.int64)
+        B = self.a.reshape(-1, bs, bs).transpose(0, 2, 1)  # [k, r, c]
+        ia = np.zeros(n * bs + 1, np.int64)
+        ia[1:] = np.cumsum(np.repeat(nb * bs, bs))
+        rowb = np.repeat(np.arange(n), nb)
+        k = np.arange(len(self.ja))[:, None, None]
+        r = np.arange(bs)[None, :, None]
+        c = np.arange(bs)[None, None, :]
+        pos = ia[bs * rowb[k] + r] + (k - self.ia[rowb[k]]) * bs + c
+        ja = np.empty(ia[-1], np.int32)
+        a = np.empty(ia[-1])
+        ja[pos] = bs * self.ja[k] + c
+        a[pos] = B
+        rows = np.repeat(np.arange(n * bs), np.diff(ia))
+        order = np.lexsort((ja, rows))
+        ja, a = ja[order], a[order]
+        return System(n * bs, 1, ia.astype(np.int32), ja, a, self.rhs, self.parts * bs, self.info)
+
     def to_scipy(self):
         import scipy.sparse as sp
         if self.bs == 1:

@@ -119,6 +119,61 @@ def test_ilu2_matches_oracle(ctx, oracle, heat, tau1, tau2):
     _factor_match(f.export(), ora)
 
 
+@pytest.mark.parametrize("case,kind", [("lame", "ilu2"), ("lame", "ich2"), ("periodic", "ich2")])
+def test_big_rows_match_oracle(ctx, oracle, case, kind):
+    """Point-expanded elasticity rows have 300-1400 contributors, beyond the
+    shared-memory workspace; they are retried in the global one and must
+    still agree bit for bit."""
+    import bsg
+    if case == "lame":
+        s = P.lame3d(10, 0.3, 1.0, 1).to_point()
+    else:
+        s = P.lame_periodic(8, 0.3, 1.5, 2.5, 0.3, 100.0, 2).to_point()
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
+    if kind == "ich2":
+        u = s.upper()
+        m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+        f = bsg.Factor(ctx, m, "ich2", p)
+        ora = oracle.fact(0, u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3, theta=0.1)
+    else:
+        m = bsg.Matrix.from_system(ctx, s)
+        f = bsg.Factor(ctx, m, "ilu2", p)
+        sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, s.a)
+        ora = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3, theta=0.1)
+    assert bsg.fact_stats()["big_rows"] > 0
+    _factor_match(f.export(), ora)
+
+
+@pytest.mark.parametrize("kind", ["ilu2", "ich2"])
+def test_block_matrix_factors_point_expansion(ctx, oracle, kind):
+    """A 3x3 block matrix is factored through its point expansion: the same
+    factor as the point CSR copy of the same operator, bit for bit; the
+    Krylov solve then runs with the block SpMV and the point factor."""
+    import bsg
+    import torch
+    s = P.lame3d(6, 0.3, 1.0, 3)
+    pt = s.to_point()
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, eps=1e-9,
+                          ittype=0, sttype=1, restart=40, krylov=1)
+    if kind == "ich2":
+        m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+        u = pt.upper()
+        ora = oracle.fact(0, u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3, theta=0.1)
+    else:
+        m = bsg.Matrix.from_system(ctx, s)
+        sia, sja, al, au = oracle.combine_lu(pt.ia, pt.ja, pt.a)
+        ora = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3, theta=0.1)
+    assert m.info()[:2] == (s.n, 3)
+    f = bsg.Factor(ctx, m, kind, p)
+    _factor_match(f.export(), ora)
+    b = s.rhs[0]
+    x = torch.zeros(pt.n, dtype=torch.float64, device="cuda")
+    (bsg.pcg if kind == "ich2" else bsg.gmres)(ctx, m, f, _t(b), x, p)
+    A = s.to_scipy()
+    xh = x.cpu().numpy()
+    assert np.linalg.norm(b - A @ xh) <= 1e-8 * np.linalg.norm(b)
+
+
 def test_trisolve_exact_matches_oracle(ctx, oracle, heat):
     import bsg
     import torch
