@@ -144,6 +144,16 @@ int bsg_fct_free(bsg_fct *f);
  * sweeps (approximate, fully parallel).  `work` may be NULL for mode 0. */
 int bsg_solve_l_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
 int bsg_solve_u_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
+/* Sweep-mode solve (lower != 0: L, else U) that allocates nothing: the same
+ * kernels as bsg_solve_l_dev / bsg_solve_u_dev with mode 1, with the work
+ * vector taken from a fixed 2^21-row device array instead of the memory
+ * pool.  For callers that cannot allocate device memory while they iterate.
+ * Factors above 2^21 rows are rejected (BSG_ERR_ARG).  The first call on a
+ * device looks the array up and should come before any stream capture; the
+ * array is shared per device, so calls must not overlap in time.  Queued on
+ * the context stream without a host synchronisation.  No counterpart in the
+ * reference (its SolveL / SolveU need no work vector). */
+int bsg_solve_sweep_static(bsg_ctx *ctx, const bsg_fct *f, int lower, int nsweeps, const double *d_x, double *d_y);
 
 /* ---- Krylov loops --------------------------------------------------------- */
 /* PCG (CSVector::Cg, Bslib/cg.cpp:31) with A symmetric and an IC2 factor;
