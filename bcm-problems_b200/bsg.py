@@ -83,6 +83,17 @@ def lib():
         "bsg_solve_symm_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
         "bsg_solver_csr": (i_, [vp, i_, ip, ip, dp, dp, dp, C.POINTER(Param)]),
         "bsg_fact_stats": (i_, [C.POINTER(C.c_ulonglong), i_]),
+        "bsg_unet_create": (i_, [vp, i_, i_, i_, i_, pp]),
+        "bsg_unet_free": (i_, [vp]),
+        "bsg_unet_nparam": (i_, [vp]),
+        "bsg_unet_set_weights": (i_, [vp, C.POINTER(C.c_float)]),
+        "bsg_unet_get_weights": (i_, [vp, C.POINTER(C.c_float)]),
+        "bsg_unet_get_grads": (i_, [vp, C.POINTER(C.c_float)]),
+        "bsg_unet_set_matrix": (i_, [vp, vp]),
+        "bsg_unet_forward_dev": (i_, [vp, vp, vp]),
+        "bsg_unet_train_sample": (i_, [vp, vp, vp, C.POINTER(C.c_double)]),
+        "bsg_unet_adam": (i_, [vp, C.c_float, C.c_float, C.c_float, C.c_float, i_]),
+        "bsg_unet_zero_grads": (i_, [vp]),
         "bsg_launch_count": (C.c_ulonglong, []),
     }
     for name, (rt, at) in sig.items():
@@ -257,6 +268,64 @@ class Factor:
     def free(self):
         if self.h:
             lib().bsg_fct_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class UNet:
+    """The learned FGMRES stage (bsg_unet_*): a 4-level 3D conv U-Net on an
+    nx x ny x nz grid, bf16 weights, FP32 accumulation, trained by the
+    library's own forward / backward kernels."""
+
+    def __init__(self, ctx, nx, ny, nz, train=False):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        self.grid = (nx, ny, nz)
+        _check(lib().bsg_unet_create(ctx.h, nx, ny, nz, int(train), C.byref(self.h)))
+        self.nparam = lib().bsg_unet_nparam(self.h)
+        ctx._adopt(self)
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        assert w.size == self.nparam
+        _check(lib().bsg_unet_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def weights(self):
+        w = np.zeros(self.nparam, np.float32)
+        _check(lib().bsg_unet_get_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float))))
+        return w
+
+    def grads(self):
+        g = np.zeros(self.nparam, np.float32)
+        _check(lib().bsg_unet_get_grads(self.h, g.ctypes.data_as(C.POINTER(C.c_float))))
+        return g
+
+    def set_matrix(self, mat):
+        _check(lib().bsg_unet_set_matrix(self.h, mat.h))
+        self._mat = mat
+
+    def forward(self, r, y):
+        _check(lib().bsg_unet_forward_dev(self.h, _ptr(r), _ptr(y)))
+
+    def train_sample(self, r, t, want_loss=False):
+        loss = C.c_double(0.0)
+        _check(lib().bsg_unet_train_sample(self.h, _ptr(r), _ptr(t), C.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    def adam(self, lr, step, beta1=0.9, beta2=0.999, eps=1e-8):
+        _check(lib().bsg_unet_adam(self.h, lr, beta1, beta2, eps, step))
+
+    def zero_grads(self):
+        _check(lib().bsg_unet_zero_grads(self.h))
+
+    def free(self):
+        if self.h:
+            lib().bsg_unet_free(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

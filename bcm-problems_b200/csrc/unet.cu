@@ -1,0 +1,832 @@
+// Learned preconditioner stage: a 4-level 3D convolutional U-Net applied
+// after the ILU2 sweep inside FGMRES, with its own training kernels.  No
+// counterpart in the reference (Bslib has no learned or reduced-precision
+// part); the network is defined by oracle/unet_ref.py, which the tests hold
+// these kernels to.
+//
+//   x0 = [r/|r|, normalised log diag(A), 0..]                 R0, 16 ch
+//   e0 = relu(conv(x0; W0 16->16))          e1 = relu(conv(pool e0; W1 16->32))
+//   e2 = relu(conv(pool e1; W2 32->64))     e3 = relu(conv(pool e2; W3 64->64))
+//   d2 = relu(conv([up e3, e2]; W4 128->32))
+//   d1 = relu(conv([up d2, e1]; W5 64->16))
+//   d0 = relu(conv([up d1, e0]; W6 32->16)) y = w7 . d0,  correction = |r| y
+//
+// Layout: activations channels-last [z][y][x][c] in bfloat16 (32 bytes per
+// voxel at 16 channels), weights bfloat16 [tap][cout][cin], accumulation in
+// FP32.  The 3x3x3 convolution is an implicit GEMM on the tensor cores
+// (mma.sync m16n8k16 bf16 -> f32): M = voxels, N = output channels (16 per
+// CTA), K = 27 taps x input channels, with the weight slice of the CTA
+// staged in shared memory (rows padded by 8 so the B-fragment reads are
+// bank-conflict free) and the A fragments read straight from the
+// channels-last tensors (L1 serves the 27-fold tap reuse).  The decoder
+// reads its upsampled input at coordinate / 2 instead of materialising it,
+// and the concatenation is two input pointers.  The backward pass reuses
+// the same kernel for the data gradient (flipped, channel-transposed
+// weights, FP32 output); weight gradients are FP32 sums on the CUDA cores.
+#include "bsg_internal.cuh"
+#include <cuda_bf16.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+typedef __nv_bfloat16 bf16;
+
+int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
+
+namespace {
+
+enum { NW = 7 };
+const int CIN[NW] = {16, 16, 32, 64, 128, 64, 32};
+const int COUT[NW] = {16, 32, 64, 64, 32, 16, 16};
+
+struct ConvArgs {
+	int nz, ny, nx;       // output dims (B has these dims; A has them >> upA)
+	const bf16 *A;
+	int Ca, upA;
+	const bf16 *B;
+	int Cb;
+	const bf16 *W;        // [27][Cout][Cin]
+	int Cout;
+	void *out;            // bf16 [v][Cout] (relu) or float [v][Cout]
+};
+
+__device__ __forceinline__ void mma_bf16(float *c, const unsigned *a, unsigned b0, unsigned b1) {
+	asm volatile(
+	    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+	    "{%0,%1,%2,%3};"
+	    : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+	    : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ unsigned ld_u32(const bf16 *p) { return __ldg(reinterpret_cast<const unsigned *>(p)); }
+
+#define CONV_MT 2 // 16-voxel tiles per warp iteration
+
+// One warp: CONV_MT tiles of 16 consecutive voxels x 16 output channels.
+template <bool F32OUT>
+__global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	bf16 *Ws = reinterpret_cast<bf16 *>(smem_raw);
+	const int Cin = a.Ca + a.Cb;
+	const int ldw = Cin + 8;
+	const int slice = blockIdx.y; // 16 output channels
+	// stage the weight slice: Ws[(tap*16 + n) * ldw + k]
+	for (int e = threadIdx.x; e < 27 * 16 * (Cin / 2); e += blockDim.x) {
+		const int k2 = e % (Cin / 2), row = e / (Cin / 2);
+		const int tap = row / 16, n = row % 16;
+		const unsigned v = ld_u32(a.W + ((size_t)tap * a.Cout + slice * 16 + n) * Cin + 2 * k2);
+		*reinterpret_cast<unsigned *>(Ws + (size_t)row * ldw + 2 * k2) = v;
+	}
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int g = lane >> 2, t4 = lane & 3;
+	const long long nvox = (long long)a.nz * a.ny * a.nx;
+	const long long ntile = (nvox + 16 * CONV_MT - 1) / (16 * CONV_MT);
+	const int nyA = a.ny >> a.upA, nxA = a.nx >> a.upA;
+	for (long long tile = (long long)blockIdx.x * 4 + warp; tile < ntile; tile += (long long)gridDim.x * 4) {
+		// rows handled by this lane: r = mt*16 + g + 8*h
+		int vz[CONV_MT][2], vy[CONV_MT][2], vx[CONV_MT][2];
+		bool vin[CONV_MT][2];
+#pragma unroll
+		for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const long long v = tile * 16 * CONV_MT + mt * 16 + g + 8 * h;
+				vin[mt][h] = v < nvox;
+				const long long vv = vin[mt][h] ? v : 0;
+				vx[mt][h] = (int)(vv % a.nx);
+				vy[mt][h] = (int)((vv / a.nx) % a.ny);
+				vz[mt][h] = (int)(vv / ((long long)a.nx * a.ny));
+			}
+		float acc[CONV_MT][2][4];
+#pragma unroll
+		for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+			for (int j = 0; j < 2; j++)
+#pragma unroll
+				for (int q = 0; q < 4; q++) acc[mt][j][q] = 0.f;
+		for (int tap = 0; tap < 27; tap++) {
+			const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+			long long ia[CONV_MT][2], ib[CONV_MT][2];
+			bool ok[CONV_MT][2];
+#pragma unroll
+			for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+				for (int h = 0; h < 2; h++) {
+					const int z = vz[mt][h] + dz, y = vy[mt][h] + dy, x = vx[mt][h] + dx;
+					ok[mt][h] = vin[mt][h] && z >= 0 && z < a.nz && y >= 0 && y < a.ny && x >= 0 && x < a.nx;
+					const int za = z >> a.upA, ya = y >> a.upA, xa = x >> a.upA;
+					ia[mt][h] = ok[mt][h] ? (((long long)za * nyA + ya) * nxA + xa) * a.Ca : 0;
+					ib[mt][h] = ok[mt][h] ? (((long long)z * a.ny + y) * a.nx + x) * a.Cb : 0;
+				}
+			const bf16 *wt = Ws + (size_t)tap * 16 * ldw;
+			for (int cb = 0; cb < Cin; cb += 16) {
+				const bool fromA = cb < a.Ca;
+				const bf16 *src = fromA ? a.A + cb : a.B + (cb - a.Ca);
+				unsigned b[2][2];
+#pragma unroll
+				for (int j = 0; j < 2; j++) {
+					const bf16 *wr = wt + (size_t)(j * 8 + g) * ldw + cb + 2 * t4;
+					b[j][0] = *reinterpret_cast<const unsigned *>(wr);
+					b[j][1] = *reinterpret_cast<const unsigned *>(wr + 8);
+				}
+#pragma unroll
+				for (int mt = 0; mt < CONV_MT; mt++) {
+					unsigned af[4];
+					const long long i0 = fromA ? ia[mt][0] : ib[mt][0];
+					const long long i1 = fromA ? ia[mt][1] : ib[mt][1];
+					af[0] = ok[mt][0] ? ld_u32(src + i0 + 2 * t4) : 0u;
+					af[1] = ok[mt][1] ? ld_u32(src + i1 + 2 * t4) : 0u;
+					af[2] = ok[mt][0] ? ld_u32(src + i0 + 2 * t4 + 8) : 0u;
+					af[3] = ok[mt][1] ? ld_u32(src + i1 + 2 * t4 + 8) : 0u;
+#pragma unroll
+					for (int j = 0; j < 2; j++) mma_bf16(acc[mt][j], af, b[j][0], b[j][1]);
+				}
+			}
+		}
+		// epilogue: rows g / g+8, columns slice*16 + j*8 + 2*t4 + {0,1}
+#pragma unroll
+		for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				if (!vin[mt][h]) continue;
+				const long long v = tile * 16 * CONV_MT + mt * 16 + g + 8 * h;
+#pragma unroll
+				for (int j = 0; j < 2; j++) {
+					const int co = slice * 16 + j * 8 + 2 * t4;
+					const float c0 = acc[mt][j][2 * h], c1 = acc[mt][j][2 * h + 1];
+					if (F32OUT) {
+						*reinterpret_cast<float2 *>(static_cast<float *>(a.out) + v * a.Cout + co) = make_float2(c0, c1);
+					} else {
+						*reinterpret_cast<__nv_bfloat162 *>(static_cast<bf16 *>(a.out) + v * a.Cout + co) =
+						    __floats2bfloat162_rn(fmaxf(c0, 0.f), fmaxf(c1, 0.f));
+					}
+				}
+			}
+	}
+}
+
+// 2x2x2 mean, bf16 in / out (dims of the input).
+__global__ void k_pool(int nz, int ny, int nx, int C, const bf16 *in, bf16 *out) {
+	const int oz = nz / 2, oy = ny / 2, ox = nx / 2;
+	const long long n = (long long)oz * oy * ox * C;
+	for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int c = (int)(e % C);
+		const long long v = e / C;
+		const int x = (int)(v % ox), y = (int)((v / ox) % oy), z = (int)(v / ((long long)ox * oy));
+		float s = 0.f;
+#pragma unroll
+		for (int k = 0; k < 8; k++) {
+			const long long u = ((long long)(2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
+			s += __bfloat162float(in[u * C + c]);
+		}
+		out[e] = __float2bfloat16_rn(s * 0.125f);
+	}
+}
+
+// x0 from r (scaled by 1/|r|, |r|^2 in *nrm2) and the log-diagonal channel.
+__global__ void k_input(long long n, const double *r, const double *nrm2, const bf16 *logd, bf16 *x0) {
+	const double s2 = *nrm2;
+	const double inv = s2 > 0.0 ? 1.0 / sqrt(s2) : 0.0;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		__align__(16) bf16 h[16];
+#pragma unroll
+		for (int c = 0; c < 16; c++) h[c] = __float2bfloat16_rn(0.f);
+		h[0] = __float2bfloat16_rn((float)(r[v] * inv));
+		h[1] = logd[v];
+		uint4 *dst = reinterpret_cast<uint4 *>(x0 + v * 16);
+		dst[0] = reinterpret_cast<const uint4 *>(h)[0];
+		dst[1] = reinterpret_cast<const uint4 *>(h)[1];
+	}
+}
+
+// y = w7 . d0 per voxel (FP32).
+__global__ void k_head(long long n, const bf16 *d0, const float *w7, float *y) {
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		float s = 0.f;
+#pragma unroll
+		for (int c = 0; c < 16; c++) s = fmaf(w7[c], __bfloat162float(d0[v * 16 + c]), s);
+		y[v] = s;
+	}
+}
+
+// z += |r| y, unless some y is not finite (then z keeps the plain ILU2 step).
+__global__ void k_check_finite(long long n, const float *y, int *flag) {
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+		if (!isfinite(y[v])) atomicExch(flag, 1);
+}
+__global__ void k_correct(long long n, const float *y, const double *nrm2, const int *flag, double *z) {
+	if (*flag) return;
+	const double s = sqrt(*nrm2);
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+		z[v] += s * (double)y[v];
+}
+__global__ void k_out(long long n, const float *y, const double *nrm2, double *out) {
+	const double s = sqrt(*nrm2);
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+		out[v] = s * (double)y[v];
+}
+
+// r1 = v - t
+__global__ void k_sub(long long n, const double *v, const double *t, double *r) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		r[i] = v[i] - t[i];
+}
+
+// sum of squares into *out (deterministic: fixed grid, block partials, one
+// final block)
+#define SQ_BLOCKS 256
+__global__ void k_sumsq_part(long long n, const double *x, double *part) {
+	__shared__ double sh[8];
+	double s = 0;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		s = fma(x[i], x[i], s);
+	s = warp_sum(s);
+	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+		part[blockIdx.x] = t;
+	}
+}
+__global__ void k_sum_final(int nb, const double *part, double *out) {
+	if (threadIdx.x == 0) {
+		double t = 0;
+		for (int b = 0; b < nb; b++) t += part[b];
+		*out = t;
+	}
+}
+
+// log |a_ii| (diagonal first in each row of the upper split), then its
+// mean and standard deviation, then the bf16 normalised channel.
+__global__ void k_logdiag(int n, const int *iu, const double *al, double *ld) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		ld[i] = log(fabs(al[iu[i]]) + 1e-300);
+}
+__global__ void k_moments(int n, const double *ld, double *out) {
+	// one block: mean and standard deviation
+	__shared__ double s1[256], s2[256];
+	double a = 0, b = 0;
+	for (int i = threadIdx.x; i < n; i += blockDim.x) { a += ld[i]; b = fma(ld[i], ld[i], b); }
+	s1[threadIdx.x] = a;
+	s2[threadIdx.x] = b;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double m = 0, q = 0;
+		for (int t = 0; t < (int)blockDim.x; t++) { m += s1[t]; q += s2[t]; }
+		m /= n;
+		q = q / n - m * m;
+		out[0] = m;
+		out[1] = q > 1e-30 ? sqrt(q) : 1.0;
+	}
+}
+__global__ void k_logd_norm(int n, const double *ld, const double *mom, bf16 *out) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		out[i] = __float2bfloat16_rn((float)((ld[i] - mom[0]) / mom[1]));
+}
+
+// ---- training --------------------------------------------------------------
+
+// target t / |r|, loss |y - t'|^2 / |t'|^2 and dL/dy; s[0] = |r|^2, s[1] = |t|^2
+__global__ void k_loss(long long n, const float *y, const double *t, const double *s, float *gy, double *lpart) {
+	__shared__ double sh[8];
+	const double inv = s[0] > 0 ? 1.0 / sqrt(s[0]) : 0.0;
+	const double tt = s[1] * inv * inv;
+	const double sc = tt > 0 ? 1.0 / tt : 0.0;
+	double l = 0;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		const double d = (double)y[v] - t[v] * inv;
+		gy[v] = (float)(2.0 * d * sc);
+		l = fma(d, d, l);
+	}
+	l = warp_sum(l);
+	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double q = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) q += sh[w];
+		lpart[blockIdx.x] = q * sc;
+	}
+}
+
+// dd0 = w7 * gy masked by d0 > 0 (bf16); dw7[c] += sum_v d0[v][c] gy[v]
+__global__ void k_head_bwd(long long n, const bf16 *d0, const float *w7, const float *gy, bf16 *dd0, float *dw7) {
+	__shared__ float sh[16][33];
+	float acc[16];
+#pragma unroll
+	for (int c = 0; c < 16; c++) acc[c] = 0.f;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		const float gv = gy[v];
+#pragma unroll
+		for (int c = 0; c < 16; c++) {
+			const float a = __bfloat162float(d0[v * 16 + c]);
+			acc[c] = fmaf(a, gv, acc[c]);
+			dd0[v * 16 + c] = __float2bfloat16_rn(a > 0.f ? w7[c] * gv : 0.f);
+		}
+	}
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int c = 0; c < 16; c++) {
+		float s = acc[c];
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) sh[c][warp] = s;
+	}
+	__syncthreads();
+	if (threadIdx.x < 16) {
+		float s = 0.f;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[threadIdx.x][w];
+		atomicAdd(dw7 + threadIdx.x, s);
+	}
+}
+
+// Gradient of an activation act [v][C] (this level's dims), bf16 out:
+//   up_t mode (fine != null): sum over the 8 children of fine[child*fs + fo + c]
+//   skip mode: skip[v*ss + so + c] + coarse[parent*C + c] / 8 (coarse may be null)
+// times (act > 0).
+__global__ void k_grad_act(int nz, int ny, int nx, int C, const float *fine, int fs, int fo, const float *skip, int ss,
+                           int so, const float *coarse, const bf16 *act, bf16 *out) {
+	const long long n = (long long)nz * ny * nx * C;
+	for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int c = (int)(e % C);
+		const long long v = e / C;
+		const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((long long)nx * ny));
+		float s = 0.f;
+		if (fine) {
+			const int fy = 2 * ny, fx = 2 * nx;
+#pragma unroll
+			for (int k = 0; k < 8; k++) {
+				const long long u = ((long long)(2 * z + (k >> 2)) * fy + 2 * y + ((k >> 1) & 1)) * fx + 2 * x + (k & 1);
+				s += fine[u * fs + fo + c];
+			}
+		} else {
+			s = skip[v * ss + so + c];
+			if (coarse) {
+				const long long p = ((long long)(z >> 1) * (ny >> 1) + (y >> 1)) * (nx >> 1) + (x >> 1);
+				s += coarse[p * C + c] * 0.125f;
+			}
+		}
+		out[e] = __float2bfloat16_rn(__bfloat162float(act[e]) > 0.f ? s : 0.f);
+	}
+}
+
+// dW[tap][co][ci] += sum_v g[v][co] in(v + off(tap))[ci], CUDA cores, FP32.
+// Each thread owns (tap, 4 output, 4 input channels) combinations over one
+// voxel chunk of the block.
+__global__ void __launch_bounds__(256) k_wgrad(ConvArgs a, const bf16 *gr, long long chunk, float *dW) {
+	const int Cin = a.Ca + a.Cb, Cout = a.Cout;
+	const long long nvox = (long long)a.nz * a.ny * a.nx;
+	const long long v0 = blockIdx.x * chunk;
+	const long long v1 = v0 + chunk < nvox ? v0 + chunk : nvox;
+	const int nci4 = Cin / 4, nco4 = Cout / 4;
+	const int ncombo = 27 * nco4 * nci4;
+	const int nyA = a.ny >> a.upA, nxA = a.nx >> a.upA;
+	for (int e = threadIdx.x; e < ncombo; e += blockDim.x) {
+		const int ci4 = e % nci4, co4 = (e / nci4) % nco4, tap = e / (nci4 * nco4);
+		const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+		const int ci = ci4 * 4;
+		const bool fromA = ci < a.Ca;
+		float acc[4][4];
+#pragma unroll
+		for (int p = 0; p < 4; p++)
+#pragma unroll
+			for (int q = 0; q < 4; q++) acc[p][q] = 0.f;
+		int x = (int)(v0 % a.nx), y = (int)((v0 / a.nx) % a.ny), z = (int)(v0 / ((long long)a.nx * a.ny));
+		for (long long v = v0; v < v1; v++) {
+			const int zz = z + dz, yy = y + dy, xx = x + dx;
+			if (zz >= 0 && zz < a.nz && yy >= 0 && yy < a.ny && xx >= 0 && xx < a.nx) {
+				const bf16 *ip;
+				if (fromA)
+					ip = a.A + (((long long)(zz >> a.upA) * nyA + (yy >> a.upA)) * nxA + (xx >> a.upA)) * a.Ca + ci;
+				else
+					ip = a.B + (((long long)zz * a.ny + yy) * a.nx + xx) * a.Cb + (ci - a.Ca);
+				const uint2 iv = __ldg(reinterpret_cast<const uint2 *>(ip));
+				const uint2 gv = __ldg(reinterpret_cast<const uint2 *>(gr + v * Cout + co4 * 4));
+				const __nv_bfloat162 i01 = *reinterpret_cast<const __nv_bfloat162 *>(&iv.x);
+				const __nv_bfloat162 i23 = *reinterpret_cast<const __nv_bfloat162 *>(&iv.y);
+				const __nv_bfloat162 g01 = *reinterpret_cast<const __nv_bfloat162 *>(&gv.x);
+				const __nv_bfloat162 g23 = *reinterpret_cast<const __nv_bfloat162 *>(&gv.y);
+				const float in4[4] = {__low2float(i01), __high2float(i01), __low2float(i23), __high2float(i23)};
+				const float g4[4] = {__low2float(g01), __high2float(g01), __low2float(g23), __high2float(g23)};
+#pragma unroll
+				for (int p = 0; p < 4; p++)
+#pragma unroll
+					for (int q = 0; q < 4; q++) acc[p][q] = fmaf(g4[p], in4[q], acc[p][q]);
+			}
+			if (++x == a.nx) { x = 0; if (++y == a.ny) { y = 0; ++z; } }
+		}
+#pragma unroll
+		for (int p = 0; p < 4; p++)
+#pragma unroll
+			for (int q = 0; q < 4; q++)
+				if (acc[p][q] != 0.f) atomicAdd(dW + ((size_t)tap * Cout + co4 * 4 + p) * Cin + ci + q, acc[p][q]);
+	}
+}
+
+// Adam on the FP32 master weights; grads are averaged over `count` samples
+// and cleared.  W0's padded input channels (ci >= 2) stay zero.
+__global__ void k_adam(int n, float *w, float *m, float *v, float *gr, float inv_count, float lr, float b1, float b2,
+                       float eps, float c1, float c2, int w0_len) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		float gi = gr[i] * inv_count;
+		gr[i] = 0.f;
+		if (i < w0_len && (i % 16) >= 2) { w[i] = 0.f; continue; }
+		m[i] = b1 * m[i] + (1.f - b1) * gi;
+		v[i] = b2 * v[i] + (1.f - b2) * gi * gi;
+		const float mh = m[i] / c1, vh = v[i] / c2;
+		w[i] -= lr * mh / (sqrtf(vh) + eps);
+	}
+}
+
+// bf16 copies of the master weights: W [tap][co][ci] and the data-gradient
+// form WT [tap][ci][co] = W[26 - tap][co][ci].
+__global__ void k_refresh(int len, int cout, int cin, const float *w, bf16 *wb, bf16 *wt) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+		const int ci = i % cin, co = (i / cin) % cout, tap = i / (cin * cout);
+		const bf16 b = __float2bfloat16_rn(w[i]);
+		wb[i] = b;
+		wt[((size_t)(26 - tap) * cin + ci) * cout + co] = b;
+	}
+}
+__global__ void k_w7(const float *w, float *w7b) {
+	if (threadIdx.x < 16) w7b[threadIdx.x] = __bfloat162float(__float2bfloat16_rn(w[threadIdx.x]));
+}
+
+inline int ew(long long n) {
+	long long b = (n + 255) / 256;
+	return (int)(b < BSG_SMS * 16 ? (b > 0 ? b : 1) : BSG_SMS * 16);
+}
+
+} // namespace
+
+// ---- the network object ------------------------------------------------------
+struct bsg_unet {
+	bsg_ctx *ctx;
+	const bsg_mat *mat;
+	int nz, ny, nx;
+	long long nv[4];            // voxels per level
+	int woff[NW + 1];           // offsets of W0..W6 in the flat parameter vector (w7 at woff[NW])
+	int nparam;
+	float *master, *adam_m, *adam_v, *grad;
+	bf16 *wb[NW], *wt[NW];
+	float *w7b;                 // bf16-rounded head weights as FP32
+	bf16 *logd;                 // normalised log-diagonal channel [R0]
+	double *ld, *mom;           // log-diagonal scratch, its moments
+	// activations
+	bf16 *x0, *e0, *p1, *e1, *p2, *e2, *p3, *e3, *d2, *d1, *d0;
+	float *y, *gy;
+	double *r1, *t1, *sc, *part; // residual, SpMV scratch, scalars [0]=|r|^2 [1]=|t|^2, reduction partials
+	int *flag;
+	// training buffers
+	bf16 *dd0, *gd1, *gd2, *ge3, *ge2, *ge1, *ge0;
+	float *gi6, *gi5, *gi4, *gp3, *gp2, *gp1;
+	int count;
+	double loss_sum;
+	bool train;
+};
+
+namespace {
+
+template <class T>
+int dalloc(bsg_ctx *c, T **p, size_t n) {
+	if (cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * (n > 0 ? n : 1)) != cudaSuccess)
+		return bsg_set_error(BSG_ERR_NOMEM, "U-Net buffers");
+	(void)c;
+	return BSG_OK;
+}
+
+int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16 *B, int Cb, const bf16 *W, int Cout,
+                void *out, bool f32out) {
+	cudaStream_t s = u->ctx->stream;
+	ConvArgs a;
+	a.nz = u->nz >> lvl; a.ny = u->ny >> lvl; a.nx = u->nx >> lvl;
+	a.A = A; a.Ca = Ca; a.upA = upA; a.B = B; a.Cb = Cb; a.W = W; a.Cout = Cout; a.out = out;
+	const int Cin = Ca + Cb;
+	const size_t smem = (size_t)27 * 16 * (Cin + 8) * sizeof(bf16);
+	const long long ntile = (u->nv[lvl] + 16 * CONV_MT - 1) / (16 * CONV_MT);
+	long long bx = (ntile + 3) / 4;
+	const long long cap = (long long)BSG_SMS * 8 / (Cout / 16);
+	if (bx > cap) bx = cap;
+	if (bx < 1) bx = 1;
+	dim3 grid((unsigned)bx, Cout / 16);
+	BSG_COUNT(1);
+	if (f32out) {
+		BSG_CUDA(cudaFuncSetAttribute(k_conv3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		k_conv3<true><<<grid, 128, smem, s>>>(a);
+	} else {
+		BSG_CUDA(cudaFuncSetAttribute(k_conv3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		k_conv3<false><<<grid, 128, smem, s>>>(a);
+	}
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+int wgrad_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16 *B, int Cb, int Cout, const bf16 *g,
+                 float *dW) {
+	ConvArgs a;
+	a.nz = u->nz >> lvl; a.ny = u->ny >> lvl; a.nx = u->nx >> lvl;
+	a.A = A; a.Ca = Ca; a.upA = upA; a.B = B; a.Cb = Cb; a.W = nullptr; a.Cout = Cout; a.out = nullptr;
+	const long long nvox = u->nv[lvl];
+	long long chunk = (nvox + 2 * BSG_SMS - 1) / (2 * BSG_SMS);
+	if (chunk < 64) chunk = 64;
+	const int blocks = (int)((nvox + chunk - 1) / chunk);
+	BSG_COUNT(1);
+	k_wgrad<<<blocks, 256, 0, u->ctx->stream>>>(a, g, chunk, dW);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+int pool_launch(bsg_unet *u, int lvl, int C, const bf16 *in, bf16 *out) {
+	BSG_COUNT(1);
+	k_pool<<<ew(u->nv[lvl + 1] * C), 256, 0, u->ctx->stream>>>(u->nz >> lvl, u->ny >> lvl, u->nx >> lvl, C, in, out);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+int sumsq(bsg_unet *u, long long n, const double *x, double *out) {
+	BSG_COUNT(2);
+	k_sumsq_part<<<SQ_BLOCKS, 256, 0, u->ctx->stream>>>(n, x, u->part);
+	k_sum_final<<<1, 32, 0, u->ctx->stream>>>(SQ_BLOCKS, u->part, out);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// Forward pass from r (FP64, |r|^2 already in u->sc[0]) to y (FP32).
+int forward(bsg_unet *u, const double *r) {
+	cudaStream_t s = u->ctx->stream;
+	int rc;
+	BSG_COUNT(1);
+	k_input<<<ew(u->nv[0]), 256, 0, s>>>(u->nv[0], r, u->sc, u->logd, u->x0);
+	if ((rc = conv_launch(u, 0, u->x0, 16, 0, nullptr, 0, u->wb[0], 16, u->e0, false))) return rc;
+	if ((rc = pool_launch(u, 0, 16, u->e0, u->p1))) return rc;
+	if ((rc = conv_launch(u, 1, u->p1, 16, 0, nullptr, 0, u->wb[1], 32, u->e1, false))) return rc;
+	if ((rc = pool_launch(u, 1, 32, u->e1, u->p2))) return rc;
+	if ((rc = conv_launch(u, 2, u->p2, 32, 0, nullptr, 0, u->wb[2], 64, u->e2, false))) return rc;
+	if ((rc = pool_launch(u, 2, 64, u->e2, u->p3))) return rc;
+	if ((rc = conv_launch(u, 3, u->p3, 64, 0, nullptr, 0, u->wb[3], 64, u->e3, false))) return rc;
+	if ((rc = conv_launch(u, 2, u->e3, 64, 1, u->e2, 64, u->wb[4], 32, u->d2, false))) return rc;
+	if ((rc = conv_launch(u, 1, u->d2, 32, 1, u->e1, 32, u->wb[5], 16, u->d1, false))) return rc;
+	if ((rc = conv_launch(u, 0, u->d1, 16, 1, u->e0, 16, u->wb[6], 16, u->d0, false))) return rc;
+	BSG_COUNT(1);
+	k_head<<<ew(u->nv[0]), 256, 0, s>>>(u->nv[0], u->d0, u->w7b, u->y);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// Backward pass from gy; accumulates into u->grad.
+int backward(bsg_unet *u) {
+	cudaStream_t s = u->ctx->stream;
+	float *G = u->grad;
+	const int *o = u->woff;
+	int rc;
+	const int R[4][3] = {{u->nz, u->ny, u->nx}, {u->nz >> 1, u->ny >> 1, u->nx >> 1},
+	                     {u->nz >> 2, u->ny >> 2, u->nx >> 2}, {u->nz >> 3, u->ny >> 3, u->nx >> 3}};
+	BSG_COUNT(1);
+	k_head_bwd<<<ew(u->nv[0]), 256, 0, s>>>(u->nv[0], u->d0, u->w7b, u->gy, u->dd0, G + o[NW]);
+	// W6: in = [up d1, e0]
+	if ((rc = wgrad_launch(u, 0, u->d1, 16, 1, u->e0, 16, 16, u->dd0, G + o[6]))) return rc;
+	if ((rc = conv_launch(u, 0, u->dd0, 16, 0, nullptr, 0, u->wt[6], 32, u->gi6, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[1] * 16), 256, 0, s>>>(R[1][0], R[1][1], R[1][2], 16, u->gi6, 32, 0, nullptr, 0, 0, nullptr,
+	                                            u->d1, u->gd1);
+	// W5: in = [up d2, e1]
+	if ((rc = wgrad_launch(u, 1, u->d2, 32, 1, u->e1, 32, 16, u->gd1, G + o[5]))) return rc;
+	if ((rc = conv_launch(u, 1, u->gd1, 16, 0, nullptr, 0, u->wt[5], 64, u->gi5, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[2] * 32), 256, 0, s>>>(R[2][0], R[2][1], R[2][2], 32, u->gi5, 64, 0, nullptr, 0, 0, nullptr,
+	                                            u->d2, u->gd2);
+	// W4: in = [up e3, e2]
+	if ((rc = wgrad_launch(u, 2, u->e3, 64, 1, u->e2, 64, 32, u->gd2, G + o[4]))) return rc;
+	if ((rc = conv_launch(u, 2, u->gd2, 32, 0, nullptr, 0, u->wt[4], 128, u->gi4, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[3] * 64), 256, 0, s>>>(R[3][0], R[3][1], R[3][2], 64, u->gi4, 128, 0, nullptr, 0, 0, nullptr,
+	                                            u->e3, u->ge3);
+	// W3: in = p3
+	if ((rc = wgrad_launch(u, 3, u->p3, 64, 0, nullptr, 0, 64, u->ge3, G + o[3]))) return rc;
+	if ((rc = conv_launch(u, 3, u->ge3, 64, 0, nullptr, 0, u->wt[3], 64, u->gp3, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[2] * 64), 256, 0, s>>>(R[2][0], R[2][1], R[2][2], 64, nullptr, 0, 0, u->gi4, 128, 64, u->gp3,
+	                                            u->e2, u->ge2);
+	// W2: in = p2
+	if ((rc = wgrad_launch(u, 2, u->p2, 32, 0, nullptr, 0, 64, u->ge2, G + o[2]))) return rc;
+	if ((rc = conv_launch(u, 2, u->ge2, 64, 0, nullptr, 0, u->wt[2], 32, u->gp2, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[1] * 32), 256, 0, s>>>(R[1][0], R[1][1], R[1][2], 32, nullptr, 0, 0, u->gi5, 64, 32, u->gp2,
+	                                            u->e1, u->ge1);
+	// W1: in = p1
+	if ((rc = wgrad_launch(u, 1, u->p1, 16, 0, nullptr, 0, 32, u->ge1, G + o[1]))) return rc;
+	if ((rc = conv_launch(u, 1, u->ge1, 32, 0, nullptr, 0, u->wt[1], 16, u->gp1, true))) return rc;
+	BSG_COUNT(1);
+	k_grad_act<<<ew(u->nv[0] * 16), 256, 0, s>>>(R[0][0], R[0][1], R[0][2], 16, nullptr, 0, 0, u->gi6, 32, 16, u->gp1,
+	                                            u->e0, u->ge0);
+	// W0: in = x0
+	if ((rc = wgrad_launch(u, 0, u->x0, 16, 0, nullptr, 0, 16, u->ge0, G + o[0]))) return rc;
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+int refresh(bsg_unet *u) {
+	cudaStream_t s = u->ctx->stream;
+	for (int k = 0; k < NW; k++) {
+		const int len = 27 * CIN[k] * COUT[k];
+		BSG_COUNT(1);
+		k_refresh<<<ew(len), 256, 0, s>>>(len, COUT[k], CIN[k], u->master + u->woff[k], u->wb[k], u->wt[k]);
+	}
+	BSG_COUNT(1);
+	k_w7<<<1, 32, 0, s>>>(u->master + u->woff[NW], u->w7b);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+} // namespace
+
+extern "C" int bsg_unet_free(bsg_unet *u);
+
+extern "C" int bsg_unet_create(bsg_ctx *c, int nx, int ny, int nz, int train, bsg_unet **out) {
+	if (!c || !out) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_create: null argument");
+	*out = nullptr;
+	if (nx < 8 || ny < 8 || nz < 8 || nx % 8 || ny % 8 || nz % 8)
+		return bsg_set_error(BSG_ERR_ARG, "bsg_unet_create: grid sides must be multiples of 8 (three poolings)");
+	BSG_CUDA(cudaSetDevice(c->device));
+	bsg_unet *u = new bsg_unet();
+	std::memset(u, 0, sizeof(*u));
+	u->ctx = c;
+	u->nz = nz; u->ny = ny; u->nx = nx;
+	for (int l = 0; l < 4; l++) u->nv[l] = (long long)(nz >> l) * (ny >> l) * (nx >> l);
+	u->train = train != 0;
+	int off = 0;
+	for (int k = 0; k < NW; k++) { u->woff[k] = off; off += 27 * CIN[k] * COUT[k]; }
+	u->woff[NW] = off;
+	u->nparam = off + 16;
+	int rc = BSG_OK;
+	auto A = [&](auto **p, size_t n) { if (!rc) rc = dalloc(c, p, n); };
+	A(&u->master, u->nparam);
+	A(&u->adam_m, u->nparam);
+	A(&u->adam_v, u->nparam);
+	A(&u->grad, u->nparam);
+	for (int k = 0; k < NW; k++) {
+		A(&u->wb[k], (size_t)27 * CIN[k] * COUT[k]);
+		A(&u->wt[k], (size_t)27 * CIN[k] * COUT[k]);
+	}
+	A(&u->w7b, 16);
+	const long long *nv = u->nv;
+	A(&u->logd, nv[0]); A(&u->ld, nv[0]); A(&u->mom, 2);
+	A(&u->x0, nv[0] * 16); A(&u->e0, nv[0] * 16); A(&u->p1, nv[1] * 16); A(&u->e1, nv[1] * 32);
+	A(&u->p2, nv[2] * 32); A(&u->e2, nv[2] * 64); A(&u->p3, nv[3] * 64); A(&u->e3, nv[3] * 64);
+	A(&u->d2, nv[2] * 32); A(&u->d1, nv[1] * 16); A(&u->d0, nv[0] * 16);
+	A(&u->y, nv[0]); A(&u->gy, nv[0]);
+	A(&u->r1, nv[0]); A(&u->t1, nv[0]); A(&u->sc, 4); A(&u->part, SQ_BLOCKS); A(&u->flag, 1);
+	if (u->train) {
+		A(&u->dd0, nv[0] * 16); A(&u->gd1, nv[1] * 16); A(&u->gd2, nv[2] * 32); A(&u->ge3, nv[3] * 64);
+		A(&u->ge2, nv[2] * 64); A(&u->ge1, nv[1] * 32); A(&u->ge0, nv[0] * 16);
+		A(&u->gi6, nv[0] * 32); A(&u->gi5, nv[1] * 64); A(&u->gi4, nv[2] * 128);
+		A(&u->gp3, nv[3] * 64); A(&u->gp2, nv[2] * 32); A(&u->gp1, nv[1] * 16);
+	}
+	if (!rc && cudaMemset(u->grad, 0, sizeof(float) * u->nparam) != cudaSuccess) rc = BSG_ERR_CUDA;
+	if (!rc && cudaMemset(u->adam_m, 0, sizeof(float) * u->nparam) != cudaSuccess) rc = BSG_ERR_CUDA;
+	if (!rc && cudaMemset(u->adam_v, 0, sizeof(float) * u->nparam) != cudaSuccess) rc = BSG_ERR_CUDA;
+	if (!rc && cudaMemset(u->logd, 0, sizeof(bf16) * nv[0]) != cudaSuccess) rc = BSG_ERR_CUDA;
+	if (rc) {
+		bsg_unet_free(u);
+		return rc;
+	}
+	*out = u;
+	return BSG_OK;
+}
+
+extern "C" int bsg_unet_free(bsg_unet *u) {
+	if (!u) return BSG_OK;
+	void *ps[] = {u->master, u->adam_m, u->adam_v, u->grad, u->w7b, u->logd, u->ld, u->mom, u->x0, u->e0, u->p1,
+	              u->e1, u->p2, u->e2, u->p3, u->e3, u->d2, u->d1, u->d0, u->y, u->gy, u->r1, u->t1, u->sc, u->part,
+	              u->flag, u->dd0, u->gd1, u->gd2, u->ge3, u->ge2, u->ge1, u->ge0, u->gi6, u->gi5, u->gi4, u->gp3,
+	              u->gp2, u->gp1};
+	cudaStreamSynchronize(u->ctx->stream);
+	for (void *p : ps)
+		if (p) cudaFree(p);
+	for (int k = 0; k < NW; k++) {
+		if (u->wb[k]) cudaFree(u->wb[k]);
+		if (u->wt[k]) cudaFree(u->wt[k]);
+	}
+	delete u;
+	return BSG_OK;
+}
+
+extern "C" int bsg_unet_nparam(const bsg_unet *u) { return u ? u->nparam : 0; }
+
+// Weights in the flat FP32 layout W0..W6 ([tap][cout][cin] each), then w7.
+extern "C" int bsg_unet_set_weights(bsg_unet *u, const float *w) {
+	if (!u || !w) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_weights: null argument");
+	BSG_CUDA(cudaMemcpyAsync(u->master, w, sizeof(float) * u->nparam, cudaMemcpyHostToDevice, u->ctx->stream));
+	int rc = refresh(u);
+	if (!rc) BSG_CUDA(cudaStreamSynchronize(u->ctx->stream));
+	return rc;
+}
+extern "C" int bsg_unet_get_weights(bsg_unet *u, float *w) {
+	if (!u || !w) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_get_weights: null argument");
+	BSG_CUDA(cudaMemcpyAsync(w, u->master, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost, u->ctx->stream));
+	BSG_CUDA(cudaStreamSynchronize(u->ctx->stream));
+	return BSG_OK;
+}
+extern "C" int bsg_unet_get_grads(bsg_unet *u, float *g) {
+	if (!u || !g) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_get_grads: null argument");
+	BSG_CUDA(cudaMemcpyAsync(g, u->grad, sizeof(float) * u->nparam, cudaMemcpyDeviceToHost, u->ctx->stream));
+	BSG_CUDA(cudaStreamSynchronize(u->ctx->stream));
+	return BSG_OK;
+}
+
+// The operator whose diagonal feeds the second input channel, and whose
+// product forms the residual after the ILU2 step inside FGMRES.  Point
+// matrices on an nx x ny x nz grid in natural order.
+extern "C" int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m) {
+	if (!u || !m) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_matrix: null argument");
+	if (m->bs != 1 || (long long)m->n != u->nv[0])
+		return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_matrix: matrix size does not match the grid");
+	u->mat = m;
+	cudaStream_t s = u->ctx->stream;
+	BSG_COUNT(3);
+	k_logdiag<<<ew(m->n), 256, 0, s>>>(m->n, m->d_iu, m->d_al, u->ld);
+	k_moments<<<1, 256, 0, s>>>(m->n, u->ld, u->mom);
+	k_logd_norm<<<ew(m->n), 256, 0, s>>>(m->n, u->ld, u->mom, u->logd);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// y_out = |r| N(r / |r|) (FP64), the network's correction for residual r.
+extern "C" int bsg_unet_forward_dev(bsg_unet *u, const double *r, double *y_out) {
+	if (!u || !r || !y_out) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_forward_dev: null argument");
+	int rc = sumsq(u, u->nv[0], r, u->sc);
+	if (!rc) rc = forward(u, r);
+	if (rc) return rc;
+	BSG_COUNT(1);
+	k_out<<<ew(u->nv[0]), 256, 0, u->ctx->stream>>>(u->nv[0], u->y, u->sc, y_out);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// One training sample: input residual r, target correction t (both FP64 on
+// the device).  Accumulates the weight gradients of |N(r/|r|) - t/|r||^2 /
+// |t/|r||^2; *loss (may be NULL) gets the sample's loss.
+extern "C" int bsg_unet_train_sample(bsg_unet *u, const double *r, const double *t, double *loss) {
+	if (!u || !r || !t) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_train_sample: null argument");
+	if (!u->train) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_train_sample: network created without training buffers");
+	cudaStream_t s = u->ctx->stream;
+	int rc = sumsq(u, u->nv[0], r, u->sc);
+	if (!rc) rc = sumsq(u, u->nv[0], t, u->sc + 1);
+	if (!rc) rc = forward(u, r);
+	if (rc) return rc;
+	BSG_COUNT(2);
+	k_loss<<<SQ_BLOCKS, 256, 0, s>>>(u->nv[0], u->y, t, u->sc, u->gy, u->part);
+	k_sum_final<<<1, 32, 0, s>>>(SQ_BLOCKS, u->part, u->sc + 2);
+	if ((rc = backward(u))) return rc;
+	u->count++;
+	if (loss) {
+		BSG_CUDA(cudaMemcpyAsync(loss, u->sc + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+		BSG_CUDA(cudaStreamSynchronize(s));
+	}
+	return BSG_OK;
+}
+
+// Adam step with the gradients accumulated since the last step (averaged).
+extern "C" int bsg_unet_adam(bsg_unet *u, float lr, float beta1, float beta2, float eps, int step) {
+	if (!u || step < 1) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_adam: bad argument");
+	const float inv = u->count > 0 ? 1.f / (float)u->count : 0.f;
+	const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+	BSG_COUNT(1);
+	k_adam<<<ew(u->nparam), 256, 0, u->ctx->stream>>>(u->nparam, u->master, u->adam_m, u->adam_v, u->grad, inv, lr,
+	                                                 beta1, beta2, eps, c1, c2, u->woff[1]);
+	BSG_CUDA(cudaGetLastError());
+	u->count = 0;
+	return refresh(u);
+}
+
+extern "C" int bsg_unet_zero_grads(bsg_unet *u) {
+	if (!u) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_zero_grads: null network");
+	BSG_CUDA(cudaMemsetAsync(u->grad, 0, sizeof(float) * u->nparam, u->ctx->stream));
+	u->count = 0;
+	return BSG_OK;
+}
+
+// FGMRES learned stage: z holds the ILU2 step M^{-1} v on entry; the
+// network corrects it with its estimate of the remaining error from the
+// residual r1 = v - A z.  A non-finite network output leaves z as it is
+// (the plain ILU2 step).  `work` is unused (own buffers).
+int bsg_unet_apply(void *net, bsg_ctx *c, const double *v, double *z, double *work) {
+	(void)work;
+	bsg_unet *u = static_cast<bsg_unet *>(net);
+	if (!u || !u->mat) return bsg_set_error(BSG_ERR_ARG, "learned stage: network has no matrix");
+	if (u->ctx != c) return bsg_set_error(BSG_ERR_ARG, "learned stage: network belongs to another context");
+	cudaStream_t s = c->stream;
+	const long long n = u->nv[0];
+	int rc = bsg_spmm_launch(u->mat, 1, z, u->t1, n, s);
+	if (rc) return bsg_set_error(rc, "learned stage: SpMV failed");
+	BSG_COUNT(1);
+	k_sub<<<ew(n), 256, 0, s>>>(n, v, u->t1, u->r1);
+	if ((rc = sumsq(u, n, u->r1, u->sc))) return rc;
+	if ((rc = forward(u, u->r1))) return rc;
+	BSG_CUDA(cudaMemsetAsync(u->flag, 0, sizeof(int), s));
+	BSG_COUNT(2);
+	k_check_finite<<<ew(n), 256, 0, s>>>(n, u->y, u->flag);
+	k_correct<<<ew(n), 256, 0, s>>>(n, u->y, u->sc, u->flag, z);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}

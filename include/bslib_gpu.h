@@ -174,6 +174,30 @@ int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const 
 int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
                    bsg_param *p);
 
+/* ---- learned preconditioner stage (no counterpart in the reference) --------
+ * A 4-level 3D convolutional U-Net (16 base channels, bf16 weights, FP32
+ * accumulation) on an nx x ny x nz grid (sides multiples of 8), natural
+ * order.  Inside FGMRES (p->krylov == 2, p->learned = the network) it follows
+ * the ILU2 step z = M^{-1} v with z += |r1| N(r1 / |r1|), r1 = v - A z; a
+ * non-finite network output leaves the plain ILU2 step.  Weights are a flat
+ * FP32 vector: W0..W6 as [27 taps][cout][cin], then the 16 head weights. */
+typedef struct bsg_unet bsg_unet;
+int bsg_unet_create(bsg_ctx *ctx, int nx, int ny, int nz, int train, bsg_unet **out);
+int bsg_unet_free(bsg_unet *u);
+int bsg_unet_nparam(const bsg_unet *u);
+int bsg_unet_set_weights(bsg_unet *u, const float *w);   /* host, nparam floats */
+int bsg_unet_get_weights(bsg_unet *u, float *w);
+int bsg_unet_get_grads(bsg_unet *u, float *g);           /* accumulated sums */
+/* the operator: its diagonal is the second input channel; FGMRES forms r1 with it */
+int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m);
+/* d_y = |r| N(r / |r|), device FP64 vectors of the grid's length */
+int bsg_unet_forward_dev(bsg_unet *u, const double *d_r, double *d_y);
+/* one training sample (device r and target t); accumulates weight gradients
+ * of |N(r/|r|) - t/|r||^2 / |t/|r||^2, writes that loss to *loss if given */
+int bsg_unet_train_sample(bsg_unet *u, const double *d_r, const double *d_t, double *loss);
+int bsg_unet_adam(bsg_unet *u, float lr, float beta1, float beta2, float eps, int step);
+int bsg_unet_zero_grads(bsg_unet *u);
+
 /* ---- measurement (no counterpart in the reference; it times with clock())  */
 /* Number of kernels this library has launched in the process so far. */
 unsigned long long bsg_launch_count(void);
