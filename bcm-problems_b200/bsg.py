@@ -90,6 +90,7 @@ def lib():
         "bsg_unet_get_weights": (i_, [vp, C.POINTER(C.c_float)]),
         "bsg_unet_get_grads": (i_, [vp, C.POINTER(C.c_float)]),
         "bsg_unet_set_matrix": (i_, [vp, vp]),
+        "bsg_unet_set_diag": (i_, [vp, vp]),
         "bsg_unet_forward_dev": (i_, [vp, vp, vp]),
         "bsg_unet_train_sample": (i_, [vp, vp, vp, C.POINTER(C.c_double)]),
         "bsg_unet_adam": (i_, [vp, C.c_float, C.c_float, C.c_float, C.c_float, i_]),
@@ -308,6 +309,10 @@ class UNet:
     def set_matrix(self, mat):
         _check(lib().bsg_unet_set_matrix(self.h, mat.h))
         self._mat = mat
+
+    def set_diag(self, d):
+        """Second input channel from a CUDA float64 tensor of diagonal values."""
+        _check(lib().bsg_unet_set_diag(self.h, _ptr(d)))
 
     def forward(self, r, y):
         _check(lib().bsg_unet_forward_dev(self.h, _ptr(r), _ptr(y)))

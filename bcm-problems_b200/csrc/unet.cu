@@ -9,7 +9,8 @@
 //   e2 = relu(conv(pool e1; W2 32->64))     e3 = relu(conv(pool e2; W3 64->64))
 //   d2 = relu(conv([up e3, e2]; W4 128->32))
 //   d1 = relu(conv([up d2, e1]; W5 64->16))
-//   d0 = relu(conv([up d1, e0]; W6 32->16)) y = w7 . d0,  correction = |r| y
+//   d0 = relu(conv([up d1, e0]; W6 32->16)) y = w7 . d0
+//   correction alpha y, alpha = (r . y) / (y . A y) (A-norm optimal step)
 //
 // Layout: activations channels-last [z][y][x][c] in bfloat16 (32 bytes per
 // voxel at 16 channels), weights bfloat16 [tap][cout][cin], accumulation in
@@ -166,6 +167,130 @@ __global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
 	}
 }
 
+// ---- shared-memory tiled convolution (grids with nx % 32 == 0) ------------
+// A CTA (8 warps) computes a 32 x 4 x 2 brick of output voxels for 16 output
+// channels.  Input channels go in chunks of CH (16 or 32): the CTA stages the
+// 34 x 6 x 4 halo brick of the chunk and the chunk's weights for all 27 taps
+// in shared memory, then every warp (one 32-voxel x-row) runs the 27 taps
+// with ldmatrix A / B fragments and mma.sync.  The halo rows are stored with
+// their 16-byte pieces XOR-swizzled by the voxel index, so the 8 row
+// addresses of an ldmatrix (8 consecutive voxels) hit 8 distinct bank
+// groups; weight rows are padded by 8 elements for the same reason.
+#define TT_X 32
+#define TT_Y 4
+#define TT_Z 2
+#define TH_X (TT_X + 2)
+#define TH_Y (TT_Y + 2)
+#define TH_Z (TT_Z + 2)
+#define TH_VOX (TH_X * TH_Y * TH_Z)
+
+template <int CH>
+__device__ __forceinline__ unsigned halo_off(int hv, int piece) {
+	const int swz = CH == 32 ? ((hv >> 1) & 3) : ((hv >> 2) & 1);
+	return (unsigned)(hv * CH * 2 + 16 * (piece ^ swz));
+}
+
+__device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned &r0, unsigned &r1, unsigned &r2, unsigned &r3) {
+	asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+	             : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+	             : "r"(addr));
+}
+
+template <bool F32OUT, int CH>
+__global__ void __launch_bounds__(256) k_conv3t(ConvArgs a) {
+	extern __shared__ __align__(128) unsigned char smem_t[];
+	unsigned char *sIn = smem_t;                                   // TH_VOX * CH bf16
+	bf16 *sW = reinterpret_cast<bf16 *>(smem_t + TH_VOX * CH * 2); // [27][16][CH + 8]
+	const int ldw = CH + 8;
+	const int Cin = a.Ca + a.Cb;
+	const int slice = blockIdx.y;
+	const int tx = a.nx / TT_X, ty = a.ny / TT_Y;
+	const int bx = blockIdx.x % tx, by = (blockIdx.x / tx) % ty, bz = blockIdx.x / (tx * ty);
+	const int x0 = bx * TT_X, y0 = by * TT_Y, z0 = bz * TT_Z;
+	const int nyA = a.ny >> a.upA, nxA = a.nx >> a.upA;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int wy = warp & 3, wz = warp >> 2;
+	const int g = lane >> 2, t4 = lane & 3;
+	const unsigned sIn_s = (unsigned)__cvta_generic_to_shared(sIn);
+	const unsigned sW_s = (unsigned)__cvta_generic_to_shared(sW);
+	float acc[2][2][4];
+#pragma unroll
+	for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+		for (int j = 0; j < 2; j++)
+#pragma unroll
+			for (int q = 0; q < 4; q++) acc[mt][j][q] = 0.f;
+	for (int c0 = 0; c0 < Cin; c0 += CH) {
+		__syncthreads(); // the previous chunk's reads are done
+		// halo brick: TH_VOX voxels x CH/8 pieces of 16 bytes
+		for (int e = threadIdx.x; e < TH_VOX * (CH / 8); e += blockDim.x) {
+			const int piece = e % (CH / 8), hv = e / (CH / 8);
+			const int hx = hv % TH_X, hy = (hv / TH_X) % TH_Y, hz = hv / (TH_X * TH_Y);
+			const int X = x0 - 1 + hx, Y = y0 - 1 + hy, Z = z0 - 1 + hz;
+			uint4 val = make_uint4(0u, 0u, 0u, 0u);
+			if (X >= 0 && X < a.nx && Y >= 0 && Y < a.ny && Z >= 0 && Z < a.nz) {
+				const int c = c0 + piece * 8;
+				const bf16 *src;
+				if (c < a.Ca)
+					src = a.A + (((long long)(Z >> a.upA) * nyA + (Y >> a.upA)) * nxA + (X >> a.upA)) * a.Ca + c;
+				else
+					src = a.B + (((long long)Z * a.ny + Y) * a.nx + X) * a.Cb + (c - a.Ca);
+				val = __ldg(reinterpret_cast<const uint4 *>(src));
+			}
+			*reinterpret_cast<uint4 *>(sIn + halo_off<CH>(hv, piece)) = val;
+		}
+		// weights of the chunk: sW[(tap*16 + n) * ldw + k] = W[tap][slice*16 + n][c0 + k]
+		for (int e = threadIdx.x; e < 27 * 16 * (CH / 8); e += blockDim.x) {
+			const int piece = e % (CH / 8), row = e / (CH / 8);
+			const int tap = row / 16, n = row % 16;
+			const uint4 val =
+			    __ldg(reinterpret_cast<const uint4 *>(a.W + ((size_t)tap * a.Cout + slice * 16 + n) * Cin + c0 + piece * 8));
+			*reinterpret_cast<uint4 *>(sW + (size_t)row * ldw + piece * 8) = val;
+		}
+		__syncthreads();
+		// lane roles in ldmatrix.x4: matrix q = lane / 8, row r = lane % 8
+		const int q = lane >> 3, r = lane & 7;
+		for (int tap = 0; tap < 27; tap++) {
+			const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3; // halo offsets (0..2)
+			const int hrow = ((wz + dz) * TH_Y + (wy + dy)) * TH_X + dx;
+#pragma unroll
+			for (int kc = 0; kc < CH / 16; kc++) {
+				unsigned b0, b1, b2, b3;
+				{
+					const int n = r + 8 * (q >> 1), k = kc * 16 + 8 * (q & 1);
+					ldsm_x4(sW_s + (unsigned)(((tap * 16 + n) * ldw + k) * 2), b0, b1, b2, b3);
+				}
+#pragma unroll
+				for (int mt = 0; mt < 2; mt++) {
+					const int hv = hrow + mt * 16 + r + 8 * (q & 1);
+					unsigned af[4];
+					ldsm_x4(sIn_s + halo_off<CH>(hv, kc * 2 + (q >> 1)), af[0], af[1], af[2], af[3]);
+					mma_bf16(acc[mt][0], af, b0, b1);
+					mma_bf16(acc[mt][1], af, b2, b3);
+				}
+			}
+		}
+	}
+	// epilogue: rows g / g+8 of m-tile mt are x = 16 mt + g (+8)
+	const long long vrow = ((long long)(z0 + wz) * a.ny + (y0 + wy)) * a.nx + x0;
+#pragma unroll
+	for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+		for (int h = 0; h < 2; h++) {
+			const long long v = vrow + mt * 16 + g + 8 * h;
+#pragma unroll
+			for (int j = 0; j < 2; j++) {
+				const int co = slice * 16 + j * 8 + 2 * t4;
+				const float c0v = acc[mt][j][2 * h], c1v = acc[mt][j][2 * h + 1];
+				if (F32OUT)
+					*reinterpret_cast<float2 *>(static_cast<float *>(a.out) + v * a.Cout + co) = make_float2(c0v, c1v);
+				else
+					*reinterpret_cast<__nv_bfloat162 *>(static_cast<bf16 *>(a.out) + v * a.Cout + co) =
+					    __floats2bfloat162_rn(fmaxf(c0v, 0.f), fmaxf(c1v, 0.f));
+			}
+		}
+}
+
 // 2x2x2 mean, bf16 in / out (dims of the input).
 __global__ void k_pool(int nz, int ny, int nx, int C, const bf16 *in, bf16 *out) {
 	const int oz = nz / 2, oy = ny / 2, ox = nx / 2;
@@ -210,21 +335,69 @@ __global__ void k_head(long long n, const bf16 *d0, const float *w7, float *y) {
 	}
 }
 
-// z += |r| y, unless some y is not finite (then z keeps the plain ILU2 step).
-__global__ void k_check_finite(long long n, const float *y, int *flag) {
+// y as FP64
+__global__ void k_widen(long long n, const float *y, double *yd) {
 	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
-		if (!isfinite(y[v])) atomicExch(flag, 1);
+		yd[v] = (double)y[v];
 }
-__global__ void k_correct(long long n, const float *y, const double *nrm2, const int *flag, double *z) {
-	if (*flag) return;
-	const double s = sqrt(*nrm2);
+// z += alpha y with alpha = (r . y) / (y . A y) = s[0] / s[1], the step that
+// minimises the A-norm of the remaining error; a step that is not finite
+// and positive (a non-finite or useless network output) leaves z as the
+// plain ILU2 step.
+__global__ void k_correct(long long n, const double *yd, const double *s, double *z) {
+	const double alpha = s[0] / s[1];
+	if (!(alpha > 0.0) || !isfinite(alpha)) return;
 	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
-		z[v] += s * (double)y[v];
+		z[v] = fma(alpha, yd[v], z[v]);
 }
-__global__ void k_out(long long n, const float *y, const double *nrm2, double *out) {
-	const double s = sqrt(*nrm2);
-	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
-		out[v] = s * (double)y[v];
+
+// Deterministic sums of NQ products over a fixed grid: block partials, then
+// one ordered final pass.  Q = 2: r . yd, yd . ay.  Q = 3 (training): y . t,
+// y . y, t . t.
+#define RED_BLOCKS 256
+__global__ void k_red2(long long n, const double *r, const double *yd, const double *ay, double *part) {
+	__shared__ double sh[2][8];
+	double a = 0, b = 0;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		a = fma(r[v], yd[v], a);
+		b = fma(yd[v], ay[v], b);
+	}
+	a = warp_sum(a);
+	b = warp_sum(b);
+	if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = a; sh[1][threadIdx.x >> 5] = b; }
+	__syncthreads();
+	if (threadIdx.x < 2) {
+		double q = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) q += sh[threadIdx.x][w];
+		part[threadIdx.x * RED_BLOCKS + blockIdx.x] = q;
+	}
+}
+__global__ void k_red3(long long n, const float *y, const double *t, double *part) {
+	__shared__ double sh[3][8];
+	double a = 0, b = 0, c = 0;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		const double yv = (double)y[v];
+		a = fma(yv, t[v], a);
+		b = fma(yv, yv, b);
+		c = fma(t[v], t[v], c);
+	}
+	a = warp_sum(a);
+	b = warp_sum(b);
+	c = warp_sum(c);
+	if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = a; sh[1][threadIdx.x >> 5] = b; sh[2][threadIdx.x >> 5] = c; }
+	__syncthreads();
+	if (threadIdx.x < 3) {
+		double q = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) q += sh[threadIdx.x][w];
+		part[threadIdx.x * RED_BLOCKS + blockIdx.x] = q;
+	}
+}
+__global__ void k_red_final(int nq, const double *part, double *out) {
+	if (threadIdx.x < nq) {
+		double q = 0;
+		for (int b = 0; b < RED_BLOCKS; b++) q += part[threadIdx.x * RED_BLOCKS + b];
+		out[threadIdx.x] = q;
+	}
 }
 
 // r1 = v - t
@@ -264,6 +437,10 @@ __global__ void k_logdiag(int n, const int *iu, const double *al, double *ld) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 		ld[i] = log(fabs(al[iu[i]]) + 1e-300);
 }
+__global__ void k_logvec(int n, const double *d, double *ld) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		ld[i] = log(fabs(d[i]) + 1e-300);
+}
 __global__ void k_moments(int n, const double *ld, double *out) {
 	// one block: mean and standard deviation
 	__shared__ double s1[256], s2[256];
@@ -288,26 +465,16 @@ __global__ void k_logd_norm(int n, const double *ld, const double *mom, bf16 *ou
 
 // ---- training --------------------------------------------------------------
 
-// target t / |r|, loss |y - t'|^2 / |t'|^2 and dL/dy; s[0] = |r|^2, s[1] = |t|^2
-__global__ void k_loss(long long n, const float *y, const double *t, const double *s, float *gy, double *lpart) {
-	__shared__ double sh[8];
-	const double inv = s[0] > 0 ? 1.0 / sqrt(s[0]) : 0.0;
-	const double tt = s[1] * inv * inv;
-	const double sc = tt > 0 ? 1.0 / tt : 0.0;
-	double l = 0;
-	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
-		const double d = (double)y[v] - t[v] * inv;
-		gy[v] = (float)(2.0 * d * sc);
-		l = fma(d, d, l);
-	}
-	l = warp_sum(l);
-	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		double q = 0;
-		for (int w = 0; w < (int)(blockDim.x >> 5); w++) q += sh[w];
-		lpart[blockIdx.x] = q * sc;
-	}
+// Loss 1 - cos^2(y, t) (only the direction of y is trained; the step length
+// is chosen when the stage is applied) and its gradient in y; s = {y.t, y.y,
+// t.t}, the loss goes to s[3].
+__global__ void k_cos_grad(long long n, const float *y, const double *t, double *s, float *gy) {
+	const double a = s[0], b = s[1], c = s[2];
+	const bool ok = b > 0.0 && c > 0.0;
+	const double ct = ok ? -2.0 * a / (b * c) : 0.0, cy = ok ? 2.0 * a * a / (b * b * c) : 0.0;
+	if (blockIdx.x == 0 && threadIdx.x == 0) s[3] = ok ? 1.0 - a * a / (b * c) : 1.0;
+	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+		gy[v] = (float)(ct * t[v] + cy * (double)y[v]);
 }
 
 // dd0 = w7 * gy masked by d0 > 0 (bf16); dw7[c] += sum_v d0[v][c] gy[v]
@@ -475,8 +642,9 @@ struct bsg_unet {
 	// activations
 	bf16 *x0, *e0, *p1, *e1, *p2, *e2, *p3, *e3, *d2, *d1, *d0;
 	float *y, *gy;
-	double *r1, *t1, *sc, *part; // residual, SpMV scratch, scalars [0]=|r|^2 [1]=|t|^2, reduction partials
-	int *flag;
+	double *r1, *t1, *ay;       // residual after the ILU2 step, SpMV scratch, A y
+	double *sc;                 // scalars: [0] |r|^2, [4..7] reductions of the step / the loss
+	double *part;               // reduction partials (3 x RED_BLOCKS)
 	// training buffers
 	bf16 *dd0, *gd1, *gd2, *ge3, *ge2, *ge1, *ge0;
 	float *gi6, *gi5, *gi4, *gp3, *gp2, *gp1;
@@ -495,6 +663,15 @@ int dalloc(bsg_ctx *c, T **p, size_t n) {
 	return BSG_OK;
 }
 
+template <bool F32OUT, int CH>
+int conv_tiled(const ConvArgs &a, cudaStream_t s) {
+	const size_t smem = (size_t)TH_VOX * CH * 2 + (size_t)27 * 16 * (CH + 8) * 2;
+	BSG_CUDA(cudaFuncSetAttribute(k_conv3t<F32OUT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	dim3 grid((unsigned)((a.nx / TT_X) * (a.ny / TT_Y) * (a.nz / TT_Z)), a.Cout / 16);
+	k_conv3t<F32OUT, CH><<<grid, 256, smem, s>>>(a);
+	return BSG_OK;
+}
+
 int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16 *B, int Cb, const bf16 *W, int Cout,
                 void *out, bool f32out) {
 	cudaStream_t s = u->ctx->stream;
@@ -502,6 +679,17 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 	a.nz = u->nz >> lvl; a.ny = u->ny >> lvl; a.nx = u->nx >> lvl;
 	a.A = A; a.Ca = Ca; a.upA = upA; a.B = B; a.Cb = Cb; a.W = W; a.Cout = Cout; a.out = out;
 	const int Cin = Ca + Cb;
+	BSG_COUNT(1);
+	if (a.nx % TT_X == 0 && a.ny % TT_Y == 0 && a.nz % TT_Z == 0) {
+		int rc;
+		if (Cin % 32 == 0)
+			rc = f32out ? conv_tiled<true, 32>(a, s) : conv_tiled<false, 32>(a, s);
+		else
+			rc = f32out ? conv_tiled<true, 16>(a, s) : conv_tiled<false, 16>(a, s);
+		if (rc) return rc;
+		BSG_CUDA(cudaGetLastError());
+		return BSG_OK;
+	}
 	const size_t smem = (size_t)27 * 16 * (Cin + 8) * sizeof(bf16);
 	const long long ntile = (u->nv[lvl] + 16 * CONV_MT - 1) / (16 * CONV_MT);
 	long long bx = (ntile + 3) / 4;
@@ -509,7 +697,6 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 	if (bx > cap) bx = cap;
 	if (bx < 1) bx = 1;
 	dim3 grid((unsigned)bx, Cout / 16);
-	BSG_COUNT(1);
 	if (f32out) {
 		BSG_CUDA(cudaFuncSetAttribute(k_conv3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 		k_conv3<true><<<grid, 128, smem, s>>>(a);
@@ -675,7 +862,7 @@ extern "C" int bsg_unet_create(bsg_ctx *c, int nx, int ny, int nz, int train, bs
 	A(&u->p2, nv[2] * 32); A(&u->e2, nv[2] * 64); A(&u->p3, nv[3] * 64); A(&u->e3, nv[3] * 64);
 	A(&u->d2, nv[2] * 32); A(&u->d1, nv[1] * 16); A(&u->d0, nv[0] * 16);
 	A(&u->y, nv[0]); A(&u->gy, nv[0]);
-	A(&u->r1, nv[0]); A(&u->t1, nv[0]); A(&u->sc, 4); A(&u->part, SQ_BLOCKS); A(&u->flag, 1);
+	A(&u->r1, nv[0]); A(&u->t1, nv[0]); A(&u->ay, nv[0]); A(&u->sc, 8); A(&u->part, 3 * RED_BLOCKS);
 	if (u->train) {
 		A(&u->dd0, nv[0] * 16); A(&u->gd1, nv[1] * 16); A(&u->gd2, nv[2] * 32); A(&u->ge3, nv[3] * 64);
 		A(&u->ge2, nv[2] * 64); A(&u->ge1, nv[1] * 32); A(&u->ge0, nv[0] * 16);
@@ -698,7 +885,7 @@ extern "C" int bsg_unet_free(bsg_unet *u) {
 	if (!u) return BSG_OK;
 	void *ps[] = {u->master, u->adam_m, u->adam_v, u->grad, u->w7b, u->logd, u->ld, u->mom, u->x0, u->e0, u->p1,
 	              u->e1, u->p2, u->e2, u->p3, u->e3, u->d2, u->d1, u->d0, u->y, u->gy, u->r1, u->t1, u->sc, u->part,
-	              u->flag, u->dd0, u->gd1, u->gd2, u->ge3, u->ge2, u->ge1, u->ge0, u->gi6, u->gi5, u->gi4, u->gp3,
+	              u->ay, u->dd0, u->gd1, u->gd2, u->ge3, u->ge2, u->ge1, u->ge0, u->gi6, u->gi5, u->gi4, u->gp3,
 	              u->gp2, u->gp1};
 	cudaStreamSynchronize(u->ctx->stream);
 	for (void *p : ps)
@@ -751,36 +938,51 @@ extern "C" int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m) {
 	return BSG_OK;
 }
 
-// y_out = |r| N(r / |r|) (FP64), the network's correction for residual r.
+// The second input channel from a device vector of diagonal values (the
+// matrix's diagonal), without binding a matrix: training switches between
+// instances this way.
+extern "C" int bsg_unet_set_diag(bsg_unet *u, const double *d_diag) {
+	if (!u || !d_diag) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_diag: null argument");
+	cudaStream_t s = u->ctx->stream;
+	const int n = (int)u->nv[0];
+	BSG_COUNT(3);
+	k_logvec<<<ew(n), 256, 0, s>>>(n, d_diag, u->ld);
+	k_moments<<<1, 256, 0, s>>>(n, u->ld, u->mom);
+	k_logd_norm<<<ew(n), 256, 0, s>>>(n, u->ld, u->mom, u->logd);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// y_out = N(r / |r|) (FP64), the network's output direction for residual r.
 extern "C" int bsg_unet_forward_dev(bsg_unet *u, const double *r, double *y_out) {
 	if (!u || !r || !y_out) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_forward_dev: null argument");
 	int rc = sumsq(u, u->nv[0], r, u->sc);
 	if (!rc) rc = forward(u, r);
 	if (rc) return rc;
 	BSG_COUNT(1);
-	k_out<<<ew(u->nv[0]), 256, 0, u->ctx->stream>>>(u->nv[0], u->y, u->sc, y_out);
+	k_widen<<<ew(u->nv[0]), 256, 0, u->ctx->stream>>>(u->nv[0], u->y, y_out);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
 
 // One training sample: input residual r, target correction t (both FP64 on
-// the device).  Accumulates the weight gradients of |N(r/|r|) - t/|r||^2 /
-// |t/|r||^2; *loss (may be NULL) gets the sample's loss.
+// the device).  Accumulates the weight gradients of 1 - cos^2(N(r/|r|), t);
+// *loss (may be NULL) gets the sample's loss.
 extern "C" int bsg_unet_train_sample(bsg_unet *u, const double *r, const double *t, double *loss) {
 	if (!u || !r || !t) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_train_sample: null argument");
 	if (!u->train) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_train_sample: network created without training buffers");
 	cudaStream_t s = u->ctx->stream;
 	int rc = sumsq(u, u->nv[0], r, u->sc);
-	if (!rc) rc = sumsq(u, u->nv[0], t, u->sc + 1);
 	if (!rc) rc = forward(u, r);
 	if (rc) return rc;
-	BSG_COUNT(2);
-	k_loss<<<SQ_BLOCKS, 256, 0, s>>>(u->nv[0], u->y, t, u->sc, u->gy, u->part);
-	k_sum_final<<<1, 32, 0, s>>>(SQ_BLOCKS, u->part, u->sc + 2);
+	BSG_COUNT(3);
+	k_red3<<<RED_BLOCKS, 256, 0, s>>>(u->nv[0], u->y, t, u->part);
+	k_red_final<<<1, 32, 0, s>>>(3, u->part, u->sc + 4);
+	k_cos_grad<<<ew(u->nv[0]), 256, 0, s>>>(u->nv[0], u->y, t, u->sc + 4, u->gy);
 	if ((rc = backward(u))) return rc;
 	u->count++;
 	if (loss) {
-		BSG_CUDA(cudaMemcpyAsync(loss, u->sc + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+		BSG_CUDA(cudaMemcpyAsync(loss, u->sc + 7, sizeof(double), cudaMemcpyDeviceToHost, s));
 		BSG_CUDA(cudaStreamSynchronize(s));
 	}
 	return BSG_OK;
@@ -807,9 +1009,11 @@ extern "C" int bsg_unet_zero_grads(bsg_unet *u) {
 }
 
 // FGMRES learned stage: z holds the ILU2 step M^{-1} v on entry; the
-// network corrects it with its estimate of the remaining error from the
-// residual r1 = v - A z.  A non-finite network output leaves z as it is
-// (the plain ILU2 step).  `work` is unused (own buffers).
+// network's direction y = N(r1/|r1|) for the remaining error, r1 = v - A z,
+// is added with the step alpha = (r1 . y) / (y . A y) that minimises the
+// A-norm of that error.  A step that is not finite and positive leaves z as
+// the plain ILU2 step.  `work` is unused (own buffers).  All on the device
+// stream, no host synchronisation.
 int bsg_unet_apply(void *net, bsg_ctx *c, const double *v, double *z, double *work) {
 	(void)work;
 	bsg_unet *u = static_cast<bsg_unet *>(net);
@@ -823,10 +1027,13 @@ int bsg_unet_apply(void *net, bsg_ctx *c, const double *v, double *z, double *wo
 	k_sub<<<ew(n), 256, 0, s>>>(n, v, u->t1, u->r1);
 	if ((rc = sumsq(u, n, u->r1, u->sc))) return rc;
 	if ((rc = forward(u, u->r1))) return rc;
-	BSG_CUDA(cudaMemsetAsync(u->flag, 0, sizeof(int), s));
-	BSG_COUNT(2);
-	k_check_finite<<<ew(n), 256, 0, s>>>(n, u->y, u->flag);
-	k_correct<<<ew(n), 256, 0, s>>>(n, u->y, u->sc, u->flag, z);
+	BSG_COUNT(1);
+	k_widen<<<ew(n), 256, 0, s>>>(n, u->y, u->t1);
+	if ((rc = bsg_spmm_launch(u->mat, 1, u->t1, u->ay, n, s))) return bsg_set_error(rc, "learned stage: SpMV failed");
+	BSG_COUNT(3);
+	k_red2<<<RED_BLOCKS, 256, 0, s>>>(n, u->r1, u->t1, u->ay, u->part);
+	k_red_final<<<1, 32, 0, s>>>(2, u->part, u->sc + 4);
+	k_correct<<<ew(n), 256, 0, s>>>(n, u->t1, u->sc + 4, z);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }

@@ -190,6 +190,8 @@ int bsg_unet_get_weights(bsg_unet *u, float *w);
 int bsg_unet_get_grads(bsg_unet *u, float *g);           /* accumulated sums */
 /* the operator: its diagonal is the second input channel; FGMRES forms r1 with it */
 int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m);
+/* the second input channel from a device vector of diagonal values only */
+int bsg_unet_set_diag(bsg_unet *u, const double *d_diag);
 /* d_y = |r| N(r / |r|), device FP64 vectors of the grid's length */
 int bsg_unet_forward_dev(bsg_unet *u, const double *d_r, double *d_y);
 /* one training sample (device r and target t); accumulates weight gradients

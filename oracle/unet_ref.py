@@ -17,12 +17,13 @@ Network (channels-last tensors [z, y, x, c]; R0 = the grid, Rl = R0 / 2^l):
     d1 = relu(conv(cat(up(d2), e1); W5:  64 -> 16))           R1
     d0 = relu(conv(cat(up(d1), e0); W6:  32 -> 16))           R0
     y  = sum_c w7[c] d0[c]                                    R0
-    correction = |r| * y
+    correction = alpha * y,  alpha = (r . y) / (y . A y)      (energy-optimal)
 
 conv: 3x3x3, zero padding, no bias, W[tap][cout][cin] with tap = 9 (dz+1) +
 3 (dy+1) + (dx+1); pool: 2x2x2 mean; up: nearest (parent = coordinate // 2).
-Without biases the network is positively homogeneous, so scaling r scales
-the correction.  The GPU stores activations in bfloat16 (round to nearest
+Training minimises 1 - cos^2(y, e) against the error e the ILU2 step left,
+so only the direction of y is learned; the step length is the minimiser of
+the A-norm of the remaining error.  The GPU stores activations in bfloat16 (round to nearest
 even) after each relu / pool and accumulates in float32; `forward(...,
 rounded=True)` reproduces those rounding points (accumulating in float64).
 """
@@ -142,10 +143,15 @@ def forward(x0, W, rounded=True):
 
 
 def loss(y, t):
-    """Relative squared error |y - t|^2 / |t|^2 and its gradient in y."""
-    tt = float(np.sum(t * t))
-    d = y - t
-    return float(np.sum(d * d)) / tt, 2.0 * d / tt
+    """Scale-free loss 1 - cos^2(y, t) and its gradient in y: the step length
+    of the correction is chosen at apply time, so only the direction of the
+    network output is trained."""
+    a = float(np.sum(y * t))
+    b = float(np.sum(y * y))
+    c = float(np.sum(t * t))
+    if b <= 0.0 or c <= 0.0:
+        return 1.0, np.zeros_like(y)
+    return 1.0 - a * a / (b * c), -2.0 * a / (b * c) * t + 2.0 * a * a / (b * b * c) * y
 
 
 def backward(A, W, gy):
