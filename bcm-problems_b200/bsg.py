@@ -340,14 +340,16 @@ class UNet:
             pass
 
 
-FACT_STAT_NAMES = ("tries", "parks", "cyc_pop", "cyc_close", "cyc_blocked", "cyc_pref", "cyc_upd", "cyc_fin",
-                   "members", "mask", "rounds", "cyc_pf", "cyc_pa", "cyc_pb", "big_rows", "warps")
+FACT_STAT_NAMES = ("tries", "parks", "cyc_pop", "cyc_close", "cyc_blocked", "cyc_tail", "cyc_upd", "cyc_fin",
+                   "members", "mask", "rounds", "cyc_pf", "cyc_pa", "cyc_pb", "big_rows", "warps",
+                   "cyc_pass_load", "cyc_pass_close", "cyc_to_publish", "cyc_post_publish", "batches", "closed",
+                   "unused22", "unused23")
 
 
 def fact_stats():
     """Scheduler counters of the last factorisation in this process."""
-    out = (C.c_ulonglong * 16)()
-    _check(lib().bsg_fact_stats(out, 16))
+    out = (C.c_ulonglong * 24)()
+    _check(lib().bsg_fact_stats(out, 24))
     return dict(zip(FACT_STAT_NAMES, list(out)))
 
 

@@ -556,10 +556,6 @@ extern "C" int bsg_solve_u_dev(bsg_ctx *c, const bsg_fct *f, int mode, int nswee
 	return rc;
 }
 
-// ---- learned stage hook (implemented in unet.cu) ---------------------------
-__attribute__((weak)) int bsg_unet_apply(void *, bsg_ctx *, const double *, double *, double *) {
-	return bsg_set_error(BSG_ERR_UNSUPPORTED, "learned preconditioner not built");
-}
 
 // ---- host-buffer drivers ----------------------------------------------------
 

@@ -14,15 +14,19 @@
 // between m and i", and a member that does not store i has dropped it.
 //
 // Schedule (dynamic, deadlock-free).  A row enters a global FIFO queue when
-// all rows of A's column i are finished (a counter per row, decremented by
-// each finishing row).  A warp pops a row and tries it: it builds C(i) over
-// finished rows (one member per lane, rows read with 16-byte loads); if it
-// meets an unfinished member m it parks the row on m's waiter list and moves
-// on; m re-queues its waiters when it finishes.  The smallest unfinished row
-// always has all its dependencies finished and is queued or being tried, so
-// the factorisation always progresses, and the queue order follows the
+// every row of A's column i has been claimed by a warp (a counter per row,
+// decremented when such a row is first claimed).  A warp pops a row and tries it: it builds C(i) over
+// finished rows (one member per lane, rows read with 16-byte loads).  An
+// unfinished member m that another warp is computing is waited for; a member
+// nobody is computing parks the row on m's waiter list and the warp moves on;
+// m re-queues its waiters when it finishes.  Waits only go from a row to a
+// smaller row that a running warp holds, so every chain of waits ends at a
+// warp that is computing; the smallest unfinished row always has all its
+// dependencies finished and is queued or being computed, so the
+// factorisation always progresses, and the queue order follows the
 // dependency levels, so the GPU works on a whole wavefront of rows at once.
-// Every spin (an empty queue slot) is bounded by globaltimer.
+// Every spin (an empty queue slot, a member being computed) is bounded by
+// globaltimer.
 //
 // Storage.  A finished row keeps only its stored part: the diagonal (inverse
 // pivot) and the U / R entries sorted by column, in a pool, published by one
@@ -31,10 +35,11 @@
 // fixed-point accumulator (scale set by tau2 * theta, bsg_comp_scale), whose
 // integer sum does not depend on the order of the pushes.
 //
-// Arithmetic order (deterministic, identical to oracle/bsl_oracle.c):
-// diagonal = scaled a_ii + (fixed-point sum of compensations received);
-// then the updates of ascending contributors, each as fma(-l, g, f); then the
-// row's own theta compensations in ascending column order.  The result does
+// Arithmetic order (deterministic, identical to oracle/bsl_oracle.c): the
+// scaled row, then the updates of ascending contributors, each as
+// fma(-l, g, f); then the diagonal gets the fixed-point sum of the
+// compensations received; then the row's own theta compensations in
+// ascending column order.  The result does
 // not depend on the schedule.  (The reference sums in its linked-list order
 // instead; that changes results only at rounding level.)
 //
@@ -52,11 +57,12 @@
 #define CF_FLAG(x) ((x) >> 30)
 
 #define FACT_WARPS 4
-#define CMAX 256   // members of C(i)
-#define HCAP 512   // distinct mask columns per row (power of two)
-#define PFCAP 1024 // prefetched contributor entries per row
-// capacities of the global-memory workspace that takes the rows that do not
-// fit the shared one (about 0.7 MB per warp)
+#define CMAX 128   // members of C(i)
+#define HCAP 256   // distinct mask columns per row (power of two)
+#define PFCAP 512  // prefetched contributor entries per row
+// capacities of the global-memory workspaces that take the rows that do not
+// fit the shared one (about 0.7 MB each), and how many there are
+#define BIG_SLOTS 64
 #define CMAX_BIG 8192
 #define HCAP_BIG 8192
 #define PFCAP_BIG 8192
@@ -86,18 +92,21 @@ struct FactArgs {
 	double acc_scale, acc_inv_scale;
 	int *lev;
 	int *nstat, *whead, *wnext;
+	int *inprog;                 // 1 while a warp is computing the row
 	int *queue;
 	long long qcap;
 	unsigned long long *qhead, *qtail;
 	int *done_count;
 	bsg_devstat *st;
 	unsigned long long *stats; // FACT_NSTAT counters (see bsg_fact_stats)
-	unsigned char *big_ws;     // GlobWS::bytes per warp of the launch
+	unsigned char *big_ws;     // BIG_SLOTS workspaces of GlobWS::bytes
+	int *big_owner;            // 1 while a warp holds that workspace
 };
 
 // Scheduler / phase counters summed over all warps of the last factorisation.
-enum { FS_TRY = 0, FS_PARK, FS_CYC_POP, FS_CYC_CLOSE, FS_CYC_BLOCKED, FS_CYC_PREF, FS_CYC_UPD, FS_CYC_FIN,
-       FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FS_BIG, FACT_NSTAT = 16 };
+enum { FS_TRY = 0, FS_PARK, FS_CYC_POP, FS_CYC_CLOSE, FS_CYC_BLOCKED, FS_CYC_TAIL, FS_CYC_UPD, FS_CYC_FIN,
+       FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FS_BIG, FS_WARPS,
+       FS_CYC_PLOAD, FS_CYC_PCLOSE, FS_CYC_TOPUB, FS_CYC_POSTPUB, FS_BATCHES, FS_CLOSED, FACT_NSTAT = 24 };
 struct PhaseClock {
 	unsigned long long v[FACT_NSTAT];
 };
@@ -117,11 +126,13 @@ struct SmemWS {
 	int Ws[CMAX], Wps[CMAX], Wes[CMAX];
 	unsigned char Wfs[CMAX];
 	int Wb[CMAX + 1];      // prefetch segment bases (sorted order)
+	unsigned char Wst[CMAX]; // member state: 0 not closed, 1 closed, 2 applied
 	int wset[CMAX * 2];    // membership hash of W (keys)
 	int hkey[HCAP];        // column accumulator
 	double hl[HCAP], hu[HCAP];
 	int lst[HCAP];         // extracted slots, then sorted
 	int lsts[HCAP];
+	int lkey[HCAP];        // columns of the extracted slots
 	unsigned pf_cf[PFCAP]; // prefetched contributor segments
 	short pf_slot[PFCAP];
 	double pf_l[PFCAP], pf_u[PFCAP];
@@ -133,24 +144,24 @@ struct GlobWS {
 	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG;
 	static constexpr size_t bytes = 8 * (2 * (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
 	                                4 * (6 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
-	                                     3 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
-	                                2 * (size_t)PFCAP_BIG + 2 * (size_t)CMAX_BIG;
+	                                     4 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
+	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG;
 	double *hl, *hu, *pf_l, *pf_u;
-	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wb, *wset, *hkey, *lst, *lsts, *sc;
+	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wb, *wset, *hkey, *lst, *lsts, *lkey, *sc;
 	unsigned *pf_cf;
 	short *pf_slot;
-	unsigned char *Wf, *Wfs;
+	unsigned char *Wf, *Wfs, *Wst;
 	__device__ explicit GlobWS(unsigned char *p) {
 		hl = reinterpret_cast<double *>(p); hu = hl + HCAP_BIG;
 		pf_l = hu + HCAP_BIG; pf_u = pf_l + PFCAP_BIG;
 		W = reinterpret_cast<int *>(pf_u + PFCAP_BIG);
 		Wp = W + CMAX_BIG; We = Wp + CMAX_BIG; Ws = We + CMAX_BIG; Wps = Ws + CMAX_BIG; Wes = Wps + CMAX_BIG;
 		Wb = Wes + CMAX_BIG; wset = Wb + CMAX_BIG + 4;
-		hkey = wset + 2 * CMAX_BIG; lst = hkey + HCAP_BIG; lsts = lst + HCAP_BIG;
-		pf_cf = reinterpret_cast<unsigned *>(lsts + HCAP_BIG);
+		hkey = wset + 2 * CMAX_BIG; lst = hkey + HCAP_BIG; lsts = lst + HCAP_BIG; lkey = lsts + HCAP_BIG;
+		pf_cf = reinterpret_cast<unsigned *>(lkey + HCAP_BIG);
 		sc = reinterpret_cast<int *>(pf_cf + PFCAP_BIG);
 		pf_slot = reinterpret_cast<short *>(sc + 4);
-		Wf = reinterpret_cast<unsigned char *>(pf_slot + PFCAP_BIG); Wfs = Wf + CMAX_BIG;
+		Wf = reinterpret_cast<unsigned char *>(pf_slot + PFCAP_BIG); Wfs = Wf + CMAX_BIG; Wst = Wfs + CMAX_BIG;
 	}
 };
 
@@ -207,34 +218,74 @@ __device__ double acc_value(const unsigned long long *acc, int j, double inv_sca
 	return __dmul_rn((double)__ldcg(acc + j), inv_scale);
 }
 
+// The queue is a ring of qcap slots (a power of two, at least twice the
+// rows): a row is in the queue at most once at a time (queued on admission,
+// or re-queued once per park), so a slot is free again long before its
+// ticket comes round; -1 marks a free slot.
 __device__ void q_push(const FactArgs &A, int row) {
-	unsigned long long t = atomicAdd(A.qtail, 1ull);
-	if ((long long)t >= A.qcap) {
-		devstat_fail(A.st, BSG_ERR_WORKSPACE, row, 1);
-		return;
+	const unsigned long long t = atomicAdd(A.qtail, 1ull);
+	int *slot = A.queue + (t & (unsigned long long)(A.qcap - 1));
+	const unsigned long long t0 = globaltimer_ns();
+	for (unsigned it = 0; atomicCAS(slot, -1, row) != -1; it++) {
+		__nanosleep(64);
+		if ((it & 31) == 31 && globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) {
+			devstat_fail(A.st, BSG_ERR_WORKSPACE, row, 1);
+			return;
+		}
 	}
-	atomicExch(A.queue + t, row);
 }
 
 // Pop the next queued row; -1 when the factorisation is finished or failed.
 __device__ int q_pop(const FactArgs &A) {
-	unsigned long long h = atomicAdd(A.qhead, 1ull);
-	if ((long long)h >= A.qcap) return -1;
-	int v = *(volatile int *)(A.queue + h);
+	const unsigned long long h = atomicAdd(A.qhead, 1ull);
+	int *slot = A.queue + (h & (unsigned long long)(A.qcap - 1));
+	int v = atomicExch(slot, -1);
 	if (v >= 0) return v;
 	unsigned long long t0 = globaltimer_ns();
 	for (unsigned it = 1;; it++) {
 		__nanosleep(64);
-		v = *(volatile int *)(A.queue + h);
-		if (v >= 0) return v;
+		if (*(volatile int *)slot >= 0) {
+			v = atomicExch(slot, -1);
+			if (v >= 0) return v;
+		}
 		if ((it & 31) == 0) {
 			if (*(volatile int *)A.done_count >= A.n) return -1;
 			if (*(volatile int *)&A.st->code != 0) return -1;
 			if (globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) {
-				devstat_fail(A.st, BSG_ERR_TIMEOUT, (int)h);
+				devstat_fail(A.st, BSG_ERR_TIMEOUT, (int)(h & 0x7fffffff));
 				return -1;
 			}
 		}
+	}
+}
+
+// Admission.  nstat[j] packs the static contributors of row j (the rows k
+// < j with A(k,j) != 0) that are unfinished (bits 0..14) and unclaimed (bits
+// 15..29); bit 31 marks j claimed once.  Row j enters the queue when all of
+// them are claimed and at most one is unfinished: it then starts while its
+// last predecessor is being computed and waits for it.  Both counts only
+// fall, so exactly one decrement makes the condition true, and that one
+// queues the row.
+#define ADM_ONE_FIN 1u
+#define ADM_ONE_CLAIM (1u << 15)
+#define ADM_CLAIMED (1u << 31)
+__device__ __forceinline__ bool admissible(unsigned v) { return ((v >> 15) & 0x7fffu) == 0 && (v & 0x7fffu) <= 1; }
+__device__ void admit_step(const FactArgs &A, int j, unsigned delta) {
+	const unsigned old = atomicSub(reinterpret_cast<unsigned *>(A.nstat) + j, delta);
+	if (!admissible(old) && admissible(old - delta)) q_push(A, j);
+}
+
+// Wait (lane 0) for row m while a warp is computing it: 1 once m is
+// finished, 0 when nobody is computing m (the caller parks), -1 on the
+// spin limit or another warp's failure.
+__device__ int wait_row(const FactArgs &A, int m) {
+	const unsigned long long t0 = globaltimer_ns();
+	for (unsigned it = 0;; it++) {
+		if (ld_acquire_u64(A.rec + m) & REC_DONE) return 1;
+		if (*(volatile int *)(A.inprog + m) == 0) return (ld_acquire_u64(A.rec + m) & REC_DONE) ? 1 : 0;
+		if (*(volatile int *)&A.st->code != 0) return -1;
+		__nanosleep(32);
+		if ((it & 63) == 63 && globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) return -1;
 	}
 }
 
@@ -249,228 +300,180 @@ __device__ void park(const FactArgs &A, int i, int m) {
 	}
 }
 
-// Examine member m of C(i) (one lane): classify it and add its candidates.
-// Returns 0, or a BSG_ERR_* code.
+// One closure pass, warp-cooperative: every unclosed member that is finished
+// gets closed.  The rows of those members are flattened into 16-byte chunks
+// spread over the lanes: a first sweep finds column i in each row (its pool
+// index and flag, or none: the member dropped i), a second inserts the
+// stored columns between the member and i (R x R skipped) into the member
+// set, new members taking slots by ballot.  Returns the number closed; the
+// smallest member still unfinished goes to *pmin.
 template <class WS>
-__device__ int close_member(const FactArgs &A, WS &s, int i, int t, int m, unsigned long long rec,
-                           int &levmax) {
-	const long long off = REC_OFF(rec);
-	const int len = REC_LEN(rec);
-	const uint4 *row4 = reinterpret_cast<const uint4 *>(A.pool_cf + off);
-	// pass 1: find column i among the stored entries 1..len-1 (sorted); the
-	// first 32 entries stay in registers for pass 2
-	uint4 v0[8];
-#pragma unroll
-	for (int r = 0; r < 8; r++) {
-		v0[r] = make_uint4(0x3fffffffu, 0x3fffffffu, 0x3fffffffu, 0x3fffffffu);
-		if (4 * r < len) v0[r] = __ldcg(row4 + r);
-	}
-	int pos = -1;
-	unsigned fi = 0;
-	bool past = false;
-#pragma unroll
-	for (int r = 0; r < 8; r++) {
-		unsigned e4[4] = {v0[r].x, v0[r].y, v0[r].z, v0[r].w};
-#pragma unroll
-		for (int c4 = 0; c4 < 4; c4++) {
-			const int e = 4 * r + c4;
-			if (e < 1 || e >= len || past || pos >= 0) continue;
-			const int c = CF_COL(e4[c4]);
-			if (c == i) { pos = e; fi = CF_FLAG(e4[c4]); }
-			else if (c > i) past = true;
+__device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax, int &pmin, int &err) {
+	const int nW = min(s.sc[0], s.cmax);
+	const unsigned lt = (1u << lane) - 1;
+	int pm = 0x7fffffff;
+	if (lane == 0) s.sc[2] = 0;
+	__syncwarp();
+	// finished unclosed members: W index, pool offset, length (scratch in Ws/Wps/Wes)
+	for (int base = 0; base < nW; base += 32) {
+		const int t = base + lane;
+		int m = -1;
+		unsigned long long rec = 0;
+		if (t < nW && s.Wst[t] == 0) {
+			m = s.W[t];
+			rec = ld_acquire_u64(A.rec + m);
 		}
-	}
-	for (int q0 = 8; pos < 0 && !past && 4 * q0 < len; q0 += 8) {
-		uint4 v[8];
-#pragma unroll
-		for (int r = 0; r < 8; r++) {
-			v[r] = make_uint4(0x3fffffffu, 0x3fffffffu, 0x3fffffffu, 0x3fffffffu);
-			if (4 * (q0 + r) < len) v[r] = __ldcg(row4 + q0 + r);
+		const bool done = m >= 0 && (rec & REC_DONE);
+		if (m >= 0 && !done) pm = min(pm, m);
+		const unsigned b = __ballot_sync(0xffffffffu, done);
+		const int q0 = s.sc[2];
+		if (done) {
+			const int q = q0 + __popc(b & lt);
+			s.Ws[q] = t;
+			s.Wps[q] = (int)REC_OFF(rec);
+			s.Wes[q] = REC_LEN(rec);
+			s.Wf[t] = (unsigned char)F_D; // until column i is found
 		}
+		__syncwarp();
+		if (lane == 0) s.sc[2] = q0 + __popc(b);
+		__syncwarp();
+	}
+	pmin = __reduce_min_sync(0xffffffffu, pm);
+	const int nd = s.sc[2];
+	if (nd == 0) return 0;
+	// chunk bases of the flattened rows
+	if (lane == 0) {
+		int acc = 0;
+		for (int d = 0; d < nd; d++) {
+			s.Wb[d] = acc;
+			acc += (s.Wes[d] + 3) >> 2;
+		}
+		s.Wb[nd] = acc;
+	}
+	__syncwarp();
+	const int T = s.Wb[nd];
+	// sweep 1: column i in each row
+	for (int k0 = 0; k0 < T; k0 += 32) {
+		const int k = k0 + lane;
+		if (k < T) {
+			int lo = 0, hi = nd - 1;
+			while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= k) lo = mid; else hi = mid - 1; }
+			const int ch = k - s.Wb[lo], len = s.Wes[lo];
+			const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
+			const unsigned e4[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-		for (int r = 0; r < 8; r++) {
-			unsigned e4[4] = {v[r].x, v[r].y, v[r].z, v[r].w};
-#pragma unroll
-			for (int c4 = 0; c4 < 4; c4++) {
-				const int e = 4 * (q0 + r) + c4;
-				if (e >= len || past || pos >= 0) continue;
-				const int c = CF_COL(e4[c4]);
-				if (c == i) { pos = e; fi = CF_FLAG(e4[c4]); }
-				else if (c > i) past = true;
+			for (int c = 0; c < 4; c++) {
+				const int e = 4 * ch + c;
+				if (e >= 1 && e < len && CF_COL(e4[c]) == i) {
+					const int t = s.Ws[lo];
+					s.Wp[t] = s.Wps[lo] + e;
+					s.Wf[t] = (unsigned char)CF_FLAG(e4[c]);
+				}
 			}
 		}
 	}
-	if (pos < 0) { // m dropped column i: compensation only, no expansion
-		s.Wf[t] = (unsigned char)F_D;
-		return 0;
-	}
-	s.Wp[t] = (int)(off + pos);
-	s.We[t] = (int)(off + len);
-	s.Wf[t] = (unsigned char)fi;
-	if (fi == F_U) levmax = max(levmax, __ldcg(A.lev + m) + 1);
-	// pass 2: the stored columns of m between m and i are members, except
-	// R entries when i is R too (R x R skip)
-	int err = 0;
+	__syncwarp();
+	// sweep 2: the stored columns between the member and i become members
+	for (int k0 = 0; k0 < T && !err; k0 += 32) {
+		const int k = k0 + lane;
+		unsigned e4[4] = {0u, 0u, 0u, 0u};
+		int pos = 0, ch = 0;
+		unsigned fi = F_D;
+		if (k < T) {
+			int lo = 0, hi = nd - 1;
+			while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= k) lo = mid; else hi = mid - 1; }
+			ch = k - s.Wb[lo];
+			const int t = s.Ws[lo];
+			fi = s.Wf[t];
+			if (fi != F_D) {
+				pos = s.Wp[t] - s.Wps[lo];
+				if (4 * ch < pos) {
+					const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
+					e4[0] = v.x; e4[1] = v.y; e4[2] = v.z; e4[3] = v.w;
+				}
+			}
+		}
 #pragma unroll
-	for (int r = 0; r < 8; r++) {
-		unsigned e4[4] = {v0[r].x, v0[r].y, v0[r].z, v0[r].w};
-#pragma unroll
-		for (int c4 = 0; c4 < 4; c4++) {
-			const int e = 4 * r + c4;
-			if (e < 1 || e >= pos || err) continue;
-			if (fi == F_R && CF_FLAG(e4[c4]) == F_R) continue;
-			const int c = CF_COL(e4[c4]);
-			const int isnew = wset_insert(s, c);
-			if (isnew < 0) { err = BSG_ERR_WORKSPACE; continue; }
+		for (int c = 0; c < 4; c++) {
+			const int e = 4 * ch + c;
+			const bool cand = e >= 1 && e < pos && !(fi == F_R && CF_FLAG(e4[c]) == F_R);
+			int isnew = 0;
+			if (cand) {
+				isnew = wset_insert(s, CF_COL(e4[c]));
+				if (isnew < 0) err = BSG_ERR_WORKSPACE;
+			}
+			const unsigned b = __ballot_sync(0xffffffffu, isnew == 1);
+			const int q0 = s.sc[0];
 			if (isnew == 1) {
-				int slot = atomicAdd(&s.sc[0], 1);
-				if (slot < s.cmax) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
-			}
-		}
-	}
-	for (int e = 32; e < pos && !err; e++) {
-		const unsigned cf = __ldcg(A.pool_cf + off + e);
-		if (fi == F_R && CF_FLAG(cf) == F_R) continue;
-		const int c = CF_COL(cf);
-		const int isnew = wset_insert(s, c);
-		if (isnew < 0) { err = BSG_ERR_WORKSPACE; continue; }
-		if (isnew == 1) {
-			int slot = atomicAdd(&s.sc[0], 1);
-			if (slot < s.cmax) s.W[slot] = c; else err = BSG_ERR_WORKSPACE;
-		}
-	}
-	return err;
-}
-
-// Factor row i.  Returns -1 when done, the unfinished row it waits for
-// (>= 0), -2 on error (reported through the status word), or -3 when the
-// row does not fit a shared-memory workspace (nothing was published yet, so
-// the caller retries it in the global one).
-template <class WS>
-__device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc) {
-	const bool ilu = A.kind == 1;
-	const long long c0 = clock64();
-	for (int t = lane; t < 2 * s.cmax; t += 32) s.wset[t] = -1;
-	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
-	if (lane == 0) { s.sc[3] = -1; s.sc[0] = 0; }
-	__syncwarp();
-
-	// ---- seed with A's column i (all finished: the row was queued)
-	const int tb = A.it[i], te = A.it[i + 1];
-	if (te - tb > s.cmax) {
-		if (!WS::big) return -3;
-		if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 2);
-		return -2;
-	}
-	for (int t = tb + lane; t < te; t += 32) {
-		int k = A.jt[t];
-		s.W[t - tb] = k;
-		wset_insert(s, k);
-	}
-	if (lane == 0) s.sc[0] = te - tb;
-	__syncwarp();
-
-	// ---- close C(i): rounds over the newest members, one member per lane
-	int err = 0, levmax = 0;
-	for (int lo = 0; lo < s.sc[0] && !err;) {
-		pc.v[FS_ROUNDS]++;
-		const int hi = min(s.sc[0], s.cmax);
-		for (int base = lo; base < hi; base += 32) {
-			const int t = base + lane;
-			int m = -1;
-			unsigned long long rec = 0;
-			if (t < hi) {
-				m = s.W[t];
-				rec = ld_acquire_u64(A.rec + m);
-				if (!(rec & REC_DONE)) { atomicCAS(&s.sc[3], -1, m); m = -1; }
+				const int slot = q0 + __popc(b & lt);
+				if (slot < s.cmax) { s.W[slot] = CF_COL(e4[c]); s.Wst[slot] = 0; } else err = BSG_ERR_WORKSPACE;
 			}
 			__syncwarp();
-			if (s.sc[3] >= 0) {
-				pc.v[FS_CYC_BLOCKED] += clock64() - c0;
-				return s.sc[3];
-			}
-			if (m >= 0) {
-				int e2 = close_member(A, s, i, t, m, rec, levmax);
-				if (e2) err = e2;
-			}
+			if (lane == 0) s.sc[0] = q0 + __popc(b);
 			__syncwarp();
 		}
 		err = __reduce_min_sync(0xffffffffu, err);
-		lo = hi;
-		__syncwarp();
 	}
-	if (err) {
-		if (!WS::big) return -3;
-		if (lane == 0) devstat_fail(A.st, err, i, 3);
-		return -2;
-	}
-	levmax = __reduce_max_sync(0xffffffffu, levmax);
-	const int nW = s.sc[0];
-	const long long c1 = clock64();
-	pc.v[FS_CYC_CLOSE] += c1 - c0;
-	pc.v[FS_CONTRIB] += nW;
-
-	// ---- sort members ascending (rank sort; rows are distinct)
-	for (int t = lane; t < nW; t += 32) {
-		int k = s.W[t], r = 0;
-		for (int u = 0; u < nW; u++) r += s.W[u] < k;
-		s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
+	// closed: pool end, state, forward-solve depth through U members
+	for (int d = lane; d < nd; d += 32) {
+		const int t = s.Ws[d];
+		s.We[t] = s.Wps[d] + s.Wes[d];
+		s.Wst[t] = 1;
+		if (s.Wf[t] == F_U) levmax = max(levmax, __ldcg(A.lev + s.W[t]) + 1);
 	}
 	__syncwarp();
+	return nd;
+}
 
-	// ---- segment bases: stored member t contributes its entries [pos, end)
+// Apply the updates of the closed members below `bound` (all members below
+// it are known by then) in ascending order, in groups of consecutive members
+// whose segments fit the prefetch buffer; marks them applied.  Returns 0, or
+// a BSG_ERR_* code (uniform over the warp).
+template <class WS>
+__device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, PhaseClock &pc) {
+	const bool ilu = A.kind == 1;
+	const int nW = min(s.sc[0], s.cmax);
+	// compact the selected members (closed, below the bound) in index order
+	if (lane == 0) s.sc[2] = 0;
+	__syncwarp();
+	for (int base = 0; base < nW; base += 32) {
+		const int t = base + lane;
+		const bool sel = t < nW && s.Wst[t] == 1 && s.W[t] < bound;
+		const unsigned b = __ballot_sync(0xffffffffu, sel);
+		const int pos0 = s.sc[2];
+		if (sel) s.lsts[pos0 + __popc(b & ((1u << lane) - 1))] = t;
+		__syncwarp();
+		if (lane == 0) s.sc[2] = pos0 + __popc(b);
+		__syncwarp();
+	}
+	const int nb = s.sc[2];
+	if (nb == 0) return 0;
+	pc.v[FS_BATCHES]++;
+	pc.v[FS_CLOSED] += nb;
+	// rank sort by row index (rows are distinct); mark applied
+	for (int q = lane; q < nb; q += 32) {
+		const int t = s.lsts[q], k = s.W[t];
+		int r = 0;
+		for (int u = 0; u < nb; u++) r += s.W[s.lsts[u]] < k;
+		s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
+		s.Wst[t] = 2;
+	}
+	__syncwarp();
+	// segment bases: stored member t contributes its entries [pos, end)
 	if (lane == 0) {
 		int b = 0;
-		for (int t = 0; t < nW; t++) {
+		for (int t = 0; t < nb; t++) {
 			s.Wb[t] = b;
 			if (s.Wfs[t] != F_D) b += s.Wes[t] - s.Wps[t];
 		}
-		s.Wb[nW] = b;
-	}
-	const double comp = acc_value(A.acc, i, A.acc_inv_scale);
-	__syncwarp();
-	const long long c2 = clock64();
-	pc.v[FS_CYC_PREF] += c2 - c1;
-
-	// ---- init the scaled row (Ich2InitRow / Ilu2InitRow); the diagonal gets
-	//      the compensations of the rows that dropped column i
-	const int ab = A.iu[i], ae = A.iu[i + 1];
-	if (lane == 0) {
-		int slot = hfind_insert(s, i);
-		const double d = __dadd_rn(A.diag0[i], comp);
-		s.hl[slot] = d;
-		s.hu[slot] = d;
+		s.Wb[nb] = b;
 	}
 	__syncwarp();
-	{
-		const double si_l = A.scll[i], si_u = A.sclu[i];
-		for (int k = ab + 1 + lane; k < ae; k += 32) {
-			int j = A.ju[k];
-			int sl = hfind_insert(s, j);
-			if (sl < 0) { err = BSG_ERR_WORKSPACE; continue; }
-			if (ilu) {
-				s.hl[sl] = __dmul_rn(__dmul_rn(A.al[k], si_u), A.scll[j]);
-				s.hu[sl] = __dmul_rn(__dmul_rn(A.au[k], si_l), A.sclu[j]);
-			} else {
-				double v = __dmul_rn(__dmul_rn(A.al[k], si_l), A.scll[j]);
-				s.hl[sl] = v;
-				s.hu[sl] = v;
-			}
-		}
-		err = __reduce_min_sync(0xffffffffu, err);
-		__syncwarp();
-	}
-
-	// ---- updates from the stored members in ascending order, in groups of
-	//      consecutive members whose segments fit the shared prefetch buffer
-	for (int t0 = 0; t0 < nW && !err;) {
+	int err = 0;
+	for (int t0 = 0; t0 < nb && !err;) {
 		int t1 = t0;
-		while (t1 < nW && s.Wb[t1 + 1] - s.Wb[t0] <= s.pfcap) t1++;
-		if (t1 == t0) { // one segment longer than the buffer
-			if (!WS::big) return -3;
-			if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 5);
-			return -2;
-		}
+		while (t1 < nb && s.Wb[t1 + 1] - s.Wb[t0] <= s.pfcap) t1++;
+		if (t1 == t0) return BSG_ERR_WORKSPACE; // one segment longer than the buffer
 		const int gb = s.Wb[t0], npf = s.Wb[t1] - gb;
 		long long g0 = clock64();
 		// prefetch: 4 independent loads per lane in flight
@@ -540,14 +543,141 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		t0 = t1;
 		__syncwarp();
 	}
-	err = __reduce_min_sync(0xffffffffu, err);
+	return __reduce_min_sync(0xffffffffu, err);
+}
+
+// Factor row i.  Returns -1 when done, the unfinished row it waits for
+// (>= 0), -2 on error (reported through the status word), or -3 when the
+// row does not fit a shared-memory workspace (nothing was published yet, so
+// the caller retries it in the global one).
+//
+// Pipelined: the row closes the members that are finished, applies the
+// updates of every closed member below the smallest unfinished one (the
+// members below it are all known: a member is only discovered from a
+// smaller member), then waits for that member while a warp computes it.
+// When the last predecessor finishes, only its own segment and the finish
+// are left.
+template <class WS>
+__device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc) {
+	const bool ilu = A.kind == 1;
+	const long long c0 = clock64();
+	for (int t = lane; t < 2 * s.cmax; t += 32) s.wset[t] = -1;
+	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
+	if (lane == 0) s.sc[0] = 0;
+	__syncwarp();
+
+	// ---- seed with A's column i
+	const int tb = A.it[i], te = A.it[i + 1];
+	if (te - tb > s.cmax) {
+		if (!WS::big) return -3;
+		if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 2);
+		return -2;
+	}
+	for (int t = tb + lane; t < te; t += 32) {
+		int k = A.jt[t];
+		s.W[t - tb] = k;
+		s.Wst[t - tb] = 0;
+		wset_insert(s, k);
+	}
+	if (lane == 0) s.sc[0] = te - tb;
+	__syncwarp();
+
+	// ---- init the scaled row (Ich2InitRow / Ilu2InitRow); the compensations
+	//      received from rows that dropped column i join the diagonal last
+	int err = 0;
+	const int ab = A.iu[i], ae = A.iu[i + 1];
+	if (lane == 0) {
+		int slot = hfind_insert(s, i);
+		s.hl[slot] = A.diag0[i];
+		s.hu[slot] = A.diag0[i];
+	}
+	__syncwarp();
+	{
+		const double si_l = A.scll[i], si_u = A.sclu[i];
+		for (int k = ab + 1 + lane; k < ae; k += 32) {
+			int j = A.ju[k];
+			int sl = hfind_insert(s, j);
+			if (sl < 0) { err = BSG_ERR_WORKSPACE; continue; }
+			if (ilu) {
+				s.hl[sl] = __dmul_rn(__dmul_rn(A.al[k], si_u), A.scll[j]);
+				s.hu[sl] = __dmul_rn(__dmul_rn(A.au[k], si_l), A.sclu[j]);
+			} else {
+				double v = __dmul_rn(__dmul_rn(A.al[k], si_l), A.scll[j]);
+				s.hl[sl] = v;
+				s.hu[sl] = v;
+			}
+		}
+		err = __reduce_min_sync(0xffffffffu, err);
+		__syncwarp();
+	}
 	if (err) {
 		if (!WS::big) return -3;
 		if (lane == 0) devstat_fail(A.st, err, i, 4);
 		return -2;
 	}
+
+	int levmax = 0;
+	long long tail0 = clock64(); // end of the last wait: the row's own latency starts here
+	for (;;) {
+		// ---- close the finished members, pass after pass, until a pass
+		//      closes none; the smallest member left is the bound
+		int bound = i;
+		const long long k0 = clock64();
+		for (;;) {
+			pc.v[FS_ROUNDS]++;
+			int pmin = 0x7fffffff;
+			const long long q0 = clock64();
+			const int closed = close_pass(A, s, i, lane, levmax, pmin, err);
+			pc.v[FS_CYC_PCLOSE] += clock64() - q0;
+			if (err) break;
+			if (!closed) {
+				bound = pmin == 0x7fffffff ? i : pmin;
+				break;
+			}
+		}
+		if (err) {
+			if (!WS::big) return -3;
+			if (lane == 0) devstat_fail(A.st, err, i, 3);
+			return -2;
+		}
+		const long long k1 = clock64();
+		pc.v[FS_CYC_CLOSE] += k1 - k0;
+		// ---- updates of the closed members below the bound
+		err = apply_members(A, s, bound, lane, pc);
+		const long long k2 = clock64();
+		pc.v[FS_CYC_UPD] += k2 - k1;
+		if (err) {
+			if (!WS::big) return -3;
+			if (lane == 0) devstat_fail(A.st, err, i, 5);
+			return -2;
+		}
+		if (bound == i) break;
+		// ---- wait for the smallest unfinished member while a warp computes
+		//      it; park when nobody does
+		int res = 0;
+		if (lane == 0) res = wait_row(A, bound);
+		res = __shfl_sync(0xffffffffu, res, 0);
+		tail0 = clock64();
+		pc.v[FS_CYC_BLOCKED] += tail0 - k2;
+		if (res == 0) return bound;
+		if (res < 0) {
+			if (lane == 0) devstat_fail(A.st, BSG_ERR_TIMEOUT, i, 7);
+			return -2;
+		}
+	}
+	levmax = __reduce_max_sync(0xffffffffu, levmax);
+	pc.v[FS_CONTRIB] += min(s.sc[0], s.cmax);
+	{
+		const double comp = acc_value(A.acc, i, A.acc_inv_scale);
+		if (lane == 0) {
+			const int di0 = hfind_insert(s, i);
+			s.hl[di0] = __dadd_rn(s.hl[di0], comp);
+			s.hu[di0] = __dadd_rn(s.hu[di0], comp);
+		}
+		__syncwarp();
+	}
 	const long long c3 = clock64();
-	pc.v[FS_CYC_UPD] += c3 - c2;
+	(void)c0;
 
 	// ---- extract the off-diagonal mask columns and sort them ascending
 	if (lane == 0) s.sc[1] = 0;
@@ -557,40 +687,74 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		bool take = c >= 0 && c != i;
 		unsigned b = __ballot_sync(0xffffffffu, take);
 		int base = s.sc[1];
-		if (take) s.lst[base + __popc(b & ((1u << lane) - 1))] = h;
+		if (take) {
+			const int q = base + __popc(b & ((1u << lane) - 1));
+			s.lst[q] = h;
+			s.lkey[q] = c;
+		}
 		__syncwarp();
 		if (lane == 0) s.sc[1] = base + __popc(b);
 		__syncwarp();
 	}
 	const int nl = s.sc[1];
-	for (int t = lane; t < nl; t += 32) {
-		int c = s.hkey[s.lst[t]], r = 0;
-		for (int u = 0; u < nl; u++) r += s.hkey[s.lst[u]] < c;
-		s.lsts[r] = s.lst[t];
+	// rank sort (columns are distinct): each lane ranks its keys against one
+	// broadcast key per step
+	for (int t0 = 0; t0 < nl; t0 += 256) {
+		int key[8], rnk[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int t = t0 + q * 32 + lane;
+			key[q] = t < nl ? s.lkey[t] : 0x7fffffff;
+			rnk[q] = 0;
+		}
+		for (int u = 0; u < nl; u++) {
+			const int x = s.lkey[u];
+#pragma unroll
+			for (int q = 0; q < 8; q++) rnk[q] += x < key[q];
+		}
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int t = t0 + q * 32 + lane;
+			if (t < nl) s.lsts[rnk[q]] = s.lst[t];
+		}
 	}
 	__syncwarp();
 	const int di = hfind_insert(s, i); // existing slot of the diagonal
 
-	// ---- filter by tau2 with theta compensation (ascending columns); the
-	//      kept columns are listed in lst[] in ascending order
-	if (lane == 0) {
-		double dl = s.hl[di], du = s.hu[di];
-		int nk = 0;
-		for (int t = 0; t < nl; t++) {
-			int h = s.lsts[t];
+	// ---- filter by tau2 with theta compensation (ascending columns): the
+	//      compensations of the dropped columns are formed in parallel (in
+	//      pf_l), the kept columns compacted into lst[] in ascending order,
+	//      and lane 0 adds the compensations to the diagonal in column order
+	if (lane == 0) s.sc[2] = 0;
+	__syncwarp();
+	for (int t0 = 0; t0 < nl; t0 += 32) {
+		const int t = t0 + lane;
+		bool keep = false;
+		if (t < nl) {
+			const int h = s.lsts[t];
 			double v = fabs(s.hl[h]);
 			if (ilu) v = fmax(v, fabs(s.hu[h]));
-			if (!(v >= A.tau2)) {
-				v = __dmul_rn(v, A.theta);
+			keep = v >= A.tau2;
+			s.pf_l[t] = keep ? 0.0 : __dmul_rn(v, A.theta);
+		}
+		const unsigned b = __ballot_sync(0xffffffffu, keep);
+		const int base = s.sc[2];
+		if (keep) s.lst[base + __popc(b & ((1u << lane) - 1))] = s.lsts[t];
+		__syncwarp();
+		if (lane == 0) s.sc[2] = base + __popc(b);
+		__syncwarp();
+	}
+	if (lane == 0) {
+		double dl = s.hl[di], du = s.hu[di];
+		for (int t = 0; t < nl; t++) {
+			const double v = s.pf_l[t];
+			if (v != 0.0) {
 				dl = __dadd_rn(dl, v);
 				du = __dadd_rn(du, v);
-			} else {
-				s.lst[nk++] = h;
 			}
 		}
 		s.hl[di] = dl;
 		s.hu[di] = du;
-		s.sc[2] = nk;
 	}
 	__syncwarp();
 	const int nk = s.sc[2];
@@ -639,18 +803,19 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	}
 	// ---- hand the dropped entries' compensations to their rows
 	for (int t = lane; t < nl; t += 32) {
-		const int h = s.lsts[t];
-		double v = fabs(s.hl[h]);
-		if (ilu) v = fmax(v, fabs(s.hu[h]));
-		if (!(v >= A.tau2)) acc_push(A.acc, s.hkey[h], __dmul_rn(v, A.theta), A.acc_scale);
+		const double v = s.pf_l[t];
+		if (v != 0.0) acc_push(A.acc, s.hkey[s.lsts[t]], v, A.acc_scale);
 	}
 	if (lane == 0) A.lev[i] = levmax;
 	__threadfence();
 	__syncwarp();
 	if (lane == 0) st_release_u64(A.rec + i, REC_DONE | ((unsigned long long)off << 32) | (unsigned long long)len);
 	__syncwarp();
+	const long long cpub = clock64();
+	pc.v[FS_CYC_TOPUB] += cpub - tail0;
 
-	// ---- wake parked rows, release A-successors, count
+	// ---- release the rows of A's row i, wake parked rows, count
+	for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) admit_step(A, A.ju[k], ADM_ONE_FIN);
 	if (lane == 0) {
 		__threadfence();
 		int w = atomicExch(A.whead + i, W_CLOSED);
@@ -660,25 +825,20 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 			w = nx;
 		}
 	}
-	for (int k = ab + 1 + lane; k < ae; k += 32) {
-		int j = A.ju[k];
-		if (atomicSub(A.nstat + j, 1) == 1) q_push(A, j);
-	}
 	__syncwarp();
-	if (lane == 0) {
-		__threadfence();
-		atomicAdd(A.done_count, 1);
-	}
-	pc.v[FS_CYC_FIN] += clock64() - c3;
+	if (lane == 0) atomicAdd(A.done_count, 1);
+	const long long c4 = clock64();
+	pc.v[FS_CYC_POSTPUB] += c4 - cpub;
+	pc.v[FS_CYC_FIN] += c4 - c3;
+	pc.v[FS_CYC_TAIL] += c4 - tail0;
 	pc.v[FS_MASK] += nl;
 	return -1;
 }
 
-__global__ void __launch_bounds__(FACT_WARPS * 32) k_fact_rows(FactArgs A) {
+__global__ void __launch_bounds__(FACT_WARPS * 32, 2) k_fact_rows(FactArgs A) {
 	extern __shared__ unsigned char smem_raw[];
 	const int warp = threadIdx.x >> 5;
 	SmemWS &s = reinterpret_cast<SmemWS *>(smem_raw)[warp];
-	GlobWS g(A.big_ws + (size_t)(blockIdx.x * FACT_WARPS + warp) * GlobWS::bytes);
 	const int lane = threadIdx.x & 31;
 	PhaseClock pc;
 #pragma unroll
@@ -691,16 +851,59 @@ __global__ void __launch_bounds__(FACT_WARPS * 32) k_fact_rows(FactArgs A) {
 		pc.v[FS_CYC_POP] += clock64() - t0;
 		if (i < 0) break;
 		pc.v[FS_TRY]++;
+		if (lane == 0) {
+			*(volatile int *)(A.inprog + i) = 1;
+			__threadfence();
+		}
+		// first claim: the rows of A's row i have one static contributor
+		// fewer that is unclaimed
+		int first = 0;
+		if (lane == 0) first = !(atomicOr(reinterpret_cast<unsigned *>(A.nstat) + i, ADM_CLAIMED) & ADM_CLAIMED);
+		first = __shfl_sync(0xffffffffu, first, 0);
+		if (first)
+			for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) admit_step(A, A.ju[k], ADM_ONE_CLAIM);
+		__syncwarp();
 		int r = try_row(A, s, i, lane, pc);
 		if (r == -3) {
+			// a shared workspace is too small: take a free global one, or
+			// give the row back to the queue (a warp never waits for a
+			// workspace, so workspace holders cannot deadlock)
 			pc.v[FS_BIG]++;
-			__syncwarp();
+			int slot = -1;
+			if (lane == 0) {
+				const int start = (int)((blockIdx.x * FACT_WARPS + warp) % BIG_SLOTS);
+				for (int k = 0; k < BIG_SLOTS && slot < 0; k++) {
+					const int q = (start + k) % BIG_SLOTS;
+					if (atomicCAS(A.big_owner + q, 0, 1) == 0) slot = q;
+				}
+			}
+			slot = __shfl_sync(0xffffffffu, slot, 0);
+			if (slot < 0) {
+				if (lane == 0) {
+					*(volatile int *)(A.inprog + i) = 0;
+					__threadfence();
+					q_push(A, i);
+				}
+				__syncwarp();
+				continue;
+			}
+			__threadfence();
+			GlobWS g(A.big_ws + (size_t)slot * GlobWS::bytes);
 			r = try_row(A, g, i, lane, pc);
+			__syncwarp();
+			if (lane == 0) {
+				__threadfence();
+				atomicExch(A.big_owner + slot, 0);
+			}
 		}
 		if (r == -2) break;
 		if (r >= 0) {
 			pc.v[FS_PARK]++;
-			if (lane == 0) park(A, i, r);
+			if (lane == 0) {
+				*(volatile int *)(A.inprog + i) = 0;
+				__threadfence();
+				park(A, i, r);
+			}
 		}
 		__syncwarp();
 	}
@@ -713,10 +916,16 @@ __global__ void __launch_bounds__(FACT_WARPS * 32) k_fact_rows(FactArgs A) {
 
 // Per-row scheduler state (counts of unfinished rows of A's column i).
 __global__ void k_fact_init(int n, const int *it, int *nstat, int *whead, unsigned long long *rec,
-                            unsigned long long *acc, int *lev) {
+                            unsigned long long *acc, int *lev, int *inprog, bsg_devstat *st) {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n) return;
-	nstat[i] = it[i + 1] - it[i];
+	int cnt = it[i + 1] - it[i];
+	if (cnt > 0x7fff) { // the admission counters hold 15 bits
+		devstat_fail(st, BSG_ERR_WORKSPACE, i, 8);
+		cnt = 0;
+	}
+	nstat[i] = (cnt << 15) | cnt;
+	inprog[i] = 0;
 	whead[i] = W_EMPTY;
 	rec[i] = 0;
 	acc[i] = 0;
@@ -826,8 +1035,9 @@ void bsg_comp_scale(double tau2, double theta, double *scale, double *inv_scale)
 static unsigned long long g_fact_stats[FACT_NSTAT];
 
 // Counters of the last factorisation in this process: [0] row tries,
-// [1] parks, [2..7] SM cycles summed over warps in queue wait, closure,
-// blocked closures, prefetch, updates, finish; [8] members of C(i),
+// [1] parks, [2..7] SM cycles summed over warps in queue wait, closure
+// passes, waits for members, a row's own latency after its last wait,
+// updates, finish; [8] members of C(i),
 // [9] mask columns, [10] closure rounds, [11..13] SM cycles in prefetch,
 // slot resolution and fma phases, [14] rows retried in the global-memory
 // workspace, [15] warps launched.
@@ -846,11 +1056,12 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	// the pool holds U + R entries padded to 4-entry rows
 	long long cap = (long long)(mem * 2.0 * (double)m->nnz_up) + 8LL * n + 1024;
 	if (cap > 0x7ffffff0LL) cap = 0x7ffffff0LL; // pool offsets are 31-bit
-	const long long qcap = 8LL * n + 65536;
+	long long qcap = 1;
+	while (qcap < 2LL * n + 65536) qcap <<= 1; // ring of slots, see q_push
 	double *scll, *sclu, *diag0, *pl, *pu = nullptr;
 	unsigned *cf;
 	unsigned long long *rec, *acc;
-	int *lev, *nstat, *whead, *wnext, *queue, *done_count;
+	int *lev, *nstat, *whead, *wnext, *queue, *done_count, *inprog;
 	unsigned long long *pool_len, *qhead, *qtail;
 	BSG_CUDA(cudaMallocAsync(&scll, sizeof(double) * n, st));
 	BSG_CUDA(cudaMallocAsync(&sclu, sizeof(double) * n, st));
@@ -865,6 +1076,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	BSG_CUDA(cudaMallocAsync(&nstat, sizeof(int) * n, st));
 	BSG_CUDA(cudaMallocAsync(&whead, sizeof(int) * n, st));
 	BSG_CUDA(cudaMallocAsync(&wnext, sizeof(int) * n, st));
+	BSG_CUDA(cudaMallocAsync(&inprog, sizeof(int) * n, st));
 	BSG_CUDA(cudaMallocAsync(&queue, sizeof(int) * qcap, st));
 	BSG_CUDA(cudaMallocAsync(&done_count, sizeof(int), st));
 	BSG_CUDA(cudaMallocAsync(&pool_len, sizeof(unsigned long long), st));
@@ -880,7 +1092,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	// scale, init, queue fill, seed, rows, count, emit, level keys (+ CUB scans/sorts)
 	BSG_COUNT(8);
 	k_fact_scale<<<nb(n, 256), 256, 0, st>>>(n, kind, m->d_iu, m->d_ju, m->d_al, p->sclmin, scll, sclu, diag0, c->d_stat);
-	k_fact_init<<<nb(n, 256), 256, 0, st>>>(n, m->d_it, nstat, whead, rec, acc, lev);
+	k_fact_init<<<nb(n, 256), 256, 0, st>>>(n, m->d_it, nstat, whead, rec, acc, lev, inprog, c->d_stat);
 	k_fill_int<<<BSG_SMS * 4, 256, 0, st>>>(qcap, queue, -1);
 	FactArgs A;
 	A.n = n; A.kind = kind;
@@ -891,7 +1103,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	A.pool_cf = cf; A.pool_l = pl; A.pool_u = pu; A.pool_cap = cap; A.pool_len = pool_len;
 	A.rec = rec; A.acc = acc; A.lev = lev;
 	bsg_comp_scale(p->tau2, p->theta, &A.acc_scale, &A.acc_inv_scale);
-	A.nstat = nstat; A.whead = whead; A.wnext = wnext; A.queue = queue; A.qcap = qcap;
+	A.nstat = nstat; A.whead = whead; A.wnext = wnext; A.inprog = inprog; A.queue = queue; A.qcap = qcap;
 	A.qhead = qhead; A.qtail = qtail; A.done_count = done_count; A.st = c->d_stat;
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
 	BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
@@ -905,16 +1117,19 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	int need = (n + FACT_WARPS - 1) / FACT_WARPS;
 	if (grid > need) grid = need;
 	if (grid < 1) grid = 1;
-	if (cudaMallocAsync(&A.big_ws, GlobWS::bytes * (size_t)grid * FACT_WARPS, st) != cudaSuccess)
+	if (cudaMallocAsync(&A.big_ws, GlobWS::bytes * (size_t)BIG_SLOTS, st) != cudaSuccess)
 		return bsg_set_error(BSG_ERR_NOMEM, "factor row workspace");
+	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * BIG_SLOTS, st));
+	BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * BIG_SLOTS, st));
 	k_fact_rows<<<grid, FACT_WARPS * 32, smem, st>>>(A);
 	BSG_CUDA(cudaGetLastError());
 	int rc = bsg_check_devstat(c);
 	cudaMemcpyAsync(g_fact_stats, A.stats, sizeof(g_fact_stats), cudaMemcpyDeviceToHost, st);
 	cudaStreamSynchronize(st);
-	g_fact_stats[FACT_NSTAT - 1] = (unsigned long long)grid * FACT_WARPS; // warps launched
+	g_fact_stats[FS_WARPS] = (unsigned long long)grid * FACT_WARPS; // warps launched
 	cudaFreeAsync(A.stats, st);
 	cudaFreeAsync(A.big_ws, st);
+	cudaFreeAsync(A.big_owner, st);
 	int ndone = 0;
 	if (!rc) {
 		BSG_CUDA(cudaMemcpy(&ndone, done_count, sizeof(int), cudaMemcpyDeviceToHost));
@@ -922,7 +1137,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	}
 	auto release = [&]() {
 		for (void *q : {(void *)scll, (void *)sclu, (void *)diag0, (void *)cf, (void *)pl, (void *)pu, (void *)rec,
-		                (void *)acc, (void *)lev, (void *)nstat, (void *)whead, (void *)wnext, (void *)queue,
+		                (void *)acc, (void *)lev, (void *)nstat, (void *)whead, (void *)wnext, (void *)inprog, (void *)queue,
 		                (void *)done_count, (void *)pool_len, (void *)qhead, (void *)qtail})
 			if (q) cudaFreeAsync(q, st);
 	};

@@ -26,6 +26,7 @@ int bsg_scale_by_launch(bsg_ctx *c, int n, const double *x, double *y, const dou
 int bsg_residual_launch(bsg_ctx *c, int n, const double *b, double *r);
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
 int bsg_unet_apply(void *net, bsg_ctx *c, const double *r, double *z, double *work);
+extern "C" int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m);
 
 // device scalar slots used by PCG
 enum { S_ENRSQ = 0, S_GAMMA = 1, S_GAMOLD = 2, S_PAP = 3, S_BREAK = 4, S_TMP = 8 };
@@ -213,6 +214,11 @@ extern "C" int bsg_gmres_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, con
 	}
 	const double target = (p->sttype == 0) ? p->eps : p->eps * bnorm;
 	const bool flexible = p->krylov == 2;
+	if (flexible && p->learned) {
+		// the learned stage works on this operator (its diagonal is an input)
+		int rc = bsg_unet_set_matrix(static_cast<bsg_unet *>(p->learned), m);
+		if (rc) return rc;
+	}
 	int it = 0, status = BSG_OK;
 	double est = 0;
 	bool converged = false;

@@ -2,15 +2,20 @@
 """Benchmark of the preconditioned Krylov path on B200.
 
 Metric: wall milliseconds from a device-resident system (A, b) to a solution x
-with FP64 true relative residual ||b - Ax|| / ||b|| <= 1e-8, for the mixed
-arm (FP32 IC2 factor + FP64 FGMRES(30)); the plain FP64 arm (FP64 IC2 +
-exact triangular solves + PCG) and the SpMV HBM bandwidth are reported
-beside it.
+with FP64 true relative residual ||b - Ax|| / ||b|| <= 1e-8, for the learned +
+mixed arm: FP32 IC2 factor (= ILU2 of the symmetric matrix) applied by
+Jacobi(6) sweeps, followed by the trained U-Net stage, inside FP64
+FGMRES(30).  Beside it, the same step with the plain FP64 arm (FP64 factor,
+exact triangular solves, PCG), the mixed PCG and the plain mixed FGMRES, and
+the HBM bandwidth of the SpMV / sweep kernels and the tensor throughput of
+the U-Net convolutions.
 
 Workload: 3-D heat, 7-point stencil, 128^3 cells (n = 2,097,152), conductivity
-lognormal(sigma=1.5) per cell from seed 4, RHS uniform[-1,1] -- the learned /
-mixed FGMRES configuration.  A step is one complete solve: factorisation of
-the device matrix, the Krylov loop, the FP64 true residual.
+lognormal(sigma=1.5) per cell from seed 4, RHS uniform[-1,1].  A step is one
+complete solve: device matrix set-up, factorisation, the Krylov loop with the
+learned stage, the FP64 true residual.  The network (weights/unet_heat64.npz,
+trained by learned.py on 2000 pairs from 64^3 instances) is loaded once
+before the timed region, like any model.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -106,16 +111,31 @@ def make_system(grid=GRID):
     return s, s.upper()
 
 
-def mixed_param(bsg):
+def mixed_param(bsg, krylov=0, learned=None):
     """FP32 IC2 factor applied by Jacobi(6) sweeps (a symmetric polynomial
-    preconditioner), FP64 PCG, stop confirmed on the FP64 true residual."""
-    return bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=TOL,
-                             niter=3000, precision=1, trisolve=1, nsweeps=6, krylov=0, true_residual=1)
+    preconditioner); krylov 0: FP64 PCG, 2: FP64 FGMRES(30) (with the learned
+    stage when `learned` is a network); stop confirmed on the FP64 true
+    residual."""
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=TOL,
+                          niter=3000, precision=1, trisolve=1, nsweeps=6, krylov=krylov, restart=30, sttype=1,
+                          true_residual=1)
+    if learned is not None:
+        p.learned = learned.h.value
+    return p
 
 
 def fp64_param(bsg):
     return bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=TOL,
                              niter=3000, precision=0, trisolve=0)
+
+
+def unet_flops(grid):
+    """FLOPs of one U-Net forward on grid^3 (W0 counted with its 16 padded
+    input channels, as the tensor cores run it)."""
+    import learned
+    vox = [grid ** 3 // 8 ** l for l in range(4)]
+    level = (0, 1, 2, 3, 2, 1, 0)
+    return sum(2 * 27 * ci * co * vox[level[k]] for k, (ci, co) in enumerate(learned.LAYERS))
 
 
 def run_reference(args, rank):
@@ -165,7 +185,7 @@ def main():
     ap.add_argument("--impl", default="bsg", choices=["bsg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lean", action="store_true",
-                    help="timed steps only (no FP64 arm, e2e, kernel timing or CPU baseline): profiling runs")
+                    help="timed steps only (no other arms, e2e, kernel timing or CPU baseline): profiling runs")
     ap.add_argument("--grid", type=int, default=GRID, help="cells per side (profiling of smaller cases)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -178,6 +198,7 @@ def main():
     import numpy as np
     import torch
     import bsg
+    import learned
 
     torch.cuda.set_device(local)
     dist = None
@@ -195,6 +216,9 @@ def main():
     d_b = torch.as_tensor(s.rhs[0], device=dev)
     L = bsg.lib()
     import ctypes as C
+
+    net = bsg.UNet(ctx, args.grid, args.grid, args.grid)
+    net.set_weights(learned.load())
 
     def solve_device(param):
         """One step: device CSR -> device matrix -> factor -> Krylov -> x."""
@@ -220,9 +244,11 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    def headline():
+        return mixed_param(bsg, krylov=2, learned=net)
+
     for _ in range(args.warmup):
-        p = mixed_param(bsg)
-        solve_device(p)
+        solve_device(headline())
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -233,7 +259,7 @@ def main():
     with ClockSampler(local) as clk:
         e0.record()
         for _ in range(args.steps):
-            p = mixed_param(bsg)
+            p = headline()
             solve_device(p)
             params.append(p)
         e1.record()
@@ -259,13 +285,18 @@ def main():
             dist.destroy_process_group()
         return 0
 
-    # ---- plain FP64 arm (IC2 FP64, exact sync-free solves, PCG): same system, same steps
-    e0.record()
-    p64 = fp64_param(bsg)
-    solve_device(p64)
-    e1.record()
-    torch.cuda.synchronize()
-    ms64 = e0.elapsed_time(e1)
+    def timed(param):
+        e0.record()
+        solve_device(param)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), param
+
+    # ---- the other arms on the same system: plain FP64 (FP64 IC2, exact
+    #      sync-free solves, PCG), mixed PCG, mixed FGMRES without the network
+    ms64, p64 = timed(fp64_param(bsg))
+    ms_pcg, p_pcg = timed(mixed_param(bsg, krylov=0))
+    ms_fg, p_fg = timed(mixed_param(bsg, krylov=2))
 
     # ---- end to end through the host-buffer C ABI (pinned host arrays)
     h_ia = torch.from_numpy(u.ia).pin_memory().numpy()
@@ -274,10 +305,12 @@ def main():
     h_b = torch.from_numpy(np.ascontiguousarray(s.rhs[0])).pin_memory().numpy()
     e2e_ms = []
     for _ in range(max(1, min(args.steps, 3))):
-        p = mixed_param(bsg)
+        p = headline()
         t0 = time.perf_counter()
         xh = bsg.solve_symm(ctx, n, h_ia, h_ja, h_a, h_b, p)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        if p.resfin > TOL:
+            raise RuntimeError(f"e2e true residual {p.resfin:.3e} above {TOL}")
     h2d = h_ia.nbytes + h_ja.nbytes + h_a.nbytes + h_b.nbytes
     d2h = xh.nbytes
 
@@ -304,6 +337,18 @@ def main():
     peak, peak_kind = peaks()
     spmv_gbs = spmv_bytes / (t_spmv.value * 1e-3) / 1e9
     sweep_gbs = sweep_bytes / (t_sweep.value * 1e-3) / 1e9
+    # U-Net forward (the learned stage's tensor-core work), same stream
+    r_t = torch.randn(n, dtype=torch.float64, device=dev)
+    y_t = torch.empty_like(r_t)
+    for _ in range(3):
+        net.forward(r_t, y_t)
+    e0.record()
+    for _ in range(20):
+        net.forward(r_t, y_t)
+    e1.record()
+    torch.cuda.synchronize()
+    t_unet = e0.elapsed_time(e1) / 20
+    conv_tflops = unet_flops(args.grid) / (t_unet * 1e-3) / 1e12
     L.bsg_fct_free(fh)
     L.bsg_mat_free(mh)
 
@@ -321,27 +366,40 @@ def main():
                    "iterations": info["iters"], "tfct_s": info["tfct"], "titr_s": info["titr"]}
 
     if rank == 0:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            bf16_peak = float(json.load(f).get("bf16_tflops", 1590.0))
         line = {
             "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": n, "nnz": int(nnz.value), "parallelism": f"replicas{world}",
-                       "solver": "IC2(tau1=tau2=1e-3) FP32 factor, Jacobi(6) triangular solves, FP64 PCG",
+                       "solver": "IC2(tau1=tau2=1e-3) FP32 factor, Jacobi(6) triangular solves, learned U-Net "
+                                 "stage (bf16, trained at 64^3), FP64 FGMRES(30)",
                        "l2": "inputs larger than L2 (matrix 175 MB, factor 420 MB)"},
             "iterations": p_last.nitperf, "true_residual": p_last.resfin,
             "fct_ms": round(p_last.timefct * 1e3, 3), "itr_ms": round(p_last.timeitr * 1e3, 3),
-            "fp64_pcg_ms": round(ms64, 3), "fp64_pcg_iterations": p64.nitperf,
+            "arms": {
+                "fp64_pcg": {"ms": round(ms64, 3), "iterations": p64.nitperf, "itr_ms": round(p64.timeitr * 1e3, 3)},
+                "mixed_pcg": {"ms": round(ms_pcg, 3), "iterations": p_pcg.nitperf,
+                              "itr_ms": round(p_pcg.timeitr * 1e3, 3)},
+                "mixed_fgmres_plain": {"ms": round(ms_fg, 3), "iterations": p_fg.nitperf,
+                                       "itr_ms": round(p_fg.timeitr * 1e3, 3)},
+            },
             "speedup_vs_fp64_pcg": round(ms64 / ms, 3),
             "e2e": {"value": round(statistics.mean(e2e_ms), 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "kernel": "k_spmv_csr (FP64 CSR SpMV)", "achieved": round(spmv_gbs, 1),
+            "roofline": {"bound": "hbm", "kernel": "k_sell_apply (FP64 SELL-8 SpMV)", "achieved": round(spmv_gbs, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(spmv_gbs / peak, 4), "traffic": None,
                          "algorithmic_bytes": spmv_bytes, "ms_per_launch": t_spmv.value,
                          "peak_source": peak_kind},
-            "roofline_trisolve": {"bound": "hbm", "kernel": "k_trsv_jacobi (one FP32 sweep)",
+            "roofline_trisolve": {"bound": "hbm", "kernel": "k_sell_apply (one FP32 Jacobi sweep)",
                                   "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                   "frac": round(sweep_gbs / peak, 4), "algorithmic_bytes": sweep_bytes,
                                   "ms_per_launch": t_sweep.value},
+            "roofline_unet": {"bound": "tensor", "kernel": "U-Net forward (k_conv3t / k_conv3, bf16 mma)",
+                              "achieved": round(conv_tflops, 1), "peak": bf16_peak, "unit": "TFLOP/s",
+                              "frac": round(conv_tflops / bf16_peak, 4), "ms_per_forward": round(t_unet, 4),
+                              "flops": unet_flops(args.grid)},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -185,9 +185,11 @@ static int pool_reserve(pool_t *p, size_t need) {
  * (Ich2StoreScaleU :910).
  *
  * Deliberate, documented difference: the reference applies the updates of
- * row i in the order of its transposed linked lists (ibegm/madj); this
- * restatement applies them in ascending order of the updating row, and sums
- * the row's own theta compensations in ascending column order.  Products are
+ * row i in the order of its transposed linked lists (ibegm/madj) and adds the
+ * compensations of the rows that dropped column i as they come; this
+ * restatement applies the updates in ascending order of the updating row,
+ * then adds the received compensations (an exact fixed-point sum), then the
+ * row's own theta compensations in ascending column order.  Products are
  * accumulated with fma().  The GPU kernel uses exactly this order, so its
  * factor can be compared bit for bit; against the reference the entries
  * agree to rounding (checked in tests/test_oracle_pin.py). */
@@ -239,7 +241,7 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 		int nl = 0;
 		/* init (Ich2InitRow / Ilu2InitRow) */
 		lst[nl++] = i; imask[i] = i;
-		fl[i] = diagg[i] + acc_value(acc, i);
+		fl[i] = diagg[i];
 		fu[i] = fl[i];
 		for (int k = ia[i] + 1; k < ia[i + 1]; k++) {
 			int j = ja[k];
@@ -296,6 +298,13 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
 				iv[r]++;
 				r = nxt;
 			}
+		}
+		/* the theta compensations received from the rows that dropped column
+		 * i, summed exactly (fixed point), join the diagonal after the updates */
+		{
+			const double cv = acc_value(acc, i);
+			fl[i] = fl[i] + cv;
+			fu[i] = fu[i] + cv;
 		}
 		if (!ilu) for (int s = 0; s < nl; s++) fu[lst[s]] = fl[lst[s]];
 		/* filter in ascending column order (Ich2FiltrRow / Ilu2FiltrRow) */
