@@ -96,6 +96,7 @@ def lib():
         "bsg_unet_adam": (i_, [vp, C.c_float, C.c_float, C.c_float, C.c_float, i_]),
         "bsg_unet_zero_grads": (i_, [vp]),
         "bsg_launch_count": (C.c_ulonglong, []),
+        "bsg_pcg_batch_dev": (i_, [vp, vp, vp, i_, i_, ip, vp, vp, C.POINTER(Param), ip, dp, ip]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -357,6 +358,26 @@ def pcg(ctx, mat, fct, b, x, param):
     """PCG on device tensors (x holds the initial guess, overwritten)."""
     _check(lib().bsg_pcg_dev(ctx.h, mat.h, fct.h, _ptr(b), _ptr(x), C.byref(param)))
     return param
+
+
+def pcg_batch(ctx, mat, fct, B, X, param, seg_off=None):
+    """Batched PCG: B, X CUDA float64 tensors [nrhs, n]; seg_off (optional)
+    the point-row offsets of independent diagonal blocks.  Returns per-system
+    iterations, FP64 true relative residuals ([nrhs * nseg], right-hand side
+    major) and the tuned shapes (chunk, group, iterations per graph, replays)."""
+    nrhs = B.shape[0]
+    if seg_off is None:
+        nseg, so = 1, None
+    else:
+        so = np.ascontiguousarray(seg_off, dtype=np.int32)
+        nseg = len(so) - 1
+    it = np.zeros(nrhs * nseg, np.int32)
+    rs = np.zeros(nrhs * nseg)
+    tn = np.zeros(4, np.int32)
+    _check(lib().bsg_pcg_batch_dev(ctx.h, mat.h, fct.h, nrhs, nseg, None if so is None else _ip(so), _ptr(B), _ptr(X),
+                                   C.byref(param), it.ctypes.data_as(C.POINTER(C.c_int)),
+                                   rs.ctypes.data_as(C.POINTER(C.c_double)), tn.ctypes.data_as(C.POINTER(C.c_int))))
+    return it, rs, tn
 
 
 def gmres(ctx, mat, fct, b, x, param):

@@ -164,6 +164,23 @@ int bsg_pcg_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *
 int bsg_gmres_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x,
                   bsg_param *p);
 
+/* Batched PCG (CSVector::Cg's recurrence, Bslib/cg.cpp:31-350, which handles
+ * one right-hand side, :375-377): nrhs right-hand sides times nseg diagonal
+ * blocks ("segments") of A that no entry couples -- e.g. the load cases of
+ * one cell, or many independent problems assembled as one block-diagonal
+ * matrix.  Each (right-hand side, segment) pair is its own system with its
+ * own scalars and stopping test (ittype 0: ||r|| <= eps ||r0||), solved
+ * together: one SpMM, one preconditioner pass per right-hand side and
+ * segmented reductions per iteration, the iterations replayed from a CUDA
+ * graph.  d_B, d_X: [nrhs][n] (n = point rows), d_X holds x0.  seg_off: host,
+ * nseg + 1 point-row offsets (whole block rows; NULL when nseg == 1).
+ * iters / res (host, nrhs * nseg, may be NULL): per-system iterations and
+ * FP64 true relative residuals; p->nitperf / p->resfin get their maxima.
+ * tuned (host, 4 ints, may be NULL): reduction chunk, SpMM group, iterations
+ * per graph, graph replays. */
+int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs, int nseg, const int *seg_off,
+                      const double *d_B, double *d_X, bsg_param *p, int *iters, double *res, int *tuned);
+
 /* ---- whole drivers with host buffers ------------------------------------- */
 /* CSVector::SolveSymm(CSMatrixR&) (Bslib/solvers.cpp:4615): upper-stored SPD
  * CSR in, IC2 + PCG (or GMRES/FGMRES per p->krylov), solution out. */
