@@ -117,6 +117,10 @@ void bsg_sell_free(bsg_sell *m, cudaStream_t s);
 int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y);
 int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const double *yin,
                    int scaled_in, double *yout);
+int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, int nsweeps,
+                      float *work32, double *yout);
+int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const float *x32,
+                          double *yout);
 
 struct bsg_mat {
 	bsg_ctx *ctx;

@@ -115,6 +115,64 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
 	}
 }
 
+// One Jacobi pass of an FP32 factor with FP32 iterates: out = (rhs - N x32)
+// * dinv, written as FP64 (the last pass, OUT64 1) or as the FP32 iterate the
+// next pass gathers (OUT64 0).  Gathering 4-byte iterates halves the
+// sector traffic of the gathers; the products and sums stay FP64.
+template <int OUT64>
+__global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restrict__ perm,
+                                                      const long long *__restrict__ off,
+                                                      const int *__restrict__ scol, const float *__restrict__ sval,
+                                                      const float *__restrict__ x32, const double *__restrict__ rhs,
+                                                      const double *__restrict__ dinv, double *__restrict__ y,
+                                                      float *__restrict__ y32) {
+	constexpr int SPW = 32 / SELL_C;
+	const int lane = threadIdx.x & 31;
+	const int grp = lane / SELL_C, l = lane % SELL_C;
+	const int nsl = (n + SELL_C - 1) / SELL_C;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * SPW; s0 < nsl; s0 += nwarps * SPW) {
+		const int slice = s0 + grp;
+		if (slice >= nsl) continue;
+		const long long base = __ldg(off + slice);
+		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+		const int *cp = scol + base + l;
+		const float *vp = sval + base + l;
+		double sum = 0.0;
+		int k = 0;
+		for (; k + 8 <= w; k += 8) {
+			int c[8];
+			float a[8], xv[8];
+#pragma unroll
+			for (int u = 0; u < 8; u++) {
+				c[u] = __ldcs(cp + SELL_C * (k + u));
+				a[u] = __ldcs(vp + SELL_C * (k + u));
+			}
+#pragma unroll
+			for (int u = 0; u < 8; u++) xv[u] = __ldg(x32 + c[u]);
+#pragma unroll
+			for (int u = 0; u < 8; u++) sum = fma((double)a[u], (double)xv[u], sum);
+		}
+		for (; k < w; k++) {
+			const int c = __ldcs(cp + SELL_C * k);
+			sum = fma((double)__ldcs(vp + SELL_C * k), (double)__ldg(x32 + c), sum);
+		}
+		const int t = slice * SELL_C + l;
+		if (t < n) {
+			const int r = perm ? __ldg(perm + t) : t;
+			const double v = (rhs[r] - sum) * dinv[r];
+			if (OUT64) y[r] = v;
+			else y32[r] = (float)v;
+		}
+	}
+}
+
+// x32 = x * dinv rounded to FP32 (the first Jacobi iterate)
+__global__ void k_scale32(int n, const double *x, const double *dinv, float *x32) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		x32[i] = (float)(x[i] * dinv[i]);
+}
+
 inline int nb(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
 
 } // namespace
@@ -235,6 +293,35 @@ int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const dou
 		if (scaled_in) k_sell_apply<double, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout);
 		else k_sell_apply<double, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout);
 	}
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
+// Jacobi sweeps of an FP32 factor with FP32 iterates: nsweeps >= 2 iterates
+// in total (the first, D^-1 x, formed by k_scale32), the last written to
+// yout in FP64.  work32 holds 2 n floats (the ping-pong iterates).
+int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, int nsweeps,
+                      float *work32, double *yout) {
+	if (!m->fp32 || nsweeps < 2) return BSG_ERR_ARG;
+	const int n = m->n, g = sell_grid(n);
+	const float *v = (const float *)m->val;
+	float *a = work32, *b = work32 + n;
+	BSG_COUNT(nsweeps);
+	k_scale32<<<nb(n, 256) < BSG_SMS * 16 ? nb(n, 256) : BSG_SMS * 16, 256, 0, s>>>(n, x, dinv, b);
+	for (int pass = 0; pass < nsweeps - 1; pass++) {
+		const bool last = pass == nsweeps - 2;
+		if (last) k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr);
+		else k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a);
+		float *t = a; a = b; b = t;
+	}
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
+// One full FP32-iterate pass (timing of the sweep kernel alone).
+int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const float *x32,
+                          double *yout) {
+	BSG_COUNT(1);
+	k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x, dinv,
+	                                                  yout, nullptr);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 

@@ -21,7 +21,9 @@
 #include "bsg_internal.cuh"
 #include "k_stream.cuh"
 
+#ifndef SELL_SIGMA
 #define SELL_SIGMA 128 // rows per length-sorting window of the factor's sliced copies
+#endif
 
 namespace {
 
@@ -198,11 +200,15 @@ int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const dou
 	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
 	const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
 	(void)n; (void)rp; (void)ci;
+	if (f->fp32) // the FP32-iterate pass of the mixed path; yin's bytes serve as its FP32 input
+		return bsg_sell_sweep32_pass(c->stream, lower ? &f->sl : &f->su, x, dinv, reinterpret_cast<const float *>(yin),
+		                             yout);
 	return bsg_sell_sweep(c->stream, lower ? &f->sl : &f->su, x, dinv, yin, 0, yout);
 }
 
 // Solve with L (lower != 0) or U.  x and y must not alias.  `work` (n
-// doubles) is needed for mode 1 with nsweeps > 1.
+// doubles) is needed for mode 1 with nsweeps > 2, and with nsweeps > 1 for an
+// FP32 factor, whose sweeps keep their intermediate iterates in FP32 there.
 int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                         double *work) {
 	cudaStream_t s = c->stream;
@@ -234,6 +240,11 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 		BSG_COUNT(1);
 		k_scale_vec<<<BSG_SMS * 8, 256, 0, s>>>(n, x, dinv, y);
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	}
+	if (use32) {
+		// FP32 factor: FP32 iterates, ping-ponged in work (2 n floats)
+		if (!work) return BSG_ERR_ARG;
+		return bsg_sell_sweeps32(s, lower ? &f->sl : &f->su, x, dinv, nsweeps, reinterpret_cast<float *>(work), y);
 	}
 	int grid = ((n + STREAM_ROWS - 1) / STREAM_ROWS + 7) / 8;
 	if (grid > BSG_SMS * 8) grid = BSG_SMS * 8;

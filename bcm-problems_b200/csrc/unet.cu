@@ -441,17 +441,30 @@ __global__ void k_logvec(int n, const double *d, double *ld) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 		ld[i] = log(fabs(d[i]) + 1e-300);
 }
-__global__ void k_moments(int n, const double *ld, double *out) {
-	// one block: mean and standard deviation
-	__shared__ double s1[256], s2[256];
+// mean and standard deviation of ld: block partials over a fixed grid
+// (SQ_BLOCKS), then one ordered final pass
+__global__ void k_moments_part(int n, const double *ld, double *part) {
+	__shared__ double s1[8], s2[8];
 	double a = 0, b = 0;
-	for (int i = threadIdx.x; i < n; i += blockDim.x) { a += ld[i]; b = fma(ld[i], ld[i], b); }
-	s1[threadIdx.x] = a;
-	s2[threadIdx.x] = b;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+		a += ld[i];
+		b = fma(ld[i], ld[i], b);
+	}
+	a = warp_sum(a);
+	b = warp_sum(b);
+	if ((threadIdx.x & 31) == 0) { s1[threadIdx.x >> 5] = a; s2[threadIdx.x >> 5] = b; }
 	__syncthreads();
 	if (threadIdx.x == 0) {
+		double p = 0, q = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) { p += s1[w]; q += s2[w]; }
+		part[blockIdx.x] = p;
+		part[gridDim.x + blockIdx.x] = q;
+	}
+}
+__global__ void k_moments_final(int n, int nb, const double *part, double *out) {
+	if (threadIdx.x == 0) {
 		double m = 0, q = 0;
-		for (int t = 0; t < (int)blockDim.x; t++) { m += s1[t]; q += s2[t]; }
+		for (int b = 0; b < nb; b++) { m += part[b]; q += part[nb + b]; }
 		m /= n;
 		q = q / n - m * m;
 		out[0] = m;
@@ -930,9 +943,10 @@ extern "C" int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m) {
 		return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_matrix: matrix size does not match the grid");
 	u->mat = m;
 	cudaStream_t s = u->ctx->stream;
-	BSG_COUNT(3);
+	BSG_COUNT(4);
 	k_logdiag<<<ew(m->n), 256, 0, s>>>(m->n, m->d_iu, m->d_al, u->ld);
-	k_moments<<<1, 256, 0, s>>>(m->n, u->ld, u->mom);
+	k_moments_part<<<SQ_BLOCKS, 256, 0, s>>>(m->n, u->ld, u->part);
+	k_moments_final<<<1, 32, 0, s>>>(m->n, SQ_BLOCKS, u->part, u->mom);
 	k_logd_norm<<<ew(m->n), 256, 0, s>>>(m->n, u->ld, u->mom, u->logd);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
@@ -945,9 +959,10 @@ extern "C" int bsg_unet_set_diag(bsg_unet *u, const double *d_diag) {
 	if (!u || !d_diag) return bsg_set_error(BSG_ERR_ARG, "bsg_unet_set_diag: null argument");
 	cudaStream_t s = u->ctx->stream;
 	const int n = (int)u->nv[0];
-	BSG_COUNT(3);
+	BSG_COUNT(4);
 	k_logvec<<<ew(n), 256, 0, s>>>(n, d_diag, u->ld);
-	k_moments<<<1, 256, 0, s>>>(n, u->ld, u->mom);
+	k_moments_part<<<SQ_BLOCKS, 256, 0, s>>>(n, u->ld, u->part);
+	k_moments_final<<<1, 32, 0, s>>>(n, SQ_BLOCKS, u->part, u->mom);
 	k_logd_norm<<<ew(n), 256, 0, s>>>(n, u->ld, u->mom, u->logd);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
