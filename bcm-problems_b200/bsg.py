@@ -97,6 +97,8 @@ def lib():
         "bsg_unet_zero_grads": (i_, [vp]),
         "bsg_launch_count": (C.c_ulonglong, []),
         "bsg_pcg_batch_dev": (i_, [vp, vp, vp, i_, i_, ip, vp, vp, C.POINTER(Param), ip, dp, ip]),
+        "bsg_lanczos_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
+        "bsg_solve_t_dev": (i_, [vp, vp, i_, i_, i_, vp, vp]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -267,6 +269,14 @@ class Factor:
     def solve_u(self, x, y, mode=0, nsweeps=3):
         _check(lib().bsg_solve_u_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))
 
+    def solve_ut(self, x, y, mode=0, nsweeps=3):
+        """y = U^{-T} x (SolveL on U's storage)."""
+        _check(lib().bsg_solve_t_dev(self.ctx.h, self.h, 0, mode, nsweeps, _ptr(x), _ptr(y)))
+
+    def solve_lt(self, x, y, mode=0, nsweeps=3):
+        """y = L^{-T} x (SolveU on L's storage)."""
+        _check(lib().bsg_solve_t_dev(self.ctx.h, self.h, 1, mode, nsweeps, _ptr(x), _ptr(y)))
+
     def free(self):
         if self.h:
             lib().bsg_fct_free(self.h)
@@ -378,6 +388,12 @@ def pcg_batch(ctx, mat, fct, B, X, param, seg_off=None):
                                    C.byref(param), it.ctypes.data_as(C.POINTER(C.c_int)),
                                    rs.ctypes.data_as(C.POINTER(C.c_double)), tn.ctypes.data_as(C.POINTER(C.c_int))))
     return it, rs, tn
+
+
+def lanczos(ctx, mat, fct, b, x, param):
+    """Two-sided Lanczos (CSVector::Lanczos) on device tensors (x holds x0)."""
+    _check(lib().bsg_lanczos_dev(ctx.h, mat.h, fct.h, _ptr(b), _ptr(x), C.byref(param)))
+    return param
 
 
 def gmres(ctx, mat, fct, b, x, param):

@@ -421,6 +421,7 @@ extern "C" int bsg_mat_free(bsg_mat *m) {
 	if (!m) return BSG_OK;
 	cudaStream_t s = m->ctx->stream;
 	bsg_sell_free(&m->sell, s);
+	bsg_sell_free(&m->sellT, s);
 	if (m->d_au && m->d_au != m->d_al) cudaFreeAsync(m->d_au, s);
 	for (void *p : {(void *)m->d_ia, (void *)m->d_ja, (void *)m->d_a, (void *)m->d_iu, (void *)m->d_ju,
 	                (void *)m->d_al, (void *)m->d_it, (void *)m->d_jt})
@@ -527,6 +528,10 @@ extern "C" int bsg_fct_free(bsg_fct *f) {
 	cudaStream_t s = f->ctx->stream;
 	bsg_sell_free(&f->sl, s);
 	bsg_sell_free(&f->su, s);
+	bsg_sell_free(&f->slt, s);
+	bsg_sell_free(&f->sut, s);
+	for (void *q : {(void *)f->d_utr_v, (void *)f->d_utr_f, (void *)f->d_l_f})
+		if (q) cudaFreeAsync(q, s);
 	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);
 	for (void *p : {(void *)f->d_iu, (void *)f->d_ju, (void *)f->d_u, (void *)f->d_dinv_l, (void *)f->d_dinv_u,
 	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f,
@@ -542,6 +547,16 @@ extern "C" int bsg_solve_l_dev(bsg_ctx *c, const bsg_fct *f, int mode, int nswee
 	double *work = nullptr;
 	if (mode == 1 && nsweeps > 1) BSG_CUDA(cudaMallocAsync(&work, sizeof(double) * f->n, c->stream));
 	int rc = bsg_trisolve_launch(c, f, 1, mode, nsweeps, x, y, work);
+	if (work) cudaFreeAsync(work, c->stream);
+	if (!rc) rc = bsg_check_devstat(c);
+	return rc;
+}
+extern "C" int bsg_solve_t_dev(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y) {
+	if (!c || !f || !x || !y || x == y || (which != 0 && which != 1))
+		return bsg_set_error(BSG_ERR_ARG, "bsg_solve_t_dev: bad argument");
+	double *work = nullptr;
+	if (mode == 1 && nsweeps > 1) BSG_CUDA(cudaMallocAsync(&work, sizeof(double) * f->n, c->stream));
+	int rc = bsg_trisolve_t_launch(c, f, which, mode, nsweeps, x, y, work);
 	if (work) cudaFreeAsync(work, c->stream);
 	if (!rc) rc = bsg_check_devstat(c);
 	return rc;
@@ -576,8 +591,9 @@ static int drive(bsg_ctx *c, int n, const int *ia, const int *ja, const double *
 	}
 	cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s);
 	cudaMemsetAsync(dx, 0, sizeof(double) * n, s);
-	bool pcg = symm && p->krylov == 0;
-	rc = pcg ? bsg_pcg_dev(c, m, f, db, dx, p) : bsg_gmres_dev(c, m, f, db, dx, p);
+	if (p->krylov != 0) rc = bsg_gmres_dev(c, m, f, db, dx, p);
+	else if (symm) rc = bsg_pcg_dev(c, m, f, db, dx, p);  // SolveSymm: Cg
+	else rc = bsg_lanczos_dev(c, m, f, db, dx, p);        // Solver: Lanczos
 	int rc2 = (int)cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
 	cudaStreamSynchronize(s);
 	cudaFreeAsync(db, s);

@@ -137,7 +137,8 @@ struct bsg_mat {
 	double *d_al, *d_au;  // ILU2 split values (al == au for symmetric input)
 	int *d_it, *d_jt;     // transpose of the strict upper pattern: rows k < i with (k,i) stored
 	int group;            // CSR SpMV sub-warp size
-	bsg_sell sell;        // SELL-32 copy of a point matrix (single-vector SpMV)
+	bsg_sell sell;        // SELL-8 copy of a point matrix (single-vector SpMV)
+	bsg_sell sellT;       // SELL-8 copy of A^T, built on first use (transposed products)
 };
 
 struct bsg_fct {
@@ -161,6 +162,12 @@ struct bsg_fct {
 	bsg_sell sl, su;              // SELL-32 strict L / U rows (Jacobi sweeps), FP64 or FP32
 	int levels_l, levels_u;       // dependency depth
 	double density, density2;
+	// transposed solves (U^T: the L-row pattern with U's values; L^T: U's
+	// pattern with L's values), built on first use for ILU2 factors
+	int has_t;
+	double *d_utr_v;
+	float *d_utr_f, *d_l_f;
+	bsg_sell slt, sut;
 };
 
 // ---- launch accounting ------------------------------------------------------
@@ -177,4 +184,8 @@ int bsg_dot_launch(bsg_ctx *c, int n, const double *x, const double *y, double *
 int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct **out);
 int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                         double *work);
+// Solve with U^T (which 0) or L^T (which 1), the transposed preconditioner of
+// the two-sided Lanczos; builds the transposed forms on first use.
+int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y,
+                          double *work);
 int bsg_check_devstat(bsg_ctx *c);

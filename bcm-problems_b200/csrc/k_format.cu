@@ -289,3 +289,39 @@ int bsg_bsr_to_point(bsg_ctx *c, int nsup, int bs, const int *ia, const int *ja,
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
+
+namespace {
+__global__ void k_transpose_keys(int n, const int *ia, const int *ja, unsigned long long *keys, int *vals) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	for (int k = ia[i]; k < ia[i + 1]; k++) {
+		keys[k] = ((unsigned long long)(unsigned)ja[k] << 32) | (unsigned)i;
+		vals[k] = k;
+	}
+}
+} // namespace
+
+// Transpose of a full square CSR matrix (rows of A^T = columns of A, columns
+// ascending), the operand of CSMatrixR::MvmAt in gather form.
+int bsg_transpose_full(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz, int **ta_o,
+                       int **tja_o, double **tv_o) {
+	unsigned long long *keys;
+	int *vals;
+	BSG_CUDA(cudaMallocAsync(&keys, sizeof(unsigned long long) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(&vals, sizeof(int) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_COUNT(1);
+	k_transpose_keys<<<nblk(n, 256), 256, 0, c->stream>>>(n, ia, ja, keys, vals);
+	int rc = bsg_sort_pairs(c, keys, vals, nnz, bits_for(n));
+	if (rc) return rc;
+	BSG_CUDA(cudaMallocAsync(ta_o, sizeof(int) * (n + 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(tja_o, sizeof(int) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_CUDA(cudaMallocAsync(tv_o, sizeof(double) * (nnz > 0 ? nnz : 1), c->stream));
+	BSG_COUNT(3);
+	k_row_ptr<<<nblk(n + 1, 256), 256, 0, c->stream>>>(n, nnz, keys, *ta_o);
+	k_cols_from_keys<<<nblk(nnz, 256), 256, 0, c->stream>>>(nnz, keys, *tja_o);
+	k_gather_vals<<<nblk(nnz, 256), 256, 0, c->stream>>>(nnz, vals, a, *tv_o);
+	BSG_CUDA(cudaGetLastError());
+	BSG_CUDA(cudaFreeAsync(keys, c->stream));
+	BSG_CUDA(cudaFreeAsync(vals, c->stream));
+	return BSG_OK;
+}

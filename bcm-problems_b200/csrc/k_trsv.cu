@@ -173,6 +173,13 @@ int bsg_fct_finish(bsg_ctx *c, bsg_fct *f) {
 int bsg_fct_make_fp32(bsg_fct *f) {
 	if (f->fp32) return BSG_OK;
 	cudaStream_t s = f->ctx->stream;
+	if (f->has_t && f->kind == 1) { // the transposed forms are rebuilt in FP32 on next use
+		bsg_sell_free(&f->slt, s);
+		bsg_sell_free(&f->sut, s);
+		if (f->d_utr_v) cudaFreeAsync(f->d_utr_v, s);
+		f->d_utr_v = nullptr;
+		f->has_t = 0;
+	}
 	BSG_CUDA(cudaMallocAsync(&f->d_ur_f, sizeof(float) * (f->nnz > 0 ? f->nnz : 1), s));
 	BSG_CUDA(cudaMallocAsync(&f->d_lr_f, sizeof(float) * (f->nnz_strict > 0 ? f->nnz_strict : 1), s));
 	BSG_COUNT(2);
@@ -206,19 +213,23 @@ int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const dou
 	return bsg_sell_sweep(c->stream, lower ? &f->sl : &f->su, x, dinv, yin, 0, yout);
 }
 
-// Solve with L (lower != 0) or U.  x and y must not alias.  `work` (n
-// doubles) is needed for mode 1 with nsweeps > 2, and with nsweeps > 1 for an
-// FP32 factor, whose sweeps keep their intermediate iterates in FP32 there.
-int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
-                        double *work) {
+namespace {
+// A triangular operand: its rows (strict part, `skip` leading diagonal
+// entries), FP64 / FP32 values, inverse pivots and sliced copy.
+struct TriOp {
+	int lower;
+	const int *rp, *ci;
+	int skip;
+	const double *vd;
+	const float *vf;
+	const double *dinv;
+	const bsg_sell *sell;
+};
+
+int trisolve_impl(bsg_ctx *c, const bsg_fct *f, const TriOp &t, int mode, int nsweeps, const double *x, double *y,
+                  double *work) {
 	cudaStream_t s = c->stream;
 	const int n = f->n;
-	const int *rp = lower ? f->d_lr_i : f->d_ur_i;
-	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
-	const int skip = lower ? 0 : 1;
-	const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
-	const double *vd = lower ? f->d_lr_v : f->d_ur_v;
-	const float *vf = lower ? f->d_lr_f : f->d_ur_f;
 	const bool use32 = f->fp32 != 0;
 	if (mode == 0) {
 		BSG_COUNT(2); // fill + solve
@@ -229,40 +240,104 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 		int need = (n + 7) / 8;
 		if (grid > need) grid = need > 0 ? need : 1;
 		if (use32)
-			k_trsv_syncfree<float><<<grid, 256, 0, s>>>(n, lower, f->d_perm, rp, ci, vf, skip, dinv, x, y, claim, c->d_stat);
+			k_trsv_syncfree<float><<<grid, 256, 0, s>>>(n, t.lower, f->d_perm, t.rp, t.ci, t.vf, t.skip, t.dinv, x, y, claim,
+			                                           c->d_stat);
 		else
-			k_trsv_syncfree<double><<<grid, 256, 0, s>>>(n, lower, f->d_perm, rp, ci, vd, skip, dinv, x, y, claim, c->d_stat);
+			k_trsv_syncfree<double><<<grid, 256, 0, s>>>(n, t.lower, f->d_perm, t.rp, t.ci, t.vd, t.skip, t.dinv, x, y,
+			                                            claim, c->d_stat);
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}
 	if (nsweeps < 1) nsweeps = 1;
 	if (nsweeps > 2 && !work) return BSG_ERR_ARG;
 	if (nsweeps == 1) { // the first iterate only: y = D^{-1} x
 		BSG_COUNT(1);
-		k_scale_vec<<<BSG_SMS * 8, 256, 0, s>>>(n, x, dinv, y);
+		k_scale_vec<<<BSG_SMS * 8, 256, 0, s>>>(n, x, t.dinv, y);
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}
 	if (use32) {
 		// FP32 factor: FP32 iterates, ping-ponged in work (2 n floats)
 		if (!work) return BSG_ERR_ARG;
-		return bsg_sell_sweeps32(s, lower ? &f->sl : &f->su, x, dinv, nsweeps, reinterpret_cast<float *>(work), y);
+		return bsg_sell_sweeps32(s, t.sell, x, t.dinv, nsweeps, reinterpret_cast<float *>(work), y);
 	}
-	int grid = ((n + STREAM_ROWS - 1) / STREAM_ROWS + 7) / 8;
-	if (grid > BSG_SMS * 8) grid = BSG_SMS * 8;
-	if (grid < 1) grid = 1;
 	// nsweeps - 1 passes (the first two iterates share one), ping-pong so
 	// that the last pass lands in y
 	const int passes = nsweeps - 1;
 	double *bufs[2] = {y, work};
 	int cur = (passes + 1) % 2;
 	const double *yin = nullptr;
-	const bsg_sell *sm = lower ? &f->sl : &f->su;
-	(void)grid; (void)rp; (void)ci; (void)vf; (void)vd; (void)skip;
 	for (int p = 0; p < passes; p++) {
 		double *out = bufs[cur];
-		int rc = bsg_sell_sweep(s, sm, x, dinv, yin, p == 0, out);
+		int rc = bsg_sell_sweep(s, t.sell, x, t.dinv, yin, p == 0, out);
 		if (rc) return rc;
 		yin = out;
 		cur ^= 1;
 	}
 	return BSG_OK;
+}
+} // namespace
+
+// Solve with L (lower != 0) or U.  x and y must not alias.  `work` (n
+// doubles) is needed for mode 1 with nsweeps > 2, and with nsweeps > 1 for an
+// FP32 factor, whose sweeps keep their intermediate iterates in FP32 there.
+int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
+                        double *work) {
+	TriOp t;
+	t.lower = lower ? 1 : 0;
+	t.rp = lower ? f->d_lr_i : f->d_ur_i;
+	t.ci = lower ? f->d_lr_j : f->d_ur_j;
+	t.skip = lower ? 0 : 1;
+	t.vd = lower ? f->d_lr_v : f->d_ur_v;
+	t.vf = lower ? f->d_lr_f : f->d_ur_f;
+	t.dinv = lower ? f->d_dinv_l : f->d_dinv_u;
+	t.sell = lower ? &f->sl : &f->su;
+	return trisolve_impl(c, f, t, mode, nsweeps, x, y, work);
+}
+
+// The transposed forms of an ILU2 factor: U^T rows are the L-row pattern
+// with U's values (the transposition that built the L rows, applied to U),
+// L^T rows are U's own pattern with L's values.  IC2 factors need none
+// (U^T = L, L^T = U).
+static int fct_build_transposes(bsg_ctx *c, bsg_fct *f) {
+	if (f->has_t || f->kind == 0) { f->has_t = 1; return BSG_OK; }
+	cudaStream_t s = c->stream;
+	const int n = f->n;
+	int *perm = nullptr, nk = 0, *ti = nullptr, *tj = nullptr;
+	int rc = bsg_strict_transpose(c, n, f->d_iu, f->d_ju, f->nnz, &ti, &tj, &perm, &nk);
+	if (rc) return rc;
+	cudaFreeAsync(ti, s);
+	cudaFreeAsync(tj, s);
+	BSG_CUDA(cudaMallocAsync(&f->d_utr_v, sizeof(double) * (nk > 0 ? nk : 1), s));
+	BSG_COUNT(1);
+	k_permute<<<nb(nk, 256), 256, 0, s>>>(nk, perm, f->d_u, f->d_utr_v);
+	BSG_CUDA(cudaFreeAsync(perm, s));
+	const int fp32 = f->fp32 ? 1 : 0;
+	if (fp32) {
+		BSG_CUDA(cudaMallocAsync(&f->d_utr_f, sizeof(float) * (nk > 0 ? nk : 1), s));
+		BSG_CUDA(cudaMallocAsync(&f->d_l_f, sizeof(float) * (f->nnz > 0 ? f->nnz : 1), s));
+		BSG_COUNT(2);
+		k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(nk, f->d_utr_v, f->d_utr_f);
+		k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz, f->d_l, f->d_l_f);
+	}
+	rc = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_utr_v, 0, fp32, &f->slt, SELL_SIGMA);
+	if (!rc) rc = bsg_sell_build(c, n, f->d_iu, f->d_ju, f->d_l, 1, fp32, &f->sut, SELL_SIGMA);
+	if (rc) return rc;
+	BSG_CUDA(cudaGetLastError());
+	f->has_t = 1;
+	return BSG_OK;
+}
+
+int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y,
+                          double *work) {
+	if (f->kind == 0) return bsg_trisolve_launch(c, f, which == 0 ? 1 : 0, mode, nsweeps, x, y, work);
+	int rc = fct_build_transposes(c, f);
+	if (rc) return rc;
+	TriOp t;
+	if (which == 0) { // U^T: lower, L-row pattern, U's values, U's inverse pivots
+		t.lower = 1; t.rp = f->d_lr_i; t.ci = f->d_lr_j; t.skip = 0;
+		t.vd = f->d_utr_v; t.vf = f->d_utr_f; t.dinv = f->d_dinv_u; t.sell = &f->slt;
+	} else {          // L^T: upper, U's pattern, L's values, L's inverse pivots
+		t.lower = 0; t.rp = f->d_iu; t.ci = f->d_ju; t.skip = 1;
+		t.vd = f->d_l; t.vf = f->d_l_f; t.dinv = f->d_dinv_l; t.sell = &f->sut;
+	}
+	return trisolve_impl(c, f, t, mode, nsweeps, x, y, work);
 }

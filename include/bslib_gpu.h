@@ -51,7 +51,8 @@ typedef struct bsg_param {
 	double sclmin;    /* minimal scaling value (ILU2)                            */
 	double pivmin;    /* minimal pivot (ILU2)                                    */
 	int ittype;       /* CG stop rule: 0 relative, 1 absolute (recursive resid.) */
-	int sttype;       /* GMRES stop rule: 0 absolute, else relative              */
+	int sttype;       /* GMRES / Lanczos stop rule: 0 absolute, 1 relative; 2 max-norm
+	                     of the residual (Lanczos; GMRES: relative)                */
 	int niter;        /* maximal number of iterations                            */
 	double eps;       /* stopping tolerance                                      */
 	int ichk;         /* iterations between convergence checks                   */
@@ -66,7 +67,7 @@ typedef struct bsg_param {
 	int precision;    /* 0: FP64 factor values; 1: FP32 factor values, FP64 pivots */
 	int trisolve;     /* 0: exact sync-free level solve; 1: Jacobi sweeps         */
 	int nsweeps;      /* Jacobi sweeps per triangular solve when trisolve == 1   */
-	int krylov;       /* 0: method of the driver (PCG symm / GMRES nonsymm),
+	int krylov;       /* 0: method of the driver (PCG symm / Lanczos nonsymm),
 	                     1: GMRES(restart), 2: FGMRES(restart)                   */
 	int restart;      /* GMRES/FGMRES restart length m                           */
 	int true_residual;/* 1: recompute r = b - Ax in FP64 at every restart/stop   */
@@ -144,6 +145,11 @@ int bsg_fct_free(bsg_fct *f);
  * sweeps (approximate, fully parallel).  `work` may be NULL for mode 0. */
 int bsg_solve_l_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
 int bsg_solve_u_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
+/* Transposed solves: which 0 with U^T (SolveL applied to U's storage), 1 with
+ * L^T (SolveU applied to L's storage) -- the transposed preconditioner of
+ * Bslib/lanczos.cpp:266-270; same modes.  The transposed forms of an ILU2
+ * factor are built on first use. */
+int bsg_solve_t_dev(bsg_ctx *ctx, bsg_fct *f, int which, int mode, int nsweeps, const double *d_x, double *d_y);
 /* Sweep-mode solve (lower != 0: L, else U) that allocates nothing: the same
  * kernels as bsg_solve_l_dev / bsg_solve_u_dev with mode 1, with the work
  * vector taken from a fixed 2^21-row device array instead of the memory
@@ -163,6 +169,13 @@ int bsg_pcg_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *
  * counterpart of CSVector::BlockGMRES, Bslib/gmres.cpp:337). */
 int bsg_gmres_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x,
                   bsg_param *p);
+
+/* Preconditioned two-sided Lanczos (CSVector::Lanczos, Bslib/lanczos.cpp:34),
+ * the reference's iteration for nonsymmetric systems: M^{-1} = U^{-1} L^{-1}
+ * and its transpose, A and A^T, the iterate of least max-norm residual
+ * returned (weights = 1); stopping per sttype (0: ||r|| <= eps, 1: ||r|| <=
+ * eps ||r0||, 2: max |r_i| <= eps).  Point matrices; x0 = d_x on entry. */
+int bsg_lanczos_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x, bsg_param *p);
 
 /* Batched PCG (CSVector::Cg's recurrence, Bslib/cg.cpp:31-350, which handles
  * one right-hand side, :375-377): nrhs right-hand sides times nseg diagonal
@@ -187,7 +200,8 @@ int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs
 int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b,
                        double *x, bsg_param *p);
 /* CSVector::Solver(CSMatrixR&) (Bslib/solvers.cpp:1339): full CSR in,
- * CombineLU + ILU2 + GMRES(restart), solution out. */
+ * CombineLU + ILU2 + Lanczos (p->krylov == 0, as the reference) or
+ * GMRES(restart) / FGMRES (krylov 1 / 2), solution out. */
 int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
                    bsg_param *p);
 

@@ -556,3 +556,97 @@ int orc_fact_levels(int kind, int n, const int *ia, const int *ja, const double 
 	}
 	return rc;
 }
+
+/* y = A^T x (the gather-free transpose product of CSMatrixR::MvmAt). */
+void orc_mvm_t(int n, const int *ia, const int *ja, const double *a, const double *x, double *y) {
+	for (int i = 0; i < n; i++) y[i] = 0.0;
+	for (int i = 0; i < n; i++)
+		for (int j = ia[i]; j < ia[i + 1]; j++) y[ja[j]] += a[j] * x[i];
+}
+
+/* Preconditioned two-sided Lanczos of CSVector::Lanczos (Bslib/lanczos.cpp:34-370)
+ * with the factor in the reference layout (l, u on the pattern iu, ju: L by
+ * columns, U by rows, inverse pivots first) and the weight vector of the
+ * max-norm error equal to one.  Per iteration: delta-products with A and
+ * M^{-1} = U^{-1} L^{-1}, the scalars gamma / ro (:148-159), the three-term
+ * updates of the solution (:163-182) and of delta (:250-262), the true
+ * residual and its max-norm (:187-205), and the transposed products
+ * L^{-T} U^{-T} (SolveL on U, SolveU on L, :266-270) and A^T (:274).  The
+ * returned solution is the iterate of least max-norm residual, as in the
+ * reference (:210-214, :364-368).  Returns the iteration count; *errmin gets
+ * the least max-norm residual. */
+int orc_lanczos(int n, const int *ia, const int *ja, const double *a, const int *iu, const int *ju, const double *l,
+                const double *u, const double *b, double *x, double eps, int sttype, int niter, double *errmin_out) {
+	double *sol = (double *)calloc((size_t)n, sizeof(double)), *r = (double *)malloc(sizeof(double) * n);
+	double *good = (double *)malloc(sizeof(double) * n), *sol1 = (double *)calloc((size_t)n, sizeof(double));
+	double *D = (double *)malloc(sizeof(double) * n), *D1 = (double *)calloc((size_t)n, sizeof(double));
+	double *d = (double *)malloc(sizeof(double) * n), *d1 = (double *)calloc((size_t)n, sizeof(double));
+	double *img = (double *)malloc(sizeof(double) * n), *p = (double *)malloc(sizeof(double) * n);
+	for (int i = 0; i < n; i++) sol[i] = x[i];
+	orc_mvm(n, ia, ja, a, sol, r);
+	for (int i = 0; i < n; i++) r[i] = b[i] - r[i];
+	double errmin = 0.0, resini = 0.0;
+	for (int i = 0; i < n; i++) {
+		errmin = fabs(r[i]) > errmin ? fabs(r[i]) : errmin;
+		resini += r[i] * r[i];
+	}
+	resini = sqrt(resini);
+	for (int i = 0; i < n; i++) { good[i] = sol[i]; D[i] = r[i]; }
+	orc_solve_l(n, iu, ju, l, r, p);
+	orc_solve_u(n, iu, ju, u, p, d);
+	double gamma = 0.0, gamma1, ro = 1.0, delDel = 0.0, delDel1, resi = resini;
+	int k;
+	for (k = 1; k < niter; k++) {
+		orc_mvm(n, ia, ja, a, d, r);
+		orc_solve_l(n, iu, ju, l, r, p);
+		orc_solve_u(n, iu, ju, u, p, img);
+		gamma1 = gamma;
+		delDel1 = delDel;
+		delDel = 0.0;
+		double dtemp = 0.0;
+		for (int i = 0; i < n; i++) delDel += d[i] * D[i];
+		for (int i = 0; i < n; i++) dtemp += img[i] * D[i];
+		gamma = delDel / dtemp;
+		if (k > 1) ro = 1.0 / (1.0 - (gamma / gamma1) * (delDel / delDel1) / ro);
+		const double rogamma = ro * gamma, unitro = 1.0 - ro;
+		for (int i = 0; i < n; i++) {
+			const double t = sol[i];
+			sol[i] = (t * ro + sol1[i] * unitro) + d[i] * rogamma;
+			sol1[i] = t;
+		}
+		orc_mvm(n, ia, ja, a, sol, r);
+		double errloc = 0.0;
+		resi = 0.0;
+		for (int i = 0; i < n; i++) {
+			r[i] = b[i] - r[i];
+			errloc = fabs(r[i]) > errloc ? fabs(r[i]) : errloc;
+			resi += r[i] * r[i];
+		}
+		resi = sqrt(resi);
+		if (errloc < errmin) {
+			for (int i = 0; i < n; i++) good[i] = sol[i];
+			errmin = errloc;
+		}
+		const int brk = fabs(delDel) < 1.e-100 && fabs(delDel1) < 1.e-100;
+		if ((sttype == 2 && errmin <= eps) || (sttype == 0 && resi <= eps) || (sttype == 1 && resi <= eps * resini) ||
+		    brk)
+			break;
+		for (int i = 0; i < n; i++) {
+			const double t = d[i];
+			d[i] = (t * ro + d1[i] * unitro) - img[i] * rogamma;
+			d1[i] = t;
+		}
+		orc_solve_l(n, iu, ju, u, D, p);   /* U^T, U's storage read as L by columns */
+		orc_solve_u(n, iu, ju, l, p, r);   /* L^T, L's storage read as U by rows */
+		orc_mvm_t(n, ia, ja, a, r, img);
+		for (int i = 0; i < n; i++) {
+			const double t = D[i];
+			D[i] = (t * ro + D1[i] * unitro) - img[i] * rogamma;
+			D1[i] = t;
+		}
+	}
+	for (int i = 0; i < n; i++) x[i] = good[i];
+	if (errmin_out) *errmin_out = errmin;
+	free(sol); free(r); free(good); free(sol1); free(D); free(D1); free(d); free(d1); free(img); free(p);
+	return k;
+}

@@ -56,6 +56,14 @@ int orc_gmres(int n, const int *ia, const int *ja, const double *a, const int *i
               const double *u, const double *b, double *x, int m, double eps, int sttype, int niter,
               double *resfin);
 
+/* y = A^T x */
+void orc_mvm_t(int n, const int *ia, const int *ja, const double *a, const double *x, double *y);
+/* Preconditioned two-sided Lanczos (CSVector::Lanczos, Bslib/lanczos.cpp:34),
+ * weight vector of the max-norm error = 1; returns the iterations, x gets
+ * the iterate of least max-norm residual. */
+int orc_lanczos(int n, const int *ia, const int *ja, const double *a, const int *iu, const int *ju, const double *l,
+                const double *u, const double *b, double *x, double eps, int sttype, int niter, double *errmin);
+
 void orc_free(void *p);
 
 #ifdef __cplusplus

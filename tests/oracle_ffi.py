@@ -126,6 +126,15 @@ class Oracle:
         return x, it, res.value
 
 
+    def lanczos(self, ia, ja, a, iu, ju, l, u, b, eps=1e-8, sttype=1, niter=2000):
+        n = len(ia) - 1
+        x = np.zeros(n)
+        em = C.c_double()
+        it = self.lib.orc_lanczos(n, _i(ia), _i(ja), _d(a), _i(iu), _i(ju), _d(l), _d(u), _d(b), _d(x),
+                                  C.c_double(eps), sttype, niter, C.byref(em))
+        return x, it, em.value
+
+
 class RefLib:
     """The reference Bslib, compiled here from its sources (oracle/Makefile)."""
 

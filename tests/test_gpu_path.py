@@ -286,3 +286,85 @@ def test_bad_csr_rejected(ctx):
     with pytest.raises(bsg.BsgError) as e:
         bsg.Matrix(ctx, 2, np.array([0, 1, 2], np.int32), np.array([0, 5], np.int32), np.ones(2))
     assert e.value.code == bsg.ERR_ARG
+
+
+@pytest.mark.parametrize("precision,trisolve", [(0, 0), (1, 1)])
+def test_lanczos_matches_oracle(ctx, oracle, heat, precision, trisolve):
+    """CSVector::Lanczos on the GPU: with the FP64 factor and exact solves it
+    follows the oracle's recurrence (iterations +-1, same solution); with the
+    FP32 factor and Jacobi sweeps it still reaches the tolerance."""
+    import bsg
+    import torch
+    s = _nonsymmetric(heat, skew=0.4)
+    b = s.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, sttype=1, eps=1e-9, niter=500,
+                          precision=precision, trisolve=trisolve, nsweeps=6)
+    m = bsg.Matrix.from_system(ctx, s)
+    f = bsg.Factor(ctx, m, "ilu2", p)
+    x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+    bsg.lanczos(ctx, m, f, _t(b), x, p)
+    A = s.to_scipy()
+    xg = x.cpu().numpy()
+    r = b - A @ xg
+    assert np.all(np.isfinite(xg))
+    assert abs(p.resfin - np.linalg.norm(r) / np.linalg.norm(b)) <= 1e-12
+    # the returned iterate is the one of least max-norm residual (the
+    # reference's goodsol), recorded in resrec
+    assert abs(np.abs(r).max() - p.resrec) <= 1e-12 * np.abs(b).max()
+    sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, s.a)
+    oiu, oju, ol, ou, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    xo, it, _ = oracle.lanczos(s.ia, s.ja, s.a, oiu, oju, ol, ou, b, eps=1e-9, sttype=1)
+    if precision == 0:
+        assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b)
+        assert np.linalg.norm(xg - xo) <= 1e-6 * np.linalg.norm(xo)
+        assert abs(p.nitperf - it) <= 1, (p.nitperf, it)
+    else:
+        # FP32 factor applied by sweeps: the recurrence is less smooth, and the
+        # least-max-norm iterate can sit a little above the 2-norm target
+        assert np.linalg.norm(r) <= 1e-7 * np.linalg.norm(b)
+        assert np.linalg.norm(xg - xo) <= 1e-5 * np.linalg.norm(xo)
+
+
+def test_solver_driver_runs_lanczos(ctx, oracle, heat):
+    """bsg_solver_csr (CSVector::Solver): CombineLU + ILU2 + Lanczos by default."""
+    import bsg
+    s = _nonsymmetric(heat, skew=0.2)
+    b = s.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, sttype=1, eps=1e-9)
+    x = bsg.solver(ctx, s.n, s.ia, s.ja, s.a, b, p)
+    sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, s.a)
+    oiu, oju, ol, ou, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    xo, it, _ = oracle.lanczos(s.ia, s.ja, s.a, oiu, oju, ol, ou, b, eps=1e-9, sttype=1)
+    assert abs(p.nitperf - it) <= 1 and p.resfin <= 1e-8
+    assert np.linalg.norm(x - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+@pytest.mark.parametrize("precision,mode", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_transposed_solves_are_adjoint(ctx, oracle, heat, precision, mode):
+    """<y, U^{-1} x> = <U^{-T} y, x> and likewise for L, for exact solves and
+    sweeps, FP64 and FP32 factors; the exact FP64 transposed solves equal the
+    oracle's SolveL on U / SolveU on L."""
+    import bsg
+    import torch
+    s = _nonsymmetric(heat, skew=0.4)
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, precision=precision)
+    m = bsg.Matrix.from_system(ctx, s)
+    f = bsg.Factor(ctx, m, "ilu2", p)
+    rng = np.random.default_rng(8)
+    x, yv = rng.standard_normal(s.n), rng.standard_normal(s.n)
+    out = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    tol = 1e-12 if precision == 0 else 1e-5
+    for fwd, adj in ((f.solve_u, f.solve_ut), (f.solve_l, f.solve_lt)):
+        fwd(_t(x), out, mode=mode, nsweeps=4)
+        a = float(np.dot(yv, out.cpu().numpy()))
+        adj(_t(yv), out, mode=mode, nsweeps=4)
+        b = float(np.dot(out.cpu().numpy(), x))
+        assert abs(a - b) <= tol * max(abs(a), 1.0), (a, b)
+    if precision == 0 and mode == 0:
+        iu, ju, l, u = f.export()
+        f.solve_ut(_t(x), out, mode=0)
+        ref = oracle.solve_l(iu, ju, u, x)
+        assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+        f.solve_lt(_t(x), out, mode=0)
+        ref = oracle.solve_u(iu, ju, l, x)
+        assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()

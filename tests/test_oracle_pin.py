@@ -95,3 +95,28 @@ def test_live_reference_larger_case(oracle, reflib):
     x, info = reflib.solve_symm(u.ia, u.ja, u.a, s.rhs[0], memory=-1.0, eps=1e-10)
     xo, it, _ = oracle.pcg(u.ia, u.ja, u.a, oiu, oju, ouu, s.rhs[0], eps=1e-10)
     assert abs(it - info["iters"]) <= 1 and rel(xo, x) < 1e-9
+
+
+def test_lanczos_matches_reference_solver(oracle, gold):
+    """The oracle's restatement of CSVector::Lanczos against the reference's
+    own Solver (CombineLU + ILU2 + Lanczos) recorded in the fixture."""
+    g = gold
+    sia, sja, al, au = oracle.combine_lu(g["ia"], g["ja"], g["ns_a"])
+    iu, ju, lv, uv, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    x, it, _ = oracle.lanczos(g["ia"], g["ja"], g["ns_a"], iu, ju, lv, uv, g["b"], eps=1e-10, sttype=1)
+    assert abs(it - int(g["nonsymm_iters"])) <= 1
+    assert rel(x, g["nonsymm_x"]) < 1e-9
+
+
+def test_live_reference_lanczos_larger_case(oracle, reflib):
+    s = P.heat3d(12, 11, 10, sigma=1.0, seed=23)
+    rows = np.repeat(np.arange(s.n), np.diff(s.ia))
+    a = s.a.copy()
+    off = s.ja != rows
+    a[off] *= 1.0 + 0.4 * np.sign(s.ja[off] - rows[off])
+    x, info = reflib.solver(s.ia, s.ja, a, s.rhs[0], tau1=1e-3, tau2=1e-3, sttype=1, eps=1e-9)
+    sia, sja, al, au = oracle.combine_lu(s.ia, s.ja, a)
+    iu, ju, lv, uv, _ = oracle.fact(1, sia, sja, al, au, tau1=1e-3, tau2=1e-3)
+    xo, it, _ = oracle.lanczos(s.ia, s.ja, a, iu, ju, lv, uv, s.rhs[0], eps=1e-9, sttype=1)
+    assert abs(it - info["iters"]) <= 1
+    assert rel(xo, x) < 1e-7
