@@ -99,6 +99,7 @@ def lib():
         "bsg_pcg_batch_dev": (i_, [vp, vp, vp, i_, i_, ip, vp, vp, C.POINTER(Param), ip, dp, ip]),
         "bsg_lanczos_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
         "bsg_solve_t_dev": (i_, [vp, vp, i_, i_, i_, vp, vp]),
+        "bsg_sell_stats": (i_, [vp, vp, C.POINTER(C.c_longlong)]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -262,6 +263,14 @@ class Factor:
 
     def to_fp32(self):
         _check(lib().bsg_fct_to_fp32(self.h))
+
+    def sell_stats(self):
+        """Sliced copies of the factor: stored entries of the strict L / U
+        rows, tiles of their tiled FP32 form (0: untiled) and the most x
+        blocks one tile stages."""
+        out = (C.c_longlong * 6)()
+        _check(lib().bsg_sell_stats(None, self.h, out))
+        return dict(entries_l=out[1], entries_u=out[2], tiles_l=out[3], tiles_u=out[4], tile_blocks=out[5])
 
     def solve_l(self, x, y, mode=0, nsweeps=3):
         _check(lib().bsg_solve_l_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))

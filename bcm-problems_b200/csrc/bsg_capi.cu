@@ -29,12 +29,17 @@ unsigned long long g_bsg_launches = 0;
 extern "C" unsigned long long bsg_launch_count(void) { return g_bsg_launches; }
 
 // Stored entries (padding included) of the SELL copies: [0] the matrix,
-// [1] strict L rows, [2] strict U rows of the factor (0 where absent).
+// [1] strict L rows, [2] strict U rows of the factor (0 where absent);
+// [3] / [4] tiles of the tiled L / U form (0: untiled), [5] most staged x
+// blocks (32 floats) of one tile over both.
 extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out) {
 	if (!out) return bsg_set_error(BSG_ERR_ARG, "bsg_sell_stats: null output");
 	out[0] = m ? m->sell.entries : 0;
 	out[1] = f ? f->sl.entries : 0;
 	out[2] = f ? f->su.entries : 0;
+	out[3] = f ? f->sl.ntile : 0;
+	out[4] = f ? f->su.ntile : 0;
+	out[5] = f ? (f->sl.tmax > f->su.tmax ? f->sl.tmax : f->su.tmax) : 0;
 	return BSG_OK;
 }
 

@@ -100,7 +100,7 @@ struct bsg_ctx {
 	int spmv_group;          // autotuned sub-warp size for CSR SpMV (0 = choose per matrix)
 };
 
-// SELL-32: slices of 32 rows, entries column-major inside a slice (k_sell.cu).
+// SELL-8: slices of 8 rows, entries column-major inside a slice (k_sell.cu).
 struct bsg_sell {
 	int n = 0;
 	int fp32 = 0;
@@ -109,10 +109,22 @@ struct bsg_sell {
 	int *col = nullptr;
 	void *val = nullptr;      // float or double
 	int *perm = nullptr;      // slot -> row when rows are sorted by length in windows (SELL-C-sigma)
+	// Tiled form (FP32 sweeps): tiles of 256 slots; tile t reads x only in the
+	// 32-float blocks tb[tb_off[t] .. tb_off[t+1]), staged in shared memory,
+	// and its columns are 16-bit indices into that staging, two per word in
+	// cpair (slice widths even).  ntile == 0: no tiled form.
+	int ntile = 0;
+	int tmax = 0;             // most blocks of one tile
+	int tgrid = 0;            // persistent grid of the tiled sweep
+	int *tb_off = nullptr;
+	int *tb = nullptr;
+	unsigned *cpair = nullptr;
 };
-// sigma > 0: sort rows by length inside windows of sigma rows first
+// sigma > 0: sort rows by length inside windows of sigma rows first;
+// tiled != 0 (FP32 only, sigma dividing 256): also build the tiled form when
+// every tile's x blocks fit the staging limit
 int bsg_sell_build(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, int fp32,
-                   bsg_sell *out, int sigma = 0);
+                   bsg_sell *out, int sigma = 0, int tiled = 0);
 void bsg_sell_free(bsg_sell *m, cudaStream_t s);
 int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y);
 int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const double *yin,

@@ -18,12 +18,13 @@
 #include "bsg_internal.cuh"
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
 
 #define SELL_C 8
 
 namespace {
 
-__global__ void k_sell_width(int n, const int *rp, int skip, const int *perm, long long *width) {
+__global__ void k_sell_width(int n, const int *rp, int skip, const int *perm, int even, long long *width) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	const int slice = t / SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
@@ -32,7 +33,199 @@ __global__ void k_sell_width(int n, const int *rp, int skip, const int *perm, lo
 	if (len < 0) len = 0;
 #pragma unroll
 	for (int o = SELL_C / 2; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o, SELL_C));
+	if (even) len = (len + 1) & ~1;
 	if ((t % SELL_C) == 0 && slice < nsl) width[slice] = (long long)SELL_C * len;
+}
+
+// ---- tiled form ----------------------------------------------------------
+// A tile is SELL_TILE consecutive row slots (32 slices).  Its entries read x
+// only inside a few 32-float blocks (for stencil factors: a band around the
+// row and one around each neighbouring plane / line), so the tiled sweep
+// copies those blocks to shared memory with coalesced loads and gathers from
+// there, and each column shrinks to a 16-bit index into the staged blocks.
+#define SELL_TILE 256
+#define TB_MAX 512    // blocks per tile: 64 KB of staging, indices < 2^14
+#define TB_HASH 2048  // open-addressing table of a tile's distinct blocks
+
+__device__ __forceinline__ unsigned tb_hash(int key) { return ((unsigned)key * 2654435761u) >> 21; }
+
+// slot of key, inserted if new (count incremented); -1 if the table is full
+__device__ int tb_insert(int *hk, int key, int *count) {
+	unsigned h = tb_hash(key);
+	for (int i = 0; i < TB_HASH; i++) {
+		const int prev = atomicCAS(hk + h, -1, key);
+		if (prev == -1) {
+			atomicAdd(count, 1);
+			return (int)h;
+		}
+		if (prev == key) return (int)h;
+		h = (h + 1) & (TB_HASH - 1);
+	}
+	return -1;
+}
+
+__device__ int tb_find(const int *hk, int key) {
+	unsigned h = tb_hash(key);
+	for (int i = 0; i < TB_HASH; i++) {
+		const int k = hk[h];
+		if (k == key) return (int)h;
+		if (k == -1) return -1;
+		h = (h + 1) & (TB_HASH - 1);
+	}
+	return -1;
+}
+
+// FILL 0: cnt[t] = distinct x blocks of tile t (bad = 1 if a tile exceeds
+// TB_MAX).  FILL 1: tb[tb_off[t] ..] = those blocks ascending, and the packed
+// 16-bit local columns of every entry (padding: index 0, value 0 in sval).
+template <int FILL>
+__global__ void __launch_bounds__(SELL_TILE) k_tile_blocks(int n, const int *rp, const int *ci, int skip,
+                                                           const int *perm, const long long *off, int ntile, int *cnt,
+                                                           int *bad, const int *tb_off, int *tb, unsigned *cpair) {
+	__shared__ int hk[TB_HASH];
+	__shared__ int hr[TB_HASH];
+	__shared__ int lst[TB_MAX];
+	__shared__ int count, pos, fail;
+	const int nsl = (n + SELL_C - 1) / SELL_C;
+	const int tid = threadIdx.x;
+	for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+		for (int i = tid; i < TB_HASH; i += SELL_TILE) hk[i] = -1;
+		if (tid == 0) {
+			count = 0;
+			pos = 0;
+			fail = 0;
+		}
+		__syncthreads();
+		const int t = tile * SELL_TILE + tid;
+		const int r = t < n ? (perm ? perm[t] : t) : -1;
+		int b = 0, e = 0;
+		if (r >= 0) {
+			b = rp[r] + skip;
+			e = rp[r + 1];
+			if (e < b) e = b;
+		}
+		for (int j = b; j < e; j++)
+			if (tb_insert(hk, ci[j] >> 5, &count) < 0) fail = 1;
+		__syncthreads();
+		if (!FILL) {
+			if (tid == 0) {
+				cnt[tile] = count;
+				if (fail || count > TB_MAX) atomicExch(bad, 1);
+			}
+			__syncthreads();
+			continue;
+		}
+		// the host checked count <= TB_MAX for every tile
+		for (int i = tid; i < TB_HASH; i += SELL_TILE)
+			if (hk[i] != -1) lst[atomicAdd(&pos, 1)] = hk[i];
+		int P = 1;
+		while (P < count) P <<= 1;
+		__syncthreads();
+		for (int i = count + tid; i < P; i += SELL_TILE) lst[i] = 0x7fffffff;
+		__syncthreads();
+		for (int k = 2; k <= P; k <<= 1) // bitonic sort, ascending
+			for (int jj = k >> 1; jj > 0; jj >>= 1) {
+				for (int i = tid; i < P; i += SELL_TILE) {
+					const int ixj = i ^ jj;
+					if (ixj > i) {
+						const int a = lst[i], c = lst[ixj];
+						if ((a > c) == ((i & k) == 0)) {
+							lst[i] = c;
+							lst[ixj] = a;
+						}
+					}
+				}
+				__syncthreads();
+			}
+		const int tb0 = tb_off[tile];
+		for (int i = tid; i < count; i += SELL_TILE) {
+			tb[tb0 + i] = lst[i];
+			hr[tb_find(hk, lst[i])] = i;
+		}
+		__syncthreads();
+		const int slice = t / SELL_C, l = t % SELL_C;
+		if (slice < nsl) {
+			const long long base = off[slice];
+			const int w = (int)((off[slice + 1] - base) / SELL_C);
+			unsigned *cp = cpair + base / 2 + l;
+			const int len = e - b;
+			for (int k = 0; k < w; k += 2) {
+				unsigned lo = 0, hi = 0;
+				if (k < len) {
+					const int c = ci[b + k];
+					lo = (unsigned)(hr[tb_find(hk, c >> 5)] * 32 + (c & 31));
+				}
+				if (k + 1 < len) {
+					const int c = ci[b + k + 1];
+					hi = (unsigned)(hr[tb_find(hk, c >> 5)] * 32 + (c & 31));
+				}
+				cp[SELL_C * (k / 2)] = lo | (hi << 16);
+			}
+		}
+		__syncthreads();
+	}
+}
+
+// The FP32-iterate Jacobi pass of k_sell_sweep32 on the tiled form: per
+// tile, stage its x blocks in shared memory, then every thread forms one
+// row slot's sum from 4-byte values and 2-byte local columns.  The products
+// are summed in the same order as k_sell_sweep32, so the results agree bit
+// for bit.
+template <int OUT64>
+__global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, const int *__restrict__ perm,
+                                                             const long long *__restrict__ off,
+                                                             const unsigned *__restrict__ cpair,
+                                                             const float *__restrict__ sval,
+                                                             const int *__restrict__ tb_off,
+                                                             const int *__restrict__ tb, const float *__restrict__ x32,
+                                                             const double *__restrict__ rhs,
+                                                             const double *__restrict__ dinv, double *__restrict__ y,
+                                                             float *__restrict__ y32) {
+	extern __shared__ float sx[];
+	const int nsl = (n + SELL_C - 1) / SELL_C;
+	for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+		const int b0 = __ldg(tb_off + tile), nbk = __ldg(tb_off + tile + 1) - b0;
+		__syncthreads(); // the previous tile's gathers are done
+		for (int i = threadIdx.x; i < nbk * 32; i += SELL_TILE) {
+			const int c = __ldg(tb + b0 + (i >> 5)) * 32 + (i & 31);
+			sx[i] = c < n ? __ldg(x32 + c) : 0.f;
+		}
+		__syncthreads();
+		const int t = tile * SELL_TILE + threadIdx.x;
+		const int slice = t / SELL_C, l = t % SELL_C;
+		if (slice < nsl) {
+			const long long base = __ldg(off + slice);
+			const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+			const float *vp = sval + base + l;
+			const unsigned *cp = cpair + base / 2 + l;
+			double sum = 0.0;
+			int k = 0;
+			for (; k + 8 <= w; k += 8) {
+				unsigned cc[4];
+				float a[8];
+#pragma unroll
+				for (int u = 0; u < 4; u++) cc[u] = __ldcs(cp + SELL_C * (k / 2 + u));
+#pragma unroll
+				for (int u = 0; u < 8; u++) a[u] = __ldcs(vp + SELL_C * (k + u));
+#pragma unroll
+				for (int u = 0; u < 4; u++) {
+					sum = fma((double)a[2 * u], (double)sx[cc[u] & 0xffffu], sum);
+					sum = fma((double)a[2 * u + 1], (double)sx[cc[u] >> 16], sum);
+				}
+			}
+			for (; k < w; k += 2) {
+				const unsigned cc = __ldcs(cp + SELL_C * (k / 2));
+				sum = fma((double)__ldcs(vp + SELL_C * k), (double)sx[cc & 0xffffu], sum);
+				sum = fma((double)__ldcs(vp + SELL_C * (k + 1)), (double)sx[cc >> 16], sum);
+			}
+			if (t < n) {
+				const int r = perm ? __ldg(perm + t) : t;
+				const double v = (rhs[r] - sum) * dinv[r];
+				if (OUT64) y[r] = v;
+				else y32[r] = (float)v;
+			}
+		}
+	}
 }
 
 template <typename VT>
@@ -190,9 +383,87 @@ __global__ void k_len_keys(int n, const int *rp, int skip, int sigma, unsigned l
 	vals[r] = r;
 }
 
+static void bsg_sell_untile(bsg_sell *m, cudaStream_t s) {
+	if (m->tb_off) cudaFreeAsync(m->tb_off, s);
+	if (m->tb) cudaFreeAsync(m->tb, s);
+	if (m->cpair) cudaFreeAsync(m->cpair, s);
+	m->tb_off = nullptr;
+	m->tb = nullptr;
+	m->cpair = nullptr;
+	m->ntile = 0;
+	m->tmax = 0;
+	m->tgrid = 0;
+}
+
+// The tiled form of a built SELL matrix (widths even).  A tile whose entries
+// touch more than TB_MAX blocks of x leaves the matrix untiled (the sweeps
+// then gather from global memory): that is not an error.
+static int bsg_sell_tile(bsg_ctx *c, int n, const int *rp, const int *ci, int skip, bsg_sell *m) {
+	cudaStream_t s = c->stream;
+	const int ntile = (n + SELL_TILE - 1) / SELL_TILE;
+	const int grid = ntile < BSG_SMS * 8 ? ntile : BSG_SMS * 8;
+	int *cnt = nullptr, *bad = nullptr;
+	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int) * (ntile + 1), s));
+	BSG_CUDA(cudaMallocAsync(&bad, sizeof(int), s));
+	BSG_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+	BSG_CUDA(cudaMemsetAsync(cnt + ntile, 0, sizeof(int), s));
+	BSG_COUNT(1);
+	k_tile_blocks<0><<<grid, SELL_TILE, 0, s>>>(n, rp, ci, skip, m->perm, m->off, ntile, cnt, bad, nullptr, nullptr,
+	                                            nullptr);
+	BSG_CUDA(cudaGetLastError());
+	int hbad = 0;
+	BSG_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	cudaFreeAsync(bad, s);
+	if (hbad) {
+		cudaFreeAsync(cnt, s);
+		return BSG_OK;
+	}
+	// most blocks of a tile, then the offsets (exclusive scan)
+	int *dmax = nullptr;
+	void *tmp = nullptr;
+	size_t t1 = 0, t2 = 0;
+	BSG_CUDA(cudaMallocAsync(&dmax, sizeof(int), s));
+	BSG_CUDA(cudaMallocAsync(&m->tb_off, sizeof(int) * (ntile + 1), s));
+	BSG_CUDA(cub::DeviceReduce::Max(nullptr, t1, cnt, dmax, ntile, s));
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, cnt, m->tb_off, ntile + 1, s));
+	BSG_CUDA(cudaMallocAsync(&tmp, (t1 > t2 ? t1 : t2) + 1, s));
+	BSG_CUDA(cub::DeviceReduce::Max(tmp, t1, cnt, dmax, ntile, s));
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, t2, cnt, m->tb_off, ntile + 1, s));
+	int h[2] = {0, 0};
+	BSG_CUDA(cudaMemcpyAsync(h, dmax, sizeof(int), cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaMemcpyAsync(h + 1, m->tb_off + ntile, sizeof(int), cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	cudaFreeAsync(tmp, s);
+	cudaFreeAsync(dmax, s);
+	cudaFreeAsync(cnt, s);
+	m->ntile = ntile;
+	m->tmax = h[0];
+	BSG_CUDA(cudaMallocAsync(&m->tb, sizeof(int) * (h[1] > 0 ? h[1] : 1), s));
+	BSG_CUDA(cudaMallocAsync(&m->cpair, sizeof(unsigned) * (m->entries / 2 > 0 ? m->entries / 2 : 1), s));
+	BSG_COUNT(1);
+	k_tile_blocks<1><<<grid, SELL_TILE, 0, s>>>(n, rp, ci, skip, m->perm, m->off, ntile, nullptr, nullptr, m->tb_off,
+	                                            m->tb, m->cpair);
+	BSG_CUDA(cudaGetLastError());
+	// persistent grid: as many tiles at once as the staging lets reside
+	const size_t smem = (size_t)m->tmax * 32 * sizeof(float);
+	if (smem > 48 * 1024)
+		BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	if (smem > 48 * 1024)
+		BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	int per_sm = 0;
+	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tsell_sweep32<0>, SELL_TILE, smem));
+	if (per_sm < 1) {
+		bsg_sell_untile(m, s);
+		return BSG_OK;
+	}
+	m->tgrid = ntile < BSG_SMS * per_sm ? ntile : BSG_SMS * per_sm;
+	return BSG_OK;
+}
+
 template <typename VT>
 int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, bsg_sell *out,
-                     int sigma) {
+                     int sigma, int tiled) {
 	cudaStream_t s = c->stream;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
 	out->perm = nullptr;
@@ -220,7 +491,7 @@ int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const doub
 	BSG_CUDA(cudaMallocAsync(&out->off, sizeof(long long) * (nsl + 1), s));
 	BSG_CUDA(cudaMemsetAsync(width + nsl, 0, sizeof(long long), s));
 	BSG_COUNT(2);
-	k_sell_width<<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, skip, out->perm, width);
+	k_sell_width<<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, skip, out->perm, tiled, width);
 	// off = exclusive scan of the slice sizes
 	size_t tmp = 0;
 	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, width, out->off, nsl + 1, s));
@@ -240,16 +511,19 @@ int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const doub
 	BSG_CUDA(cudaGetLastError());
 	BSG_CUDA(cudaFreeAsync(width, s));
 	BSG_CUDA(cudaFreeAsync(d_tmp, s));
-	return BSG_OK;
+	return tiled ? bsg_sell_tile(c, n, rp, ci, skip, out) : BSG_OK;
 }
 
 int bsg_sell_build(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, int fp32,
-                   bsg_sell *out, int sigma) {
-	return fp32 ? bsg_sell_build_t<float>(c, n, rp, ci, v, skip, out, sigma)
-	            : bsg_sell_build_t<double>(c, n, rp, ci, v, skip, out, sigma);
+                   bsg_sell *out, int sigma, int tiled) {
+	// the tiles must hold whole sorting windows
+	tiled = tiled && fp32 && n > 0 && (sigma <= 0 || (SELL_TILE % sigma) == 0);
+	return fp32 ? bsg_sell_build_t<float>(c, n, rp, ci, v, skip, out, sigma, tiled)
+	            : bsg_sell_build_t<double>(c, n, rp, ci, v, skip, out, sigma, 0);
 }
 
 void bsg_sell_free(bsg_sell *m, cudaStream_t s) {
+	bsg_sell_untile(m, s);
 	if (m->perm) cudaFreeAsync(m->perm, s);
 	m->perm = nullptr;
 	if (m->off) cudaFreeAsync(m->off, s);
@@ -307,10 +581,21 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 	float *a = work32, *b = work32 + n;
 	BSG_COUNT(nsweeps);
 	k_scale32<<<nb(n, 256) < BSG_SMS * 16 ? nb(n, 256) : BSG_SMS * 16, 256, 0, s>>>(n, x, dinv, b);
+	const size_t smem = (size_t)m->tmax * 32 * sizeof(float);
 	for (int pass = 0; pass < nsweeps - 1; pass++) {
 		const bool last = pass == nsweeps - 2;
-		if (last) k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr);
-		else k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a);
+		if (m->ntile) {
+			if (last)
+				k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
+				                                                     m->tb, b, x, dinv, yout, nullptr);
+			else
+				k_tsell_sweep32<0><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
+				                                                     m->tb, b, x, dinv, nullptr, a);
+		} else if (last) {
+			k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr);
+		} else {
+			k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a);
+		}
 		float *t = a; a = b; b = t;
 	}
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
@@ -320,8 +605,12 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const float *x32,
                           double *yout) {
 	BSG_COUNT(1);
-	k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x, dinv,
-	                                                  yout, nullptr);
+	if (m->ntile)
+		k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, (size_t)m->tmax * 32 * sizeof(float), s>>>(
+		    m->n, m->ntile, m->perm, m->off, m->cpair, (const float *)m->val, m->tb_off, m->tb, x32, x, dinv, yout, nullptr);
+	else
+		k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x,
+		                                                  dinv, yout, nullptr);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
 

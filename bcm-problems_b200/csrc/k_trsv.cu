@@ -189,8 +189,8 @@ int bsg_fct_make_fp32(bsg_fct *f) {
 	// the sweeps read the SELL copies: rebuild them with FP32 values
 	bsg_sell_free(&f->sl, s);
 	bsg_sell_free(&f->su, s);
-	int rc = bsg_sell_build(f->ctx, f->n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 1, &f->sl, SELL_SIGMA);
-	if (!rc) rc = bsg_sell_build(f->ctx, f->n, f->d_iu, f->d_ju, f->d_u, 1, 1, &f->su, SELL_SIGMA);
+	int rc = bsg_sell_build(f->ctx, f->n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 1, &f->sl, SELL_SIGMA, 1);
+	if (!rc) rc = bsg_sell_build(f->ctx, f->n, f->d_iu, f->d_ju, f->d_u, 1, 1, &f->su, SELL_SIGMA, 1);
 	if (rc) return rc;
 	f->fp32 = 1;
 	return BSG_OK;
@@ -318,8 +318,8 @@ static int fct_build_transposes(bsg_ctx *c, bsg_fct *f) {
 		k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(nk, f->d_utr_v, f->d_utr_f);
 		k_to_f32<<<BSG_SMS * 4, 256, 0, s>>>(f->nnz, f->d_l, f->d_l_f);
 	}
-	rc = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_utr_v, 0, fp32, &f->slt, SELL_SIGMA);
-	if (!rc) rc = bsg_sell_build(c, n, f->d_iu, f->d_ju, f->d_l, 1, fp32, &f->sut, SELL_SIGMA);
+	rc = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_utr_v, 0, fp32, &f->slt, SELL_SIGMA, fp32);
+	if (!rc) rc = bsg_sell_build(c, n, f->d_iu, f->d_ju, f->d_l, 1, fp32, &f->sut, SELL_SIGMA, fp32);
 	if (rc) return rc;
 	BSG_CUDA(cudaGetLastError());
 	f->has_t = 1;

@@ -333,7 +333,13 @@ def main():
     L.bsg_fct_info(fh, C.byref(fn), C.byref(fnnz), None, None, None, None)
     nnz_strict = fnnz.value - n
     spmv_bytes = nnz.value * 12 + (n + 1) * 4 + 2 * n * 8
-    sweep_bytes = nnz_strict * 8 + (n + 1) * 4 + 3 * n * 8 + n * 4  # fp32 value + col, dinv, x, y_out, fp32 y_in
+    st = (C.c_longlong * 6)()
+    bsg._check(L.bsg_sell_stats(None, fh, st))
+    tiled = st[4] > 0  # the backward sweep timed below
+    if tiled:  # fp32 value + 16-bit local column; rhs, dinv, y_out; fp32 y_in (staged once per tile)
+        sweep_bytes = nnz_strict * 6 + 3 * n * 8 + n * 4
+    else:  # fp32 value + int32 column, row pointers; rhs, dinv, y_out; fp32 y_in
+        sweep_bytes = nnz_strict * 8 + (n + 1) * 4 + 3 * n * 8 + n * 4
     peak, peak_kind = peaks()
     spmv_gbs = spmv_bytes / (t_spmv.value * 1e-3) / 1e9
     sweep_gbs = sweep_bytes / (t_sweep.value * 1e-3) / 1e9
@@ -392,7 +398,9 @@ def main():
                          "peak": peak, "unit": "GB/s", "frac": round(spmv_gbs / peak, 4), "traffic": None,
                          "algorithmic_bytes": spmv_bytes, "ms_per_launch": t_spmv.value,
                          "peak_source": peak_kind},
-            "roofline_trisolve": {"bound": "hbm", "kernel": "k_sell_sweep32 (one FP32 Jacobi sweep)",
+            "roofline_trisolve": {"bound": "hbm",
+                                  "kernel": ("k_tsell_sweep32 (one FP32 Jacobi sweep, x staged in shared memory)"
+                                             if tiled else "k_sell_sweep32 (one FP32 Jacobi sweep)"),
                                   "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                   "frac": round(sweep_gbs / peak, 4), "algorithmic_bytes": sweep_bytes,
                                   "ms_per_launch": t_sweep.value},

@@ -241,7 +241,10 @@ int bsg_time_kernel(bsg_ctx *ctx, int kind, const bsg_mat *m, const bsg_fct *f, 
 /* Scheduler counters of the last factorisation (see k_fact.cu). */
 int bsg_fact_stats(unsigned long long *out, int nout);
 /* Stored entries, padding included, of the sliced copies the bandwidth-bound
- * products read: out[0] matrix, out[1] strict L, out[2] strict U. */
+ * products read: out[0] matrix, out[1] strict L, out[2] strict U; out[3] /
+ * out[4] tiles of the tiled FP32 L / U sweeps (0: untiled, columns gathered
+ * from global memory), out[5] most 32-float x blocks one tile stages.
+ * out holds 6 values. */
 int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out);
 
 #ifdef __cplusplus

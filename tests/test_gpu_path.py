@@ -209,6 +209,81 @@ def test_trisolve_jacobi_converges(ctx, oracle, heat):
     assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-10
 
 
+def _sweeps_fp32(N, dinv, x, nsweeps):
+    """The FP32-iterate Jacobi recurrence of a triangular solve: y0 =
+    fl32(D^-1 x), y_k = D^-1 (x - N y_(k-1)) with FP32 values of N and FP64
+    products, rounded to FP32 except the last of nsweeps iterates."""
+    y = (x * dinv).astype(np.float32)
+    for k in range(nsweeps - 1):
+        v = (x - N @ y.astype(np.float64)) * dinv
+        y = v if k == nsweeps - 2 else v.astype(np.float32)
+    return y
+
+
+def _strict_parts32(iu, ju, l, u):
+    """Strict lower rows (from L's columns) and strict upper rows of a factor
+    in the reference layout, values rounded to FP32; inverse pivots."""
+    import scipy.sparse as sp
+    n = len(iu) - 1
+    rows = np.repeat(np.arange(n), np.diff(iu))
+    off = ju != rows
+    f32 = lambda v: v[off].astype(np.float32).astype(np.float64)
+    NU = sp.csr_matrix((f32(u), (rows[off], ju[off])), shape=(n, n))
+    NL = sp.csr_matrix((f32(l), (ju[off], rows[off])), shape=(n, n))
+    return NL, NU, l[iu[:-1]], u[iu[:-1]]
+
+
+def _random_graph(n, deg, seed):
+    """SPD matrix on a random graph (each row joined to `deg` random rows, weak
+    couplings): the columns a row tile reads are spread over the whole vector."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    i = np.repeat(np.arange(n), deg)
+    j = rng.integers(0, n, n * deg)
+    keep = i != j
+    W = sp.coo_matrix((-rng.uniform(0.02, 0.05, keep.sum()), (i[keep], j[keep])), shape=(n, n)).tocsr()
+    W = (W + W.T).tocsr()
+    W.sum_duplicates()
+    A = (W + sp.diags(np.asarray(abs(W).sum(axis=1)).ravel() + 1.0)).tocsr()
+    A.sort_indices()
+    ia, ja, a = [], [], []
+    for r in range(n):  # each row's diagonal first
+        c, v = A.indices[A.indptr[r]:A.indptr[r + 1]], A.data[A.indptr[r]:A.indptr[r + 1]]
+        d = c == r
+        ja.append(np.concatenate([c[d], c[~d]]))
+        a.append(np.concatenate([v[d], v[~d]]))
+    ia = np.concatenate([[0], np.cumsum([len(c) for c in ja])]).astype(np.int32)
+    return P.System(n, 1, ia, np.concatenate(ja).astype(np.int32), np.concatenate(a), np.zeros((1, n)), None)
+
+
+@pytest.mark.parametrize("case", ["heat", "random"])
+def test_fp32_sweeps_match_restated_recurrence(ctx, heat, case):
+    """The FP32-factor sweeps (tiled, with x staged in shared memory, for the
+    stencil factor; gathered from global memory where a tile would stage too
+    many x blocks, for the random graph) equal the restated recurrence."""
+    import bsg
+    import torch
+    s = heat if case == "heat" else _random_graph(60000, 4, 21)
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, precision=1)
+    m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    st = f.sell_stats()
+    if case == "heat":
+        assert st["tiles_l"] > 0 and st["tiles_u"] > 0
+    else:
+        assert st["tiles_l"] == 0 and st["tiles_u"] == 0
+    NL, NU, dl, du = _strict_parts32(*f.export())
+    x = np.random.default_rng(6).standard_normal(s.n)
+    y = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    for sw in (2, 3, 6):
+        f.solve_l(_t(x), y, mode=1, nsweeps=sw)
+        ref = _sweeps_fp32(NL, dl, x, sw)
+        assert np.abs(y.cpu().numpy() - ref).max() <= 1e-6 * np.abs(ref).max(), ("L", sw)
+        f.solve_u(_t(x), y, mode=1, nsweeps=sw)
+        ref = _sweeps_fp32(NU, du, x, sw)
+        assert np.abs(y.cpu().numpy() - ref).max() <= 1e-6 * np.abs(ref).max(), ("U", sw)
+
+
 def test_pcg_matches_oracle(ctx, oracle, heat):
     import bsg
     import torch
