@@ -446,11 +446,13 @@ static int bsg_sell_tile(bsg_ctx *c, int n, const int *rp, const int *ci, int sk
 	                                            m->tb, m->cpair);
 	BSG_CUDA(cudaGetLastError());
 	// persistent grid: as many tiles at once as the staging lets reside
+	// the limit covers every tiled form: the L and U copies of one factor
+	// (and other factors) stage different amounts, and the attribute is per
+	// kernel, not per launch
 	const size_t smem = (size_t)m->tmax * 32 * sizeof(float);
-	if (smem > 48 * 1024)
-		BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	if (smem > 48 * 1024)
-		BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	const int smem_cap = TB_MAX * 32 * (int)sizeof(float);
+	BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+	BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
 	int per_sm = 0;
 	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tsell_sweep32<0>, SELL_TILE, smem));
 	if (per_sm < 1) {
@@ -550,7 +552,8 @@ int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y)
 	else
 		k_sell_apply<double, 0, 0><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const double *)m->val, x,
 		                                                           nullptr, nullptr, nullptr, y);
-	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
 }
 
 // One Jacobi pass yout = (x - N yin) * dinv; scaled_in: yin = x * dinv.
@@ -567,7 +570,8 @@ int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const dou
 		if (scaled_in) k_sell_apply<double, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout);
 		else k_sell_apply<double, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout);
 	}
-	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
 }
 
 // Jacobi sweeps of an FP32 factor with FP32 iterates: nsweeps >= 2 iterates
@@ -598,7 +602,8 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 		}
 		float *t = a; a = b; b = t;
 	}
-	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
 }
 
 // One full FP32-iterate pass (timing of the sweep kernel alone).
@@ -611,7 +616,8 @@ int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, co
 	else
 		k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x,
 		                                                  dinv, yout, nullptr);
-	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
 }
 
 // Stored entries (with padding) of a SELL matrix: the bytes a product reads.
