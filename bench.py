@@ -403,6 +403,9 @@ def main():
                                              if tiled else "k_sell_sweep32 (one FP32 Jacobi sweep)"),
                                   "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
                                   "frac": round(sweep_gbs / peak, 4), "algorithmic_bytes": sweep_bytes,
+                                  # dram read + write of one launch, ncu at this workload (128^3)
+                                  "traffic": (382960000 if tiled and args.grid == 128 else None),
+                                  "traffic_source": "profiles/k_tsell_sweep32_heat128.md",
                                   "ms_per_launch": t_sweep.value},
             "roofline_unet": {"bound": "tensor", "kernel": "U-Net forward (k_conv3t / k_conv3, bf16 mma)",
                               "achieved": round(conv_tflops, 1), "peak": bf16_peak, "unit": "TFLOP/s",
