@@ -57,6 +57,43 @@ int fail(const char *msg) {
 	return -1;
 }
 
+// Block CSR (CSMatrixRS, Bslib/smatrix.h:1040-1048) with a uniform block
+// size: blocks column-major, block k of the arrays at a[k * bs * bs].  The
+// reference keeps the partition in protected members, so a derived type
+// fills them.
+struct RSBuild : public CSMatrixRS {
+	RSBuild(int nsup, int bs, const int *ia_, const int *ja_, const double *a_)
+	    : CSMatrixRS(nsup, ia_[nsup], ia_[nsup] * bs * bs) {
+		const int nzj = ia_[nsup], nz = nzj * bs * bs;
+		m = n = nsup * bs;
+		nsupr = nsupc = nsup;
+		nlist = nsup;
+		nzja = nzj;
+		nza = nzatot = nz;
+		blamx = bs;
+		for (int i = 0; i < nsup; i++) list[i] = i;
+		std::memcpy(ia, ia_, sizeof(int) * (nsup + 1));
+		std::memcpy(ja, ja_, sizeof(int) * nzj);
+		std::memcpy(a, a_, sizeof(double) * nz);
+		for (int j = 0; j < nzj; j++) bsa[j] = j * bs * bs;
+		for (int i = 0; i <= nsup; i++) sprndr[i] = sprndc[i] = i * bs;
+	}
+	// block CSR of any CSMatrixRS with a uniform block size, blocks in row order
+	static void export_rs(const CSMatrixRS &m, int bs, int **ia_o, int **ja_o, double **a_o) {
+		CSMatrixRS &mm = const_cast<CSMatrixRS &>(m);
+		const int nsup = mm.GetNsupr();
+		const int *ia = mm.GetIa(), *ja = mm.GetJa(), *bsa = mm.GetBsa();
+		const double *a = mm.GetA();
+		const int nzj = ia[nsup], b2 = bs * bs;
+		*ia_o = (int *)std::malloc(sizeof(int) * (nsup + 1));
+		*ja_o = (int *)std::malloc(sizeof(int) * (nzj > 0 ? nzj : 1));
+		*a_o = (double *)std::malloc(sizeof(double) * (nzj > 0 ? nzj * b2 : 1));
+		std::memcpy(*ia_o, ia, sizeof(int) * (nsup + 1));
+		std::memcpy(*ja_o, ja, sizeof(int) * nzj);
+		for (int j = 0; j < nzj; j++) std::memcpy(*a_o + (size_t)j * b2, a + bsa[j], sizeof(double) * b2);
+	}
+};
+
 } // namespace
 
 extern "C" {
@@ -216,6 +253,70 @@ int ref_solver(int n, const int *ia, const int *ja, const double *a, const doubl
 	} catch (const char *e) {
 		return fail(e);
 	}
+}
+
+// CombineLU of a block matrix (Bslib/smatrixrs.cpp:1645): upper blocks as
+// they are, lower blocks transposed, both patterns extended to their union.
+int ref_combine_lu_block(int nsup, int bs, const int *ia, const int *ja, const double *a, int **ia_s, int **ja_s,
+                         double **al, double **au) {
+	try {
+		RSBuild m(nsup, bs, ia, ja, a);
+		CSMatrixRS l, u;
+		m.CombineLU(l, u);
+		int *ial, *jal;
+		RSBuild::export_rs(l, bs, &ial, &jal, al);
+		RSBuild::export_rs(u, bs, ia_s, ja_s, au);
+		std::free(ial);
+		std::free(jal);
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// CombineLU + block ILU2 (Bslib/ilu2rs.cpp:1458) of a full-stored block
+// matrix; L and U come back with the same pattern (diagonal block first).
+int ref_ilu2_block(int nsup, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
+                   double theta, double memory, double sclmin, double pivmin, int **ia_f, int **ja_f, double **a_l,
+                   double **a_u, double *stats) {
+	try {
+		RSBuild m(nsup, bs, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		p.sclmin = sclmin; p.pivmin = pivmin;
+		CSMatrixRS al, au, l, u, dummy;
+		m.CombineLU(al, au);
+		std::ofstream fout("/dev/null");
+		double t0 = now_s();
+		dummy.Ilu2(fout, p, al, au, l, u);
+		double t1 = now_s();
+		int *ial, *jal;
+		RSBuild::export_rs(l, bs, &ial, &jal, a_l);
+		RSBuild::export_rs(u, bs, ia_f, ja_f, a_u);
+		std::free(ial);
+		std::free(jal);
+		if (stats) { stats[0] = p.density; stats[1] = p.density2; stats[2] = t1 - t0; }
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// Block triangular solves with a block factor (CSMatrixRS::SolveL,
+// Bslib/mvm.cpp:3140; SolveU, :3410).
+int ref_solve_l_block(int nsup, int bs, const int *ia, const int *ja, const double *a, const double *x, double *y) {
+	RSBuild m(nsup, bs, ia, ja, a);
+	CSVector vx = make_vec(nsup * bs, x), vy(nsup * bs);
+	m.SolveL(vx, vy);
+	std::memcpy(y, vy.GetVect(), sizeof(double) * nsup * bs);
+	return 0;
+}
+int ref_solve_u_block(int nsup, int bs, const int *ia, const int *ja, const double *a, const double *x, double *y) {
+	RSBuild m(nsup, bs, ia, ja, a);
+	CSVector vx = make_vec(nsup * bs, x), vy(nsup * bs);
+	m.SolveU(vx, vy);
+	std::memcpy(y, vy.GetVect(), sizeof(double) * nsup * bs);
+	return 0;
 }
 
 } // extern "C"

@@ -6,7 +6,8 @@ solver, compiled from its sources into oracle/_ref/libbslib_ref.so
 are stored as fixtures.  The GPU box has no reference sources; the fixtures
 let every machine check the oracle against the reference.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (all fixtures)
+    python tests/golden/make_golden.py --block    (lame_block.npz only)
 """
 import os
 import sys
@@ -66,5 +67,41 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def nonsymmetric_blocks(s, skew=0.3):
+    a = s.a.reshape(-1, s.bs, s.bs).copy()
+    rows = np.repeat(np.arange(s.n), np.diff(s.ia))
+    off = s.ja != rows
+    a[off] *= (1.0 + skew * np.sign(s.ja[off] - rows[off]))[:, None, None]
+    return a.reshape(-1)
+
+
+def main_block():
+    """Block (CSMatrixRS) fixtures: CombineLU, block ILU2 with its SVD scaling,
+    block SolveL / SolveU, on a small Lame block matrix and a nonsymmetric
+    variant of it."""
+    ref = RefLib()
+    out = {}
+    s = P.lame3d(4, sigma=1.0, seed=31)
+    bs = s.bs
+    x = np.random.default_rng(32).standard_normal(s.n * bs)
+    out["nb"], out["bs"] = s.n, bs
+    out["ia"], out["ja"], out["a"] = s.ia, s.ja, s.a
+    out["ns_a"] = nonsymmetric_blocks(s)
+    out["x"] = x
+    ia_s, ja_s, al, au = ref.combine_lu_block(s.ia, s.ja, s.a, bs)
+    out["clu_ia"], out["clu_ja"], out["clu_l"], out["clu_u"] = ia_s, ja_s, al, au
+    for tag, vals, t1, t2 in (("bilu_a", "a", 1e-3, 1e-3), ("bilu_b", "a", 1e-2, 1e-5), ("bilu_ns", "ns_a", 1e-3, 1e-4)):
+        ia_f, ja_f, l, u, st = ref.ilu2_block(s.ia, s.ja, out[vals], bs, tau1=t1, tau2=t2, theta=0.1)
+        out[f"{tag}_ia"], out[f"{tag}_ja"], out[f"{tag}_l"], out[f"{tag}_u"] = ia_f, ja_f, l, u
+        out[f"{tag}_density"] = np.array(st[:2])
+        out[f"{tag}_solve_l"] = ref.solve_l_block(ia_f, ja_f, l, bs, x)
+        out[f"{tag}_solve_u"] = ref.solve_u_block(ia_f, ja_f, u, bs, x)
+    path = os.path.join(HERE, "lame_block.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if "--block" not in sys.argv:
+        main()
+    main_block()

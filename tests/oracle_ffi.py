@@ -39,6 +39,15 @@ def _take_csr(lib, n, pia, pja, pa, pb=None):
     return ia, ja, a, b
 
 
+def _take_bsr(nb, bs, pia, pja, *pvals):
+    """Block CSR arrays handed back by the C side (malloc'ed): copies."""
+    ia = np.ctypeslib.as_array(pia, (nb + 1,)).copy()
+    nz = int(ia[-1])
+    ja = np.ctypeslib.as_array(pja, (max(nz, 1),))[:nz].copy()
+    vals = [np.ctypeslib.as_array(p, (max(nz, 1) * bs * bs,))[:nz * bs * bs].copy() for p in pvals]
+    return ia, ja, vals
+
+
 class Oracle:
     def __init__(self, path=ORACLE_SO):
         self.lib = C.CDLL(path)
@@ -135,6 +144,46 @@ class Oracle:
         return x, it, em.value
 
 
+    # ---- block (CSMatrixRS) part ----
+    def combine_lu_block(self, ia, ja, a, bs):
+        nb = len(ia) - 1
+        pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
+        if self.lib.orc_combine_lu_block(nb, bs, _i(ia), _i(ja), _d(a), C.byref(pia), C.byref(pja), C.byref(pl),
+                                         C.byref(pu)) != 0:
+            raise MemoryError("combine_lu_block")
+        ia_s, ja_s, (al, au) = _take_bsr(nb, bs, pia, pja, pl, pu)
+        for p in (pia, pja, pl, pu):
+            self.lib.orc_free(p)
+        return ia_s, ja_s, al, au
+
+    def ilu2_block(self, ia_s, ja_s, al, au, bs, tau1=1e-3, tau2=1e-3, theta=0.1, sclmin=1e-8, pivmin=1e-8):
+        """Block ILU2 of a CombineLU'd block matrix: (ia, ja, l, u, (density, density2))."""
+        nb = len(ia_s) - 1
+        pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
+        st = (C.c_double * 3)()
+        rc = self.lib.orc_ilu2_block(nb, bs, _i(ia_s), _i(ja_s), _d(al), _d(au), C.c_double(tau1), C.c_double(tau2),
+                                     C.c_double(theta), C.c_double(sclmin), C.c_double(pivmin), C.byref(pia),
+                                     C.byref(pja), C.byref(pl), C.byref(pu), st)
+        if rc != 0:
+            raise RuntimeError(f"orc_ilu2_block failed ({rc})")
+        ia_f, ja_f, (l, u) = _take_bsr(nb, bs, pia, pja, pl, pu)
+        for p in (pia, pja, pl, pu):
+            self.lib.orc_free(p)
+        return ia_f, ja_f, l, u, (st[0], st[1])
+
+    def solve_l_block(self, ia, ja, a, bs, x):
+        nb = len(ia) - 1
+        y = np.zeros(nb * bs)
+        self.lib.orc_solve_l_block(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y))
+        return y
+
+    def solve_u_block(self, ia, ja, a, bs, x):
+        nb = len(ia) - 1
+        y = np.zeros(nb * bs)
+        self.lib.orc_solve_u_block(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y))
+        return y
+
+
 class RefLib:
     """The reference Bslib, compiled here from its sources (oracle/Makefile)."""
 
@@ -219,3 +268,40 @@ class RefLib:
                                       C.c_double(pivmin), sttype, C.c_double(eps), niter, ichk, st))
         return x, dict(iters=int(st[0]), resfin=st[1], tfct=st[2], titr=st[3], density=st[4], density2=st[5],
                        wall=st[6])
+
+    # ---- block (CSMatrixRS) part ----
+    def combine_lu_block(self, ia, ja, a, bs):
+        nb = len(ia) - 1
+        pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
+        self._err(self.lib.ref_combine_lu_block(nb, bs, _i(ia), _i(ja), _d(a), C.byref(pia), C.byref(pja),
+                                                C.byref(pl), C.byref(pu)))
+        ia_s, ja_s, (al, au) = _take_bsr(nb, bs, pia, pja, pl, pu)
+        for p in (pia, pja, pl, pu):
+            self.lib.ref_free(p)
+        return ia_s, ja_s, al, au
+
+    def ilu2_block(self, ia, ja, a, bs, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, sclmin=1e-8, pivmin=1e-8):
+        """CombineLU + CSMatrixRS::Ilu2: (ia, ja, l, u, (density, density2, seconds))."""
+        nb = len(ia) - 1
+        pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
+        st = (C.c_double * 3)()
+        self._err(self.lib.ref_ilu2_block(nb, bs, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+                                          C.c_double(theta), C.c_double(memory), C.c_double(sclmin),
+                                          C.c_double(pivmin), C.byref(pia), C.byref(pja), C.byref(pl),
+                                          C.byref(pu), st))
+        ia_f, ja_f, (l, u) = _take_bsr(nb, bs, pia, pja, pl, pu)
+        for p in (pia, pja, pl, pu):
+            self.lib.ref_free(p)
+        return ia_f, ja_f, l, u, (st[0], st[1], st[2])
+
+    def solve_l_block(self, ia, ja, a, bs, x):
+        nb = len(ia) - 1
+        y = np.zeros(nb * bs)
+        self._err(self.lib.ref_solve_l_block(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y)))
+        return y
+
+    def solve_u_block(self, ia, ja, a, bs, x):
+        nb = len(ia) - 1
+        y = np.zeros(nb * bs)
+        self._err(self.lib.ref_solve_u_block(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y)))
+        return y

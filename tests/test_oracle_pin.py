@@ -17,6 +17,7 @@ import pytest
 import problems as P
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "heat_8x8x6.npz")
+GOLD_BLOCK = os.path.join(os.path.dirname(__file__), "golden", "lame_block.npz")
 
 
 @pytest.fixture(scope="module")
@@ -120,3 +121,43 @@ def test_live_reference_lanczos_larger_case(oracle, reflib):
     xo, it, _ = oracle.lanczos(s.ia, s.ja, a, iu, ju, lv, uv, s.rhs[0], eps=1e-9, sttype=1)
     assert abs(it - info["iters"]) <= 1
     assert rel(xo, x) < 1e-7
+
+
+# ---- block (CSMatrixRS) ILU2: the oracle replays the reference's own update
+#      order and calls the same LAPACK dgesvd, so it agrees bit for bit ----
+
+@pytest.fixture(scope="module")
+def gold_block():
+    return np.load(GOLD_BLOCK)
+
+
+def test_block_combine_lu_matches_reference(oracle, gold_block):
+    g = gold_block
+    ia_s, ja_s, al, au = oracle.combine_lu_block(g["ia"], g["ja"], g["a"], int(g["bs"]))
+    assert np.array_equal(ia_s, g["clu_ia"]) and np.array_equal(ja_s, g["clu_ja"])
+    assert np.array_equal(al, g["clu_l"]) and np.array_equal(au, g["clu_u"])
+
+
+@pytest.mark.parametrize("tag,vals,t1,t2", [("bilu_a", "a", 1e-3, 1e-3), ("bilu_b", "a", 1e-2, 1e-5),
+                                            ("bilu_ns", "ns_a", 1e-3, 1e-4)])
+def test_block_ilu2_matches_reference(oracle, gold_block, tag, vals, t1, t2):
+    g = gold_block
+    bs = int(g["bs"])
+    clu = oracle.combine_lu_block(g["ia"], g["ja"], g[vals], bs)
+    ia_f, ja_f, l, u, st = oracle.ilu2_block(*clu, bs, tau1=t1, tau2=t2, theta=0.1)
+    assert np.array_equal(ia_f, g[f"{tag}_ia"]) and np.array_equal(ja_f, g[f"{tag}_ja"])
+    assert np.array_equal(l, g[f"{tag}_l"]) and np.array_equal(u, g[f"{tag}_u"])
+    assert np.allclose(st, g[f"{tag}_density"], rtol=0, atol=1e-14)
+    x = g["x"]
+    assert np.array_equal(oracle.solve_l_block(ia_f, ja_f, l, bs, x), g[f"{tag}_solve_l"])
+    assert np.array_equal(oracle.solve_u_block(ia_f, ja_f, u, bs, x), g[f"{tag}_solve_u"])
+
+
+def test_live_reference_block_ilu2_larger_cases(oracle, reflib):
+    cases = [(P.lame3d(9, sigma=1.0, seed=33), 1e-3, 1e-3),
+             (P.lame_periodic(10, rmin=1.5, rmax=3.0, seed=34), 1e-2, 1e-4)]
+    for s, t1, t2 in cases:
+        ia_f, ja_f, l, u, st = reflib.ilu2_block(s.ia, s.ja, s.a, 3, tau1=t1, tau2=t2)
+        o = oracle.ilu2_block(*oracle.combine_lu_block(s.ia, s.ja, s.a, 3), 3, tau1=t1, tau2=t2)
+        assert np.array_equal(o[0], ia_f) and np.array_equal(o[1], ja_f)
+        assert np.array_equal(o[2], l) and np.array_equal(o[3], u)
