@@ -38,7 +38,7 @@ class Param(C.Structure):
         ("density", C.c_double), ("density2", C.c_double), ("timefct", C.c_double), ("timeitr", C.c_double),
         ("precision", C.c_int), ("trisolve", C.c_int), ("nsweeps", C.c_int), ("krylov", C.c_int),
         ("restart", C.c_int), ("true_residual", C.c_int), ("learned", C.c_void_p), ("resrec", C.c_double),
-        ("pad", C.c_int * 4),
+        ("blockfct", C.c_int), ("pad", C.c_int * 3),
     ]
 
 
@@ -100,6 +100,7 @@ def lib():
         "bsg_lanczos_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
         "bsg_solve_t_dev": (i_, [vp, vp, i_, i_, i_, vp, vp]),
         "bsg_sell_stats": (i_, [vp, vp, C.POINTER(C.c_longlong)]),
+        "bsg_fct_export_block": (i_, [vp, ip, ip, ip, ip, dp, dp]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -263,6 +264,20 @@ class Factor:
 
     def to_fp32(self):
         _check(lib().bsg_fct_to_fp32(self.h))
+
+    def export_block(self):
+        """Block factor of a block ILU2: (ia, ja, l, u), 3x3 column-major blocks."""
+        nb, nz = C.c_int(), C.c_int()
+        _check(lib().bsg_fct_export_block(self.h, C.byref(nb), C.byref(nz), None, None, None, None))
+        ia = np.zeros(nb.value + 1, np.int32)
+        ja = np.zeros(nz.value, np.int32)
+        l = np.zeros(9 * nz.value)
+        u = np.zeros(9 * nz.value)
+        _check(lib().bsg_fct_export_block(self.h, None, None, ia.ctypes.data_as(C.POINTER(C.c_int)),
+                                          ja.ctypes.data_as(C.POINTER(C.c_int)),
+                                          l.ctypes.data_as(C.POINTER(C.c_double)),
+                                          u.ctypes.data_as(C.POINTER(C.c_double))))
+        return ia, ja, l, u
 
     def sell_stats(self):
         """Sliced copies of the factor: stored entries of the strict L / U

@@ -143,6 +143,7 @@ extern "C" void bsg_param_default(bsg_param *p) {
 	p->krylov = 0;
 	p->restart = 50;
 	p->true_residual = 1;
+	p->blockfct = 1;
 	p->learned = nullptr;
 }
 
@@ -482,7 +483,9 @@ static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **
 	if (kind == 0 && p->fcttyp == 1)
 		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) is not on the GPU path; use fcttyp = 2");
 	bsg_fct *f = nullptr;
-	int rc = bsg_fact_run(c, m, kind, p, &f);
+	// a 3x3 block matrix gets the reference's block ILU2 (CSMatrixRS::Ilu2)
+	const bool block = kind == 1 && m->bs == 3 && p->blockfct != 0;
+	int rc = block ? bsg_bfact_run(c, m, p, &f) : bsg_fact_run(c, m, kind, p, &f);
 	if (rc) return rc;
 	float ms = 0;
 	cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -490,7 +493,7 @@ static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **
 	p->density = f->density;
 	p->density2 = f->density2;
 	if (p->precision == 1) {
-		rc = bsg_fct_make_fp32(f);
+		rc = block ? bsg_bfact_make_fp32(f) : bsg_fct_make_fp32(f);
 		if (rc) { bsg_fct_free(f); return rc; }
 	}
 	*out = f;
@@ -501,17 +504,32 @@ extern "C" int bsg_fct_ich2(bsg_ctx *c, bsg_mat *m, bsg_param *p, bsg_fct **out)
 extern "C" int bsg_fct_ilu2(bsg_ctx *c, bsg_mat *m, bsg_param *p, bsg_fct **out) { return fct_common(c, m, p, 1, out); }
 extern "C" int bsg_fct_to_fp32(bsg_fct *f) {
 	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_to_fp32: null factor");
-	return bsg_fct_make_fp32(f);
+	return f->d_bia ? bsg_bfact_make_fp32(f) : bsg_fct_make_fp32(f);
 }
 
 extern "C" int bsg_fct_export(const bsg_fct *f, int *nnz, int *iu, int *ju, double *l, double *u) {
 	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_export: null factor");
+	if (f->d_bia) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_export: block factor (use bsg_fct_export_block)");
 	if (nnz) *nnz = f->nnz;
 	cudaStream_t s = f->ctx->stream;
 	if (iu) BSG_CUDA(cudaMemcpyAsync(iu, f->d_iu, sizeof(int) * (f->n + 1), cudaMemcpyDeviceToHost, s));
 	if (ju) BSG_CUDA(cudaMemcpyAsync(ju, f->d_ju, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, s));
 	if (l) BSG_CUDA(cudaMemcpyAsync(l, f->d_l, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, s));
 	if (u) BSG_CUDA(cudaMemcpyAsync(u, f->d_u, sizeof(double) * f->nnz, cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	return BSG_OK;
+}
+
+extern "C" int bsg_fct_export_block(const bsg_fct *f, int *nb, int *nnzb, int *ia, int *ja, double *l, double *u) {
+	if (!f) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_export_block: null factor");
+	if (!f->d_bia) return bsg_set_error(BSG_ERR_ARG, "bsg_fct_export_block: point factor (use bsg_fct_export)");
+	if (nb) *nb = f->nb;
+	if (nnzb) *nnzb = f->nnz;
+	cudaStream_t s = f->ctx->stream;
+	if (ia) BSG_CUDA(cudaMemcpyAsync(ia, f->d_bia, sizeof(int) * (f->nb + 1), cudaMemcpyDeviceToHost, s));
+	if (ja) BSG_CUDA(cudaMemcpyAsync(ja, f->d_bja, sizeof(int) * f->nnz, cudaMemcpyDeviceToHost, s));
+	if (l) BSG_CUDA(cudaMemcpyAsync(l, f->d_bl, sizeof(double) * 9 * (size_t)f->nnz, cudaMemcpyDeviceToHost, s));
+	if (u) BSG_CUDA(cudaMemcpyAsync(u, f->d_bu, sizeof(double) * 9 * (size_t)f->nnz, cudaMemcpyDeviceToHost, s));
 	BSG_CUDA(cudaStreamSynchronize(s));
 	return BSG_OK;
 }
@@ -542,6 +560,10 @@ extern "C" int bsg_fct_free(bsg_fct *f) {
 	                (void *)f->d_lr_i, (void *)f->d_lr_j, (void *)f->d_lr_v, (void *)f->d_ur_f, (void *)f->d_lr_f,
 	                (void *)f->d_perm})
 		if (p) cudaFreeAsync(p, s);
+	if (f->d_bia) // block factor: its strict U rows are separate arrays
+		for (void *p : {(void *)f->d_bia, (void *)f->d_bja, (void *)f->d_bl, (void *)f->d_bu, (void *)f->d_bdl,
+		                (void *)f->d_bdu, (void *)f->d_ones, (void *)f->d_ur_i, (void *)f->d_ur_j, (void *)f->d_ur_v})
+			if (p) cudaFreeAsync(p, s);
 	cudaStreamSynchronize(s);
 	delete f;
 	return BSG_OK;

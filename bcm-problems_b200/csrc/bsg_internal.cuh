@@ -180,6 +180,14 @@ struct bsg_fct {
 	double *d_utr_v;
 	float *d_utr_f, *d_l_f;
 	bsg_sell slt, sut;
+	// block factor (k_bfact.cu): nb block rows, nnz = blocks; 3x3 column-major
+	// blocks, pivot block first; the strict parts' point rows live in
+	// d_lr_* / d_ur_* and sl / su, the diagonal action of the solves in
+	// d_bdl (L_ii^T) / d_bdu (U_ii)
+	int nb;
+	int *d_bia, *d_bja;
+	double *d_bl, *d_bu;
+	double *d_bdl, *d_bdu, *d_ones;
 };
 
 // ---- launch accounting ------------------------------------------------------
@@ -201,3 +209,8 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y,
                           double *work);
 int bsg_check_devstat(bsg_ctx *c);
+// block ILU2 of a 3x3 block matrix (k_bfact.cu) and its solves
+int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out);
+int bsg_bfact_make_fp32(bsg_fct *f);
+int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
+                         double *work);

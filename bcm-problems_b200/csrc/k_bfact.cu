@@ -1,0 +1,897 @@
+// Block (3 x 3) second-order incomplete LU: the reference's CSMatrixRS::Ilu2
+// (Bslib/ilu2rs.cpp:1458-1820) on the GPU, with its SVD scaling of the
+// diagonal blocks (Ilu2AllocScale, :25-315), block filtering with diagonal
+// compensation (Ilu2FiltrRow, :616-692), SVD pivots (Ilu2PivScaleRow,
+// :694-852) and the final back-scaling (Ich2StoreScaleU,
+// Bslib/ich2rs.cpp:822-943); and the block triangular solves of its factor
+// (CSMatrixRS::SolveL / SolveU, Bslib/mvm.cpp:3140 / 3410).
+//
+// Blocks are column-major 3 x 3 (entry (r, c) at r + 3 c), as CSMatrixRS
+// keeps them.
+//
+// Schedule.  Block rows of a natural-order 3-D elasticity matrix form a
+// dependency chain (every block row couples to the previous one), so rows
+// are factored in order by one persistent CTA that spreads each row's work
+// over its 512 threads:
+//   1. the members of the row -- earlier rows that stored an element in this
+//      column -- come from per-column lists that every stored element
+//      appended to (the reference walks linked lists instead, :1578-1617);
+//   2. the scaled row of A goes into dense per-column accumulators;
+//   3. every (member, element) pair registers its column, then subtracts its
+//      two 3 x 3 products (L and U side) with atomics;
+//   4. one thread per touched column filters it, adding the compensation to
+//      the pivot block and to that column's future diagonal block;
+//   5. one thread takes the SVD of the pivot block; the kept blocks are
+//      scaled, ranked by column, stored as U (max-norm >= tau1) or R, and
+//      appended to their columns' member lists.
+// The updates are summed in arrival order, and the SVD is this file's own,
+// so the factor agrees with the reference to rounding, not bit for bit; a
+// singular vector's sign cancels in L U, but for (nearly) repeated singular
+// values the reference's vectors and these differ by a rotation, which can
+// move a block across a threshold.
+#include "bsg_internal.cuh"
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+namespace {
+
+constexpr int BT = 512;       // threads of the row kernel
+constexpr int LMAX = 4096;    // distinct columns one row may touch
+constexpr int MMAX = 4096;    // members of one row
+constexpr int CH = 32;        // entries per member-list chunk
+
+inline int nb_(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
+
+// ---- 3 x 3 helpers (column-major) -----------------------------------------
+// out = p q with p given by strides: p(r, k) at p[r * pr + k * pc]; q(k, c)
+// at q[k * qr + c * qc]; sums in k order from zero
+__device__ __forceinline__ void mm3(const double *p, int pr, int pc, const double *q, int qr, int qc, double *out) {
+#pragma unroll
+	for (int r = 0; r < 3; r++)
+#pragma unroll
+		for (int c = 0; c < 3; c++) {
+			double s = 0.0;
+#pragma unroll
+			for (int k = 0; k < 3; k++) s += p[r * pr + k * pc] * q[k * qr + c * qc];
+			out[r + 3 * c] = s;
+		}
+}
+
+// A = U diag(s) V^T of a 3 x 3 matrix (column-major), s descending, U and V
+// orthogonal: one-sided Jacobi (Hestenes), rotating column pairs of W = A V
+// until they are orthogonal; U = the normalised columns of W, completed to an
+// orthonormal basis (Gram-Schmidt of unit vectors) where a singular value
+// vanishes.
+__device__ void svd3(const double *a, double *u, double *s, double *v) {
+	double w[9], vw[9];
+	for (int k = 0; k < 9; k++) {
+		w[k] = a[k];
+		vw[k] = (k % 4) == 0 ? 1.0 : 0.0;
+	}
+	for (int sweep = 0; sweep < 30; sweep++) {
+		double off = 0.0;
+		for (int pq = 0; pq < 3; pq++) {
+			const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+			double al = 0.0, be = 0.0, ga = 0.0;
+			for (int r = 0; r < 3; r++) {
+				al += w[r + 3 * p] * w[r + 3 * p];
+				be += w[r + 3 * q] * w[r + 3 * q];
+				ga += w[r + 3 * p] * w[r + 3 * q];
+			}
+			const double nrm = sqrt(al * be);
+			if (nrm == 0.0 || fabs(ga) <= 1e-16 * nrm) continue;
+			off = fmax(off, fabs(ga) / nrm);
+			const double zeta = (be - al) / (2.0 * ga);
+			const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+			const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+			for (int r = 0; r < 3; r++) {
+				const double wp = w[r + 3 * p], wq = w[r + 3 * q];
+				w[r + 3 * p] = cs * wp - sn * wq;
+				w[r + 3 * q] = sn * wp + cs * wq;
+				const double vp = vw[r + 3 * p], vq = vw[r + 3 * q];
+				vw[r + 3 * p] = cs * vp - sn * vq;
+				vw[r + 3 * q] = sn * vp + cs * vq;
+			}
+		}
+		if (off <= 1e-15) break;
+	}
+	double sv[3];
+	for (int c = 0; c < 3; c++) sv[c] = sqrt(w[3 * c] * w[3 * c] + w[1 + 3 * c] * w[1 + 3 * c] + w[2 + 3 * c] * w[2 + 3 * c]);
+	int o[3] = {0, 1, 2}; // descending order
+	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
+	if (sv[o[1]] < sv[o[2]]) { const int t = o[1]; o[1] = o[2]; o[2] = t; }
+	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
+	const double smax = sv[o[0]];
+	int good[3];
+	for (int c = 0; c < 3; c++) {
+		const int k = o[c];
+		s[c] = sv[k];
+		good[c] = sv[k] > 1e-300 && sv[k] > 1e-14 * smax;
+		for (int r = 0; r < 3; r++) {
+			u[r + 3 * c] = good[c] ? w[r + 3 * k] / sv[k] : 0.0;
+			v[r + 3 * c] = vw[r + 3 * k];
+		}
+	}
+	for (int c = 0; c < 3; c++) {
+		if (good[c]) continue;
+		for (int e = 0; e < 3; e++) {
+			double x[3] = {e == 0 ? 1.0 : 0.0, e == 1 ? 1.0 : 0.0, e == 2 ? 1.0 : 0.0};
+			for (int d = 0; d < 3; d++) {
+				if (d == c || !good[d]) continue;
+				const double pr = u[3 * d] * x[0] + u[1 + 3 * d] * x[1] + u[2 + 3 * d] * x[2];
+				for (int r = 0; r < 3; r++) x[r] -= pr * u[r + 3 * d];
+			}
+			const double nx = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+			if (nx > 0.5) {
+				for (int r = 0; r < 3; r++) u[r + 3 * c] = x[r] / nx;
+				good[c] = 1;
+				break;
+			}
+		}
+	}
+}
+
+// ---- CombineLU of a block matrix on the device ----------------------------
+// keys (row, col) of the union pattern: upper blocks (j >= i) at (i, j),
+// lower blocks (j <= i) transposed to (j, i); the source is 2 p (upper) or
+// 2 p + 1 (lower) for the block p of A
+__global__ void k_bc_keys(int nb, const int *ia, const int *ja, const int *off, unsigned long long *keys, int *src) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	int o = off[i];
+	for (int p = ia[i]; p < ia[i + 1]; p++) {
+		const int j = ja[p];
+		if (j >= i) {
+			keys[o] = ((unsigned long long)i << 32) | (unsigned)j;
+			src[o++] = 2 * p;
+		}
+		if (j <= i) {
+			keys[o] = ((unsigned long long)j << 32) | (unsigned)i;
+			src[o++] = 2 * p + 1;
+		}
+	}
+}
+__global__ void k_bc_count(int nb, const int *ia, const int *ja, int *cnt) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	int c = 0;
+	for (int p = ia[i]; p < ia[i + 1]; p++) c += (ja[p] >= i) + (ja[p] <= i);
+	cnt[i] = c;
+}
+__global__ void k_bc_flags(int nk, const unsigned long long *keys, int *flag) {
+	const int e = blockIdx.x * blockDim.x + threadIdx.x;
+	if (e < nk) flag[e] = (e == 0 || keys[e] != keys[e - 1]) ? 1 : 0;
+}
+// id[e] = inclusive count of distinct keys - 1; row counts of the pattern
+__global__ void k_bc_pattern(int nk, const unsigned long long *keys, const int *id, const int *flag, int *bja,
+                             int *rowcnt) {
+	const int e = blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= nk || !flag[e]) return;
+	bja[id[e] - 1] = (int)(keys[e] & 0xffffffffu);
+	atomicAdd(rowcnt + (int)(keys[e] >> 32), 1);
+}
+// values: au = the block (column-major), al = the block transposed
+// (column-major); A's blocks arrive row-major
+__global__ void k_bc_values(int nk, const int *src, const int *id, const double *a, double *al, double *au) {
+	const int e = blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= nk) return;
+	const int s = src[e], p = s >> 1;
+	const double *b = a + (size_t)p * 9; // row-major: (r, c) at 3 r + c
+	double *o = ((s & 1) ? al : au) + (size_t)(id[e] - 1) * 9;
+	for (int r = 0; r < 3; r++)
+		for (int c = 0; c < 3; c++) o[r + 3 * c] = (s & 1) ? b[3 * c + r] : b[3 * r + c];
+}
+
+// ---- scaling of the diagonal blocks (Ilu2AllocScale) ----------------------
+__global__ void k_bscale(int nb, const int *bia, const double *au, double sclmin, double *scll, double *sclu,
+                         double *sinvl, double *sinvu, double *diagg) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	const double *d = au + (size_t)bia[i] * 9;
+	double u[9], v[9], s[3];
+	svd3(d, u, s, v);
+	for (int k = 0; k < 3; k++) s[k] = sqrt(s[k] < sclmin ? sclmin : s[k]);
+	double *il = sinvl + (size_t)i * 9, *iu = sinvu + (size_t)i * 9, *sl = scll + (size_t)i * 9,
+	       *su = sclu + (size_t)i * 9;
+	for (int r = 0; r < 3; r++)
+		for (int c = 0; c < 3; c++) {
+			il[r + 3 * c] = u[r + 3 * c] * s[c]; // U diag(s^1/2)
+			iu[r + 3 * c] = v[r + 3 * c] * s[c]; // V diag(s^1/2)
+			sl[r + 3 * c] = u[c + 3 * r] / s[r]; // diag(s^-1/2) U^T
+			su[r + 3 * c] = v[c + 3 * r] / s[r]; // diag(s^-1/2) V^T
+		}
+	double t[9];
+	mm3(sl, 1, 3, d, 1, 3, t);                 // scll D
+	mm3(t, 1, 3, su, 3, 1, diagg + (size_t)i * 9); // ... sclu^T
+}
+
+// ---- the row kernel ---------------------------------------------------------
+struct BArgs {
+	int nb;
+	const int *bia, *bja;     // CombineLU pattern (diagonal block first)
+	const double *al, *au;    // transposed lower / upper blocks
+	const double *scll, *sclu;
+	double *diagg;            // scaled diagonal blocks, plus compensations
+	double *fml, *fmu;        // dense accumulators, 9 per block column
+	int *imask;               // row that last registered a column
+	int *ig, *jg;             // stored rows: pivot, then +col (U) / -col (R)
+	double *gl, *gu;
+	long long cap;            // stored blocks available
+	int *mhead, *mtail, *mcnt; // per-column member lists (chunks)
+	int *chk, *chq, *chnext;  // chunk entries: member row, stored position; next chunk
+	int *pool;                // chunks in use
+	int pool_cap;
+	double tau1, tau2, theta, pivmin;
+	unsigned long long *nstored; // [0] U blocks, [1] R blocks
+	bsg_devstat *st;
+};
+
+__device__ int upper_index(const int *pre, int n, int w) { // largest m with pre[m] <= w
+	int lo = 0, hi = n - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (pre[mid] <= w) lo = mid;
+		else hi = mid - 1;
+	}
+	return lo;
+}
+
+// loads of data this kernel writes: L2 only (atomics update L2, not L1)
+__device__ __forceinline__ void ld9(const double *p, double *o) {
+#pragma unroll
+	for (int k = 0; k < 9; k++) o[k] = __ldcg(p + k);
+}
+
+// shared memory of the row kernel, carved from the dynamic allocation
+constexpr size_t BSMEM = sizeof(int) * (3 * MMAX + 1 + 3 * LMAX) + MMAX;
+
+__global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
+	extern __shared__ __align__(16) int bsm[];
+	int *mk = bsm, *mq = mk + MMAX, *mpre = mq + MMAX, *lst = mpre + MMAX + 1, *keep = lst + LMAX,
+	    *rank_ = keep + LMAX;
+	unsigned char *mr = reinterpret_cast<unsigned char *>(rank_ + LMAX);
+	__shared__ double dsum[BT / 32][3];
+	__shared__ double dl[9], du[9];
+	__shared__ int nm, nl, nk, W, base, fail;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	if (tid == 0) {
+		base = 0;
+		fail = 0;
+		A.ig[0] = 0;
+	}
+	__syncthreads();
+	for (int irow = 0; irow < A.nb; irow++) {
+		// ---- members of the row (warp 0) and the scaled row of A (the rest)
+		if (tid == 0) {
+			nm = __ldcg(A.mcnt + irow);
+			nl = 0;
+			if (nm > MMAX) fail = 1;
+		}
+		__syncthreads();
+		if (fail) break;
+		if (warp == 0) {
+			int c = __ldcg(A.mhead + irow), o = 0;
+			while (c >= 0 && o < nm) {
+				if (o + lane < nm) {
+					mk[o + lane] = __ldcg(A.chk + (size_t)c * CH + lane);
+					mq[o + lane] = __ldcg(A.chq + (size_t)c * CH + lane);
+				}
+				o += CH;
+				c = __ldcg(A.chnext + c);
+			}
+		} else {
+			const double *sli = A.scll + (size_t)irow * 9, *sui = A.sclu + (size_t)irow * 9;
+			for (int p = A.bia[irow] + tid - 32; p < A.bia[irow + 1]; p += BT - 32) {
+				const int j = A.bja[p];
+				double t[9];
+				if (j == irow) {
+					double dg[9];
+					ld9(A.diagg + (size_t)j * 9, dg);
+					for (int k = 0; k < 9; k++) A.fml[(size_t)j * 9 + k] = A.fmu[(size_t)j * 9 + k] = dg[k];
+				} else {
+					mm3(sli, 1, 3, A.au + (size_t)p * 9, 1, 3, t);
+					mm3(t, 1, 3, A.sclu + (size_t)j * 9, 3, 1, A.fmu + (size_t)j * 9);
+					mm3(sui, 1, 3, A.al + (size_t)p * 9, 1, 3, t);
+					mm3(t, 1, 3, A.scll + (size_t)j * 9, 3, 1, A.fml + (size_t)j * 9);
+				}
+				atomicExch(A.imask + j, irow);
+				const int slot = atomicAdd(&nl, 1);
+				if (slot < LMAX) lst[slot] = j;
+			}
+		}
+		__syncthreads();
+		// ---- member segments [q, end of the member's row) and their prefix (warp 0)
+		for (int m = tid; m < nm; m += BT) {
+			const int k = mk[m], q = mq[m];
+			mpre[m + 1] = __ldcg(A.ig + k + 1) - q;
+			mr[m] = __ldcg(A.jg + q) < 0;
+		}
+		__syncthreads();
+		if (warp == 0) {
+			int carry = 0;
+			if (lane == 0) mpre[0] = 0;
+			for (int o = 0; o < nm; o += 32) {
+				int v = o + lane < nm ? mpre[o + lane + 1] : 0;
+				for (int d = 1; d < 32; d <<= 1) {
+					const int y = __shfl_up_sync(0xffffffffu, v, d);
+					if (lane >= d) v += y;
+				}
+				if (o + lane < nm) mpre[o + lane + 1] = v + carry;
+				carry += __shfl_sync(0xffffffffu, v, 31);
+			}
+			if (lane == 0) W = carry;
+		}
+		__syncthreads();
+		// ---- register the members' columns (first registration zeroes them)
+		for (int w = tid; w < W; w += BT) {
+			const int m = upper_index(mpre, nm, w);
+			const int e = mq[m] + (w - mpre[m]);
+			int c = __ldcg(A.jg + e);
+			if (mr[m] && c < 0) continue;
+			c = c < 0 ? -c : c;
+			if (atomicExch(A.imask + c, irow) != irow) {
+				for (int k = 0; k < 9; k++) A.fml[(size_t)c * 9 + k] = A.fmu[(size_t)c * 9 + k] = 0.0;
+				const int slot = atomicAdd(&nl, 1);
+				if (slot < LMAX) lst[slot] = c;
+			}
+		}
+		__syncthreads();
+		if (nl > LMAX) {
+			if (tid == 0) fail = 2;
+			break;
+		}
+		// ---- updates: fmu[c] -= Lki^T Ukc, fml[c] -= Uki^T Lkc
+		for (int w = tid; w < W; w += BT) {
+			const int m = upper_index(mpre, nm, w);
+			const int q = mq[m], e = q + (w - mpre[m]);
+			int c = __ldcg(A.jg + e);
+			if (mr[m] && c < 0) continue;
+			c = c < 0 ? -c : c;
+			double lel[9], uel[9], gu[9], gl[9], tu[9], tl[9];
+			ld9(A.gl + (size_t)q * 9, lel);
+			ld9(A.gu + (size_t)q * 9, uel);
+			ld9(A.gu + (size_t)e * 9, gu);
+			ld9(A.gl + (size_t)e * 9, gl);
+			mm3(lel, 3, 1, gu, 1, 3, tu); // lel^T gu
+			mm3(uel, 3, 1, gl, 1, 3, tl); // uel^T gl
+			for (int k = 0; k < 9; k++) {
+				atomicAdd(A.fmu + (size_t)c * 9 + k, -tu[k]);
+				atomicAdd(A.fml + (size_t)c * 9 + k, -tl[k]);
+			}
+		}
+		__syncthreads();
+		// ---- filter: keep max-norm >= tau2, else compensate both diagonals
+		double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0;
+		for (int t = tid; t < nl; t += BT) {
+			const int c = lst[t];
+			keep[t] = 0;
+			if (c == irow) continue;
+			double fl[9], fu[9];
+			ld9(A.fml + (size_t)c * 9, fl);
+			ld9(A.fmu + (size_t)c * 9, fu);
+			double mx = 0.0;
+			for (int k = 0; k < 9; k++) mx = fmax(mx, fmax(fabs(fl[k]), fabs(fu[k])));
+			if (mx >= A.tau2) {
+				keep[t] = 1;
+			} else {
+				double dg[9];
+				ld9(A.diagg + (size_t)c * 9, dg);
+				for (int r = 0; r < 3; r++)
+					for (int cc = 0; cc < 3; cc++) {
+						const double v = A.theta * fmax(fabs(fl[r + 3 * cc]), fabs(fu[r + 3 * cc]));
+						if (r == 0) ds0 += v;
+						else if (r == 1) ds1 += v;
+						else ds2 += v;
+						dg[4 * cc] += v;
+					}
+				for (int cc = 0; cc < 3; cc++) A.diagg[(size_t)c * 9 + 4 * cc] = dg[4 * cc];
+			}
+		}
+		ds0 = warp_sum(ds0);
+		ds1 = warp_sum(ds1);
+		ds2 = warp_sum(ds2);
+		if (lane == 0) {
+			dsum[warp][0] = ds0;
+			dsum[warp][1] = ds1;
+			dsum[warp][2] = ds2;
+		}
+		__syncthreads();
+		// ---- pivot block (thread 0)
+		if (tid == 0) {
+			double fd[9];
+			ld9(A.fmu + (size_t)irow * 9, fd);
+			for (int r = 0; r < 3; r++) {
+				double sm = 0.0;
+				for (int w2 = 0; w2 < BT / 32; w2++) sm += dsum[w2][r];
+				fd[4 * r] += sm;
+			}
+			double u[9], v[9], sv[3];
+			svd3(fd, u, sv, v);
+			for (int k = 0; k < 3; k++) sv[k] = 1.0 / sqrt(sv[k] < A.pivmin ? A.pivmin : sv[k]);
+			for (int r = 0; r < 3; r++)
+				for (int c = 0; c < 3; c++) {
+					dl[r + 3 * c] = u[c + 3 * r] * sv[r]; // diag(s^-1/2) U^T
+					du[r + 3 * c] = v[c + 3 * r] * sv[r]; // diag(s^-1/2) V^T
+				}
+			int K = 0;
+			for (int t = 0; t < nl; t++) K += keep[t];
+			nk = K;
+		}
+		__syncthreads();
+		if ((long long)base + 1 + nk > A.cap) {
+			if (tid == 0) fail = 3;
+			break;
+		}
+		for (int t = tid; t < nl; t += BT) { // rank = kept blocks of smaller column
+			if (!keep[t]) continue;
+			const int c = lst[t];
+			int r = 0;
+			for (int t2 = 0; t2 < nl; t2++) r += keep[t2] && lst[t2] < c;
+			rank_[t] = r;
+		}
+		if (tid == 0) { // the pivot block: gl = dl^T, gu = du^T
+			A.jg[base] = irow;
+			for (int r = 0; r < 3; r++)
+				for (int c = 0; c < 3; c++) {
+					A.gl[(size_t)base * 9 + r + 3 * c] = dl[c + 3 * r];
+					A.gu[(size_t)base * 9 + r + 3 * c] = du[c + 3 * r];
+				}
+		}
+		__syncthreads();
+		// ---- scale, store, and append to the columns' member lists
+		unsigned long long nu = 0, nr = 0;
+		for (int t = tid; t < nl; t += BT) {
+			if (!keep[t]) continue;
+			const int c = lst[t];
+			const int pos = base + 1 + rank_[t];
+			double fl[9], fu[9], tl[9], tu[9];
+			ld9(A.fml + (size_t)c * 9, fl);
+			ld9(A.fmu + (size_t)c * 9, fu);
+			mm3(du, 1, 3, fl, 1, 3, tl);
+			mm3(dl, 1, 3, fu, 1, 3, tu);
+			double mx = 0.0;
+			for (int k = 0; k < 9; k++) {
+				A.gl[(size_t)pos * 9 + k] = tl[k];
+				A.gu[(size_t)pos * 9 + k] = tu[k];
+				mx = fmax(mx, fmax(fabs(tl[k]), fabs(tu[k])));
+			}
+			const int isu = mx >= A.tau1;
+			A.jg[pos] = isu ? c : -c;
+			nu += isu;
+			nr += !isu;
+			// member entry (irow, pos) for column c: only this thread owns c now
+			const int n0 = __ldcg(A.mcnt + c);
+			int ch = __ldcg(A.mtail + c);
+			if ((n0 % CH) == 0) {
+				const int nc = atomicAdd(A.pool, 1);
+				if (nc >= A.pool_cap) {
+					fail = 4;
+					continue;
+				}
+				A.chnext[nc] = -1;
+				if (ch >= 0) A.chnext[ch] = nc;
+				else A.mhead[c] = nc;
+				A.mtail[c] = nc;
+				ch = nc;
+			}
+			A.chk[(size_t)ch * CH + (n0 % CH)] = irow;
+			A.chq[(size_t)ch * CH + (n0 % CH)] = pos;
+			A.mcnt[c] = n0 + 1;
+		}
+		if (nu) atomicAdd(A.nstored, nu);
+		if (nr) atomicAdd(A.nstored + 1, nr);
+		__syncthreads();
+		if (tid == 0) {
+			base += 1 + nk;
+			A.ig[irow + 1] = base;
+			atomicAdd(A.nstored, 1ull); // the pivot block
+		}
+		__syncthreads();
+		if (fail) break;
+	}
+	if (tid == 0 && fail) devstat_fail(A.st, BSG_ERR_WORKSPACE, 0, 100 + fail);
+}
+
+// ---- final: the U part scaled back (Ich2StoreScaleU) ----------------------
+__global__ void k_bfin_count(int nb, const int *ig, const int *jg, int *cnt) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	int c = 0;
+	for (int q = ig[i]; q < ig[i + 1]; q++) c += jg[q] >= 0;
+	cnt[i] = c;
+}
+__global__ void k_bfin_fill(int nb, const int *ig, const int *jg, const double *gl, const double *gu,
+                            const double *scll, const double *sclu, const double *sinvl, const double *sinvu,
+                            const int *fi, int *fj, double *fl, double *fu) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	int o = fi[i];
+	for (int q = ig[i]; q < ig[i + 1]; q++) {
+		const int j = jg[q];
+		if (j < 0) continue;
+		fj[o] = j;
+		if (j == i) { // scl^T g
+			mm3(scll + (size_t)i * 9, 3, 1, gl + (size_t)q * 9, 1, 3, fl + (size_t)o * 9);
+			mm3(sclu + (size_t)i * 9, 3, 1, gu + (size_t)q * 9, 1, 3, fu + (size_t)o * 9);
+		} else { // g sclinv^T
+			mm3(gl + (size_t)q * 9, 1, 3, sinvl + (size_t)j * 9, 3, 1, fl + (size_t)o * 9);
+			mm3(gu + (size_t)q * 9, 1, 3, sinvu + (size_t)j * 9, 3, 1, fu + (size_t)o * 9);
+		}
+		o++;
+	}
+}
+
+// ---- solve-ready forms ------------------------------------------------------
+// point rows of the strict parts: the U solve reads row 3 i + r of U's
+// strict blocks (U_ik(r, c) at column 3 k + c); the L solve reads the
+// transpose of L's strict blocks (L_ki(c, r) at row 3 i + r, column 3 k + c),
+// built here by first writing each entry under its (row, column) key
+__global__ void k_bsu_count(int nb, const int *fi, int *cnt) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	const int nbk = fi[i + 1] - fi[i] - 1;
+	for (int r = 0; r < 3; r++) cnt[3 * i + r] = 3 * nbk;
+}
+__global__ void k_bsu_fill(int nb, const int *fi, const int *fj, const double *fu, const int *rp, int *ci,
+                           double *v) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	for (int r = 0; r < 3; r++) {
+		int o = rp[3 * i + r];
+		for (int q = fi[i] + 1; q < fi[i + 1]; q++)
+			for (int c = 0; c < 3; c++) {
+				ci[o] = 3 * fj[q] + c;
+				v[o++] = fu[(size_t)q * 9 + r + 3 * c];
+			}
+	}
+}
+// keys (row, col) and values of the transposed strict L entries
+__global__ void k_bsl_keys(int nb, const int *fi, const int *fj, const double *fl, unsigned long long *keys,
+                           double *vals) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x; // block row k of the storage
+	if (i >= nb) return;
+	long long o = 9LL * (fi[i] - i); // strict blocks before row i
+	for (int q = fi[i] + 1; q < fi[i + 1]; q++) {
+		const int j = fj[q];
+		for (int c = 0; c < 3; c++)
+			for (int r = 0; r < 3; r++) { // entry (c, r) of L_ij lands at row 3 j + r, column 3 i + c
+				keys[o] = ((unsigned long long)(3 * j + r) << 32) | (unsigned)(3 * i + c);
+				vals[o++] = fl[(size_t)q * 9 + c + 3 * r];
+			}
+	}
+}
+__global__ void k_keys_to_csr(long long nk, const unsigned long long *keys, int *ci, int *cnt) {
+	const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (e >= nk) return;
+	ci[e] = (int)(keys[e] & 0xffffffffu);
+	atomicAdd(cnt + (int)(keys[e] >> 32), 1);
+}
+// diagonal action of the solves: L: y_i = L_ii^T t_i; U: y_i = U_ii t_i
+__global__ void k_bdiag_pack(int nb, const int *fi, const double *fl, const double *fu, double *dlt, double *du) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	const double *l = fl + (size_t)fi[i] * 9, *u = fu + (size_t)fi[i] * 9;
+	for (int r = 0; r < 3; r++)
+		for (int c = 0; c < 3; c++) {
+			dlt[(size_t)i * 9 + r + 3 * c] = l[c + 3 * r];
+			du[(size_t)i * 9 + r + 3 * c] = u[r + 3 * c];
+		}
+}
+// y = D t per block (D column-major), t and y may alias
+__global__ void k_bdiag_apply(int nb, const double *d, const double *t, double *y) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	const double *b = d + (size_t)i * 9;
+	const double t0 = t[3 * i], t1 = t[3 * i + 1], t2 = t[3 * i + 2];
+	for (int r = 0; r < 3; r++) y[3 * i + r] = b[r] * t0 + b[r + 3] * t1 + b[r + 6] * t2;
+}
+__global__ void k_fill_d(long long n, double *x, double v) {
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		x[i] = v;
+}
+// Exact block solve, one warp walking the block rows in dependency order
+// (lower: ascending, upper: descending): y_i = D_i (x_i - N_i y) with N's
+// point rows 3 i .. 3 i + 2 gathered by the lanes.  Latency-bound: the
+// parity mode of the block factor.
+__global__ void k_bsolve_seq(int nb, int lower, const int *rp, const int *ci, const double *v, const double *d,
+                             const double *x, double *y) {
+	const int lane = threadIdx.x;
+	for (int s = 0; s < nb; s++) {
+		const int i = lower ? s : nb - 1 - s;
+		double t[3];
+		for (int r = 0; r < 3; r++) {
+			double acc = 0.0;
+			for (int p = rp[3 * i + r] + lane; p < rp[3 * i + r + 1]; p += 32) acc += v[p] * __ldcg(y + ci[p]);
+			t[r] = x[3 * i + r] - warp_sum(acc);
+		}
+		if (lane < 3) {
+			const double *b = d + (size_t)i * 9;
+			__stcg(y + 3 * i + lane, b[lane] * t[0] + b[lane + 3] * t[1] + b[lane + 6] * t[2]);
+		}
+		__threadfence_block();
+		__syncwarp();
+	}
+}
+
+} // namespace
+
+// ---- host ------------------------------------------------------------------
+struct DevVec {
+	void *p = nullptr;
+	cudaStream_t s = nullptr;
+	~DevVec() { if (p) cudaFreeAsync(p, s); }
+};
+#define BALLOC(var, type, count)                                                                           \
+	type *var = nullptr;                                                                                   \
+	DevVec var##_h;                                                                                        \
+	BSG_CUDA(cudaMallocAsync(&var, sizeof(type) * (size_t)((count) > 0 ? (count) : 1), st));             \
+	var##_h.p = var;                                                                                       \
+	var##_h.s = st;
+
+// point CSR from sorted (row, col) keys
+static int keys_csr(cudaStream_t st, int n, long long nk, unsigned long long *keys, double *vals, int **rp,
+                    int **ci, double **v) {
+	unsigned long long *k2;
+	double *v2;
+	BSG_CUDA(cudaMallocAsync(&k2, sizeof(unsigned long long) * (nk > 0 ? nk : 1), st));
+	BSG_CUDA(cudaMallocAsync(&v2, sizeof(double) * (nk > 0 ? nk : 1), st));
+	size_t tmp = 0;
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, k2, vals, v2, (int)nk, 0, 64, st));
+	void *dt;
+	BSG_CUDA(cudaMallocAsync(&dt, tmp + 1, st));
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(dt, tmp, keys, k2, vals, v2, (int)nk, 0, 64, st));
+	cudaFreeAsync(dt, st);
+	int *cnt;
+	BSG_CUDA(cudaMallocAsync(&cnt, sizeof(int) * (n + 1), st));
+	BSG_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (n + 1), st));
+	BSG_CUDA(cudaMallocAsync(ci, sizeof(int) * (nk > 0 ? nk : 1), st));
+	BSG_COUNT(1);
+	if (nk > 0) k_keys_to_csr<<<nb_(nk, 256), 256, 0, st>>>(nk, k2, *ci, cnt);
+	BSG_CUDA(cudaMallocAsync(rp, sizeof(int) * (n + 1), st));
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, *rp, n + 1, st));
+	BSG_CUDA(cudaMallocAsync(&dt, tmp + 1, st));
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(dt, tmp, cnt, *rp, n + 1, st));
+	cudaFreeAsync(dt, st);
+	cudaFreeAsync(cnt, st);
+	cudaFreeAsync(k2, st);
+	*v = v2;
+	return BSG_OK;
+}
+
+// Block ILU2 of a 3 x 3 block matrix: the factor f gets the block form
+// (d_bia / d_bja / d_bl / d_bu, column-major blocks) and the solve-ready
+// forms (strict parts as point CSR + SELL copies, block diagonals).
+int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out) {
+	if (m->bs != 3) return bsg_set_error(BSG_ERR_UNSUPPORTED, "block factorisation: 3 x 3 blocks only");
+	cudaStream_t st = c->stream;
+	const int nb = m->n;
+	BSG_CUDA(cudaMemsetAsync(c->d_stat, 0, sizeof(bsg_devstat), st));
+	BSG_CUDA(cudaEventRecord(c->ev0, st));
+	// ---- CombineLU on the device
+	BALLOC(cnt, int, nb + 1);
+	BALLOC(koff, int, nb + 1);
+	BSG_CUDA(cudaMemsetAsync(cnt + nb, 0, sizeof(int), st));
+	BSG_COUNT(1);
+	k_bc_count<<<nb_(nb, 256), 256, 0, st>>>(nb, m->d_ia, m->d_ja, cnt);
+	size_t tmp = 0;
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, koff, nb + 1, st));
+	BALLOC(dtmp, char, tmp + 1);
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(dtmp, tmp, cnt, koff, nb + 1, st));
+	int nk = 0;
+	BSG_CUDA(cudaMemcpyAsync(&nk, koff + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+	BSG_CUDA(cudaStreamSynchronize(st));
+	BALLOC(keys, unsigned long long, nk);
+	BALLOC(keys2, unsigned long long, nk);
+	BALLOC(src, int, nk);
+	BALLOC(src2, int, nk);
+	BSG_COUNT(1);
+	k_bc_keys<<<nb_(nb, 256), 256, 0, st>>>(nb, m->d_ia, m->d_ja, koff, keys, src);
+	size_t t2 = 0;
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, keys, keys2, src, src2, nk, 0, 64, st));
+	BALLOC(dtmp2, char, t2 + 1);
+	BSG_CUDA(cub::DeviceRadixSort::SortPairs(dtmp2, t2, keys, keys2, src, src2, nk, 0, 64, st));
+	BALLOC(flag, int, nk);
+	BALLOC(id, int, nk);
+	BSG_COUNT(1);
+	k_bc_flags<<<nb_(nk, 256), 256, 0, st>>>(nk, keys2, flag);
+	size_t t3 = 0;
+	BSG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, t3, flag, id, nk, st));
+	BALLOC(dtmp3, char, t3 + 1);
+	BSG_CUDA(cub::DeviceScan::InclusiveSum(dtmp3, t3, flag, id, nk, st));
+	int nnzb = 0;
+	BSG_CUDA(cudaMemcpyAsync(&nnzb, id + nk - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+	BSG_CUDA(cudaStreamSynchronize(st));
+	BALLOC(bja, int, nnzb);
+	BALLOC(bia, int, nb + 1);
+	BALLOC(rowcnt, int, nb + 1);
+	BSG_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(int) * (nb + 1), st));
+	BALLOC(bal, double, (long long)nnzb * 9);
+	BALLOC(bau, double, (long long)nnzb * 9);
+	BSG_CUDA(cudaMemsetAsync(bal, 0, sizeof(double) * 9 * (size_t)nnzb, st));
+	BSG_CUDA(cudaMemsetAsync(bau, 0, sizeof(double) * 9 * (size_t)nnzb, st));
+	BSG_COUNT(2);
+	k_bc_pattern<<<nb_(nk, 256), 256, 0, st>>>(nk, keys2, id, flag, bja, rowcnt);
+	k_bc_values<<<nb_(nk, 256), 256, 0, st>>>(nk, src2, id, m->d_a, bal, bau);
+	size_t t4 = 0;
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t4, rowcnt, bia, nb + 1, st));
+	BALLOC(dtmp4, char, t4 + 1);
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(dtmp4, t4, rowcnt, bia, nb + 1, st));
+	// ---- scaling
+	BALLOC(scll, double, (long long)nb * 9);
+	BALLOC(sclu, double, (long long)nb * 9);
+	BALLOC(sinvl, double, (long long)nb * 9);
+	BALLOC(sinvu, double, (long long)nb * 9);
+	BALLOC(diagg, double, (long long)nb * 9);
+	BSG_COUNT(1);
+	k_bscale<<<nb_(nb, 128), 128, 0, st>>>(nb, bia, bau, p->sclmin, scll, sclu, sinvl, sinvu, diagg);
+	// ---- row kernel workspace
+	const double mem = fabs(p->memory) > 1.0 ? fabs(p->memory) : 1.0;
+	const long long cap = (long long)(mem * (double)nnzb) + nb + 16;
+	if (cap > 0x7fffffffLL) return bsg_set_error(BSG_ERR_ARG, "block factorisation: workspace above 2^31 blocks");
+	const int pool_cap = (int)(nb + cap / CH + 16);
+	BALLOC(fml, double, (long long)nb * 9);
+	BALLOC(fmu, double, (long long)nb * 9);
+	BALLOC(imask, int, nb);
+	BALLOC(ig, int, nb + 1);
+	BALLOC(jg, int, cap);
+	BALLOC(gl, double, cap * 9);
+	BALLOC(gu, double, cap * 9);
+	BALLOC(mhead, int, nb);
+	BALLOC(mtail, int, nb);
+	BALLOC(mcnt, int, nb);
+	BALLOC(chk, int, (long long)pool_cap * CH);
+	BALLOC(chq, int, (long long)pool_cap * CH);
+	BALLOC(chnext, int, pool_cap);
+	BALLOC(pool, int, 1);
+	BALLOC(nstored, unsigned long long, 2);
+	BSG_CUDA(cudaMemsetAsync(imask, 0xff, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMemsetAsync(mhead, 0xff, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMemsetAsync(mtail, 0xff, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMemsetAsync(mcnt, 0, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMemsetAsync(pool, 0, sizeof(int), st));
+	BSG_CUDA(cudaMemsetAsync(nstored, 0, sizeof(unsigned long long) * 2, st));
+	BArgs A;
+	A.nb = nb; A.bia = bia; A.bja = bja; A.al = bal; A.au = bau; A.scll = scll; A.sclu = sclu; A.diagg = diagg;
+	A.fml = fml; A.fmu = fmu; A.imask = imask; A.ig = ig; A.jg = jg; A.gl = gl; A.gu = gu; A.cap = cap;
+	A.mhead = mhead; A.mtail = mtail; A.mcnt = mcnt; A.chk = chk; A.chq = chq; A.chnext = chnext; A.pool = pool;
+	A.pool_cap = pool_cap; A.tau1 = p->tau1; A.tau2 = p->tau2; A.theta = p->theta; A.pivmin = p->pivmin;
+	A.nstored = nstored; A.st = c->d_stat;
+	BSG_CUDA(cudaFuncSetAttribute(k_bilu2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BSMEM));
+	BSG_COUNT(1);
+	k_bilu2_rows<<<1, BT, BSMEM, st>>>(A);
+	BSG_CUDA(cudaGetLastError());
+	int rc = bsg_check_devstat(c);
+	if (rc) return rc;
+	// ---- U part scaled back
+	BALLOC(fcnt, int, nb + 1);
+	BSG_CUDA(cudaMemsetAsync(fcnt + nb, 0, sizeof(int), st));
+	BSG_COUNT(1);
+	k_bfin_count<<<nb_(nb, 256), 256, 0, st>>>(nb, ig, jg, fcnt);
+	bsg_fct *f = new bsg_fct();
+	f->ctx = c;
+	f->n = 3 * nb;
+	f->bs = 3;
+	f->nb = nb;
+	f->kind = 1;
+	auto fail = [&](int code) {
+		bsg_fct_free(f);
+		return code;
+	};
+#define FCUDA(call)                                                             \
+	do {                                                                        \
+		cudaError_t e_ = (call);                                                \
+		if (e_ != cudaSuccess) return fail(bsg_set_cuda_error(e_, #call, __FILE__, __LINE__)); \
+	} while (0)
+	FCUDA(cudaMallocAsync(&f->d_bia, sizeof(int) * (nb + 1), st));
+	size_t t5 = 0;
+	FCUDA(cub::DeviceScan::ExclusiveSum(nullptr, t5, fcnt, f->d_bia, nb + 1, st));
+	void *dt5;
+	FCUDA(cudaMallocAsync(&dt5, t5 + 1, st));
+	FCUDA(cub::DeviceScan::ExclusiveSum(dt5, t5, fcnt, f->d_bia, nb + 1, st));
+	cudaFreeAsync(dt5, st);
+	int nf = 0;
+	FCUDA(cudaMemcpyAsync(&nf, f->d_bia + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+	unsigned long long hs[2];
+	FCUDA(cudaMemcpyAsync(hs, nstored, sizeof(hs), cudaMemcpyDeviceToHost, st));
+	FCUDA(cudaStreamSynchronize(st));
+	f->nnz = nf;
+	FCUDA(cudaMallocAsync(&f->d_bja, sizeof(int) * (nf > 0 ? nf : 1), st));
+	FCUDA(cudaMallocAsync(&f->d_bl, sizeof(double) * 9 * (size_t)(nf > 0 ? nf : 1), st));
+	FCUDA(cudaMallocAsync(&f->d_bu, sizeof(double) * 9 * (size_t)(nf > 0 ? nf : 1), st));
+	BSG_COUNT(1);
+	k_bfin_fill<<<nb_(nb, 128), 128, 0, st>>>(nb, ig, jg, gl, gu, scll, sclu, sinvl, sinvu, f->d_bia, f->d_bja,
+	                                           f->d_bl, f->d_bu);
+	FCUDA(cudaGetLastError());
+	f->density = 9.0 * (double)hs[0] / (9.0 * (double)nnzb);
+	f->density2 = 9.0 * (double)hs[1] / (9.0 * (double)nnzb);
+	FCUDA(cudaEventRecord(c->ev1, st));
+	// ---- solve-ready forms
+	const int n = 3 * nb;
+	const long long nstrict = 9LL * (nf - nb);
+	FCUDA(cudaMallocAsync(&f->d_ur_i, sizeof(int) * (n + 1), st));
+	{
+		int *ucnt;
+		FCUDA(cudaMallocAsync(&ucnt, sizeof(int) * (n + 1), st));
+		FCUDA(cudaMemsetAsync(ucnt + n, 0, sizeof(int), st));
+		BSG_COUNT(1);
+		k_bsu_count<<<nb_(nb, 256), 256, 0, st>>>(nb, f->d_bia, ucnt);
+		size_t t6 = 0;
+		FCUDA(cub::DeviceScan::ExclusiveSum(nullptr, t6, ucnt, f->d_ur_i, n + 1, st));
+		void *dt6;
+		FCUDA(cudaMallocAsync(&dt6, t6 + 1, st));
+		FCUDA(cub::DeviceScan::ExclusiveSum(dt6, t6, ucnt, f->d_ur_i, n + 1, st));
+		cudaFreeAsync(dt6, st);
+		cudaFreeAsync(ucnt, st);
+	}
+	FCUDA(cudaMallocAsync(&f->d_ur_j, sizeof(int) * (nstrict > 0 ? nstrict : 1), st));
+	FCUDA(cudaMallocAsync(&f->d_ur_v, sizeof(double) * (nstrict > 0 ? nstrict : 1), st));
+	BSG_COUNT(1);
+	k_bsu_fill<<<nb_(nb, 256), 256, 0, st>>>(nb, f->d_bia, f->d_bja, f->d_bu, f->d_ur_i, f->d_ur_j, f->d_ur_v);
+	{
+		unsigned long long *lk;
+		double *lv;
+		FCUDA(cudaMallocAsync(&lk, sizeof(unsigned long long) * (nstrict > 0 ? nstrict : 1), st));
+		FCUDA(cudaMallocAsync(&lv, sizeof(double) * (nstrict > 0 ? nstrict : 1), st));
+		BSG_COUNT(1);
+		k_bsl_keys<<<nb_(nb, 256), 256, 0, st>>>(nb, f->d_bia, f->d_bja, f->d_bl, lk, lv);
+		int rc2 = keys_csr(st, n, nstrict, lk, lv, &f->d_lr_i, &f->d_lr_j, &f->d_lr_v);
+		cudaFreeAsync(lk, st);
+		cudaFreeAsync(lv, st);
+		if (rc2) return fail(rc2);
+	}
+	f->nnz_strict = (int)nstrict;
+	FCUDA(cudaMallocAsync(&f->d_bdl, sizeof(double) * 9 * (size_t)nb, st));
+	FCUDA(cudaMallocAsync(&f->d_bdu, sizeof(double) * 9 * (size_t)nb, st));
+	FCUDA(cudaMallocAsync(&f->d_ones, sizeof(double) * n, st));
+	BSG_COUNT(2);
+	k_bdiag_pack<<<nb_(nb, 256), 256, 0, st>>>(nb, f->d_bia, f->d_bl, f->d_bu, f->d_bdl, f->d_bdu);
+	k_fill_d<<<nb_(n, 256) < BSG_SMS * 8 ? nb_(n, 256) : BSG_SMS * 8, 256, 0, st>>>(n, f->d_ones, 1.0);
+	int rc3 = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 0, &f->sl, 0);
+	if (!rc3) rc3 = bsg_sell_build(c, n, f->d_ur_i, f->d_ur_j, f->d_ur_v, 0, 0, &f->su, 0);
+	if (rc3) return fail(rc3);
+	FCUDA(cudaStreamSynchronize(st));
+#undef FCUDA
+	*out = f;
+	return BSG_OK;
+}
+
+// FP32 values for the sweeps' strict parts (block diagonals stay FP64)
+int bsg_bfact_make_fp32(bsg_fct *f) {
+	cudaStream_t s = f->ctx->stream;
+	bsg_sell_free(&f->sl, s);
+	bsg_sell_free(&f->su, s);
+	int rc = bsg_sell_build(f->ctx, f->n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 1, &f->sl, 0);
+	if (!rc) rc = bsg_sell_build(f->ctx, f->n, f->d_ur_i, f->d_ur_j, f->d_ur_v, 0, 1, &f->su, 0);
+	if (rc) return rc;
+	f->fp32 = 1;
+	return BSG_OK;
+}
+
+// Block triangular solve (lower: SolveL, else SolveU).  mode 0: exact (one
+// warp, rows in order); mode 1: nsweeps Jacobi iterates y <- D (x - N y)
+// from y = D x, work = n doubles.
+int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
+                         double *work) {
+	cudaStream_t s = c->stream;
+	const int nb = f->nb;
+	const double *d = lower ? f->d_bdl : f->d_bdu;
+	if (mode == 0) {
+		BSG_COUNT(1);
+		if (lower) k_bsolve_seq<<<1, 32, 0, s>>>(nb, 1, f->d_lr_i, f->d_lr_j, f->d_lr_v, d, x, y);
+		else k_bsolve_seq<<<1, 32, 0, s>>>(nb, 0, f->d_ur_i, f->d_ur_j, f->d_ur_v, d, x, y);
+		BSG_CUDA(cudaGetLastError());
+		return BSG_OK;
+	}
+	if (nsweeps < 1) return bsg_set_error(BSG_ERR_ARG, "block sweeps: nsweeps >= 1");
+	if (nsweeps > 1 && !work) return bsg_set_error(BSG_ERR_ARG, "block sweeps: work vector missing");
+	BSG_COUNT(1);
+	k_bdiag_apply<<<nb_(nb, 256), 256, 0, s>>>(nb, d, x, y);
+	for (int k = 1; k < nsweeps; k++) {
+		int rc = bsg_sell_sweep(s, lower ? &f->sl : &f->su, x, f->d_ones, y, 0, work); // work = x - N y
+		if (rc) return rc;
+		BSG_COUNT(1);
+		k_bdiag_apply<<<nb_(nb, 256), 256, 0, s>>>(nb, d, work, y);
+	}
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}

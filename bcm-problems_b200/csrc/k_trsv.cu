@@ -202,6 +202,7 @@ int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
 // used to time the sweep kernel on its own.
 int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const double *x, const double *yin,
                               double *yout) {
+	if (f->d_bia) return bsg_set_error(BSG_ERR_UNSUPPORTED, "single sweep timing of a block factor");
 	const int n = f->n;
 	const int *rp = lower ? f->d_lr_i : f->d_ur_i;
 	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
@@ -281,6 +282,7 @@ int trisolve_impl(bsg_ctx *c, const bsg_fct *f, const TriOp &t, int mode, int ns
 // FP32 factor, whose sweeps keep their intermediate iterates in FP32 there.
 int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                         double *work) {
+	if (f->d_bia) return bsg_btrisolve_launch(c, f, lower, mode, nsweeps, x, y, work);
 	TriOp t;
 	t.lower = lower ? 1 : 0;
 	t.rp = lower ? f->d_lr_i : f->d_ur_i;
@@ -329,6 +331,7 @@ static int fct_build_transposes(bsg_ctx *c, bsg_fct *f) {
 int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y,
                           double *work) {
 	if (f->kind == 0) return bsg_trisolve_launch(c, f, which == 0 ? 1 : 0, mode, nsweeps, x, y, work);
+	if (f->d_bia) return bsg_set_error(BSG_ERR_UNSUPPORTED, "transposed solves of a block factor");
 	int rc = fct_build_transposes(c, f);
 	if (rc) return rc;
 	TriOp t;

@@ -56,6 +56,7 @@ static int sweep_scratch(int device, double **out) {
 extern "C" int bsg_solve_sweep_static(bsg_ctx *c, const bsg_fct *f, int lower, int nsweeps, const double *x,
                                       double *y) {
 	if (!c || !f || !x || !y || x == y) return bsg_set_error(BSG_ERR_ARG, "bsg_solve_sweep_static: bad argument");
+	if (f->d_bia) return bsg_set_error(BSG_ERR_UNSUPPORTED, "bsg_solve_sweep_static: block factor");
 	if (f->n > BSG_SWEEP_STATIC_ROWS) {
 		char msg[160];
 		std::snprintf(msg, sizeof msg, "bsg_solve_sweep_static: %d rows exceed the static scratch of %d rows", f->n,

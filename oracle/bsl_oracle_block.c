@@ -96,10 +96,92 @@ int orc_combine_lu_block(int nb, int bs, const int *ia, const int *ja, const dou
 	return 0;
 }
 
+/* One-sided Jacobi (Hestenes) SVD of a 3 x 3 block, s descending, U
+ * completed by Gram-Schmidt of unit vectors where a singular value vanishes:
+ * the algorithm the GPU path uses for its pivot and scaling blocks
+ * (bcm-problems_b200/csrc/k_bfact.cu, svd3).  Restated here so that the GPU
+ * factor can be checked against an oracle that takes the same SVD; vt holds
+ * V^T like dgesvd's output. */
+static void svd3_jacobi(const double *a, double *s, double *u, double *vt) {
+	double w[9], vw[9];
+	for (int k = 0; k < 9; k++) {
+		w[k] = a[k];
+		vw[k] = (k % 4) == 0 ? 1.0 : 0.0;
+	}
+	for (int sweep = 0; sweep < 30; sweep++) {
+		double off = 0.0;
+		for (int pq = 0; pq < 3; pq++) {
+			const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+			double al = 0.0, be = 0.0, ga = 0.0;
+			for (int r = 0; r < 3; r++) {
+				al += w[r + 3 * p] * w[r + 3 * p];
+				be += w[r + 3 * q] * w[r + 3 * q];
+				ga += w[r + 3 * p] * w[r + 3 * q];
+			}
+			const double nrm = sqrt(al * be);
+			if (nrm == 0.0 || fabs(ga) <= 1e-16 * nrm) continue;
+			if (fabs(ga) / nrm > off) off = fabs(ga) / nrm;
+			const double zeta = (be - al) / (2.0 * ga);
+			const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+			const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+			for (int r = 0; r < 3; r++) {
+				const double wp = w[r + 3 * p], wq = w[r + 3 * q];
+				w[r + 3 * p] = cs * wp - sn * wq;
+				w[r + 3 * q] = sn * wp + cs * wq;
+				const double vp = vw[r + 3 * p], vq = vw[r + 3 * q];
+				vw[r + 3 * p] = cs * vp - sn * vq;
+				vw[r + 3 * q] = sn * vp + cs * vq;
+			}
+		}
+		if (off <= 1e-15) break;
+	}
+	double sv[3];
+	for (int c = 0; c < 3; c++) sv[c] = sqrt(w[3 * c] * w[3 * c] + w[1 + 3 * c] * w[1 + 3 * c] + w[2 + 3 * c] * w[2 + 3 * c]);
+	int o[3] = {0, 1, 2}, good[3];
+	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
+	if (sv[o[1]] < sv[o[2]]) { const int t = o[1]; o[1] = o[2]; o[2] = t; }
+	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
+	const double smax = sv[o[0]];
+	for (int c = 0; c < 3; c++) {
+		const int k = o[c];
+		s[c] = sv[k];
+		good[c] = sv[k] > 1e-300 && sv[k] > 1e-14 * smax;
+		for (int r = 0; r < 3; r++) {
+			u[r + 3 * c] = good[c] ? w[r + 3 * k] / sv[k] : 0.0;
+			vt[c + 3 * r] = vw[r + 3 * k]; /* V^T(c, r) = V(r, c) */
+		}
+	}
+	for (int c = 0; c < 3; c++) {
+		if (good[c]) continue;
+		for (int e = 0; e < 3; e++) {
+			double x[3] = {e == 0 ? 1.0 : 0.0, e == 1 ? 1.0 : 0.0, e == 2 ? 1.0 : 0.0};
+			for (int d = 0; d < 3; d++) {
+				if (d == c || !good[d]) continue;
+				const double pr = u[3 * d] * x[0] + u[1 + 3 * d] * x[1] + u[2 + 3 * d] * x[2];
+				for (int r = 0; r < 3; r++) x[r] -= pr * u[r + 3 * d];
+			}
+			const double nx = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+			if (nx > 0.5) {
+				for (int r = 0; r < 3; r++) u[r + 3 * c] = x[r] / nx;
+				good[c] = 1;
+				break;
+			}
+		}
+	}
+}
+
+static int g_svd_jacobi = 0; /* orc_ilu2_block_jacobi sets it for one call */
+
 /* The SVD of one B x B block as the reference takes it: dgesvd for B > 1,
  * the sign split for B == 1 (Bslib/ilu2rs.cpp:118-140, :717-740).  a is
  * overwritten; u and vt are column-major (vt holds V^T). */
 static int block_svd(int bs, double *a, double *s, double *u, double *vt, double *work, int lwork) {
+	if (bs == 3 && g_svd_jacobi) {
+		double a0[9];
+		memcpy(a0, a, sizeof a0);
+		svd3_jacobi(a0, s, u, vt);
+		return 0;
+	}
 	if (bs > 1) {
 		int info = 0;
 		dgesvd_("A", "A", &bs, &bs, a, &bs, s, u, &bs, vt, &bs, work, &lwork, &info);
@@ -451,4 +533,16 @@ void orc_solve_u_block(int nb, int bs, const int *ia, const int *ja, const doubl
 			yi[r] = s;
 		}
 	}
+}
+
+/* orc_ilu2_block with the GPU path's Jacobi SVD in place of dgesvd (3 x 3
+ * blocks): the oracle that the GPU block factor is checked against value by
+ * value. */
+int orc_ilu2_block_jacobi(int nb, int bs, const int *is, const int *js, const double *al, const double *au,
+                          double tau1, double tau2, double theta, double sclmin, double pivmin, int **ia_f, int **ja_f,
+                          double **l, double **u, double *stats) {
+	g_svd_jacobi = 1;
+	const int rc = orc_ilu2_block(nb, bs, is, js, al, au, tau1, tau2, theta, sclmin, pivmin, ia_f, ja_f, l, u, stats);
+	g_svd_jacobi = 0;
+	return rc;
 }

@@ -156,12 +156,15 @@ class Oracle:
             self.lib.orc_free(p)
         return ia_s, ja_s, al, au
 
-    def ilu2_block(self, ia_s, ja_s, al, au, bs, tau1=1e-3, tau2=1e-3, theta=0.1, sclmin=1e-8, pivmin=1e-8):
-        """Block ILU2 of a CombineLU'd block matrix: (ia, ja, l, u, (density, density2))."""
+    def ilu2_block(self, ia_s, ja_s, al, au, bs, tau1=1e-3, tau2=1e-3, theta=0.1, sclmin=1e-8, pivmin=1e-8,
+                   jacobi_svd=False):
+        """Block ILU2 of a CombineLU'd block matrix: (ia, ja, l, u, (density, density2)).
+        jacobi_svd: the GPU path's one-sided Jacobi SVD instead of LAPACK's dgesvd."""
         nb = len(ia_s) - 1
         pia, pja, pl, pu = _ip(), _ip(), _dp(), _dp()
         st = (C.c_double * 3)()
-        rc = self.lib.orc_ilu2_block(nb, bs, _i(ia_s), _i(ja_s), _d(al), _d(au), C.c_double(tau1), C.c_double(tau2),
+        f = self.lib.orc_ilu2_block_jacobi if jacobi_svd else self.lib.orc_ilu2_block
+        rc = f(nb, bs, _i(ia_s), _i(ja_s), _d(al), _d(au), C.c_double(tau1), C.c_double(tau2),
                                      C.c_double(theta), C.c_double(sclmin), C.c_double(pivmin), C.byref(pia),
                                      C.byref(pja), C.byref(pl), C.byref(pu), st)
         if rc != 0:

@@ -146,15 +146,16 @@ def test_big_rows_match_oracle(ctx, oracle, case, kind):
 
 @pytest.mark.parametrize("kind", ["ilu2", "ich2"])
 def test_block_matrix_factors_point_expansion(ctx, oracle, kind):
-    """A 3x3 block matrix is factored through its point expansion: the same
-    factor as the point CSR copy of the same operator, bit for bit; the
-    Krylov solve then runs with the block SpMV and the point factor."""
+    """With blockfct = 0 a 3x3 block matrix is factored through its point
+    expansion: the same factor as the point CSR copy of the same operator, bit
+    for bit; the Krylov solve then runs with the block SpMV and the point
+    factor.  (IC2 of a block matrix always takes this path.)"""
     import bsg
     import torch
     s = P.lame3d(6, 0.3, 1.0, 3)
     pt = s.to_point()
     p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, eps=1e-9,
-                          ittype=0, sttype=1, restart=40, krylov=1)
+                          ittype=0, sttype=1, restart=40, krylov=1, blockfct=0)
     if kind == "ich2":
         m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
         u = pt.upper()
