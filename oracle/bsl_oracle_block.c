@@ -24,6 +24,8 @@
 
 #include "bsl_oracle.h"
 
+extern void dsyev_(const char *jobz, const char *uplo, const int *n, double *a, const int *lda, double *w,
+                   double *work, const int *lwork, int *info);
 extern void dgesvd_(const char *jobu, const char *jobvt, const int *m, const int *n, double *a, const int *lda,
                     double *s, double *u, const int *ldu, double *vt, const int *ldvt, double *work, const int *lwork,
                     int *info);
@@ -545,4 +547,226 @@ int orc_ilu2_block_jacobi(int nb, int bs, const int *is, const int *js, const do
 	const int rc = orc_ilu2_block(nb, bs, is, js, al, au, tau1, tau2, theta, sclmin, pivmin, ia_f, ja_f, l, u, stats);
 	g_svd_jacobi = 0;
 	return rc;
+}
+
+/* Block IC2 of an upper-stored symmetric block matrix (CSMatrixRS::Ich2,
+ * Bslib/ich2rs.cpp:1075-1380): the symmetric form of the block ILU2 above
+ * with one mask, the diagonal blocks scaled by their eigenvectors (LAPACK
+ * dsyev, Ich2AllocScale :26-250) and the pivots taken from the
+ * eigendecomposition of the pivot block, eigenvalues in descending order
+ * (Ich2PivScaleRow :532-647).  A negative eigenvalue is an error (-2), as
+ * the reference throws.  Output: U (L = U^T) on its pattern, scaled back
+ * (Ich2StoreScaleU :822-943); stats as orc_ilu2_block. */
+int orc_ich2_block(int nb, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
+                   double theta, int **ia_f, int **ja_f, double **uo, double *stats) {
+	const int b2 = bs * bs, lwork = 10 * bs;
+	double *scl = malloc(sizeof(double) * (size_t)nb * b2), *sinv = malloc(sizeof(double) * (size_t)nb * b2);
+	double *diagg = malloc(sizeof(double) * (size_t)nb * b2), *fm = calloc((size_t)nb * b2, sizeof(double));
+	int *imask = malloc(sizeof(int) * nb), *lstloc = malloc(sizeof(int) * nb), *lstupd = malloc(sizeof(int) * nb);
+	int *indlst = malloc(sizeof(int) * nb), *iv = malloc(sizeof(int) * nb), *madj = malloc(sizeof(int) * nb);
+	int *ibegm = malloc(sizeof(int) * nb);
+	double aloc[64], vloc[64], eig[8], work[80], delem[64], lel[64];
+	if (bs > 8 || !scl || !sinv || !diagg || !fm || !imask || !lstloc || !lstupd || !indlst || !iv || !madj || !ibegm)
+		return -1;
+	for (int i = 0; i < nb; i++) { /* Ich2AllocScale */
+		const double *d = a + (size_t)ia[i] * b2;
+		double *sl = scl + (size_t)i * b2, *si = sinv + (size_t)i * b2;
+		int info = 0;
+		memcpy(aloc, d, sizeof(double) * b2);
+		dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
+		if (info) return -3;
+		for (int k = 0; k < bs; k++)
+			if (eig[k] < 0.0) return -2;
+		for (int k = 0; k < bs; k++) eig[k] = sqrt(eig[k]);
+		for (int r = 0; r < bs; r++)
+			for (int c = 0; c < bs; c++) si[r + c * bs] = aloc[r + c * bs] * eig[c]; /* Q diag(l^1/2) */
+		for (int k = 0; k < bs; k++) eig[k] = 1.0 / eig[k];
+		for (int r = 0; r < bs; r++)
+			for (int c = 0; c < bs; c++) sl[r + c * bs] = aloc[c + r * bs] * eig[r]; /* diag(l^-1/2) Q^T */
+		mm(bs, sl, 1, bs, d, 1, bs, aloc);
+		mm(bs, aloc, 1, bs, sl, bs, 1, diagg + (size_t)i * b2);
+	}
+	int cap = ia[nb] * 2 + nb + 16, nzjg = 0;
+	int *ig = malloc(sizeof(int) * ((size_t)nb + 1)), *jg = malloc(sizeof(int) * cap), *addrg = malloc(sizeof(int) * cap);
+	double *g = malloc(sizeof(double) * (size_t)cap * b2);
+	if (!ig || !jg || !addrg || !g) return -1;
+	ig[0] = 0;
+	int icycle = -1;
+	for (int i = 0; i < nb; i++) {
+		imask[i] = -1;
+		iv[i] = -1;
+		madj[i] = -1;
+		ibegm[i] = -1;
+	}
+	long long nzu = 0, nzr = 0;
+	for (int irow = 0; irow < nb; irow++) {
+		icycle++;
+		int nlist1 = 0; /* Ich2InitRow */
+		lstloc[nlist1++] = irow;
+		imask[irow] = icycle;
+		memcpy(fm + (size_t)irow * b2, diagg + (size_t)irow * b2, sizeof(double) * b2);
+		for (int p = ia[irow] + 1; p < ia[irow + 1]; p++) {
+			const int jj = ja[p];
+			lstloc[nlist1++] = jj;
+			imask[jj] = icycle;
+			mm(bs, scl + (size_t)irow * b2, 1, bs, a + (size_t)p * b2, 1, bs, aloc);
+			mm(bs, aloc, 1, bs, scl + (size_t)jj * b2, bs, 1, fm + (size_t)jj * b2);
+		}
+		for (int k = ibegm[irow]; k != -1; k = madj[k]) { /* updates, linked-list order */
+			const int j0 = iv[k];
+			const int elmisr = jg[j0] < 0;
+			memcpy(lel, g + (size_t)addrg[j0] * b2, sizeof(double) * b2);
+			int nupd = 0;
+			for (int q = j0; q < ig[k + 1]; q++) {
+				int jc = jg[q];
+				if (elmisr && jc < 0) continue;
+				if (jc < 0) jc = -jc;
+				if (imask[jc] != icycle) {
+					imask[jc] = icycle;
+					lstloc[nlist1++] = jc;
+					memset(fm + (size_t)jc * b2, 0, sizeof(double) * b2);
+				}
+				lstupd[nupd] = jc;
+				indlst[nupd] = q;
+				nupd++;
+			}
+			for (int t = 0; t < nupd; t++) {
+				double *f = fm + (size_t)lstupd[t] * b2;
+				const double *gg = g + (size_t)addrg[indlst[t]] * b2;
+				for (int r = 0; r < bs; r++)
+					for (int c = 0; c < bs; c++)
+						for (int m2 = 0; m2 < bs; m2++) f[r + c * bs] -= lel[m2 + r * bs] * gg[m2 + c * bs];
+			}
+		}
+		{
+			int k = ibegm[irow];
+			while (k != -1) {
+				const int k1 = madj[k];
+				if (iv[k] >= ig[k + 1] - 1) {
+					madj[k] = -1;
+				} else {
+					int c = jg[iv[k] + 1];
+					if (c < 0) c = -c;
+					madj[k] = ibegm[c];
+					ibegm[c] = k;
+				}
+				iv[k]++;
+				k = k1;
+			}
+		}
+		int nlist2 = 0; /* Ich2FiltrRow */
+		double *fdi = fm + (size_t)irow * b2;
+		for (int t = 1; t < nlist1; t++) {
+			const int j = lstloc[t];
+			const double *f = fm + (size_t)j * b2;
+			double mx = 0.0;
+			for (int k = 0; k < b2; k++) {
+				const double v = fabs(f[k]);
+				if (v > mx) mx = v;
+			}
+			if (mx >= tau2) {
+				lstupd[nlist2++] = j;
+			} else {
+				double *dj = diagg + (size_t)j * b2;
+				for (int r = 0; r < bs; r++)
+					for (int c = 0; c < bs; c++) {
+						const double v = fabs(f[r + c * bs]) * theta;
+						fdi[r + r * bs] += v;
+						dj[c + c * bs] += v;
+					}
+			}
+		}
+		nlist1 = nlist2;
+		{ /* Ich2PivScaleRow */
+			int info = 0;
+			memcpy(aloc, fdi, sizeof(double) * b2);
+			dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
+			if (info) return -3;
+			for (int r = 0; r < bs; r++) /* eigenpairs in descending order */
+				for (int c = 0; c < bs; c++) delem[(bs - r - 1) * bs + c] = aloc[r * bs + c];
+			memcpy(aloc, delem, sizeof(double) * b2);
+			for (int k = 0; k < bs; k++) work[bs - k - 1] = eig[k];
+			for (int k = 0; k < bs; k++) eig[k] = work[k];
+			for (int k = 0; k < bs; k++) {
+				if (eig[k] < 0.0) return -2;
+				eig[k] = sqrt(eig[k]);
+				eig[k] = 1.0 / eig[k];
+			}
+			for (int r = 0; r < bs; r++)
+				for (int c = 0; c < bs; c++) delem[r + c * bs] = aloc[c + r * bs] * eig[r];
+			for (int t = 0; t < nlist1; t++) {
+				double *f = fm + (size_t)lstupd[t] * b2;
+				mm(bs, delem, 1, bs, f, 1, bs, vloc);
+				memcpy(f, vloc, sizeof(double) * b2);
+			}
+		}
+		if (nlist1) qsort(lstupd, nlist1, sizeof(int), cmp_int);
+		if (nzjg + nlist1 + 1 > cap) {
+			while (nzjg + nlist1 + 1 > cap) cap *= 2;
+			jg = realloc(jg, sizeof(int) * cap);
+			addrg = realloc(addrg, sizeof(int) * cap);
+			g = realloc(g, sizeof(double) * (size_t)cap * b2);
+			if (!jg || !addrg || !g) return -1;
+		}
+		if (nlist1) {
+			iv[irow] = nzjg + 1;
+			madj[irow] = ibegm[lstupd[0]];
+			ibegm[lstupd[0]] = irow;
+		}
+		jg[nzjg] = irow; /* Ich2StoreRow */
+		addrg[nzjg] = nzjg;
+		for (int r = 0; r < bs; r++)
+			for (int c = 0; c < bs; c++) g[(size_t)nzjg * b2 + r + c * bs] = delem[c + r * bs];
+		nzjg++;
+		nzu += b2;
+		for (int t = 0; t < nlist1; t++) {
+			const int j = lstupd[t];
+			const double *f = fm + (size_t)j * b2;
+			double mx = 0.0;
+			for (int k = 0; k < b2; k++) {
+				const double v = fabs(f[k]);
+				if (v > mx) mx = v;
+			}
+			const int keep = mx >= tau1;
+			jg[nzjg] = keep ? j : -j;
+			addrg[nzjg] = nzjg;
+			memcpy(g + (size_t)nzjg * b2, f, sizeof(double) * b2);
+			if (keep) nzu += b2;
+			else nzr += b2;
+			nzjg++;
+		}
+		ig[irow + 1] = nzjg;
+	}
+	int nkeep = 0;
+	for (int q = 0; q < nzjg; q++)
+		if (jg[q] >= 0) nkeep++;
+	int *fi = malloc(sizeof(int) * ((size_t)nb + 1)), *fj = malloc(sizeof(int) * (nkeep > 0 ? nkeep : 1));
+	double *fu = malloc(sizeof(double) * (size_t)(nkeep > 0 ? nkeep : 1) * b2);
+	if (!fi || !fj || !fu) return -1;
+	int o = 0;
+	fi[0] = 0;
+	for (int i = 0; i < nb; i++) {
+		for (int q = ig[i]; q < ig[i + 1]; q++) {
+			const int jj = jg[q];
+			if (jj < 0) continue;
+			fj[o] = jj;
+			const double *gg = g + (size_t)addrg[q] * b2;
+			if (jj == i) mm(bs, scl + (size_t)i * b2, bs, 1, gg, 1, bs, fu + (size_t)o * b2);
+			else mm(bs, gg, 1, bs, sinv + (size_t)jj * b2, bs, 1, fu + (size_t)o * b2);
+			o++;
+		}
+		fi[i + 1] = o;
+	}
+	if (stats) {
+		const double nza = (double)ia[nb] * b2;
+		stats[0] = (double)nzu / nza;
+		stats[1] = (double)nzr / nza;
+		stats[2] = 0.0;
+	}
+	*ia_f = fi;
+	*ja_f = fj;
+	*uo = fu;
+	free(scl); free(sinv); free(diagg); free(fm); free(imask); free(lstloc); free(lstupd); free(indlst);
+	free(iv); free(madj); free(ibegm); free(ig); free(jg); free(addrg); free(g);
+	return 0;
 }

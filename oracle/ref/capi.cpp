@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iostream>
 #include <chrono>
 #include "smatrix.h"
 #include "slvparam.h"
@@ -317,6 +318,39 @@ int ref_solve_u_block(int nsup, int bs, const int *ia, const int *ja, const doub
 	m.SolveU(vx, vy);
 	std::memcpy(y, vy.GetVect(), sizeof(double) * nsup * bs);
 	return 0;
+}
+
+// Block IC2 (CSMatrixRS::Ich2, Bslib/ich2rs.cpp:1075) of an upper-stored
+// symmetric block matrix; U comes back (L = U^T).
+int ref_ich2_block(int nsup, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
+                   double theta, double memory, int **ia_f, int **ja_f, double **a_u, double *stats) {
+	try {
+		RSBuild m(nsup, bs, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+		std::ofstream fout("/dev/null");
+		// CSMatrixRS::Ich2 prints its histograms and statistics to cout and to
+		// the log stream whatever msglev says (Bslib/ich2rs.cpp:244-245,
+		// :1276-1297); failed streams format nothing
+		fout.setstate(std::ios::badbit);
+		const std::ios::iostate cst = std::cout.rdstate();
+		std::cout.setstate(std::ios::badbit);
+		double t0 = now_s();
+		CSMatrixRS u;
+		try {
+			u = m.Ich2(fout, p);
+		} catch (...) {
+			std::cout.clear(cst);
+			throw;
+		}
+		double t1 = now_s();
+		std::cout.clear(cst);
+		RSBuild::export_rs(u, bs, ia_f, ja_f, a_u);
+		if (stats) { stats[0] = p.density; stats[1] = p.density2; stats[2] = t1 - t0; }
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
 }
 
 } // extern "C"

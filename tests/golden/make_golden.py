@@ -77,8 +77,8 @@ def nonsymmetric_blocks(s, skew=0.3):
 
 def main_block():
     """Block (CSMatrixRS) fixtures: CombineLU, block ILU2 with its SVD scaling,
-    block SolveL / SolveU, on a small Lame block matrix and a nonsymmetric
-    variant of it."""
+    block IC2 with its eigenvector scaling, block SolveL / SolveU, on a small
+    Lame block matrix and a nonsymmetric variant of it."""
     ref = RefLib()
     out = {}
     s = P.lame3d(4, sigma=1.0, seed=31)
@@ -96,6 +96,13 @@ def main_block():
         out[f"{tag}_density"] = np.array(st[:2])
         out[f"{tag}_solve_l"] = ref.solve_l_block(ia_f, ja_f, l, bs, x)
         out[f"{tag}_solve_u"] = ref.solve_u_block(ia_f, ja_f, u, bs, x)
+    u = s.upper()
+    out["ua_ia"], out["ua_ja"], out["ua_a"] = u.ia, u.ja, u.a
+    for tag, t1, t2 in (("bic_a", 1e-3, 1e-3), ("bic_b", 1e-2, 1e-5)):
+        ia_f, ja_f, uf, st = ref.ich2_block(u.ia, u.ja, u.a, bs, tau1=t1, tau2=t2, theta=0.1)
+        out[f"{tag}_ia"], out[f"{tag}_ja"], out[f"{tag}_u"] = ia_f, ja_f, uf
+        out[f"{tag}_solve_l"] = ref.solve_l_block(ia_f, ja_f, uf, bs, x)
+        out[f"{tag}_solve_u"] = ref.solve_u_block(ia_f, ja_f, uf, bs, x)
     path = os.path.join(HERE, "lame_block.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -174,6 +174,22 @@ class Oracle:
             self.lib.orc_free(p)
         return ia_f, ja_f, l, u, (st[0], st[1])
 
+    def ich2_block(self, ia, ja, a, bs, tau1=1e-3, tau2=1e-3, theta=0.1):
+        """Block IC2 of an upper-stored symmetric block matrix: (ia, ja, u, (density, density2))."""
+        nb = len(ia) - 1
+        pia, pja, pu = _ip(), _ip(), _dp()
+        st = (C.c_double * 3)()
+        rc = self.lib.orc_ich2_block(nb, bs, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+                                     C.c_double(theta), C.byref(pia), C.byref(pja), C.byref(pu), st)
+        if rc == -2:
+            raise ArithmeticError("negative pivot in block IC2")
+        if rc != 0:
+            raise RuntimeError(f"orc_ich2_block failed ({rc})")
+        ia_f, ja_f, (u,) = _take_bsr(nb, bs, pia, pja, pu)
+        for p in (pia, pja, pu):
+            self.lib.orc_free(p)
+        return ia_f, ja_f, u, (st[0], st[1])
+
     def solve_l_block(self, ia, ja, a, bs, x):
         nb = len(ia) - 1
         y = np.zeros(nb * bs)
@@ -308,3 +324,16 @@ class RefLib:
         y = np.zeros(nb * bs)
         self._err(self.lib.ref_solve_u_block(nb, bs, _i(ia), _i(ja), _d(a), _d(x), _d(y)))
         return y
+
+    def ich2_block(self, ia, ja, a, bs, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0):
+        """CSMatrixRS::Ich2 of an upper-stored block matrix: (ia, ja, u, (density, density2, seconds))."""
+        nb = len(ia) - 1
+        pia, pja, pu = _ip(), _ip(), _dp()
+        st = (C.c_double * 3)()
+        self._err(self.lib.ref_ich2_block(nb, bs, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+                                          C.c_double(theta), C.c_double(memory), C.byref(pia), C.byref(pja),
+                                          C.byref(pu), st))
+        ia_f, ja_f, (u,) = _take_bsr(nb, bs, pia, pja, pu)
+        for p in (pia, pja, pu):
+            self.lib.ref_free(p)
+        return ia_f, ja_f, u, (st[0], st[1], st[2])

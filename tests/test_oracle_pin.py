@@ -161,3 +161,24 @@ def test_live_reference_block_ilu2_larger_cases(oracle, reflib):
         o = oracle.ilu2_block(*oracle.combine_lu_block(s.ia, s.ja, s.a, 3), 3, tau1=t1, tau2=t2)
         assert np.array_equal(o[0], ia_f) and np.array_equal(o[1], ja_f)
         assert np.array_equal(o[2], l) and np.array_equal(o[3], u)
+
+
+@pytest.mark.parametrize("tag,t1,t2", [("bic_a", 1e-3, 1e-3), ("bic_b", 1e-2, 1e-5)])
+def test_block_ich2_matches_reference(oracle, gold_block, tag, t1, t2):
+    g = gold_block
+    bs = int(g["bs"])
+    ia_f, ja_f, u, st = oracle.ich2_block(g["ua_ia"], g["ua_ja"], g["ua_a"], bs, tau1=t1, tau2=t2, theta=0.1)
+    assert np.array_equal(ia_f, g[f"{tag}_ia"]) and np.array_equal(ja_f, g[f"{tag}_ja"])
+    assert np.array_equal(u, g[f"{tag}_u"])
+    x = g["x"]
+    assert np.array_equal(oracle.solve_l_block(ia_f, ja_f, u, bs, x), g[f"{tag}_solve_l"])
+    assert np.array_equal(oracle.solve_u_block(ia_f, ja_f, u, bs, x), g[f"{tag}_solve_u"])
+
+
+def test_live_reference_block_ich2_larger_cases(oracle, reflib):
+    for s, t1, t2 in [(P.lame3d(9, sigma=1.0, seed=35), 1e-3, 1e-3),
+                      (P.lame_periodic(10, rmin=1.5, rmax=3.0, seed=36), 1e-2, 1e-4)]:
+        u = s.upper()
+        ia_f, ja_f, uf, _ = reflib.ich2_block(u.ia, u.ja, u.a, 3, tau1=t1, tau2=t2)
+        o = oracle.ich2_block(u.ia, u.ja, u.a, 3, tau1=t1, tau2=t2)
+        assert np.array_equal(o[0], ia_f) and np.array_equal(o[1], ja_f) and np.array_equal(o[2], uf)
