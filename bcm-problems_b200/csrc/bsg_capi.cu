@@ -483,9 +483,10 @@ static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **
 	if (kind == 0 && p->fcttyp == 1)
 		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) is not on the GPU path; use fcttyp = 2");
 	bsg_fct *f = nullptr;
-	// a 3x3 block matrix gets the reference's block ILU2 (CSMatrixRS::Ilu2)
-	const bool block = kind == 1 && m->bs == 3 && p->blockfct != 0;
-	int rc = block ? bsg_bfact_run(c, m, p, &f) : bsg_fact_run(c, m, kind, p, &f);
+	// a 3x3 block matrix gets the reference's block factorisations
+	// (CSMatrixRS::Ilu2 / CSMatrixRS::Ich2)
+	const bool block = m->bs == 3 && p->blockfct != 0;
+	int rc = block ? bsg_bfact_run(c, m, kind == 0, p, &f) : bsg_fact_run(c, m, kind, p, &f);
 	if (rc) return rc;
 	float ms = 0;
 	cudaEventElapsedTime(&ms, c->ev0, c->ev1);

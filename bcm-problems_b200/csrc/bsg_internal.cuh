@@ -209,8 +209,8 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y,
                           double *work);
 int bsg_check_devstat(bsg_ctx *c);
-// block ILU2 of a 3x3 block matrix (k_bfact.cu) and its solves
-int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out);
+// block ILU2 / IC2 of a 3x3 block matrix (k_bfact.cu) and its solves
+int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct **out);
 int bsg_bfact_make_fp32(bsg_fct *f);
 int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                          double *work);

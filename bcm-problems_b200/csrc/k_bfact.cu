@@ -183,14 +183,26 @@ __global__ void k_bc_values(int nk, const int *src, const int *id, const double 
 }
 
 // ---- scaling of the diagonal blocks (Ilu2AllocScale) ----------------------
-__global__ void k_bscale(int nb, const int *bia, const double *au, double sclmin, double *scll, double *sclu,
-                         double *sinvl, double *sinvu, double *diagg) {
+// sym (block IC2, Ich2AllocScale Bslib/ich2rs.cpp:26-250): the diagonal
+// block is symmetric; its eigenvectors (V) scale both sides, no sclmin
+// clamp, and a negative eigenvalue (u_k . v_k < 0) is a pivot error
+__global__ void k_bscale(int nb, int sym, const int *bia, const double *au, double sclmin, double *scll, double *sclu,
+                         double *sinvl, double *sinvu, double *diagg, bsg_devstat *st) {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= nb) return;
 	const double *d = au + (size_t)bia[i] * 9;
 	double u[9], v[9], s[3];
 	svd3(d, u, s, v);
-	for (int k = 0; k < 3; k++) s[k] = sqrt(s[k] < sclmin ? sclmin : s[k]);
+	if (sym) {
+		for (int k = 0; k < 3; k++) {
+			if (u[3 * k] * v[3 * k] + u[1 + 3 * k] * v[1 + 3 * k] + u[2 + 3 * k] * v[2 + 3 * k] < 0.0 && s[k] > 0.0)
+				devstat_fail(st, BSG_ERR_PIVOT, i, 1);
+			for (int r = 0; r < 3; r++) u[r + 3 * k] = v[r + 3 * k];
+		}
+		for (int k = 0; k < 3; k++) s[k] = sqrt(s[k]);
+	} else {
+		for (int k = 0; k < 3; k++) s[k] = sqrt(s[k] < sclmin ? sclmin : s[k]);
+	}
 	double *il = sinvl + (size_t)i * 9, *iu = sinvu + (size_t)i * 9, *sl = scll + (size_t)i * 9,
 	       *su = sclu + (size_t)i * 9;
 	for (int r = 0; r < 3; r++)
@@ -222,6 +234,7 @@ struct BArgs {
 	int *pool;                // chunks in use
 	int pool_cap;
 	double tau1, tau2, theta, pivmin;
+	int sym;                  // block IC2: eigendecomposition pivots, L = U^T
 	unsigned long long *nstored; // [0] U blocks, [1] R blocks
 	bsg_devstat *st;
 };
@@ -252,7 +265,7 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 	unsigned char *mr = reinterpret_cast<unsigned char *>(rank_ + LMAX);
 	__shared__ double dsum[BT / 32][3];
 	__shared__ double dl[9], du[9];
-	__shared__ int nm, nl, nk, W, base, fail;
+	__shared__ int nm, nl, nk, W, base, fail, failrow;
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	if (tid == 0) {
 		base = 0;
@@ -291,8 +304,10 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 				} else {
 					mm3(sli, 1, 3, A.au + (size_t)p * 9, 1, 3, t);
 					mm3(t, 1, 3, A.sclu + (size_t)j * 9, 3, 1, A.fmu + (size_t)j * 9);
-					mm3(sui, 1, 3, A.al + (size_t)p * 9, 1, 3, t);
-					mm3(t, 1, 3, A.scll + (size_t)j * 9, 3, 1, A.fml + (size_t)j * 9);
+					if (!A.sym) { // the symmetric form keeps one mask (L = U^T)
+						mm3(sui, 1, 3, A.al + (size_t)p * 9, 1, 3, t);
+						mm3(t, 1, 3, A.scll + (size_t)j * 9, 3, 1, A.fml + (size_t)j * 9);
+					}
 				}
 				atomicExch(A.imask + j, irow);
 				const int slot = atomicAdd(&nl, 1);
@@ -353,10 +368,10 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 			ld9(A.gu + (size_t)e * 9, gu);
 			ld9(A.gl + (size_t)e * 9, gl);
 			mm3(lel, 3, 1, gu, 1, 3, tu); // lel^T gu
-			mm3(uel, 3, 1, gl, 1, 3, tl); // uel^T gl
-			for (int k = 0; k < 9; k++) {
-				atomicAdd(A.fmu + (size_t)c * 9 + k, -tu[k]);
-				atomicAdd(A.fml + (size_t)c * 9 + k, -tl[k]);
+			for (int k = 0; k < 9; k++) atomicAdd(A.fmu + (size_t)c * 9 + k, -tu[k]);
+			if (!A.sym) {
+				mm3(uel, 3, 1, gl, 1, 3, tl); // uel^T gl
+				for (int k = 0; k < 9; k++) atomicAdd(A.fml + (size_t)c * 9 + k, -tl[k]);
 			}
 		}
 		__syncthreads();
@@ -367,7 +382,7 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 			keep[t] = 0;
 			if (c == irow) continue;
 			double fl[9], fu[9];
-			ld9(A.fml + (size_t)c * 9, fl);
+			ld9((A.sym ? A.fmu : A.fml) + (size_t)c * 9, fl);
 			ld9(A.fmu + (size_t)c * 9, fu);
 			double mx = 0.0;
 			for (int k = 0; k < 9; k++) mx = fmax(mx, fmax(fabs(fl[k]), fabs(fu[k])));
@@ -407,7 +422,18 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 			}
 			double u[9], v[9], sv[3];
 			svd3(fd, u, sv, v);
-			for (int k = 0; k < 3; k++) sv[k] = 1.0 / sqrt(sv[k] < A.pivmin ? A.pivmin : sv[k]);
+			if (A.sym) { // Ich2PivScaleRow (Bslib/ich2rs.cpp:532-647): eigenpairs, no clamp
+				for (int k = 0; k < 3; k++) {
+					if (u[3 * k] * v[3 * k] + u[1 + 3 * k] * v[1 + 3 * k] + u[2 + 3 * k] * v[2 + 3 * k] < 0.0 && sv[k] > 0.0) {
+						fail = 5;
+						failrow = irow;
+					}
+					for (int r = 0; r < 3; r++) u[r + 3 * k] = v[r + 3 * k];
+					sv[k] = 1.0 / sqrt(sv[k]);
+				}
+			} else {
+				for (int k = 0; k < 3; k++) sv[k] = 1.0 / sqrt(sv[k] < A.pivmin ? A.pivmin : sv[k]);
+			}
 			for (int r = 0; r < 3; r++)
 				for (int c = 0; c < 3; c++) {
 					dl[r + 3 * c] = u[c + 3 * r] * sv[r]; // diag(s^-1/2) U^T
@@ -418,6 +444,7 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 			nk = K;
 		}
 		__syncthreads();
+		if (fail) break;
 		if ((long long)base + 1 + nk > A.cap) {
 			if (tid == 0) fail = 3;
 			break;
@@ -445,10 +472,14 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 			const int c = lst[t];
 			const int pos = base + 1 + rank_[t];
 			double fl[9], fu[9], tl[9], tu[9];
-			ld9(A.fml + (size_t)c * 9, fl);
 			ld9(A.fmu + (size_t)c * 9, fu);
-			mm3(du, 1, 3, fl, 1, 3, tl);
 			mm3(dl, 1, 3, fu, 1, 3, tu);
+			if (A.sym) {
+				for (int k = 0; k < 9; k++) tl[k] = tu[k];
+			} else {
+				ld9(A.fml + (size_t)c * 9, fl);
+				mm3(du, 1, 3, fl, 1, 3, tl);
+			}
 			double mx = 0.0;
 			for (int k = 0; k < 9; k++) {
 				A.gl[(size_t)pos * 9 + k] = tl[k];
@@ -489,7 +520,10 @@ __global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
 		__syncthreads();
 		if (fail) break;
 	}
-	if (tid == 0 && fail) devstat_fail(A.st, BSG_ERR_WORKSPACE, 0, 100 + fail);
+	if (tid == 0 && fail) {
+		if (fail == 5) devstat_fail(A.st, BSG_ERR_PIVOT, failrow, 2);
+		else devstat_fail(A.st, BSG_ERR_WORKSPACE, 0, 100 + fail);
+	}
 }
 
 // ---- final: the U part scaled back (Ich2StoreScaleU) ----------------------
@@ -658,10 +692,11 @@ static int keys_csr(cudaStream_t st, int n, long long nk, unsigned long long *ke
 	return BSG_OK;
 }
 
-// Block ILU2 of a 3 x 3 block matrix: the factor f gets the block form
+// Block ILU2 (sym 0) or block IC2 (sym 1, the matrix symmetric) of a 3 x 3
+// block matrix: the factor f gets the block form
 // (d_bia / d_bja / d_bl / d_bu, column-major blocks) and the solve-ready
 // forms (strict parts as point CSR + SELL copies, block diagonals).
-int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out) {
+int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct **out) {
 	if (m->bs != 3) return bsg_set_error(BSG_ERR_UNSUPPORTED, "block factorisation: 3 x 3 blocks only");
 	cudaStream_t st = c->stream;
 	const int nb = m->n;
@@ -723,7 +758,7 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out) {
 	BALLOC(sinvu, double, (long long)nb * 9);
 	BALLOC(diagg, double, (long long)nb * 9);
 	BSG_COUNT(1);
-	k_bscale<<<nb_(nb, 128), 128, 0, st>>>(nb, bia, bau, p->sclmin, scll, sclu, sinvl, sinvu, diagg);
+	k_bscale<<<nb_(nb, 128), 128, 0, st>>>(nb, sym, bia, bau, p->sclmin, scll, sclu, sinvl, sinvu, diagg, c->d_stat);
 	// ---- row kernel workspace
 	const double mem = fabs(p->memory) > 1.0 ? fabs(p->memory) : 1.0;
 	const long long cap = (long long)(mem * (double)nnzb) + nb + 16;
@@ -755,7 +790,7 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out) {
 	A.fml = fml; A.fmu = fmu; A.imask = imask; A.ig = ig; A.jg = jg; A.gl = gl; A.gu = gu; A.cap = cap;
 	A.mhead = mhead; A.mtail = mtail; A.mcnt = mcnt; A.chk = chk; A.chq = chq; A.chnext = chnext; A.pool = pool;
 	A.pool_cap = pool_cap; A.tau1 = p->tau1; A.tau2 = p->tau2; A.theta = p->theta; A.pivmin = p->pivmin;
-	A.nstored = nstored; A.st = c->d_stat;
+	A.nstored = nstored; A.st = c->d_stat; A.sym = sym;
 	BSG_CUDA(cudaFuncSetAttribute(k_bilu2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BSMEM));
 	BSG_COUNT(1);
 	k_bilu2_rows<<<1, BT, BSMEM, st>>>(A);
@@ -772,7 +807,7 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, const bsg_param *p, bsg_fct **out) {
 	f->n = 3 * nb;
 	f->bs = 3;
 	f->nb = nb;
-	f->kind = 1;
+	f->kind = sym ? 0 : 1;
 	auto fail = [&](int code) {
 		bsg_fct_free(f);
 		return code;

@@ -73,9 +73,9 @@ typedef struct bsg_param {
 	int true_residual;/* 1: recompute r = b - Ax in FP64 at every restart/stop   */
 	void *learned;    /* optional learned preconditioner stage (bsg_unet*) for FGMRES */
 	double resrec;    /* output: last recursive residual estimate (relative)     */
-	int blockfct;     /* 3x3 block matrices: 1 (default) block ILU2 with SVD-scaled
-	                     diagonal blocks (CSMatrixRS::Ilu2), 0 point ILU2 of the
-	                     point expansion; IC2 of a block matrix is always point */
+	int blockfct;     /* 3x3 block matrices: 1 (default) block factorisation with
+	                     SVD / eigenvector-scaled diagonal blocks (CSMatrixRS::Ilu2
+	                     / Ich2), 0 point factorisation of the point expansion */
 	int pad[3];
 } bsg_param;
 
@@ -138,7 +138,8 @@ int bsg_fct_to_fp32(bsg_fct *f);
  * l[nnz] (L by columns) and u[nnz] (U by rows), inverse pivots first.  Call
  * with NULL arrays to get nnz only. */
 int bsg_fct_export(const bsg_fct *f, int *nnz, int *iu, int *ju, double *l, double *u);
-/* The block factor of a block ILU2 (CSMatrixRS layout, Bslib/smatrix.h:1040):
+/* The block factor of a block ILU2 / IC2 (CSMatrixRS layout,
+ * Bslib/smatrix.h:1040; for IC2, l == u and L = U^T):
  * nb block rows, *nnzb blocks, ia[nb + 1], ja[nnzb], l / u [9 nnzb] column-
  * major 3x3 blocks, the pivot block first in each row (SolveL / SolveU apply
  * it as Bslib/mvm.cpp:3140 / 3410 do).  BSG_ERR_ARG for a point factor.

@@ -134,3 +134,55 @@ def test_block_gmres_lame(ctx, precision, trisolve):
     r = b - A @ x.cpu().numpy()
     assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b), (p.nitperf, np.linalg.norm(r) / np.linalg.norm(b))
     assert abs(p.resfin - np.linalg.norm(r) / np.linalg.norm(b)) <= 1e-12
+
+
+# ---- block IC2 (CSMatrixRS::Ich2): the symmetric form, eigenvector scaling ----
+
+def _gpu_ich2(ctx, s, **kw):
+    import bsg
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, **kw)
+    m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+    f = bsg.Factor(ctx, m, "ich2", p)
+    return m, f, p
+
+
+@pytest.mark.parametrize("case", ["lame7", "periodic8"])
+def test_block_ich2_matches_reference_preconditioner(ctx, oracle, case):
+    s = CASES[case]()
+    m, f, p = _gpu_ich2(ctx, s)
+    ia, ja, l, u = f.export_block()
+    assert np.array_equal(l, u)  # L = U^T: one set of blocks
+    uu = s.upper()
+    o = oracle.ich2_block(uu.ia, uu.ja, uu.a, 3, tau1=1e-3, tau2=1e-3, theta=0.1)
+    assert abs(p.density - o[3][0]) <= 0.01 * o[3][0]
+    assert _precond_diff(oracle, (ia, ja, u, u), (o[0], o[1], o[2], o[2]), s.n) <= 2e-2
+
+
+@pytest.mark.parametrize("precision,trisolve", [(0, 0), (1, 1)])
+def test_block_ich2_pcg(ctx, precision, trisolve):
+    import bsg
+    import torch
+    s = P.lame3d(8, sigma=1.0, seed=45)
+    m, f, p = _gpu_ich2(ctx, s, eps=1e-8, ittype=0, niter=3000, precision=precision, trisolve=trisolve, nsweeps=6)
+    b = s.rhs[0]
+    x = torch.zeros(3 * s.n, dtype=torch.float64, device="cuda")
+    bsg.pcg(ctx, m, f, _t(b), x, p)
+    A = s.to_scipy()
+    r = b - A @ x.cpu().numpy()
+    assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b), (p.nitperf, np.linalg.norm(r) / np.linalg.norm(b))
+
+
+def test_block_ich2_negative_pivot_is_reported(ctx):
+    """A symmetric block matrix with a negative definite diagonal block: the
+    reference throws (" Negative eigenvalue when scaling"); here the factor
+    call returns BSG_ERR_PIVOT and the context stays usable."""
+    import bsg
+    s = P.lame3d(4, sigma=1.0, seed=46)
+    a = s.a.reshape(-1, 9).copy()
+    a[s.ia[10]] *= -1.0  # block row 10's diagonal block (diagonal first)
+    bad = P.System(s.n, 3, s.ia, s.ja, a.reshape(-1), s.rhs, s.parts)
+    with pytest.raises(bsg.BsgError) as e:
+        _gpu_ich2(ctx, bad)
+    assert e.value.code == bsg.ERR_PIVOT
+    m, f, p = _gpu_ich2(ctx, s)  # the next factorisation works
+    assert p.density > 1.0
