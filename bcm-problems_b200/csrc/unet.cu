@@ -26,6 +26,7 @@
 // weights, FP32 output); weight gradients are FP32 sums on the CUDA cores.
 #include "bsg_internal.cuh"
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -637,6 +638,437 @@ inline int ew(long long n) {
 	return (int)(b < BSG_SMS * 16 ? (b > 0 ? b : 1) : BSG_SMS * 16);
 }
 
+// ---- 5th-generation tensor cores (tcgen05) for the level-0 convolutions ----
+// Level 0 of the network has 16 output channels and x-lines of 128 voxels.
+// For a staged input line (y', z') of 128 voxels the tensor cores compute,
+// one MMA per z tap dz and 16-channel K chunk,
+//     D[x'][(dy, dx, n)] = sum_cin in[x'][y'][z'][cin] W[dz][dy][dx][n][cin],
+// M = 128 voxels, N = 3 x 3 x 16 = 144 (an N = 16 MMA costs as many cycles
+// as an N = 48 one; N = 144 runs the tensor cores at full rate).  Line y'
+// feeds output rows y' + 1 (dy = 0), y' (dy = 1) and y' - 1 (dy = 2), so
+// each output row owns a 48-column accumulator block T[x'][(dx, n)] in
+// tensor memory and the blocks of consecutive rows are laid out at
+// descending column offsets: the three blocks a line feeds are contiguous,
+// and one MMA adds into all of them (two when the ring of 10 blocks wraps).
+// The epilogue forms out[x] = T0[x - 1] + T1[x] + T2[x + 1] with warp
+// shuffles (the grid's x boundary is the tile's: nx = 128 only).
+//
+// Warp roles (288 threads, two CTAs per SM):
+//   warps 0-3  epilogue: TMEM lanes 32w .. 32w + 31; read a finished row's
+//              block, zero it for its next use, shift-add, ReLU, store;
+//   warps 4-7  producers: stage the three z lines of each input line y' into
+//              a ring of slots.  A 16-channel input at full resolution is one
+//              TMA box per z line (4 KB; planes outside the grid read as
+//              zeros); an upsampled one is gathered with cp.async;
+//   warp 8     one thread issues the MMAs and commits them to mbarriers.
+// Each 16-channel part of a staged z line is a 128 x 32-byte K-major tile in
+// the 32-byte swizzle (16-byte halves of row r exchanged when bit 2 of r is
+// set), the layout TMA writes and the tensor cores read with SWIZZLE_32B
+// descriptors.  The weights are K-major without swizzle: core matrices of
+// 8 rows x 16 bytes, rows 16 bytes apart, 8-channel chunks LBO bytes apart.  Every wait is an mbarrier wait bounded
+// by BSG_SPIN_LIMIT_NS; one that expires raises BSG_ERR_TIMEOUT and makes
+// all roles leave their loops.
+namespace tc {
+constexpr int YRUN = 16;  // output rows (y) of one work unit at fixed z
+constexpr int NB = 5;     // 48-column accumulator blocks in the TMEM ring (256 columns allocated)
+constexpr int CTAS = 2;   // CTAs per SM: two pipelines share the tensor cores
+constexpr int THREADS = 288;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address, leading (K-chunk) and
+// stride (8-row group) byte offsets, descriptor version 1, no swizzle
+__device__ __forceinline__ unsigned long long sdesc(unsigned addr, unsigned lbo, unsigned sbo) {
+	return (unsigned long long)((addr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+	       ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// descriptor of a 128-row K-major tile of 32-byte rows in the 32-byte swizzle
+// (SBO = 8 rows x 32 bytes; the leading offset is unused)
+__device__ __forceinline__ unsigned long long sdesc_sw32(unsigned addr) {
+	return (unsigned long long)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((unsigned long long)(256 >> 4) << 32) |
+	       (1ull << 46) | (6ull << 61);
+}
+
+// instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major, M = 128
+__device__ __forceinline__ unsigned idesc(int n) {
+	return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(unsigned tmem, unsigned long long ad, unsigned long long bd, unsigned id) {
+	asm volatile("{\n\t.reg .pred p;\n\tsetp.eq.u32 p, 1, 1;\n\t"
+	             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+	             "l"(ad), "l"(bd), "r"(id));
+}
+__device__ __forceinline__ void commit(unsigned mb) {
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mb) : "memory");
+}
+__device__ __forceinline__ void arrive(unsigned mb) {
+	asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(mb) : "memory");
+}
+__device__ __forceinline__ void arrive_tx(unsigned mb, unsigned bytes) {
+	asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(mb), "r"(bytes)
+	             : "memory");
+}
+// TMA: the 128-voxel x 16-channel box at voxel v0 of a 2D [voxel][16] map
+__device__ __forceinline__ void tma_line(unsigned dst, const CUtensorMap *map, int v0, unsigned mb) {
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+	             "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(v0), "r"(mb)
+	             : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned mb, int count) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count));
+}
+
+// bounded wait on the mbarrier phase `parity`: 1 when it completed, 0 when
+// *abort was raised (here on expiry, or by another role).  The timer is read
+// only once the phase has not completed after 64 polls.
+__device__ __forceinline__ int mbar_wait(unsigned mb, unsigned parity, volatile int *abort) {
+	unsigned long long t0 = 0;
+	for (unsigned it = 0;; it++) {
+		unsigned done;
+		asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		             "selp.u32 %0, 1, 0, p;\n\t}\n"
+		             : "=r"(done)
+		             : "r"(mb), "r"(parity)
+		             : "memory");
+		if (done) return 1;
+		if ((it & 63) == 63) {
+			if (*abort) return 0;
+			const unsigned long long now = globaltimer_ns();
+			if (t0 == 0)
+				t0 = now;
+			else if (now - t0 > BSG_SPIN_LIMIT_NS) {
+				*abort = 1;
+				return 0;
+			}
+		}
+	}
+}
+// TMEM column of the accumulator block of the q-th output row of a CTA
+__device__ __forceinline__ unsigned blk_col(long long q) { return 48u * (unsigned)(NB - 1 - (int)(q % NB)); }
+
+// shared-memory plan of k_conv3_tc<CIN>
+template <int CIN>
+struct Plan {
+	static constexpr int NCH = CIN / 8;                 // 16-byte chunks of a voxel
+	static constexpr int NK = CIN / 16;                 // 16-channel parts (K steps)
+	static constexpr int WDZ = NCH * 144 * 16;          // weights of one z tap: [chunk][(dy,dx,n)][8]
+	static constexpr int TILE = 128 * 32;               // one part of one z line (swizzled)
+	static constexpr int SLOT = 3 * NK * TILE;          // an input line: [dz][part] tiles
+	static constexpr int NSLOT = CIN == 16 ? 6 : 3;     // ring depth (two CTAs per SM either way)
+	static constexpr int XCH = 2 * 4 * 2 * 16 * 4;      // warp-edge exchange: [row parity][warp][side][16] floats
+	// slots first (1024-byte aligned for the swizzle), then weights, exchange
+	static constexpr size_t BYTES = 1024 + (size_t)NSLOT * SLOT + (size_t)3 * WDZ + XCH;
+};
+} // namespace tc
+
+// tmA / tmB: [voxel][16] maps of the A part (when not upsampled) and the B part
+template <int CIN, bool F32OUT>
+__global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
+    k_conv3_tc(ConvArgs a, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+               bsg_devstat *st) {
+	using PL = tc::Plan<CIN>;
+	constexpr int NCH = PL::NCH, NK = PL::NK, NSLOT = PL::NSLOT, NB = tc::NB;
+	extern __shared__ __align__(128) unsigned char sm_raw[];
+	unsigned char *sl = sm_raw + ((1024u - (tc::smem_u32(sm_raw) & 1023u)) & 1023u);
+	unsigned char *sw = sl + (size_t)NSLOT * PL::SLOT;
+	float *xch = reinterpret_cast<float *>(sw + 3 * PL::WDZ);
+	const bool up = a.upA != 0; // A part gathered with cp.async (else TMA, like B)
+	__shared__ __align__(8) unsigned long long bar[2 * NSLOT + 2 * NB + 3];
+	__shared__ unsigned tmem_base;
+	__shared__ volatile int abort_;
+	const unsigned b_full = tc::smem_u32(&bar[0]), b_free = b_full + 8 * NSLOT; // slots
+	const unsigned k_full = b_free + 8 * NSLOT, k_free = k_full + 8 * NB;        // accumulator blocks
+	const unsigned x_bar = k_free + 8 * NB, f_bar = x_bar + 16;                  // edge exchange, drain
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const int ny = a.ny, nz = a.nz, nyc = (ny + tc::YRUN - 1) / tc::YRUN;
+	const long long nunits = (long long)nz * nyc;
+	if (warp == 0) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(tc::smem_u32(&tmem_base)));
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	if (tid == 0) {
+		for (int i = 0; i < NSLOT; i++) {
+			tc::mbar_init(b_full + 8 * i, 1 + (up ? 128 : 0)); // TMA issuer (+ gatherers)
+			tc::mbar_init(b_free + 8 * i, 1);
+		}
+		for (int i = 0; i < NB; i++) {
+			tc::mbar_init(k_full + 8 * i, 1);
+			tc::mbar_init(k_free + 8 * i, 128);
+		}
+		tc::mbar_init(x_bar, 8); // lanes 0 and 31 of the four epilogue warps
+		tc::mbar_init(x_bar + 8, 8);
+		tc::mbar_init(f_bar, 1);
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		abort_ = 0;
+	}
+	// weights: sw[dz][chunk][(dy, dx, n)][8] = W[(dz, dy, dx)][n][chunk * 8 ..]
+	for (int e = tid; e < 27 * 16 * NCH; e += tc::THREADS) {
+		const int ch = e % NCH, r = e / NCH, n = r % 16, tap = r / 16, dz = tap / 9, t9 = tap % 9;
+		const uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.W + ((size_t)tap * 16 + n) * CIN + ch * 8));
+		*reinterpret_cast<uint4 *>(sw + dz * PL::WDZ + ch * (144 * 16) + (t9 * 16 + n) * 16) = v;
+	}
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	const unsigned tmem = tmem_base;
+
+	if (warp < 4) {
+		// ---- epilogue ----
+		const unsigned lanes = (unsigned)(32 * warp) << 16;
+		unsigned zero[16];
+#pragma unroll
+		for (int i = 0; i < 16; i++) zero[i] = 0u;
+		// accumulators start at zero (every MMA accumulates)
+		for (int c = 0; c < NB * 48; c += 16)
+			asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+			                 tmem + lanes + c),
+			             "r"(zero[0]), "r"(zero[1]), "r"(zero[2]), "r"(zero[3]), "r"(zero[4]), "r"(zero[5]), "r"(zero[6]),
+			             "r"(zero[7]), "r"(zero[8]), "r"(zero[9]), "r"(zero[10]), "r"(zero[11]), "r"(zero[12]), "r"(zero[13]),
+			             "r"(zero[14]), "r"(zero[15]));
+		asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+		asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+		for (int i = 0; i < NB; i++) tc::arrive(k_free + 8 * i); // use 0 of every block: free
+		long long q = 0;
+		bool quit = false; // warp-uniform
+		for (long long u = blockIdx.x; u < nunits && !quit; u += gridDim.x) {
+			const int z = (int)(u / nyc), ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+			for (int r = ya; r < yb; r++, q++) {
+				const int b = (int)(q % NB);
+				const bool ok = tc::mbar_wait(k_full + 8 * b, (unsigned)((q / NB) & 1), &abort_);
+				if (!__all_sync(0xffffffffu, ok)) {
+					quit = true;
+					break;
+				}
+				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+				const unsigned col = tmem + lanes + tc::blk_col(q);
+				float t[3][16];
+#pragma unroll
+				for (int dx = 0; dx < 3; dx++) {
+					unsigned rr[16];
+					asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+					             : "=r"(rr[0]), "=r"(rr[1]), "=r"(rr[2]), "=r"(rr[3]), "=r"(rr[4]), "=r"(rr[5]), "=r"(rr[6]),
+					               "=r"(rr[7]), "=r"(rr[8]), "=r"(rr[9]), "=r"(rr[10]), "=r"(rr[11]), "=r"(rr[12]), "=r"(rr[13]),
+					               "=r"(rr[14]), "=r"(rr[15])
+					             : "r"(col + 16 * dx));
+					asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+					for (int i = 0; i < 16; i++) t[dx][i] = __uint_as_float(rr[i]);
+				}
+#pragma unroll
+				for (int dx = 0; dx < 3; dx++)
+					asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+					                 col + 16 * dx),
+					             "r"(zero[0]), "r"(zero[1]), "r"(zero[2]), "r"(zero[3]), "r"(zero[4]), "r"(zero[5]),
+					             "r"(zero[6]), "r"(zero[7]), "r"(zero[8]), "r"(zero[9]), "r"(zero[10]), "r"(zero[11]),
+					             "r"(zero[12]), "r"(zero[13]), "r"(zero[14]), "r"(zero[15]));
+				asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+				asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+				tc::arrive(k_free + 8 * b);
+				// warp edges: lane 31's T0 goes to the next warp, lane 0's T2 to the previous
+				float *xr = xch + (q & 1) * 128;
+				if (lane == 31)
+#pragma unroll
+					for (int i = 0; i < 16; i++) xr[(warp * 2 + 0) * 16 + i] = t[0][i];
+				if (lane == 0)
+#pragma unroll
+					for (int i = 0; i < 16; i++) xr[(warp * 2 + 1) * 16 + i] = t[2][i];
+				if (lane == 0 || lane == 31) tc::arrive(x_bar + 8 * (unsigned)(q & 1));
+				const bool xok = tc::mbar_wait(x_bar + 8 * (unsigned)(q & 1), (unsigned)((q >> 1) & 1), &abort_);
+				if (!__all_sync(0xffffffffu, xok)) {
+					quit = true;
+					break;
+				}
+				// branch-free edges: every lane reads the neighbour warps' values
+				// (one broadcast each), lanes 0 and 31 select them
+				const float4 *xl = reinterpret_cast<const float4 *>(xr + ((warp > 0 ? warp - 1 : 0) * 2 + 0) * 16);
+				const float4 *xg = reinterpret_cast<const float4 *>(xr + ((warp < 3 ? warp + 1 : 3) * 2 + 1) * 16);
+				const bool has_l = lane == 0 && warp > 0, has_r = lane == 31 && warp < 3;
+				const bool zero_l = lane == 0 && warp == 0, zero_r = lane == 31 && warp == 3;
+				float o[16];
+#pragma unroll
+				for (int i4 = 0; i4 < 4; i4++) {
+					const float4 el = xl[i4], er = xg[i4];
+					const float ev_l[4] = {el.x, el.y, el.z, el.w}, ev_r[4] = {er.x, er.y, er.z, er.w};
+#pragma unroll
+					for (int k = 0; k < 4; k++) {
+						const int i = 4 * i4 + k;
+						float lf = __shfl_up_sync(0xffffffffu, t[0][i], 1);
+						float rt = __shfl_down_sync(0xffffffffu, t[2][i], 1);
+						lf = has_l ? ev_l[k] : (zero_l ? 0.f : lf);
+						rt = has_r ? ev_r[k] : (zero_r ? 0.f : rt);
+						o[i] = lf + t[1][i] + rt;
+					}
+				}
+				const long long v = ((long long)z * ny + r) * 128 + 32 * warp + lane;
+				if (F32OUT) {
+					float4 *op = reinterpret_cast<float4 *>(static_cast<float *>(a.out) + v * 16);
+#pragma unroll
+					for (int k = 0; k < 4; k++) op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
+				} else {
+					unsigned pk[8];
+#pragma unroll
+					for (int k = 0; k < 8; k++) {
+						const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(o[2 * k], 0.f), fmaxf(o[2 * k + 1], 0.f));
+						pk[k] = *reinterpret_cast<const unsigned *>(&h);
+					}
+					uint4 *op = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.out) + v * 16);
+					op[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+					op[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+				}
+			}
+		}
+	} else if (warp < 8) {
+		// ---- producers: thread 128 issues the TMA boxes; with an upsampled A
+		// part, thread p also gathers voxel x = p of its three z lines ----
+		const int p = tid - 128;
+		const bool tma_thread = p == 0;
+		const unsigned tx_bytes = 3u * PL::TILE * (unsigned)(NK - (up ? 1 : 0));
+		const int nyA = ny >> a.upA, nxA = 128 >> a.upA;
+		if (tma_thread) {
+			asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tmA)) : "memory");
+			if (NK == 2) asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tmB)) : "memory");
+		}
+		long long g = 0; // lines staged
+		if (up || tma_thread) {
+			bool pending = false;
+			for (long long u = blockIdx.x; u < nunits && !abort_; u += gridDim.x) {
+				const int z = (int)(u / nyc), ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+				const int l0 = max(ya - 1, 0), l1 = min(yb, ny - 1);
+				for (int y = l0; y <= l1; y++, g++) {
+					const int s = (int)(g % NSLOT);
+					const long long k = g / NSLOT;
+					if (k >= 1 && !tc::mbar_wait(b_free + 8 * s, (unsigned)((k - 1) & 1), &abort_)) break;
+					unsigned char *slot = sl + (size_t)s * PL::SLOT;
+					if (tma_thread) {
+						tc::arrive_tx(b_full + 8 * s, tx_bytes);
+#pragma unroll
+						for (int dz = 0; dz < 3; dz++) {
+							const int v0 = ((z + dz - 1) * ny + y) * 128; // outside the grid: zeros
+							if (!up) tc::tma_line(tc::smem_u32(slot + (dz * NK) * PL::TILE), &tmA, v0, b_full + 8 * s);
+							if (NK == 2) tc::tma_line(tc::smem_u32(slot + (dz * NK + 1) * PL::TILE), &tmB, v0, b_full + 8 * s);
+						}
+					}
+					if (up) {
+						// row p of part 0, 16-byte halves h stored at h ^ bit 2 of p
+#pragma unroll
+						for (int dz = 0; dz < 3; dz++) {
+							const int Z = z + dz - 1;
+							const bool in = Z >= 0 && Z < nz;
+							const bf16 *src = in ? a.A + (((long long)(Z >> a.upA) * nyA + (y >> a.upA)) * nxA + (p >> a.upA)) * 16 : a.W;
+							unsigned char *row = slot + (dz * NK) * PL::TILE + p * 32;
+#pragma unroll
+							for (int h = 0; h < 2; h++)
+								asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+								                 tc::smem_u32(row + ((h ^ ((p >> 2) & 1)) << 4))),
+								             "l"(src + 8 * h), "r"(in ? 16u : 0u)
+								             : "memory");
+						}
+						asm volatile("cp.async.commit_group;" ::: "memory");
+						// the previous line's gathers have landed: hand them on
+						if (pending) {
+							asm volatile("cp.async.wait_group 1;" ::: "memory");
+							asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+							tc::arrive(b_full + 8 * (unsigned)((g - 1) % NSLOT));
+						}
+						pending = true;
+					}
+				}
+			}
+			if (up) {
+				asm volatile("cp.async.wait_group 0;" ::: "memory");
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				if (pending) tc::arrive(b_full + 8 * (unsigned)((g - 1) % NSLOT));
+			}
+		}
+		// no TMA copy may still be in flight when the CTA leaves: wait (bounded)
+		// for the last lines' slots
+		if (tma_thread)
+			for (long long h = g > NSLOT ? g - NSLOT : 0; h < g; h++) {
+				volatile int never = 0;
+				tc::mbar_wait(b_full + 8 * (unsigned)(h % NSLOT), (unsigned)((h / NSLOT) & 1), &never);
+			}
+	} else if (lane == 0) {
+		// ---- MMA issue (warp 8, one thread) ----
+		// descriptors of slot 0 / z tap 0 / K chunk 0; offsets add to the start field
+		const unsigned long long adesc0 = tc::sdesc_sw32(tc::smem_u32(sl));
+		const unsigned long long bdesc0 = tc::sdesc(tc::smem_u32(sw), 144 * 16, 128);
+		int q0 = 0, gs = 0;   // rows of earlier units; slot of the current line
+		unsigned gph = 0;     // phase parity of that slot
+		bool issued = false, ok = true;
+		for (long long u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+			const int ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+			const int l0 = max(ya - 1, 0), l1 = min(yb, ny - 1);
+			int acq = ya, done = ya; // next row to acquire / to release
+			for (int y = l0; y <= l1; y++) {
+				const int rlo = max(y - 1, ya), rhi = min(y + 1, yb - 1); // rows this line feeds
+				// the epilogue frees blocks in row order: the newest row's block
+				// being free implies the blocks of the rows before it are
+				if (acq <= rhi) {
+					const int q = q0 + (rhi - ya);
+					ok = tc::mbar_wait(k_free + 8 * (unsigned)(q % NB), (unsigned)((q / NB) & 1), &abort_);
+					acq = rhi + 1;
+				}
+				if (!ok || !(ok = tc::mbar_wait(b_full + 8 * (unsigned)gs, gph, &abort_))) break;
+				asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+				// rows rhi, rhi - 1, .., rlo take dy = jlo, jlo + 1, ..; their blocks
+				// (one less each) sit at ascending columns up to block 0, then the
+				// rest starts again at column 0 (block NB - 1)
+				const int jlo = y + 1 - rhi, nrow = rhi - rlo + 1;
+				const int b0 = (q0 + (rhi - ya)) % NB;
+				const int n1 = min(nrow, b0 + 1), n2 = nrow - n1;
+				const unsigned c1 = tmem + 48u * (unsigned)(NB - 1 - b0);
+				const unsigned id1 = tc::idesc(48 * n1), id2 = tc::idesc(48 * max(n2, 1));
+				const unsigned long long ad = adesc0 + (unsigned)(gs * (PL::SLOT >> 4));
+				const unsigned long long bd1 = bdesc0 + (unsigned)(jlo * 48), bd2 = bdesc0 + (unsigned)((jlo + n1) * 48);
+				// straight-line issue (the issuing thread's instructions between
+				// MMAs cost tensor-core time at this size)
+				if (n2 == 0) {
+#pragma unroll
+					for (int dz = 0; dz < 3; dz++)
+#pragma unroll
+						for (int kc = 0; kc < NK; kc++)
+							tc::mma(c1, ad + (unsigned)(((dz * NK + kc) * PL::TILE) >> 4),
+							        bd1 + (unsigned)((dz * PL::WDZ + kc * 2 * 2304) >> 4), id1);
+				} else {
+#pragma unroll
+					for (int dz = 0; dz < 3; dz++)
+#pragma unroll
+						for (int kc = 0; kc < NK; kc++) {
+							const unsigned ao = (unsigned)(((dz * NK + kc) * PL::TILE) >> 4);
+							const unsigned bo = (unsigned)((dz * PL::WDZ + kc * 2 * 2304) >> 4);
+							tc::mma(c1, ad + ao, bd1 + bo, id1);
+							tc::mma(tmem, ad + ao, bd2 + bo, id2);
+						}
+				}
+				tc::commit(b_free + 8 * (unsigned)gs);
+				issued = true;
+				if (++gs == NSLOT) {
+					gs = 0;
+					gph ^= 1u;
+				}
+				// rows whose last input line this was
+				const int last = y == l1 ? yb - 1 : y - 1;
+				for (; done <= last; done++) tc::commit(k_full + 8 * (unsigned)((q0 + (done - ya)) % NB));
+			}
+			q0 += yb - ya;
+		}
+		if (issued) { // drain before the accumulators are released
+			tc::commit(f_bar);
+			volatile int never = 0;
+			tc::mbar_wait(f_bar, 0, &never);
+		}
+	}
+	__syncwarp();
+	if (abort_ && tid == 0) devstat_fail(st, BSG_ERR_TIMEOUT, (int)blockIdx.x, 30);
+	asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+	__syncthreads();
+	asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+	if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem_base));
+}
+
 } // namespace
 
 // ---- the network object ------------------------------------------------------
@@ -685,6 +1117,60 @@ int conv_tiled(const ConvArgs &a, cudaStream_t s) {
 	return BSG_OK;
 }
 
+// cuTensorMapEncodeTiled, through the runtime's driver entry point
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static bool tried = false;
+	if (!tried) {
+		tried = true;
+		void *f = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+	}
+	return fn;
+}
+
+// 2D map of a [nv][16] bf16 array: boxes of 128 voxels x 16 channels in the
+// 32-byte swizzle; boxes outside [0, nv) read as zeros
+int tmap_lines(CUtensorMap *m, const bf16 *p, long long nv) {
+	const PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+	if (!enc) return bsg_set_error(BSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+	const cuuint64_t dim[2] = {16, (cuuint64_t)nv};
+	const cuuint64_t stride[1] = {16 * sizeof(bf16)};
+	const cuuint32_t box[2] = {16, 128}, estride[2] = {1, 1};
+	if (enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(p), dim, stride, box, estride,
+	        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+	        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+		return bsg_set_error(BSG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+	return BSG_OK;
+}
+
+// the tensor-core (tcgen05) convolution: a persistent grid, two CTAs per SM;
+// A has 16 channels (full or half resolution), B none or 16
+template <int CIN, bool F32OUT>
+int conv_tc(const ConvArgs &a, bsg_ctx *c) {
+	constexpr size_t smem = tc::Plan<CIN>::BYTES;
+	const long long nv = (long long)a.nz * a.ny * a.nx;
+	CUtensorMap ta, tb;
+	int rc;
+	// an upsampled A is gathered instead; its map is only a valid placeholder
+	if ((rc = tmap_lines(&ta, a.A, a.upA ? nv >> (3 * a.upA) : nv))) return rc;
+	if (CIN == 32) {
+		if ((rc = tmap_lines(&tb, a.B, nv))) return rc;
+	} else {
+		tb = ta;
+	}
+	BSG_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, F32OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	const long long nunits = (long long)a.nz * ((a.ny + tc::YRUN - 1) / tc::YRUN);
+	const long long cap = (long long)BSG_SMS * tc::CTAS;
+	const long long grid = nunits < cap ? nunits : cap;
+	k_conv3_tc<CIN, F32OUT><<<(unsigned)grid, tc::THREADS, smem, c->stream>>>(a, ta, tb, c->d_stat);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
 int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16 *B, int Cb, const bf16 *W, int Cout,
                 void *out, bool f32out) {
 	cudaStream_t s = u->ctx->stream;
@@ -693,6 +1179,9 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 	a.A = A; a.Ca = Ca; a.upA = upA; a.B = B; a.Cb = Cb; a.W = W; a.Cout = Cout; a.out = out;
 	const int Cin = Ca + Cb;
 	BSG_COUNT(1);
+	// 16 outputs from 16 or 32 inputs on x-lines of 128 voxels: tcgen05
+	if (Cout == 16 && !f32out && a.nx == 128 && Ca == 16 && (Cb == 0 || Cb == 16) && upA <= 1)
+		return Cin == 16 ? conv_tc<16, false>(a, u->ctx) : conv_tc<32, false>(a, u->ctx);
 	if (a.nx % TT_X == 0 && a.ny % TT_Y == 0 && a.nz % TT_Z == 0) {
 		int rc;
 		if (Cin % 32 == 0)

@@ -109,3 +109,37 @@ def test_unet_adam_step_lowers_loss(ctx, setup):
     assert losses[-1] < 0.95 * losses[0], losses[::10]
     w = net.weights()
     assert np.all(_unflat(w)["W0"][:, :, 2:] == 0.0)
+
+
+@pytest.mark.parametrize("ny,nz", [(16, 8), (120, 40)])
+def test_unet_forward_tensor_core_level_matches_oracle(ctx, ny, nz):
+    """A grid 128 voxels wide puts the level-0 convolutions (16 -> 16 and the
+    decoder's 32 -> 16 with its upsampled half) on the tcgen05 kernel (x-lines
+    of 128 voxels, TMA-staged, the accumulators in tensor memory); the whole
+    forward still matches the oracle within the bf16 tolerance of the other
+    forward test.  120 x 40 gives 320 work units of up to 16 y-rows (the last
+    of each plane 8 rows) on at most 296 CTAs: CTAs take several units and
+    the ring of row accumulators wraps across them."""
+    import bsg
+    import torch
+    nx = 128
+    s = P.heat3d(nx, ny, nz, sigma=1.0, seed=19)
+    m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+    W = U.init_weights(3)
+    r = np.random.default_rng(14).standard_normal(s.n)
+    u = s.upper()
+    d = u.a[u.ia[:-1]]
+    ld = np.log(np.abs(d) + 1e-300)
+    logd = U.bf16((ld - ld.mean()) / ld.std()).reshape(nz, ny, nx)
+    net = bsg.UNet(ctx, nx, ny, nz)
+    net.set_weights(_flat(W))
+    net.set_matrix(m)
+    y = torch.empty(s.n, dtype=torch.float64, device="cuda")
+    for _ in range(2):  # the second call reuses the kernels' state (TMEM, barriers)
+        net.forward(torch.as_tensor(r, device="cuda"), y)
+    x0, nr = U.make_input(r.reshape(nz, ny, nx), logd)
+    want = U.forward(x0, W)["y"].reshape(-1)
+    got = y.cpu().numpy()
+    assert np.all(np.isfinite(got))
+    assert np.abs(got - want).max() <= 1e-2 * np.abs(want).max()
+    assert np.linalg.norm(got - want) <= 5e-3 * np.linalg.norm(want)
