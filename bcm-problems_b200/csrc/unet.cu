@@ -669,7 +669,6 @@ inline int ew(long long n) {
 // by BSG_SPIN_LIMIT_NS; one that expires raises BSG_ERR_TIMEOUT and makes
 // all roles leave their loops.
 namespace tc {
-constexpr int YRUN = 16;  // output rows (y) of one work unit at fixed z
 constexpr int NB = 5;     // 48-column accumulator blocks in the TMEM ring (256 columns allocated)
 constexpr int CTAS = 2;   // CTAs per SM: two pipelines share the tensor cores
 constexpr int THREADS = 288;
@@ -782,8 +781,11 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
 	const unsigned k_full = b_free + 8 * NSLOT, k_free = k_full + 8 * NB;        // accumulator blocks
 	const unsigned x_bar = k_free + 8 * NB, f_bar = x_bar + 16;                  // edge exchange, drain
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-	const int ny = a.ny, nz = a.nz, nyc = (ny + tc::YRUN - 1) / tc::YRUN;
-	const long long nunits = (long long)nz * nyc;
+	const int ny = a.ny, nz = a.nz;
+	// this CTA's share of the level's nz * ny output rows: one contiguous range,
+	// walked as one segment [ya, yb) per z plane it touches
+	const long long nrow = (long long)nz * ny;
+	const long long r0 = nrow * blockIdx.x / gridDim.x, r1 = nrow * (blockIdx.x + 1) / gridDim.x;
 	if (warp == 0) {
 		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(tc::smem_u32(&tmem_base)));
 		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -833,8 +835,10 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
 		for (int i = 0; i < NB; i++) tc::arrive(k_free + 8 * i); // use 0 of every block: free
 		long long q = 0;
 		bool quit = false; // warp-uniform
-		for (long long u = blockIdx.x; u < nunits && !quit; u += gridDim.x) {
-			const int z = (int)(u / nyc), ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+		for (long long rs = r0, re; rs < r1 && !quit; rs = re) {
+			const int z = (int)(rs / ny), ya = (int)(rs % ny);
+			re = min(r1, (long long)(z + 1) * ny);
+			const int yb = (int)(re - (long long)z * ny);
 			for (int r = ya; r < yb; r++, q++) {
 				const int b = (int)(q % NB);
 				const bool ok = tc::mbar_wait(k_full + 8 * b, (unsigned)((q / NB) & 1), &abort_);
@@ -934,8 +938,10 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
 		long long g = 0; // lines staged
 		if (up || tma_thread) {
 			bool pending = false;
-			for (long long u = blockIdx.x; u < nunits && !abort_; u += gridDim.x) {
-				const int z = (int)(u / nyc), ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+			for (long long rs = r0, re; rs < r1 && !abort_; rs = re) {
+				const int z = (int)(rs / ny), ya = (int)(rs % ny);
+				re = min(r1, (long long)(z + 1) * ny);
+				const int yb = (int)(re - (long long)z * ny);
 				const int l0 = max(ya - 1, 0), l1 = min(yb, ny - 1);
 				for (int y = l0; y <= l1; y++, g++) {
 					const int s = (int)(g % NSLOT);
@@ -998,8 +1004,10 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
 		int q0 = 0, gs = 0;   // rows of earlier units; slot of the current line
 		unsigned gph = 0;     // phase parity of that slot
 		bool issued = false, ok = true;
-		for (long long u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-			const int ya = (int)(u % nyc) * tc::YRUN, yb = min(ny, ya + tc::YRUN);
+		for (long long rs = r0, re; rs < r1 && ok; rs = re) {
+			const int z = (int)(rs / ny), ya = (int)(rs % ny);
+			re = min(r1, (long long)(z + 1) * ny);
+			const int yb = (int)(re - (long long)z * ny);
 			const int l0 = max(ya - 1, 0), l1 = min(yb, ny - 1);
 			int acq = ya, done = ya; // next row to acquire / to release
 			for (int y = l0; y <= l1; y++) {
@@ -1163,9 +1171,9 @@ int conv_tc(const ConvArgs &a, bsg_ctx *c) {
 		tb = ta;
 	}
 	BSG_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, F32OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-	const long long nunits = (long long)a.nz * ((a.ny + tc::YRUN - 1) / tc::YRUN);
+	const long long nrow = (long long)a.nz * a.ny;
 	const long long cap = (long long)BSG_SMS * tc::CTAS;
-	const long long grid = nunits < cap ? nunits : cap;
+	const long long grid = nrow < cap ? nrow : cap;
 	k_conv3_tc<CIN, F32OUT><<<(unsigned)grid, tc::THREADS, smem, c->stream>>>(a, ta, tb, c->d_stat);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;

@@ -407,7 +407,7 @@ def main():
                                   "traffic": (382960000 if tiled and args.grid == 128 else None),
                                   "traffic_source": "profiles/k_tsell_sweep32_heat128.md",
                                   "ms_per_launch": t_sweep.value},
-            "roofline_unet": {"bound": "tensor", "kernel": "U-Net forward (k_conv3t / k_conv3, bf16 mma)",
+            "roofline_unet": {"bound": "tensor", "kernel": "U-Net forward (level 0: k_conv3_tc, tcgen05 + TMA; deeper levels: k_conv3t / k_conv3, mma.sync)",
                               "achieved": round(conv_tflops, 1), "peak": bf16_peak, "unit": "TFLOP/s",
                               "frac": round(conv_tflops / bf16_peak, 4), "ms_per_forward": round(t_unet, 4),
                               "flops": unet_flops(args.grid)},

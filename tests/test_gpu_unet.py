@@ -117,9 +117,10 @@ def test_unet_forward_tensor_core_level_matches_oracle(ctx, ny, nz):
     decoder's 32 -> 16 with its upsampled half) on the tcgen05 kernel (x-lines
     of 128 voxels, TMA-staged, the accumulators in tensor memory); the whole
     forward still matches the oracle within the bf16 tolerance of the other
-    forward test.  120 x 40 gives 320 work units of up to 16 y-rows (the last
-    of each plane 8 rows) on at most 296 CTAs: CTAs take several units and
-    the ring of row accumulators wraps across them."""
+    forward test.  Each CTA takes a contiguous range of the nz * ny output
+    rows: at 16 x 8 one row each (128 CTAs), at 120 x 40 about 16 rows
+    (296 CTAs) that often span two z planes, so the ring of row accumulators
+    wraps across segments."""
     import bsg
     import torch
     nx = 128
