@@ -14,6 +14,7 @@ Every product, solve and training step runs in the library's kernels through
 bsg; this module only drives them.
 
     python learned.py --grid 64 --instances 100 --per 20 --epochs 6 --out weights/unet_heat64.npz
+    python learned.py --time-forward 128     # time the committed network's forward at 128^3
 """
 import argparse
 import math
@@ -179,6 +180,33 @@ def load(path=DEFAULT_WEIGHTS):
     return w
 
 
+def time_forward(grid, reps=20, sigma=1.5, seed=4, log=print):
+    """Time the forward pass of the committed network bound to the grid^3 heat
+    system (CUDA events on the library stream, after 3 warm-up calls)."""
+    import torch
+    ctx = bsg.Context(0)
+    s = P.heat3d(grid, sigma=sigma, seed=seed)
+    m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+    net = bsg.UNet(ctx, grid, grid, grid)
+    net.set_weights(load())
+    net.set_matrix(m)
+    r = torch.as_tensor(np.random.default_rng(seed).standard_normal(s.n), device="cuda")
+    y = torch.empty_like(r)
+    for _ in range(3):
+        net.forward(r, y)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        net.forward(r, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    log(f"U-Net forward at {grid}^3: {ms:.3f} ms ({reps} calls)")
+    net.free()
+    return ms
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--grid", type=int, default=64)
@@ -191,7 +219,12 @@ def main():
     ap.add_argument("--nsweeps", type=int, default=6)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--time-forward", type=int, default=0, metavar="GRID",
+                    help="only time the committed network's forward on the GRID^3 heat system")
     a = ap.parse_args()
+    if a.time_forward:
+        time_forward(a.time_forward)
+        return
     ctx = bsg.Context(0)
     data = make_pairs(ctx, a.grid, a.instances, a.per, a.sigma, nsweeps=a.nsweeps)
     w, hist = train(ctx, data, a.grid, a.epochs, a.batch, a.lr, a.seed)
