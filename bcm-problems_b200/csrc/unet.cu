@@ -763,7 +763,7 @@ struct Plan {
 } // namespace tc
 
 // tmA / tmB: [voxel][16] maps of the A part (when not upsampled) and the B part
-template <int CIN, bool F32OUT>
+template <int CIN>
 __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
     k_conv3_tc(ConvArgs a, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                bsg_devstat *st) {
@@ -906,22 +906,17 @@ __global__ void __launch_bounds__(tc::THREADS, tc::CTAS)
 						o[i] = lf + t[1][i] + rt;
 					}
 				}
+				// ReLU, bf16
 				const long long v = ((long long)z * ny + r) * 128 + 32 * warp + lane;
-				if (F32OUT) {
-					float4 *op = reinterpret_cast<float4 *>(static_cast<float *>(a.out) + v * 16);
+				unsigned pk[8];
 #pragma unroll
-					for (int k = 0; k < 4; k++) op[k] = make_float4(o[4 * k], o[4 * k + 1], o[4 * k + 2], o[4 * k + 3]);
-				} else {
-					unsigned pk[8];
-#pragma unroll
-					for (int k = 0; k < 8; k++) {
-						const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(o[2 * k], 0.f), fmaxf(o[2 * k + 1], 0.f));
-						pk[k] = *reinterpret_cast<const unsigned *>(&h);
-					}
-					uint4 *op = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.out) + v * 16);
-					op[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-					op[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+				for (int k = 0; k < 8; k++) {
+					const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(o[2 * k], 0.f), fmaxf(o[2 * k + 1], 0.f));
+					pk[k] = *reinterpret_cast<const unsigned *>(&h);
 				}
+				uint4 *op = reinterpret_cast<uint4 *>(static_cast<bf16 *>(a.out) + v * 16);
+				op[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+				op[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
 			}
 		}
 	} else if (warp < 8) {
@@ -1156,8 +1151,8 @@ int tmap_lines(CUtensorMap *m, const bf16 *p, long long nv) {
 }
 
 // the tensor-core (tcgen05) convolution: a persistent grid, two CTAs per SM;
-// A has 16 channels (full or half resolution), B none or 16
-template <int CIN, bool F32OUT>
+// A has 16 channels (full or half resolution), B none or 16; ReLU, bf16 out
+template <int CIN>
 int conv_tc(const ConvArgs &a, bsg_ctx *c) {
 	constexpr size_t smem = tc::Plan<CIN>::BYTES;
 	const long long nv = (long long)a.nz * a.ny * a.nx;
@@ -1170,11 +1165,11 @@ int conv_tc(const ConvArgs &a, bsg_ctx *c) {
 	} else {
 		tb = ta;
 	}
-	BSG_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, F32OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	BSG_CUDA(cudaFuncSetAttribute(k_conv3_tc<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	const long long nrow = (long long)a.nz * a.ny;
 	const long long cap = (long long)BSG_SMS * tc::CTAS;
 	const long long grid = nrow < cap ? nrow : cap;
-	k_conv3_tc<CIN, F32OUT><<<(unsigned)grid, tc::THREADS, smem, c->stream>>>(a, ta, tb, c->d_stat);
+	k_conv3_tc<CIN><<<(unsigned)grid, tc::THREADS, smem, c->stream>>>(a, ta, tb, c->d_stat);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
@@ -1189,7 +1184,7 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 	BSG_COUNT(1);
 	// 16 outputs from 16 or 32 inputs on x-lines of 128 voxels: tcgen05
 	if (Cout == 16 && !f32out && a.nx == 128 && Ca == 16 && (Cb == 0 || Cb == 16) && upA <= 1)
-		return Cin == 16 ? conv_tc<16, false>(a, u->ctx) : conv_tc<32, false>(a, u->ctx);
+		return Cin == 16 ? conv_tc<16>(a, u->ctx) : conv_tc<32>(a, u->ctx);
 	if (a.nx % TT_X == 0 && a.ny % TT_Y == 0 && a.nz % TT_Z == 0) {
 		int rc;
 		if (Cin % 32 == 0)
