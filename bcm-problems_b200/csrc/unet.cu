@@ -64,20 +64,25 @@ __device__ __forceinline__ unsigned ld_u32(const bf16 *p) { return __ldg(reinter
 
 #define CONV_MT 2 // 16-voxel tiles per warp iteration
 
-// One warp: CONV_MT tiles of 16 consecutive voxels x 16 output channels.
+// One CTA: CONV_MT tiles of 16 consecutive voxels x 16 output channels; its
+// four warps take every fourth tap (7, 7, 7, 6 of the 27) of the same tile,
+// which shortens each warp's chain of dependent gathers fourfold, and their
+// FP32 partial sums meet in shared memory (red[3][CONV_MT * 8][32]).
 template <bool F32OUT>
 __global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	bf16 *Ws = reinterpret_cast<bf16 *>(smem_raw);
 	const int Cin = a.Ca + a.Cb;
 	const int ldw = Cin + 8;
+	float *red = reinterpret_cast<float *>(smem_raw);
+	bf16 *Ws = reinterpret_cast<bf16 *>(smem_raw + 3 * CONV_MT * 8 * 32 * sizeof(float));
 	const int slice = blockIdx.y; // 16 output channels
-	// stage the weight slice: Ws[(tap*16 + n) * ldw + k]
-	for (int e = threadIdx.x; e < 27 * 16 * (Cin / 2); e += blockDim.x) {
-		const int k2 = e % (Cin / 2), row = e / (Cin / 2);
+	// stage the weight slice, 16 bytes per load: Ws[(tap*16 + n) * ldw + k]
+	// (Cin is a multiple of 8, so rows of both layouts start on 16 bytes)
+	for (int e = threadIdx.x; e < 27 * 16 * (Cin / 8); e += blockDim.x) {
+		const int k8 = e % (Cin / 8), row = e / (Cin / 8);
 		const int tap = row / 16, n = row % 16;
-		const unsigned v = ld_u32(a.W + ((size_t)tap * a.Cout + slice * 16 + n) * Cin + 2 * k2);
-		*reinterpret_cast<unsigned *>(Ws + (size_t)row * ldw + 2 * k2) = v;
+		const uint4 v = __ldg(reinterpret_cast<const uint4 *>(a.W + ((size_t)tap * a.Cout + slice * 16 + n) * Cin + 8 * k8));
+		*reinterpret_cast<uint4 *>(Ws + (size_t)row * ldw + 8 * k8) = v;
 	}
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -85,7 +90,7 @@ __global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
 	const long long nvox = (long long)a.nz * a.ny * a.nx;
 	const long long ntile = (nvox + 16 * CONV_MT - 1) / (16 * CONV_MT);
 	const int nyA = a.ny >> a.upA, nxA = a.nx >> a.upA;
-	for (long long tile = (long long)blockIdx.x * 4 + warp; tile < ntile; tile += (long long)gridDim.x * 4) {
+	for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
 		// rows handled by this lane: r = mt*16 + g + 8*h
 		int vz[CONV_MT][2], vy[CONV_MT][2], vx[CONV_MT][2];
 		bool vin[CONV_MT][2];
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
 			for (int j = 0; j < 2; j++)
 #pragma unroll
 				for (int q = 0; q < 4; q++) acc[mt][j][q] = 0.f;
-		for (int tap = 0; tap < 27; tap++) {
+		for (int tap = warp; tap < 27; tap += 4) {
 			const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
 			long long ia[CONV_MT][2], ib[CONV_MT][2];
 			bool ok[CONV_MT][2];
@@ -146,7 +151,28 @@ __global__ void __launch_bounds__(128) k_conv3(ConvArgs a) {
 				}
 			}
 		}
-		// epilogue: rows g / g+8, columns slice*16 + j*8 + 2*t4 + {0,1}
+		// warps 1-3 hand their partial sums to warp 0
+		if (warp > 0)
+#pragma unroll
+			for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+				for (int j = 0; j < 2; j++)
+#pragma unroll
+					for (int q = 0; q < 4; q++) red[((warp - 1) * CONV_MT * 8 + (mt * 2 + j) * 4 + q) * 32 + lane] = acc[mt][j][q];
+		__syncthreads();
+		if (warp == 0) {
+#pragma unroll
+			for (int w = 0; w < 3; w++)
+#pragma unroll
+				for (int mt = 0; mt < CONV_MT; mt++)
+#pragma unroll
+					for (int j = 0; j < 2; j++)
+#pragma unroll
+						for (int q = 0; q < 4; q++) acc[mt][j][q] += red[(w * CONV_MT * 8 + (mt * 2 + j) * 4 + q) * 32 + lane];
+		}
+		__syncthreads(); // red is free for the next tile
+		if (warp > 0) continue;
+		// epilogue (warp 0): rows g / g+8, columns slice*16 + j*8 + 2*t4 + {0,1}
 #pragma unroll
 		for (int mt = 0; mt < CONV_MT; mt++)
 #pragma unroll
@@ -1195,9 +1221,9 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 		BSG_CUDA(cudaGetLastError());
 		return BSG_OK;
 	}
-	const size_t smem = (size_t)27 * 16 * (Cin + 8) * sizeof(bf16);
+	const size_t smem = (size_t)3 * CONV_MT * 8 * 32 * sizeof(float) + (size_t)27 * 16 * (Cin + 8) * sizeof(bf16);
 	const long long ntile = (u->nv[lvl] + 16 * CONV_MT - 1) / (16 * CONV_MT);
-	long long bx = (ntile + 3) / 4;
+	long long bx = ntile;
 	const long long cap = (long long)BSG_SMS * 8 / (Cout / 16);
 	if (bx > cap) bx = cap;
 	if (bx < 1) bx = 1;
