@@ -1208,8 +1208,10 @@ int conv_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf16
 	a.A = A; a.Ca = Ca; a.upA = upA; a.B = B; a.Cb = Cb; a.W = W; a.Cout = Cout; a.out = out;
 	const int Cin = Ca + Cb;
 	BSG_COUNT(1);
-	// 16 outputs from 16 or 32 inputs on x-lines of 128 voxels: tcgen05
-	if (Cout == 16 && !f32out && a.nx == 128 && Ca == 16 && (Cb == 0 || Cb == 16) && upA <= 1)
+	// 16 outputs from 16 or 32 inputs on x-lines of 128 voxels: tcgen05 (TMA
+	// line coordinates are 32-bit voxel indices)
+	if (Cout == 16 && !f32out && a.nx == 128 && Ca == 16 && (Cb == 0 || Cb == 16) && upA <= 1 &&
+	    (long long)a.nz * a.ny * 128 < (1ll << 31))
 		return Cin == 16 ? conv_tc<16>(a, u->ctx) : conv_tc<32>(a, u->ctx);
 	if (a.nx % TT_X == 0 && a.ny % TT_Y == 0 && a.nz % TT_Z == 0) {
 		int rc;
