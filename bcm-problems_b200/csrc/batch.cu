@@ -340,8 +340,9 @@ extern "C" int bsg_pcg_batch_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f,
 		*ptr = keep.back().p;
 		return BSG_OK;
 	};
-	double *r, *z, *pp, *q, *t, *w, *sc, *part;
-	int *si, *segid, *dseg, *cnt;
+	double *r = nullptr, *z = nullptr, *pp = nullptr, *q = nullptr, *t = nullptr, *w = nullptr, *sc = nullptr,
+	       *part = nullptr;
+	int *si = nullptr, *segid = nullptr, *dseg = nullptr, *cnt = nullptr;
 	int rc = BSG_OK;
 	if (!rc) rc = alloc((void **)&r, sizeof(double) * N);
 	if (!rc) rc = alloc((void **)&z, sizeof(double) * N);

@@ -203,11 +203,7 @@ int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
 int bsg_trisolve_sweep_launch(bsg_ctx *c, const bsg_fct *f, int lower, const double *x, const double *yin,
                               double *yout) {
 	if (f->d_bia) return bsg_set_error(BSG_ERR_UNSUPPORTED, "single sweep timing of a block factor");
-	const int n = f->n;
-	const int *rp = lower ? f->d_lr_i : f->d_ur_i;
-	const int *ci = lower ? f->d_lr_j : f->d_ur_j;
 	const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
-	(void)n; (void)rp; (void)ci;
 	if (f->fp32) // the FP32-iterate pass of the mixed path; yin's bytes serve as its FP32 input
 		return bsg_sell_sweep32_pass(c->stream, lower ? &f->sl : &f->su, x, dinv, reinterpret_cast<const float *>(yin),
 		                             yout);
