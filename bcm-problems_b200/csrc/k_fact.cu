@@ -1042,6 +1042,7 @@ static unsigned long long g_fact_stats[FACT_NSTAT];
 // slot resolution and fma phases, [14] rows retried in the global-memory
 // workspace, [15] warps launched.
 extern "C" int bsg_fact_stats(unsigned long long *out, int nout) {
+	if (!out && nout > 0) return bsg_set_error(BSG_ERR_ARG, "bsg_fact_stats: null output");
 	for (int k = 0; k < nout && k < FACT_NSTAT; k++) out[k] = g_fact_stats[k];
 	return BSG_OK;
 }

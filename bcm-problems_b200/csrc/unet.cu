@@ -1431,7 +1431,9 @@ extern "C" int bsg_unet_free(bsg_unet *u) {
 	return BSG_OK;
 }
 
-extern "C" int bsg_unet_nparam(const bsg_unet *u) { return u ? u->nparam : 0; }
+extern "C" int bsg_unet_nparam(const bsg_unet *u) {
+	return u ? u->nparam : bsg_set_error(BSG_ERR_ARG, "bsg_unet_nparam: null network");
+}
 
 // Weights in the flat FP32 layout W0..W6 ([tap][cout][cin] each), then w7.
 extern "C" int bsg_unet_set_weights(bsg_unet *u, const float *w) {

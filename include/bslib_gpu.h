@@ -225,7 +225,7 @@ int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const doub
 typedef struct bsg_unet bsg_unet;
 int bsg_unet_create(bsg_ctx *ctx, int nx, int ny, int nz, int train, bsg_unet **out);
 int bsg_unet_free(bsg_unet *u);
-int bsg_unet_nparam(const bsg_unet *u);
+int bsg_unet_nparam(const bsg_unet *u);                   /* BSG_ERR_ARG for a null network */
 int bsg_unet_set_weights(bsg_unet *u, const float *w);   /* host, nparam floats */
 int bsg_unet_get_weights(bsg_unet *u, float *w);
 int bsg_unet_get_grads(bsg_unet *u, float *g);           /* accumulated sums */
@@ -248,7 +248,8 @@ unsigned long long bsg_launch_count(void);
  * 1 / 2: forward / backward solve with f in `mode`/`nsweeps`), CUDA events. */
 int bsg_time_kernel(bsg_ctx *ctx, int kind, const bsg_mat *m, const bsg_fct *f, int mode, int nsweeps, int reps,
                     double *ms_per_launch);
-/* Scheduler counters of the last factorisation (see k_fact.cu). */
+/* Scheduler counters of the last factorisation (see k_fact.cu); the first
+ * nout of them (BSG_ERR_ARG for a null out with nout > 0). */
 int bsg_fact_stats(unsigned long long *out, int nout);
 /* Stored entries, padding included, of the sliced copies the bandwidth-bound
  * products read: out[0] matrix, out[1] strict L, out[2] strict U; out[3] /

@@ -3,6 +3,7 @@ include/bslib_gpu.h declares, and its host-side logic answers as documented."""
 import ctypes as C
 import os
 import re
+import sys
 
 import pytest
 
@@ -64,3 +65,55 @@ def test_no_cpu_fallback_without_gpu():
         bsg.Context(0)
     h = C.c_void_p()
     assert bsg.lib().bsg_create(C.byref(h), 0, None) == bsg.ERR_CUDA
+
+
+_NULL_SWEEP = r'''
+import ctypes as C, re, sys
+sys.path.insert(0, sys.argv[1])
+import bsg
+L = bsg.lib()
+hdr = open(sys.argv[2]).read()
+names = re.findall(r"^(?:int|unsigned long long|const char \*|void) \*?(bsg_\w+)\(", hdr, re.M)
+skip = {"bsg_create", "bsg_param_default", "bsg_last_error", "bsg_version", "bsg_launch_count"}
+extra = {  # entry points the Python binding does not declare
+    "bsg_solve_sweep_static": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p],
+    "bsg_time_kernel": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p],
+}
+def dflt(t):
+    if t in (C.c_int, C.c_long, C.c_longlong, C.c_uint, C.c_ulonglong, C.c_size_t):
+        return 0
+    if t in (C.c_float, C.c_double):
+        return 0.0
+    return None
+for nm in names:
+    if nm in skip:
+        continue
+    f = getattr(L, nm)
+    if f.argtypes is None:
+        f.argtypes = extra[nm]
+    f.restype = C.c_int
+    print(nm, f(*[dflt(t) for t in f.argtypes]), flush=True)
+# a null output with a positive count
+f = L.bsg_fact_stats
+print("bsg_fact_stats/24", f(None, 24), flush=True)
+'''
+
+
+def test_every_entry_point_rejects_null_handles():
+    """Every declared entry point, called with null handles and buffers and
+    zero sizes, returns BSG_ERR_ARG (the release functions: BSG_OK, as free()
+    of NULL), touches no device and does not crash -- run in a child process
+    so that a crash is reported, not fatal to the test run."""
+    import subprocess
+    import bsg
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _NULL_SWEEP, os.path.join(root, "bcm-problems_b200"),
+                        os.path.join(root, "include", "bslib_gpu.h")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    got = dict(line.split() for line in r.stdout.splitlines())
+    releases = {"bsg_destroy", "bsg_mat_free", "bsg_fct_free", "bsg_unet_free"}
+    ok_when_empty = {"bsg_fact_stats"}  # nothing requested, nothing written
+    assert len(got) >= 35
+    for nm, v in got.items():
+        want = bsg.OK if nm in releases | ok_when_empty else bsg.ERR_ARG
+        assert int(v) == want, (nm, v)
