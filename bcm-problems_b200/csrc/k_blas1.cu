@@ -116,6 +116,35 @@ __global__ void k_residual(int n, const double *b, double *r) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r[i] = b[i] - r[i];
 }
 
+// out = max_i |x_i| (CSVector::MaxProdSVect with unit weights,
+// Bslib/svector.cpp:376): one partial per block, the last block takes the
+// maximum of the partials.  Max is order-independent, so the result is exact.
+__global__ void __launch_bounds__(RED_THREADS) k_maxabs(int n, const double *x, double *partials,
+                                                        unsigned int *counter, double *out) {
+	__shared__ double sh[32];
+	__shared__ bool last;
+	double v = 0.0;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v = fmax(v, fabs(x[i]));
+	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+	if (l == 0) sh[w] = v;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int k = 0; k < (int)(blockDim.x >> 5); k++) t = fmax(t, sh[k]);
+		partials[blockIdx.x] = t;
+		__threadfence();
+		last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+	}
+	__syncthreads();
+	if (!last || threadIdx.x != 0) return;
+	__threadfence();
+	double t = 0.0;
+	for (int b = 0; b < (int)gridDim.x; b++) t = fmax(t, __ldcg(partials + b));
+	*out = t;
+	*counter = 0;
+}
+
 __global__ void k_fill(int n, double *x, double v) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
 }
@@ -181,6 +210,12 @@ int bsg_residual_launch(bsg_ctx *c, int n, const double *b, double *r) {
 	k_residual<<<ew_grid(n), 256, 0, c->stream>>>(n, b, r);
 	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }
+int bsg_maxabs_launch(bsg_ctx *c, int n, const double *x, double *d_out) {
+	BSG_COUNT(1);
+	k_maxabs<<<RED_BLOCKS, RED_THREADS, 0, c->stream>>>(n, x, c->d_partials, c->d_counters, d_out);
+	return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v) {
 	BSG_COUNT(1);
 	k_fill<<<ew_grid(n), 256, 0, s>>>((int)n, x, v);

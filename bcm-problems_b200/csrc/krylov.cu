@@ -24,12 +24,13 @@ int bsg_gemv_add_launch(bsg_ctx *c, int n, const double *V, long long ld, int k,
 int bsg_scale_by_launch(bsg_ctx *c, int n, const double *x, double *y, const double *num, const double *den,
                         int sqrt_den);
 int bsg_residual_launch(bsg_ctx *c, int n, const double *b, double *r);
+int bsg_maxabs_launch(bsg_ctx *c, int n, const double *x, double *d_out);
 int bsg_fill_launch(cudaStream_t s, long long n, double *x, double v);
 int bsg_unet_apply(void *net, bsg_ctx *c, const double *r, double *z, double *work);
 extern "C" int bsg_unet_set_matrix(bsg_unet *u, const bsg_mat *m);
 
 // device scalar slots used by PCG
-enum { S_ENRSQ = 0, S_GAMMA = 1, S_GAMOLD = 2, S_PAP = 3, S_BREAK = 4, S_TMP = 8 };
+enum { S_ENRSQ = 0, S_GAMMA = 1, S_GAMOLD = 2, S_PAP = 3, S_BREAK = 4, S_ERR = 5, S_TMP = 8 };
 
 namespace {
 
@@ -100,6 +101,7 @@ int bsg_true_residual(bsg_ctx *c, const bsg_mat *m, const double *b, const doubl
 extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x,
                            bsg_param *p) {
 	if (!c || !m || !f || !d_b || !d_x || !p) return bsg_set_error(BSG_ERR_ARG, "bsg_pcg_dev: null argument");
+	if (p->ittype < 0 || p->ittype > 2) return bsg_set_error(BSG_ERR_UNSUPPORTED, "PCG: ittype must be 0, 1 or 2");
 	const int N = m->n * m->bs;
 	cudaStream_t s = c->stream;
 	Buf r, q, z, pp, t, w;
@@ -119,13 +121,17 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 	int rc = bsg_spmm_launch(m, 1, d_x, r.p, N, s);
 	if (!rc) rc = bsg_residual_launch(c, N, d_b, r.p);
 	if (rc) return rc;
-	double enrsq0 = 0.0, enrsq = 0.0;
+	double enrsq0 = 0.0, enrsq = 0.0, errmin = 0.0;
+	const bool maxnorm = p->ittype == 2;
 	int k, nit = 0, status = BSG_OK, replacements = 0;
 	const int g = ew_grid(N);
 	for (k = 1; k < p->niter; k++) {
 		rc = bsg_precond_apply(c, f, p, r.p, z.p, t.p, w.p);
 		if (rc) return rc;
 		rc = bsg_dots_launch(c, 2, N, r.p, r.p, r.p, z.p, nullptr, nullptr, c->d_scalars + S_ENRSQ);
+		// ittype 2: weighted max-norm of the recursive residual, unit weights
+		// (Bslib/cg.cpp:195-198, the weights of AbstractSymmSolver are 1)
+		if (!rc && maxnorm) rc = bsg_maxabs_launch(c, N, r.p, c->d_scalars + S_ERR);
 		if (rc) return rc;
 		BSG_CUDA(cudaMemcpyAsync(c->h_pinned, c->d_scalars, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
 		BSG_CUDA(cudaStreamSynchronize(s));
@@ -133,17 +139,21 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 		if (rc) return rc;
 		enrsq = c->h_pinned[S_ENRSQ];
 		if (k == 1) enrsq0 = enrsq;
+		errmin = c->h_pinned[S_ERR];
 		nit = k;
 		if (c->h_pinned[S_BREAK] != 0.0) { status = BSG_ERR_BREAKDOWN; break; }
-		const double goal = p->ittype == 0 ? p->eps * p->eps * enrsq0 : p->eps * p->eps;
-		if ((p->ittype == 0 || p->ittype == 1) && enrsq <= goal) {
+		// stop rules of Bslib/cg.cpp:239-241: 0 relative and 1 absolute on
+		// ||r||^2, 2 on max |r_i| <= |eps|
+		const double goal = maxnorm ? std::fabs(p->eps) : (p->ittype == 0 ? p->eps * p->eps * enrsq0 : p->eps * p->eps);
+		if ((maxnorm ? errmin : enrsq) <= goal) {
 			if (!p->true_residual || replacements >= 5) break;
 			// the recursive residual says converged: confirm with the FP64
-			// true residual; if it drifted (FP32 preconditioner), continue
-			// from the true residual
+			// true residual in the same norm; if it drifted (FP32
+			// preconditioner), continue from the true residual
 			rc = bsg_spmm_launch(m, 1, d_x, t.p, N, s);
 			if (!rc) rc = bsg_residual_launch(c, N, d_b, t.p);
-			if (!rc) rc = bsg_dots_launch(c, 1, N, t.p, t.p, nullptr, nullptr, nullptr, nullptr, c->d_scalars + S_TMP);
+			if (!rc) rc = maxnorm ? bsg_maxabs_launch(c, N, t.p, c->d_scalars + S_TMP)
+			                      : bsg_dots_launch(c, 1, N, t.p, t.p, nullptr, nullptr, nullptr, nullptr, c->d_scalars + S_TMP);
 			if (rc) return rc;
 			BSG_CUDA(cudaMemcpyAsync(c->h_pinned + 8, c->d_scalars + S_TMP, sizeof(double), cudaMemcpyDeviceToHost, s));
 			BSG_CUDA(cudaStreamSynchronize(s));
@@ -174,7 +184,7 @@ extern "C" int bsg_pcg_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const
 	p->timeitr = ms * 1e-3;
 	p->nitperf = nit;
 	p->resfin = res;
-	p->resrec = enrsq0 > 0 ? std::sqrt(enrsq / enrsq0) : 0.0;
+	p->resrec = maxnorm ? errmin : (enrsq0 > 0 ? std::sqrt(enrsq / enrsq0) : 0.0);
 	(void)t0;
 	if (status == BSG_ERR_BREAKDOWN) return bsg_set_error(status, " Matrix is not positive definite");
 	if (status == BSG_ERR_NOCONV) return bsg_set_error(status, "iteration limit reached");

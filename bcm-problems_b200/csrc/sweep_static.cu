@@ -16,6 +16,10 @@
 //   * the first call on a device looks up the array's address with
 //     cudaGetSymbolAddress (which can load this module); make that first call
 //     before any stream capture;
+//   * the address is kept for the life of the process: a cudaDeviceReset (or
+//     any reset of the device's primary context) unloads the module and
+//     leaves the kept address stale, so after such a reset this entry point
+//     must not be called again until the process restarts;
 //   * the array is shared by every call on the device: calls that overlap in
 //     time (other threads, other streams) race on it and give wrong results;
 //     keep the calls on one stream, one after another;
@@ -66,6 +70,6 @@ extern "C" int bsg_solve_sweep_static(bsg_ctx *c, const bsg_fct *f, int lower, i
 	double *work = nullptr;
 	int rc = sweep_scratch(c->device, &work);
 	if (rc) return rc;
-	rc = bsg_trisolve_launch(c, f, lower ? 1 : 0, 1, nsweeps, x, y, work);
-	return rc ? bsg_set_error(rc, "sweep solve launch failed") : BSG_OK;
+	// a failed launch has already recorded its own cause (bsg_last_error)
+	return bsg_trisolve_launch(c, f, lower ? 1 : 0, 1, nsweeps, x, y, work);
 }

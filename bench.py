@@ -5,10 +5,12 @@ Metric: wall milliseconds from a device-resident system (A, b) to a solution x
 with FP64 true relative residual ||b - Ax|| / ||b|| <= 1e-8, for the learned +
 mixed arm: FP32 IC2 factor (= ILU2 of the symmetric matrix) applied by
 Jacobi(6) sweeps, followed by the trained U-Net stage, inside FP64
-FGMRES(30).  Beside it, the same step with the plain FP64 arm (FP64 factor,
-exact triangular solves, PCG), the mixed PCG and the plain mixed FGMRES, and
-the HBM bandwidth of the SpMV / sweep kernels and the tensor throughput of
-the U-Net convolutions.
+FGMRES(30).  Beside it, the same step with the FP64 arms (FP64 factor with
+exact triangular solves, the reference's algorithm, and with Jacobi(6)
+sweeps, PCG), the mixed PCG and the plain mixed FGMRES, each with its
+relative error against the reference Bslib's own solution of the same system;
+the HBM bandwidth of the sweep / SpMV kernels and the tensor throughput of the
+U-Net convolutions.
 
 Workload: 3-D heat, 7-point stencil, 128^3 cells (n = 2,097,152), conductivity
 lognormal(sigma=1.5) per cell from seed 4, RHS uniform[-1,1].  A step is one
@@ -52,6 +54,21 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def profile_traffic(name, grid):
+    """DRAM read + write bytes per launch of one kernel, from its committed ncu
+    summary profiles/<name>.md (the line `dram_bytes_per_launch = N`), when
+    the summary's workload (128^3) is the one being run; else None."""
+    import re
+    if grid != 128:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", name + ".md")) as f:
+            m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9]+)", f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
 
 
 class ClockSampler:
@@ -124,9 +141,12 @@ def mixed_param(bsg, krylov=0, learned=None):
     return p
 
 
-def fp64_param(bsg):
+def fp64_param(bsg, trisolve=0):
+    """All-FP64 IC2-PCG: exact sync-free triangular solves (trisolve 0, the
+    reference's SolveL / SolveU) or Jacobi(6) sweeps of the FP64 factor
+    (trisolve 1, the fastest FP64 arm)."""
     return bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=TOL,
-                             niter=3000, precision=0, trisolve=0)
+                             niter=3000, precision=0, trisolve=trisolve, nsweeps=6, true_residual=1)
 
 
 def unet_flops(grid):
@@ -139,7 +159,13 @@ def unet_flops(grid):
 
 
 def run_reference(args, rank):
-    """Reference arm: the reference Bslib's own CPU solver on the same system."""
+    """Reference arm: the reference Bslib's own CPU solver on the same system.
+
+    Bslib is single-threaded, so one step (one full solve, ~15 s at 128^3)
+    runs on one host core.  To keep the whole run within a few minutes, one
+    untimed warm-up solve is run (the CPU needs no more) and the timed steps
+    stop once 150 s of solves are done (at least one): `steps` in the line is
+    the number actually timed, `steps_requested` the K asked for."""
     if rank != 0:
         return 0
     from oracle_ffi import RefLib, REF_SO
@@ -151,25 +177,30 @@ def run_reference(args, rank):
     s, u = make_system()
     b = s.rhs[0]
     ref = RefLib()
+
+    def solve():
+        return ref.solve_symm(u.ia, u.ja, u.a, b, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=-1.0, ittype=0,
+                              eps=TOL, niter=3000)
+
+    if args.warmup > 0:
+        solve()
     times = []
-    info = None
-    for it in range(args.warmup + args.steps):
+    info = x = None
+    while len(times) < args.steps and (not times or sum(times) < 150e3):
         t0 = time.perf_counter()
-        x, info = ref.solve_symm(u.ia, u.ja, u.a, b, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=-1.0,
-                                 ittype=0, eps=TOL, niter=3000)
-        dt = (time.perf_counter() - t0) * 1e3
-        if it >= args.warmup:
-            times.append(dt)
+        x, info = solve()
+        times.append((time.perf_counter() - t0) * 1e3)
     r = b - s.to_scipy() @ x
     res = float(np.linalg.norm(r) / np.linalg.norm(b))
     ms = statistics.mean(times)
     line = {"impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+            "steps": len(times), "steps_requested": args.steps, "warmup": min(args.warmup, 1),
+            "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "solver": "Bslib SolveSymm: IC2 (tau1=tau2=1e-3) + PCG, natural order",
                        "n": s.n, "nnz": s.nnz},
             "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": 1, "kind": "reference",
-                             "sample": "the full system, one solve per step"},
+                             "sample": "the full system, one solve per step (single-threaded Bslib)"},
             "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "iterations": info["iters"], "true_residual": res, "tfct_s": info["tfct"], "titr_s": info["titr"],
             "host_cores_available": os.cpu_count()}
@@ -256,11 +287,12 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     launches0 = bsg.lib().bsg_launch_count()
     params = []
+    x_head = None
     with ClockSampler(local) as clk:
         e0.record()
         for _ in range(args.steps):
             p = headline()
-            solve_device(p)
+            x_head = solve_device(p)
             params.append(p)
         e1.record()
         torch.cuda.synchronize()
@@ -287,16 +319,19 @@ def main():
 
     def timed(param):
         e0.record()
-        solve_device(param)
+        x = solve_device(param)
         e1.record()
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1), param
+        return e0.elapsed_time(e1), param, x.cpu().numpy()
 
-    # ---- the other arms on the same system: plain FP64 (FP64 IC2, exact
-    #      sync-free solves, PCG), mixed PCG, mixed FGMRES without the network
-    ms64, p64 = timed(fp64_param(bsg))
-    ms_pcg, p_pcg = timed(mixed_param(bsg, krylov=0))
-    ms_fg, p_fg = timed(mixed_param(bsg, krylov=2))
+    # ---- the other arms on the same system: FP64 IC2-PCG with exact
+    #      sync-free solves (the reference's algorithm) and with Jacobi(6)
+    #      sweeps of the FP64 factor, mixed PCG, mixed FGMRES without the network
+    arms = {"fp64_pcg": timed(fp64_param(bsg, trisolve=0)),
+            "fp64_pcg_sweeps": timed(fp64_param(bsg, trisolve=1)),
+            "mixed_pcg": timed(mixed_param(bsg, krylov=0)),
+            "mixed_fgmres_plain": timed(mixed_param(bsg, krylov=2))}
+    x_head = x_head.cpu().numpy()
 
     # ---- end to end through the host-buffer C ABI (pinned host arrays)
     h_ia = torch.from_numpy(u.ia).pin_memory().numpy()
@@ -358,22 +393,39 @@ def main():
     L.bsg_fct_free(fh)
     L.bsg_mat_free(mh)
 
-    # ---- CPU baseline: the reference Bslib (oracle/_ref) on the same system, rank 0, N = 1
+    # ---- CPU baseline: the reference Bslib (oracle/_ref) on the same system, rank 0, N = 1;
+    #      its solution is the FP64 oracle every arm's error is stated against
     cpu = None
+    x_ref = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle_ffi import RefLib, REF_SO
         if os.path.exists(REF_SO):
             t0 = time.perf_counter()
-            _, info = RefLib().solve_symm(u.ia, u.ja, u.a, s.rhs[0], fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1,
-                                          memory=-1.0, ittype=0, eps=TOL, niter=3000)
+            x_ref, info = RefLib().solve_symm(u.ia, u.ja, u.a, s.rhs[0], fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1,
+                                              memory=-1.0, ittype=0, eps=TOL, niter=3000)
             cpu = {"value": round((time.perf_counter() - t0) * 1e3, 1), "unit": "ms", "cores": 1,
                    "kind": "reference",
                    "sample": "one full solve of the benchmark system (IC2 + PCG, natural order)",
-                   "iterations": info["iters"], "tfct_s": info["tfct"], "titr_s": info["titr"]}
+                   "iterations": info["iters"], "tfct_s": info["tfct"], "titr_s": info["titr"],
+                   "true_residual": float(np.linalg.norm(s.rhs[0] - s.to_scipy() @ x_ref)
+                                          / np.linalg.norm(s.rhs[0]))}
+
+    def rel_err(x):
+        if x_ref is None:
+            return None
+        return float(np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref))
 
     if rank == 0:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             bf16_peak = float(json.load(f).get("bf16_tflops", 1590.0))
+        arm_lines = {k: {"ms": round(t, 3), "iterations": pa.nitperf, "fct_ms": round(pa.timefct * 1e3, 3),
+                         "itr_ms": round(pa.timeitr * 1e3, 3), "true_residual": pa.resfin,
+                         "rel_err_vs_reference": rel_err(xa)}
+                     for k, (t, pa, xa) in arms.items()}
+        fp64_best = min(("fp64_pcg", "fp64_pcg_sweeps"), key=lambda k: arms[k][0])
+        nonlearned_best = min(arms, key=lambda k: arms[k][0])
+        sweep_traffic = profile_traffic("k_tsell_sweep32_heat128", args.grid) if tiled else None
+        spmv_traffic = profile_traffic("k_sell_apply_heat128", args.grid)
         line = {
             "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
@@ -383,30 +435,31 @@ def main():
                                  "stage (bf16, trained at 64^3), FP64 FGMRES(30)",
                        "l2": "inputs larger than L2 (matrix 175 MB, factor 420 MB)"},
             "iterations": p_last.nitperf, "true_residual": p_last.resfin,
+            "rel_err_vs_reference": rel_err(x_head),
             "fct_ms": round(p_last.timefct * 1e3, 3), "itr_ms": round(p_last.timeitr * 1e3, 3),
-            "arms": {
-                "fp64_pcg": {"ms": round(ms64, 3), "iterations": p64.nitperf, "itr_ms": round(p64.timeitr * 1e3, 3)},
-                "mixed_pcg": {"ms": round(ms_pcg, 3), "iterations": p_pcg.nitperf,
-                              "itr_ms": round(p_pcg.timeitr * 1e3, 3)},
-                "mixed_fgmres_plain": {"ms": round(ms_fg, 3), "iterations": p_fg.nitperf,
-                                       "itr_ms": round(p_fg.timeitr * 1e3, 3)},
-            },
-            "speedup_vs_fp64_pcg": round(ms64 / ms, 3),
+            "arms": arm_lines,
+            "speedup_vs_fp64_pcg": round(arms["fp64_pcg"][0] / ms, 3),
+            "speedup_vs_fastest_fp64": {"arm": fp64_best, "speedup": round(arms[fp64_best][0] / ms, 3)},
+            "fastest_non_learned": {"arm": nonlearned_best, "ms": round(arms[nonlearned_best][0], 3),
+                                    "learned_speedup": round(arms[nonlearned_best][0] / ms, 3)},
             "e2e": {"value": round(statistics.mean(e2e_ms), 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "kernel": "k_sell_apply (FP64 SELL-8 SpMV)", "achieved": round(spmv_gbs, 1),
-                         "peak": peak, "unit": "GB/s", "frac": round(spmv_gbs / peak, 4), "traffic": None,
-                         "algorithmic_bytes": spmv_bytes, "ms_per_launch": t_spmv.value,
-                         "peak_source": peak_kind},
-            "roofline_trisolve": {"bound": "hbm",
-                                  "kernel": ("k_tsell_sweep32 (one FP32 Jacobi sweep, x staged in shared memory)"
-                                             if tiled else "k_sell_sweep32 (one FP32 Jacobi sweep)"),
-                                  "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
-                                  "frac": round(sweep_gbs / peak, 4), "algorithmic_bytes": sweep_bytes,
-                                  # dram read + write of one launch, ncu at this workload (128^3)
-                                  "traffic": (382960000 if tiled and args.grid == 128 else None),
-                                  "traffic_source": "profiles/k_tsell_sweep32_heat128.md",
-                                  "ms_per_launch": t_sweep.value},
+            # the step's largest kernel, k_fact_rows (the IC2 factorisation), is
+            # bound by its dependency chain, not by bytes; the largest
+            # bandwidth-bound kernel is the Jacobi sweep of the triangular solves
+            "roofline": {"bound": "hbm",
+                         "kernel": ("k_tsell_sweep32 (one FP32 Jacobi sweep, x staged in shared memory)"
+                                    if tiled else "k_sell_sweep32 (one FP32 Jacobi sweep)"),
+                         "achieved": round(sweep_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(sweep_gbs / peak, 4), "traffic": sweep_traffic,
+                         "traffic_source": "profiles/k_tsell_sweep32_heat128.md" if sweep_traffic else None,
+                         "algorithmic_bytes": sweep_bytes, "ms_per_launch": t_sweep.value, "peak_source": peak_kind},
+            "roofline_spmv": {"bound": "hbm", "kernel": "k_sell_apply (FP64 SELL-8 SpMV)",
+                              "achieved": round(spmv_gbs, 1), "peak": peak, "unit": "GB/s",
+                              "frac": round(spmv_gbs / peak, 4), "traffic": spmv_traffic,
+                              "traffic_source": "profiles/k_sell_apply_heat128.md" if spmv_traffic else None,
+                              "algorithmic_bytes": spmv_bytes, "ms_per_launch": t_spmv.value,
+                              "peak_source": peak_kind},
             "roofline_unet": {"bound": "tensor", "kernel": "U-Net forward (level 0: k_conv3_tc, tcgen05 + TMA; deeper levels: k_conv3t / k_conv3, mma.sync)",
                               "achieved": round(conv_tflops, 1), "peak": bf16_peak, "unit": "TFLOP/s",
                               "frac": round(conv_tflops / bf16_peak, 4), "ms_per_forward": round(t_unet, 4),

@@ -166,9 +166,12 @@ int bsg_solve_t_dev(bsg_ctx *ctx, bsg_fct *f, int which, int mode, int nsweeps, 
  * pool.  For callers that cannot allocate device memory while they iterate.
  * Factors above 2^21 rows are rejected (BSG_ERR_ARG).  The first call on a
  * device looks the array up and should come before any stream capture; the
- * array is shared per device, so calls must not overlap in time.  Queued on
- * the context stream without a host synchronisation.  No counterpart in the
- * reference (its SolveL / SolveU need no work vector). */
+ * array is shared per device, so calls must not overlap in time.  The
+ * array's address is kept for the life of the process: after a device reset
+ * (cudaDeviceReset) the entry point must not be used until the process
+ * restarts.  Queued on the context stream without a host synchronisation.
+ * No counterpart in the reference (its SolveL / SolveU need no work
+ * vector). */
 int bsg_solve_sweep_static(bsg_ctx *ctx, const bsg_fct *f, int lower, int nsweeps, const double *d_x, double *d_y);
 
 /* ---- Krylov loops --------------------------------------------------------- */

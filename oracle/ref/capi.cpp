@@ -353,4 +353,45 @@ int ref_ich2_block(int nsup, int bs, const int *ia, const int *ja, const double 
 	}
 }
 
+// Whole symmetric block driver CSVector::SolveSymm(CSMatrixRS&)
+// (Bslib/solvers.cpp:4452) with natural ordering: block IC2, then PCG, one
+// right-hand side per call as the reference takes them (Bslib/cg.cpp:375-377);
+// nrhs load cases solved one after another from x = 0.  a: upper-stored
+// blocks, column-major.  stats[4 * k + 0..3] per case: iterations, resfin,
+// wall seconds, density.
+int ref_solve_symm_block(int nsup, int bs, const int *ia, const int *ja, const double *a, int nrhs, const double *b,
+                         double *x, double tau1, double tau2, double theta, double memory, int ittype, double eps,
+                         int niter, double *stats) {
+	const std::ios::iostate cst = std::cout.rdstate();
+	try {
+		const int n = nsup * bs;
+		std::ofstream fout("/dev/null");
+		fout.setstate(std::ios::badbit);
+		std::cout.setstate(std::ios::badbit);
+		for (int k = 0; k < nrhs; k++) {
+			RSBuild m(nsup, bs, ia, ja, a);
+			CSlvParam p;
+			p.msglev = 0; p.ordtype = 0;
+			p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = memory;
+			p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = 1;
+			CSVector vb = make_vec(n, b + (size_t)k * n), norm(n), sol(n);
+			norm.SetSVect(1.0);
+			sol.SetSVect(0.0);
+			double t0 = now_s();
+			sol.SolveSymm(fout, m, vb, p, norm);
+			double t1 = now_s();
+			std::memcpy(x + (size_t)k * n, sol.GetVect(), sizeof(double) * n);
+			if (stats) {
+				stats[4 * k + 0] = p.nitperf; stats[4 * k + 1] = p.resfin; stats[4 * k + 2] = t1 - t0;
+				stats[4 * k + 3] = p.density;
+			}
+		}
+		std::cout.clear(cst);
+		return 0;
+	} catch (const char *e) {
+		std::cout.clear(cst);
+		return fail(e);
+	}
+}
+
 } // extern "C"

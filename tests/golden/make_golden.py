@@ -8,7 +8,11 @@ let every machine check the oracle against the reference.
 
     python tests/golden/make_golden.py            (all fixtures)
     python tests/golden/make_golden.py --block    (lame_block.npz only)
+    python tests/golden/make_golden.py --cfg      (the benchmark-configuration
+                                                  fixtures cfg1_heat32.npz and
+                                                  cell12_lame_periodic.npz only)
 """
+import hashlib
 import os
 import sys
 
@@ -108,7 +112,75 @@ def main_block():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def sha(*arrays):
+    """sha256 over the raw bytes of the arrays, in order (a generator pin)."""
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def main_cfg():
+    """The reference's own solves at benchmark configurations.
+
+    cfg1_heat32.npz: the first benchmark configuration exactly -- 3-D heat,
+    7-point stencil, 32^3 (n = 32768), unit conductivity, RHS uniform[-1,1]
+    from seed 0; CSVector::SolveSymm(CSMatrixR&) with IC2 tau1 = tau2 = 1e-3,
+    theta = 0.1, PCG to relative residual 1e-10 (ittype 0).  Holds the
+    solution, the iteration count, the factor density, a hash of the factor
+    pattern and the factor's action through SolveL / SolveU on a seeded probe
+    vector (4096 sampled entries: the 7.5 MB of factor values stay out).
+
+    cell12_lame_periodic.npz: the homogenisation cell's shape at a size the
+    CPU solves in seconds -- periodic Q1 Lame on 12^3 nodes, inclusions of
+    radius 1-2 cells at 30% volume fraction, contrast 100, seed 2, node 0
+    pinned; its six unit macro-strain load cases each solved by
+    CSVector::SolveSymm(CSMatrixRS&) (block IC2 + PCG, tau 1e-3, relative
+    residual 1e-8).  Holds the six solutions and each one's distance to a
+    sparse direct solve, the accuracy the reference itself reached.
+    """
+    import scipy.sparse.linalg as spla
+    ref = RefLib()
+    s = P.config(1)
+    u = s.upper()
+    b = s.rhs[0]
+    x, info = ref.solve_symm(u.ia, u.ja, u.a, b, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=-1.0, ittype=0,
+                             eps=1e-10, niter=3000)
+    iu, ju, uu, st = ref.ich2(u.ia, u.ja, u.a, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
+    rng = np.random.default_rng(101)
+    probe = rng.standard_normal(s.n)
+    idx = np.sort(rng.choice(s.n, 4096, replace=False)).astype(np.int32)
+    out = dict(system_sha=sha(s.ia, s.ja, s.a, b), upper_sha=sha(u.ia, u.ja, u.a), x_ref=x,
+               iters=np.array(info["iters"]),
+               true_res=np.array(np.linalg.norm(b - s.to_scipy() @ x) / np.linalg.norm(b)),
+               density=np.array(st[0]), factor_nnz=np.array(len(ju)), factor_pattern_sha=sha(iu, ju),
+               probe_idx=idx, probe_solve_l=ref.solve_l(iu, ju, uu, probe)[idx],
+               probe_solve_u=ref.solve_u(iu, ju, uu, probe)[idx])
+    path = os.path.join(HERE, "cfg1_heat32.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+    c = P.lame_periodic(12, 0.3, 1.0, 2.0, 0.3, 100.0, 2)
+    cu = c.upper()
+    X, infos = ref.solve_symm_block(cu.ia, cu.ja, cu.a, c.bs, c.rhs, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0,
+                                    ittype=0, eps=1e-8, niter=3000)
+    A = c.to_scipy().tocsc()
+    lu = spla.splu(A)
+    ref_err = []
+    for k in range(c.rhs.shape[0]):
+        xd = lu.solve(c.rhs[k])
+        ref_err.append(np.linalg.norm(X[k] - xd) / np.linalg.norm(xd))
+    out = dict(system_sha=sha(c.ia, c.ja, c.a, c.rhs), X_ref=X, iters=np.array([i["iters"] for i in infos]),
+               ref_err_vs_direct=np.array(ref_err))
+    path = os.path.join(HERE, "cell12_lame_periodic.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes", "ref errors", ref_err)
+
+
 if __name__ == "__main__":
-    if "--block" not in sys.argv:
-        main()
-    main_block()
+    if "--cfg" in sys.argv:
+        main_cfg()
+    else:
+        if "--block" not in sys.argv:
+            main()
+        main_block()

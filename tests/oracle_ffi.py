@@ -337,3 +337,19 @@ class RefLib:
         for p in (pia, pja, pu):
             self.lib.ref_free(p)
         return ia_f, ja_f, u, (st[0], st[1], st[2])
+
+    def solve_symm_block(self, ia, ja, a, bs, B, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, ittype=0, eps=1e-8,
+                         niter=1000):
+        """CSVector::SolveSymm(CSMatrixRS&) (block IC2 + PCG) for each row of B
+        (load cases), x0 = 0: (X, [dict(iters, resfin, wall, density)])."""
+        nb = len(ia) - 1
+        B = np.ascontiguousarray(np.atleast_2d(B), dtype=np.float64)
+        nrhs = B.shape[0]
+        X = np.zeros_like(B)
+        st = (C.c_double * (4 * nrhs))()
+        self._err(self.lib.ref_solve_symm_block(nb, bs, _i(ia), _i(ja), _d(a), nrhs, _d(B), _d(X),
+                                                C.c_double(tau1), C.c_double(tau2), C.c_double(theta),
+                                                C.c_double(memory), ittype, C.c_double(eps), niter, st))
+        info = [dict(iters=int(st[4 * k]), resfin=st[4 * k + 1], wall=st[4 * k + 2], density=st[4 * k + 3])
+                for k in range(nrhs)]
+        return X, info

@@ -3,7 +3,10 @@ allocating entry points bsg_solve_l_dev / bsg_solve_u_dev in sweep mode.
 
 Both run the same kernels in the same order, so the results agree to the
 last bit; the test allows 1e-14 relative.  Two calls in a row check that the
-shared static work array carries nothing from one call to the next.
+shared static work array carries nothing from one call to the next.  The
+library allocates from the device's default stream-ordered memory pool; the
+pool's high-water mark, reset before each call, shows that the static entry
+point takes nothing from it while the allocating entry point does.
 """
 import ctypes as C
 
@@ -15,6 +18,26 @@ import problems as P
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-14
+
+
+def _pool_marks(device=0):
+    """(used bytes now, high-water mark) of the device's default memory pool."""
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, cur = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, high = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(cur), int(high)
+
+
+def _reset_high_mark(device=0):
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device)
+    assert err == rt.cudaError_t.cudaSuccess
+    (err,) = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, rt.cuuint64_t(0))
+    assert err == rt.cudaError_t.cudaSuccess
 
 
 def _static_solve(ctx, f, lower, nsweeps, x, y):
@@ -41,9 +64,18 @@ def test_static_sweep_matches_allocating_solve(ctx, precision):
                 x = torch.as_tensor(rng.standard_normal(s.n), device="cuda")
                 want = torch.empty_like(x)
                 got = torch.full_like(x, np.nan)
+                ctx.sync()
+                _reset_high_mark()
+                base, _ = _pool_marks()
                 (f.solve_l if lower else f.solve_u)(x, want, mode=1, nsweeps=nsweeps)
+                ctx.sync()
+                _, high_alloc = _pool_marks()
+                assert high_alloc > base, "the allocating solve should draw its work vector from the pool"
+                _reset_high_mark()
                 assert _static_solve(ctx, f, lower, nsweeps, x, got) == bsg.OK, bsg.lib().bsg_last_error()
                 ctx.sync()
+                cur, high = _pool_marks()
+                assert cur == base and high == base, ("the static solve took pool memory", base, cur, high)
                 w, g = want.cpu().numpy(), got.cpu().numpy()
                 assert np.all(np.isfinite(g))
                 assert np.abs(g - w).max() <= TOL * np.abs(w).max(), (lower, nsweeps, call)
