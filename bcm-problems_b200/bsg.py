@@ -101,6 +101,14 @@ def lib():
         "bsg_solve_t_dev": (i_, [vp, vp, i_, i_, i_, vp, vp]),
         "bsg_sell_stats": (i_, [vp, vp, C.POINTER(C.c_longlong)]),
         "bsg_fct_export_block": (i_, [vp, ip, ip, ip, ip, dp, dp]),
+        "bsg_mat_vbsr": (i_, [vp, i_, ip, ip, ip, dp, i_, pp]),
+        "bsg_read_mtr_bin": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, ip, ip, ip, ip, dp]),
+        "bsg_write_mtr_bin": (i_, [C.c_char_p, i_, i_, i_, i_, ip, ip, ip, dp]),
+        "bsg_read_mtr": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, ip, dp]),
+        "bsg_read_vect": (i_, [C.c_char_p, C.POINTER(C.c_longlong), i_, dp]),
+        "bsg_write_vect_bin": (i_, [C.c_char_p, i_, i_, i_, i_, dp, ip, ip]),
+        "bsg_read_vect_bin": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, dp, ip, ip]),
+        "bsg_solve": (i_, [vp, vp, vp, dp, dp, C.POINTER(Param)]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -431,6 +439,104 @@ def solve_symm(ctx, n, ia, ja, a, b, param):
     x = np.zeros(n)
     _check(lib().bsg_solve_symm_csr(ctx.h, n, _ip(ia), _ip(ja), _dp(a), _dp(b), _dp(x), C.byref(param)))
     return x
+
+
+def solve(ctx, mat, fct, b, x0, param):
+    """The Krylov solve of bsg_solve with host buffers: x0 the initial guess;
+    returns the solution (also when the iteration limit stopped the loop,
+    which then raises after the copy is taken)."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    _check(lib().bsg_solve(ctx.h, mat.h, fct.h, _dp(b), x.ctypes.data_as(C.POINTER(C.c_double)), C.byref(param)))
+    return x
+
+
+# ---- files in the reference's formats (CSMatrixR::ReadMtrBin / WriteMtrBin /
+#      ReadMtr, CSVector::ReadVect / WriteVectBin / ReadVectBin)
+
+def _ni(n):
+    return np.zeros(max(n, 0), np.int32)
+
+
+def read_system_bin(path, nvec=0):
+    """A CSMatrixR in binary form followed by nvec CSVectors in binary form
+    (the layout of CSMatrixR::ConvertToBinary): returns (m, n, list, ia, ja,
+    a, [vectors])."""
+    L = lib()
+    pb = os.fsencode(path)
+    off = C.c_longlong(0)
+    m, n, nl, nz = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(L.bsg_read_mtr_bin(pb, C.byref(off), C.byref(m), C.byref(n), C.byref(nl), C.byref(nz), None, None, None,
+                              None))
+    lst, ia, ja, a = _ni(nl.value), _ni(nl.value + 1), _ni(nz.value), np.zeros(nz.value)
+    ptr = lambda v: v.ctypes.data_as(C.POINTER(C.c_int if v.dtype == np.int32 else C.c_double))  # noqa: E731
+    _check(L.bsg_read_mtr_bin(pb, C.byref(off), None, None, None, None, ptr(lst), ptr(ia), ptr(ja), ptr(a)))
+    vecs = []
+    for _ in range(nvec):
+        nv, nr, npart = C.c_int(), C.c_int(), C.c_int()
+        _check(L.bsg_read_vect_bin(pb, C.byref(off), C.byref(nv), C.byref(nr), C.byref(npart), None, None, None))
+        v, bl, ind = np.zeros(nv.value * nr.value), _ni(npart.value + 1), _ni(npart.value)
+        _check(L.bsg_read_vect_bin(pb, C.byref(off), None, None, None, ptr(v), ptr(bl), ptr(ind)))
+        vecs.append(v)
+    return m.value, n.value, lst, ia, ja, a, vecs
+
+
+def write_system_bin(path, ia, ja, a, vecs=(), lst=None):
+    """Write a CSMatrixR (binary form) and then the vectors (CSVector binary
+    form, one part each), as CSMatrixR::ConvertToBinary lays a system out."""
+    L = lib()
+    pb = os.fsencode(path)
+    n = len(ia) - 1
+    lst = np.arange(n, dtype=np.int32) if lst is None else lst
+    _check(L.bsg_write_mtr_bin(pb, 0, n, n, n, _ip(lst), _ip(ia), _ip(ja), _dp(a)))
+    for v in vecs:
+        v = np.ascontiguousarray(v, np.float64)
+        _check(L.bsg_write_vect_bin(pb, 1, len(v), 1, 1, _dp(v), _ip(np.array([0, len(v)])), _ip(np.array([0]))))
+
+
+def read_system_text(path, nvec=0):
+    """The text form CSMatrixR::ReadMtr reads, then nvec vectors as
+    CSVector::ReadVect reads them: returns (n, ia, ja, a, [vectors])."""
+    L = lib()
+    pb = os.fsencode(path)
+    off = C.c_longlong(0)
+    n, nz = C.c_int(), C.c_int()
+    _check(L.bsg_read_mtr(pb, C.byref(off), C.byref(n), C.byref(nz), None, None, None))
+    ia, ja, a = _ni(n.value + 1), _ni(nz.value), np.zeros(nz.value)
+    _check(L.bsg_read_mtr(pb, C.byref(off), None, None, ia.ctypes.data_as(C.POINTER(C.c_int)),
+                          ja.ctypes.data_as(C.POINTER(C.c_int)), a.ctypes.data_as(C.POINTER(C.c_double))))
+    vecs = []
+    for _ in range(nvec):
+        v = np.zeros(n.value)
+        _check(L.bsg_read_vect(pb, C.byref(off), n.value, v.ctypes.data_as(C.POINTER(C.c_double))))
+        vecs.append(v)
+    return n.value, ia, ja, a, vecs
+
+
+_bslib = None
+
+
+def bslib():
+    """Load libbsg_bslib.so, the drop-ins for Bslib's AbstractSymmSolver /
+    AbstractSolver (built against the reference's headers)."""
+    global _bslib
+    if _bslib is None:
+        lib()
+        path = os.path.join(os.path.dirname(LIB_SO), "libbsg_bslib.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is not built; build with BSLIB_INCLUDE (or BSG_REFERENCE) set")
+        L = C.CDLL(path)
+        L.bsg_bslib_abstract.restype = C.c_int
+        L.bsg_bslib_abstract.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(Param)]
+        L.bsg_bslib_last_error.restype = C.c_char_p
+        _bslib = L
+    return _bslib
+
+
+def abstract_solve(symm, gener, fns, param):
+    """bsg_bslib_abstract: the GPU AbstractSymmSolver (symm) / AbstractSolver
+    on a generator object and its seven callbacks; returns the status code
+    (the solution goes through the generator's store callback)."""
+    return bslib().bsg_bslib_abstract(int(symm), gener, fns, C.byref(param))
 
 
 def solver(ctx, n, ia, ja, a, b, param):

@@ -2,6 +2,11 @@
 
 * ``libbsg.so``          -- the sm_100a solver library (csrc/*.cu), nvcc.
 * ``libbsg_problems.so`` -- the host-side problem generators (csrc/problems.cpp).
+* ``libbsg_bslib.so``    -- the drop-ins for Bslib's AbstractSymmSolver /
+  AbstractSolver (csrc/bsg_bslib.cpp), compiled against the reference's own
+  headers (slvparam.h, smatrix.h): built only when BSLIB_INCLUDE names the
+  directory that holds them (or BSG_REFERENCE the reference source tree, whose
+  Bslib/ it is); a library built earlier is kept otherwise.
 
 Objects are compiled in parallel into ``_build/`` and linked next to this
 file, so the shared objects travel with a copy of the repository.
@@ -33,6 +38,17 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources)
 
 
+def bslib_include():
+    """Directory of the reference's Bslib headers, from BSLIB_INCLUDE or
+    BSG_REFERENCE (the reference source tree); None when neither is set."""
+    inc = os.environ.get("BSLIB_INCLUDE")
+    if not inc and os.environ.get("BSG_REFERENCE"):
+        inc = os.path.join(os.environ["BSG_REFERENCE"], "Bslib")
+    if inc and not os.path.isfile(os.path.join(inc, "slvparam.h")):
+        raise RuntimeError(f"BSLIB_INCLUDE / BSG_REFERENCE: no slvparam.h in {inc}")
+    return inc
+
+
 def build(verbose=False, ptxas_info=False):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
@@ -57,6 +73,13 @@ def build(verbose=False, ptxas_info=False):
     gen_lib = os.path.join(HERE, "libbsg_problems.so")
     if _stale(gen_lib, [gen_src]):
         _run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-o", gen_lib, gen_src])
+    inc = bslib_include()
+    shim_src = os.path.join(CSRC, "bsg_bslib.cpp")
+    shim_lib = os.path.join(HERE, "libbsg_bslib.so")
+    if inc and _stale(shim_lib, [shim_src, lib, os.path.join(os.path.dirname(HERE), "include", "bsg_bslib.h")]):
+        _run(["g++", "-O2", "-fPIC", "-shared", "-std=gnu++14", "-fpermissive", "-w", "-I", inc, "-I",
+              os.path.join(os.path.dirname(HERE), "include"), "-o", shim_lib, shim_src, "-L", HERE, "-lbsg",
+              "-Wl,-rpath,$ORIGIN"])
     if verbose or ptxas_info:
         for k, v in logs.items():
             if v.strip():

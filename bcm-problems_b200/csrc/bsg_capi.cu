@@ -7,6 +7,7 @@
 #include <cmath>
 #include <new>
 #include <vector>
+#include <algorithm>
 
 int bsg_expand_symmetric(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz_up, int **ia_o,
                          int **ja_o, double **a_o, int *nnz_o);
@@ -334,11 +335,107 @@ extern "C" int bsg_mat_csr_dev(bsg_ctx *c, int n, const int *ia, const int *ja, 
 	return mat_csr_common(c, n, ia, ja, a, symm_upper, false, out);
 }
 
+// Point CSR of a block matrix with block sizes sprnd[i+1] - sprnd[i]
+// (CSMatrixRS with sprndr = sprndc, Bslib/smatrix.h:1040-1048): the blocks of
+// block row i follow one another in `a`, each column-major, columns ascending.
+// Symmetric (upper) input keeps the upper triangle of each diagonal block, so
+// every point row starts with its diagonal; rows come out column-sorted.
+static int vbsr_to_point_host(int nsup, const int *sprnd, const int *ia, const int *ja, const double *a,
+                              int symm_upper, std::vector<int> &pia, std::vector<int> &pja, std::vector<double> &pa) {
+	const int n = sprnd[nsup];
+	std::vector<long long> cnt(n + 1, 0);
+	size_t off = 0;
+	std::vector<size_t> bsa(ia[nsup] + 1, 0);
+	for (int i = 0; i < nsup; i++) {
+		const int bi = sprnd[i + 1] - sprnd[i];
+		for (int k = ia[i]; k < ia[i + 1]; k++) {
+			const int j = ja[k], bj = sprnd[j + 1] - sprnd[j];
+			bsa[k] = off;
+			off += (size_t)bi * bj;
+			for (int r = 0; r < bi; r++) {
+				const int nr = (symm_upper && j == i) ? bj - r : bj;
+				cnt[sprnd[i] + r + 1] += nr;
+			}
+		}
+	}
+	for (int r = 0; r < n; r++) cnt[r + 1] += cnt[r];
+	if (cnt[n] > 0x7fffffffLL) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: more than 2^31 point entries");
+	pia.assign(cnt.begin(), cnt.end());
+	pja.resize(pia[n]);
+	pa.resize(pia[n]);
+	std::vector<int> pos(pia.begin(), pia.end() - 1);
+	for (int i = 0; i < nsup; i++) {
+		const int bi = sprnd[i + 1] - sprnd[i];
+		for (int k = ia[i]; k < ia[i + 1]; k++) {
+			const int j = ja[k], bj = sprnd[j + 1] - sprnd[j];
+			const double *blk = a + bsa[k];
+			for (int r = 0; r < bi; r++)
+				for (int cc = (symm_upper && j == i) ? r : 0; cc < bj; cc++) {
+					const int q = pos[sprnd[i] + r]++;
+					pja[q] = sprnd[j] + cc;
+					pa[q] = blk[(size_t)cc * bi + r];
+				}
+		}
+	}
+	return BSG_OK;
+}
+
+extern "C" int bsg_mat_vbsr(bsg_ctx *c, int nsup, const int *sprnd, const int *ia, const int *ja, const double *a,
+                            int symm_upper, bsg_mat **out) {
+	if (!c || !out || !sprnd) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: null argument");
+	*out = nullptr;
+	int rc = check_csr_host(nsup, ia, ja, 1);
+	if (rc) return rc;
+	if (sprnd[0] != 0) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: sprnd[0] != 0");
+	bool all3 = true, all1 = true;
+	for (int i = 0; i < nsup; i++) {
+		const int b = sprnd[i + 1] - sprnd[i];
+		if (b < 1) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: empty block");
+		all3 = all3 && b == 3;
+		all1 = all1 && b == 1;
+	}
+	for (int i = 0; i < nsup; i++)
+		for (int k = ia[i] + 1; k < ia[i + 1]; k++)
+			if (ja[k] <= ja[k - 1]) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: block columns must ascend");
+	if (symm_upper) {
+		rc = check_upper_host(nsup, ia, ja);
+		if (rc) return rc;
+	}
+	if (all1) return bsg_mat_csr(c, nsup, ia, ja, a, symm_upper, out);
+	if (all3) return bsg_mat_bsr(c, nsup, 3, ia, ja, a, symm_upper, out);
+	std::vector<int> pia, pja;
+	std::vector<double> pa;
+	rc = vbsr_to_point_host(nsup, sprnd, ia, ja, a, symm_upper, pia, pja, pa);
+	if (rc) return rc;
+	return bsg_mat_csr(c, sprnd[nsup], pia.data(), pja.data(), pa.data(), symm_upper, out);
+}
+
 extern "C" int bsg_mat_bsr(bsg_ctx *c, int nsup, int bs, const int *ia, const int *ja, const double *a,
                            int symm_upper, bsg_mat **out) {
 	if (!c || !out) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_bsr: null argument");
+	if (bs < 1) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_bsr: block size must be positive");
 	if (bs == 1) return bsg_mat_csr(c, nsup, ia, ja, a, symm_upper, out);
-	if (bs != 3) return bsg_set_error(BSG_ERR_UNSUPPORTED, "bsg_mat_bsr: block size must be 1 or 3");
+	if (bs != 3) {
+		// other uniform sizes: the point expansion (columns sorted per row first)
+		if (nsup < 0 || (long long)nsup * bs > 0x7fffffffLL) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_bsr: too large");
+		int rc = check_csr_host(nsup, ia, ja, bs);
+		if (rc) return rc;
+		std::vector<int> sprnd(nsup + 1), sja(ia[nsup]);
+		std::vector<double> sa((size_t)ia[nsup] * bs * bs);
+		for (int i = 0; i <= nsup; i++) sprnd[i] = i * bs;
+		std::vector<std::pair<int, int>> row;
+		for (int i = 0; i < nsup; i++) {
+			row.clear();
+			for (int k = ia[i]; k < ia[i + 1]; k++) row.push_back({ja[k], k});
+			std::sort(row.begin(), row.end());
+			for (size_t q = 0; q < row.size(); q++) {
+				sja[ia[i] + q] = row[q].first;
+				std::copy(a + (size_t)row[q].second * bs * bs, a + (size_t)(row[q].second + 1) * bs * bs,
+				          sa.begin() + (size_t)(ia[i] + q) * bs * bs);
+			}
+		}
+		return bsg_mat_vbsr(c, nsup, sprnd.data(), ia, sja.data(), sa.data(), symm_upper, out);
+	}
 	int rc = check_csr_host(nsup, ia, ja, bs);
 	if (!rc && symm_upper) rc = check_upper_host(nsup, ia, ja);
 	if (rc) return rc;
@@ -629,6 +726,37 @@ static int drive(bsg_ctx *c, int n, const int *ia, const int *ja, const double *
 	bsg_fct_free(f);
 	bsg_mat_free(m);
 	if (!rc && rc2) rc = bsg_set_error(BSG_ERR_CUDA, "copy of the solution failed");
+	return rc;
+}
+
+extern "C" int bsg_solve(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const double *b, double *x, bsg_param *p) {
+	if (!c || !m || !f || !p || !b || !x) return bsg_set_error(BSG_ERR_ARG, "bsg_solve: null argument");
+	const size_t n = (size_t)m->n * m->bs;
+	double *db = nullptr, *dx = nullptr;
+	cudaStream_t s = c->stream;
+	if (cudaMallocAsync(&db, sizeof(double) * (n ? n : 1), s) != cudaSuccess ||
+	    cudaMallocAsync(&dx, sizeof(double) * (n ? n : 1), s) != cudaSuccess) {
+		if (db) cudaFreeAsync(db, s);
+		return bsg_set_error(BSG_ERR_NOMEM, "bsg_solve: vectors");
+	}
+	int rc = BSG_OK;
+	if (cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+	    cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+		rc = bsg_set_error(BSG_ERR_CUDA, "bsg_solve: copy to the device failed");
+	if (!rc) {
+		if (p->krylov != 0) rc = bsg_gmres_dev(c, m, f, db, dx, p);
+		else if (m->symm) rc = bsg_pcg_dev(c, m, f, db, dx, p);              // CSVector::Cg
+		else if (m->bs == 1 && !f->d_bia) rc = bsg_lanczos_dev(c, m, f, db, dx, p); // CSVector::Lanczos
+		else rc = bsg_gmres_dev(c, m, f, db, dx, p);
+	}
+	// the last iterate comes back also when the iteration limit was reached
+	if (rc == BSG_OK || rc == BSG_ERR_NOCONV) {
+		if (cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess && rc == BSG_OK)
+			rc = bsg_set_error(BSG_ERR_CUDA, "bsg_solve: copy of the solution failed");
+	}
+	cudaStreamSynchronize(s);
+	cudaFreeAsync(db, s);
+	cudaFreeAsync(dx, s);
 	return rc;
 }
 

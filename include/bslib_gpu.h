@@ -108,10 +108,23 @@ int bsg_mat_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double 
 /* Same from device arrays (copied device-to-device). */
 int bsg_mat_csr_dev(bsg_ctx *ctx, int n, const int *d_ia, const int *d_ja, const double *d_a, int symm_upper,
                     bsg_mat **out);
-/* Block CSR with uniform block size bs (1..4), blocks column-major as in
- * CSMatrixRS (a[9*j + 3*c + r] for bs == 3). */
+/* Block CSR with uniform block size bs >= 1, blocks column-major as in
+ * CSMatrixRS (a[9*j + 3*c + r] for bs == 3).  bs == 3 keeps the 3x3 block
+ * path (block SpMV, the block IC2 / ILU2 of CSMatrixRS); bs == 1 is point
+ * CSR; any other size is expanded to point CSR on the host, and the point
+ * factorisations then apply to it. */
 int bsg_mat_bsr(bsg_ctx *ctx, int nsup, int bs, const int *ia, const int *ja, const double *a, int symm_upper,
                 bsg_mat **out);
+/* Block CSR with variable block sizes: the CSMatrixRS layout with
+ * sprndr = sprndc = sprnd (Bslib/smatrix.h:1040-1048), as the reference's
+ * AbstractSolver / AbstractSymmSolver assemble it (Bslib/solvers.cpp:
+ * 5638-5736).  Block row i has sprnd[i+1] - sprnd[i] rows; its blocks follow
+ * one another in `a`, each column-major, columns ascending in every block row
+ * (symm_upper: upper blocks only, the diagonal block first).  All blocks 3x3:
+ * the block path of bsg_mat_bsr; all 1x1: point CSR; otherwise the point
+ * expansion (upper triangle of each diagonal block when symm_upper). */
+int bsg_mat_vbsr(bsg_ctx *ctx, int nsup, const int *sprnd, const int *ia, const int *ja, const double *a,
+                 int symm_upper, bsg_mat **out);
 int bsg_mat_free(bsg_mat *m);
 int bsg_mat_info(const bsg_mat *m, int *n, int *bs, int *nnz);
 
@@ -208,6 +221,14 @@ int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs
                       const double *d_B, double *d_X, bsg_param *p, int *iters, double *res, int *tuned);
 
 /* ---- whole drivers with host buffers ------------------------------------- */
+/* The iteration of CSVector::SolveSymm / Solver (Bslib/solvers.cpp:4452,
+ * :4615, :1339, :1568) on a matrix and its factor, host buffers: x holds the
+ * initial guess on entry (the drivers start from the vector itself) and the
+ * solution on exit, also when the iteration limit stopped the loop
+ * (BSG_ERR_NOCONV).  p->krylov 0: PCG (CSVector::Cg) for a symmetric matrix,
+ * the two-sided Lanczos (CSVector::Lanczos) for a nonsymmetric point matrix,
+ * GMRES(restart) for a nonsymmetric block matrix; 1 / 2: GMRES / FGMRES. */
+int bsg_solve(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *b, double *x, bsg_param *p);
 /* CSVector::SolveSymm(CSMatrixR&) (Bslib/solvers.cpp:4615): upper-stored SPD
  * CSR in, IC2 + PCG (or GMRES/FGMRES per p->krylov), solution out. */
 int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b,
@@ -217,6 +238,33 @@ int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const 
  * GMRES(restart) / FGMRES (krylov 1 / 2), solution out. */
 int bsg_solver_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
                    bsg_param *p);
+
+/* ---- matrix and vector files in the reference's formats (host only) -------
+ * Each reader works at the byte offset *offset of the file; with every array
+ * NULL it returns the sizes only (offset unchanged), else it fills the arrays
+ * and moves *offset past what it read, so the pieces of one file (a matrix
+ * followed by its vectors, as ConvertToBinary writes them,
+ * Bslib/smatrixr.cpp:4010) are read one after another.  Writers truncate the
+ * file, or append when append != 0.  BSG_ERR_ARG for a malformed or
+ * truncated file, with its path in the message. */
+/* CSMatrixR::ReadMtrBin (Bslib/smatrixr.cpp:3852): int m, n, nlist, nzja;
+ * int list[nlist], ia[nlist+1], ja[nzja]; double a[nzja], native order. */
+int bsg_read_mtr_bin(const char *path, long long *offset, int *m, int *n, int *nlist, int *nzja, int *list, int *ia,
+                     int *ja, double *a);
+/* CSMatrixR::WriteMtrBin (Bslib/smatrixr.cpp:3984), the same layout. */
+int bsg_write_mtr_bin(const char *path, int append, int m, int n, int nlist, const int *list, const int *ia,
+                      const int *ja, const double *a);
+/* CSMatrixR::ReadMtr (Bslib/smatrixr.cpp:3888), the text form: n and nzja,
+ * a label line, ia[n+1], a label line, ja[nzja], a label line, a[nzja]. */
+int bsg_read_mtr(const char *path, long long *offset, int *n, int *nzja, int *ia, int *ja, double *a);
+/* CSVector::ReadVect (Bslib/svector.cpp:465): a label line, then nv values. */
+int bsg_read_vect(const char *path, long long *offset, int nv, double *v);
+/* CSVector::WriteVectBin / ReadVectBin (Bslib/svector.cpp:537 / :488):
+ * int nparts, nrhs, nv; double v[nv*nrhs]; int blksv[nparts+1], inda[nparts]. */
+int bsg_write_vect_bin(const char *path, int append, int nv, int nrhs, int nparts, const double *v, const int *blksv,
+                       const int *inda);
+int bsg_read_vect_bin(const char *path, long long *offset, int *nv, int *nrhs, int *nparts, double *v, int *blksv,
+                      int *inda);
 
 /* ---- learned preconditioner stage (no counterpart in the reference) --------
  * A 4-level 3D convolutional U-Net (16 base channels, bf16 weights, FP32

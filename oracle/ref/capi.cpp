@@ -394,4 +394,52 @@ int ref_solve_symm_block(int nsup, int bs, const int *ia, const int *ja, const d
 	}
 }
 
+// ---- files in the reference's own formats (CSMatrixR::WriteMtrBin / ReadMtrBin,
+// Bslib/smatrixr.cpp:3984 / :3852; CSVector::WriteVectBin / ReadVectBin,
+// Bslib/svector.cpp:537 / :488; CSMatrixR::ConvertToBinary, :4010).  They print
+// to cout; the harness silences it around the calls.
+struct QuietCout {
+	std::ios::iostate st = std::cout.rdstate();
+	QuietCout() { std::cout.setstate(std::ios::badbit); }
+	~QuietCout() { std::cout.clear(st); }
+};
+
+int ref_write_mtr_bin(const char *path, int n, const int *ia, const int *ja, const double *a) {
+	QuietCout q;
+	CSMatrixR m = make_csr(n, ia, ja, a);
+	std::ofstream f(path, std::ios::binary | std::ios::trunc);
+	m.WriteMtrBin(f);
+	return f ? 0 : fail("write failed");
+}
+
+int ref_write_vect_bin(const char *path, int append, int n, const double *v) {
+	QuietCout q;
+	CSVector vv = make_vec(n, v);
+	std::ofstream f(path, std::ios::binary | (append ? std::ios::app : std::ios::trunc));
+	vv.WriteVectBin(f);
+	return f ? 0 : fail("write failed");
+}
+
+// A binary file holding a matrix and then nvec vectors, read with the
+// reference's readers: ia / ja / a are malloc'ed (ref_free), vectors go to
+// vecs (nvec * n values, n the matrix size).
+int ref_read_system_bin(const char *path, int nvec, int *n_out, int **ia, int **ja, double **a, double *vecs) {
+	QuietCout q;
+	try {
+		std::ifstream f(path, std::ios::binary);
+		CSMatrixR m = CSMatrixR::ReadMtrBin(f);
+		export_csr(m, ia, ja, a);
+		const int n = m.GetNlist();
+		*n_out = n;
+		CSVector dummy;
+		for (int k = 0; k < nvec; k++) {
+			CSVector v = dummy.ReadVectBin(f);
+			if (vecs) std::memcpy(vecs + (size_t)k * n, v.GetVect(), sizeof(double) * n);
+		}
+		return f ? 0 : fail("read failed");
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
 } // extern "C"

@@ -353,3 +353,77 @@ class RefLib:
         info = [dict(iters=int(st[4 * k]), resfin=st[4 * k + 1], wall=st[4 * k + 2], density=st[4 * k + 3])
                 for k in range(nrhs)]
         return X, info
+
+    # ---- generator behind the abstract-interface callbacks (oracle/ref/abstract_gen.cpp) ----
+    def gen_create(self, sprnd, ia, ja, a, b, x0, seed=1):
+        """A generator serving block CSR (blocks column-major, sizes from
+        sprnd) through Bslib's seven callbacks, each block row's blocks in a
+        shuffled order.  Returns an opaque handle (free with gen_free)."""
+        self.lib.ref_gen_create.restype = C.c_void_p
+        self._gen_keep = [np.ascontiguousarray(v, dt) for v, dt in
+                          ((sprnd, np.int32), (ia, np.int32), (ja, np.int32), (a, np.float64), (b, np.float64),
+                           (x0, np.float64))]
+        sp_, ia_, ja_, a_, b_, x_ = self._gen_keep
+        h = self.lib.ref_gen_create(len(ia_) - 1, _i(sp_), _i(ia_), _i(ja_), _d(a_), _d(b_), _d(x_),
+                                    C.c_uint(seed))
+        return C.c_void_p(h)
+
+    def gen_free(self, h):
+        self.lib.ref_gen_free(h)
+
+    def gen_solution(self, h, n):
+        x = np.zeros(n)
+        self.lib.ref_gen_solution(h, _d(x))
+        return x
+
+    def gen_calls(self, h):
+        c = np.zeros(7, np.int32)
+        self.lib.ref_gen_calls(h, _i(c))
+        return c
+
+    def gen_fns(self):
+        fns = (C.c_void_p * 7)()
+        self.lib.ref_gen_fns(fns)
+        return fns
+
+    def abstract(self, symm, h, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, ittype=0, sttype=1, eps=1e-10,
+                 niter=3000):
+        """The reference's AbstractSymmSolver (symm) / AbstractSolver on generator h."""
+        out = (C.c_double * 4)()
+        rc = self.lib.ref_abstract(int(symm), h, C.c_double(tau1), C.c_double(tau2), C.c_double(theta),
+                                   C.c_double(memory), ittype, sttype, C.c_double(eps), niter, out)
+        if rc != 0:
+            self.lib.ref_abstract_error.restype = C.c_char_p
+            raise RuntimeError(self.lib.ref_abstract_error().decode())
+        return dict(iters=int(out[0]), resfin=out[1], density=out[2], wall=out[3])
+
+    # ---- the reference's own file readers / writers ----
+    def write_system_bin(self, path, ia, ja, a, vecs=()):
+        """CSMatrixR::WriteMtrBin, then CSVector::WriteVectBin per vector."""
+        n = len(ia) - 1
+        pb = os.fsencode(path)
+        self._err(self.lib.ref_write_mtr_bin(pb, n, _i(ia), _i(ja), _d(a)))
+        for v in vecs:
+            self._err(self.lib.ref_write_vect_bin(pb, 1, len(v), _d(v)))
+
+    def read_system_bin(self, path, nvec, n):
+        """CSMatrixR::ReadMtrBin then nvec CSVector::ReadVectBin: (ia, ja, a, vecs)."""
+        pia, pja, pa = _ip(), _ip(), _dp()
+        nn = C.c_int()
+        vecs = np.zeros(max(nvec * n, 1))
+        self._err(self.lib.ref_read_system_bin(os.fsencode(path), nvec, C.byref(nn), C.byref(pia), C.byref(pja),
+                                               C.byref(pa), _d(vecs)))
+        ia, ja, a, _ = _take_csr(self.lib, nn.value, pia, pja, pa)
+        for p in (pia, pja, pa):
+            self.lib.ref_free(p)
+        return ia, ja, a, [vecs[k * n:(k + 1) * n].copy() for k in range(nvec)]
+
+    def convert_to_binary(self, text_path, bin_path):
+        """CSMatrixR::ConvertToBinary (text matrix + rhs + norm -> binary), run
+        as the separate program oracle/_ref/ref_convert (the reference's text
+        streams crash inside a Python process)."""
+        import subprocess
+        tool = os.path.join(os.path.dirname(REF_SO), "ref_convert")
+        r = subprocess.run([tool, text_path, bin_path], capture_output=True, text=True, timeout=120)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_convert failed: {r.stderr.strip()}")

@@ -117,3 +117,32 @@ def test_every_entry_point_rejects_null_handles():
     for nm, v in got.items():
         want = bsg.OK if nm in releases | ok_when_empty else bsg.ERR_ARG
         assert int(v) == want, (nm, v)
+
+
+def test_bslib_dropins_export_the_reference_signatures():
+    """libbsg_bslib.so exports the C form of the Abstract*Solver drop-ins and
+    the C++ drop-ins with the reference's parameter types
+    (Bslib/smatrix.h:27-34: void *, ofstream &, CSlvParam &, then the seven
+    callback types)."""
+    import subprocess
+    import bsg
+    L = bsg.bslib()
+    for nm in ("bsg_bslib_abstract", "bsg_bslib_last_error"):
+        assert hasattr(L, nm)
+    path = os.path.join(os.path.dirname(bsg.LIB_SO), "libbsg_bslib.so")
+    syms = subprocess.run(["nm", "-DC", path], capture_output=True, text=True, check=True).stdout
+    cb = ("void (*)(void*, int&), void (*)(void*, int*), void (*)(void*, int*&, int*&), "
+          "void (*)(void*, int, double*), void (*)(void*, int, double*), void (*)(void*, int, double*), "
+          "void (*)(void*, int, double*)")
+    for fn in ("AbstractSymmSolver", "AbstractSolver"):
+        sig = f"bsg_bslib::{fn}(void*, std::basic_ofstream<char, std::char_traits<char> >&, CSlvParam&, {cb})"
+        assert sig in syms, fn
+
+
+def test_bslib_dropin_rejects_null_arguments_without_a_device():
+    import bsg
+    p = bsg.default_param()
+    assert bsg.abstract_solve(True, None, None, p) == bsg.ERR_ARG
+    fns = (C.c_void_p * 7)()
+    assert bsg.abstract_solve(True, None, fns, p) == bsg.ERR_ARG
+    assert b"callback 1 is null" in bsg.bslib().bsg_bslib_last_error()
