@@ -146,3 +146,15 @@ def test_bslib_dropin_rejects_null_arguments_without_a_device():
     fns = (C.c_void_p * 7)()
     assert bsg.abstract_solve(True, None, fns, p) == bsg.ERR_ARG
     assert b"callback 1 is null" in bsg.bslib().bsg_bslib_last_error()
+
+
+def test_parfbss_header_symbols_are_exported():
+    """Every bsg_parfbss_* function include/bsg_parfbss.h declares is exported
+    by libbsg.so."""
+    import bsg
+    src = open(os.path.join(ROOT, "include", "bsg_parfbss.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = sorted(set(re.findall(r"\b(bsg_parfbss_[a-z_]+)\s*\(", src)))
+    assert len(names) == 15
+    L = C.CDLL(bsg.LIB_SO)
+    assert not [n for n in names if not hasattr(L, n)]
