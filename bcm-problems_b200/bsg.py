@@ -109,6 +109,7 @@ def lib():
         "bsg_write_vect_bin": (i_, [C.c_char_p, i_, i_, i_, i_, dp, ip, ip]),
         "bsg_read_vect_bin": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, dp, ip, ip]),
         "bsg_solve": (i_, [vp, vp, vp, dp, dp, C.POINTER(Param)]),
+        "bsg_solve_lu": (i_, [vp, vp, i_, i_, i_, dp, dp]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -528,6 +529,12 @@ def bslib():
         L.bsg_bslib_abstract.restype = C.c_int
         L.bsg_bslib_abstract.argtypes = [C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(Param)]
         L.bsg_bslib_last_error.restype = C.c_char_p
+        L.bsg_bslib_operator_create.restype = C.c_int
+        L.bsg_bslib_operator_create.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                C.POINTER(C.c_double), C.c_int, C.POINTER(Param),
+                                                C.POINTER(C.c_void_p)]
+        L.bsg_bslib_operator_free.argtypes = [C.c_void_p]
+        L.bsg_bslib_operator_fns.argtypes = [C.POINTER(C.c_void_p)]
         _bslib = L
     return _bslib
 
@@ -537,6 +544,27 @@ def abstract_solve(symm, gener, fns, param):
     on a generator object and its seven callbacks; returns the status code
     (the solution goes through the generator's store callback)."""
     return bslib().bsg_bslib_abstract(int(symm), gener, fns, C.byref(param))
+
+
+class GpuOperator:
+    """The matrix and its IC2 / ILU2 factor on the GPU behind the reference's
+    CMVM / CSOLVELU callbacks (bsg_bslib::MvmA / SolveLU / SolveL / SolveU):
+    .h is the operator object, .fns the four function pointers."""
+
+    def __init__(self, n, ia, ja, a, symm_upper, param):
+        L = bslib()
+        self.h = C.c_void_p()
+        rc = L.bsg_bslib_operator_create(n, _ip(ia), _ip(ja), _dp(a), int(symm_upper), C.byref(param),
+                                         C.byref(self.h))
+        if rc != OK:
+            raise BsgError(rc, L.bsg_bslib_last_error().decode(errors="replace"))
+        self.fns = (C.c_void_p * 4)()
+        L.bsg_bslib_operator_fns(self.fns)
+
+    def free(self):
+        if self.h:
+            bslib().bsg_bslib_operator_free(self.h)
+            self.h = C.c_void_p()
 
 
 def solver(ctx, n, ia, ja, a, b, param):

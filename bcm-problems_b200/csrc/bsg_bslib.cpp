@@ -17,10 +17,12 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <new>
 #include <vector>
 
 #include "slvparam.h"
 #include "smatrix.h"
+#include "ExchangeMPI.h"
 #include "bsg_bslib.h"
 
 namespace {
@@ -203,12 +205,118 @@ void AbstractSolver(void *_pgener, std::ofstream &_fout, CSlvParam &_param, CNSU
 	solve(false, _pgener, _param, _fnsup, _fsprnds, _fiaja, _fblockrow, _frhs, _finiguess, _fstoresol);
 }
 
+void AbstractParSolver(void *_pgener, void *_comm, std::ofstream &_fout, CSlvParam &_param, CNSUP _fnsup,
+                       CSPRNDS _fsprnds, CIAJA _fiaja, CBLOCKROW _fblockrow, CRHS _frhs, CINIGUESS _finiguess,
+                       CSTORESOL _fstoresol) {
+	(void)_fout;
+	if (_comm && static_cast<CMPIComm *>(_comm)->GetNproc() != 1)
+		raise(BSG_ERR_UNSUPPORTED, "AbstractParSolver: the GPU path runs on one process (nproc must be 1)");
+	solve(false, _pgener, _param, _fnsup, _fsprnds, _fiaja, _fblockrow, _frhs, _finiguess, _fstoresol);
+}
+
 void SetGpuOptions(const bsg_param &ext) {
 	g_ext = ext;
 	g_ext_set = true;
 }
 
 } // namespace bsg_bslib
+
+// ---- GPU operators for the reference's callback Krylov loops -----------------
+
+namespace {
+
+struct Operator {
+	bsg_ctx *c = nullptr;
+	bsg_mat *m = nullptr;
+	bsg_fct *f = nullptr;
+	int n = 0;
+	int mode = 0, nsweeps = 3;
+	std::vector<double> tmp;
+};
+
+// The vector's columns (nv entries each, nrhs of them) one after another.
+template <class F>
+void each_column(CSVector &x, CSVector &y, int n, F fn) {
+	const int nv = x.GetNv(), nr = x.GetNrhs();
+	if (nv != n || y.GetNv() != n || y.GetNrhs() != nr) raise(BSG_ERR_ARG, "GPU operator: vector of the wrong size");
+	for (int k = 0; k < nr; k++) check(fn(x.GetVect() + (size_t)k * n, y.GetVect() + (size_t)k * n));
+}
+
+} // namespace
+
+namespace bsg_bslib {
+
+void MvmA(void *_obj, CSVector &_x, CSVector &_ax) {
+	Operator *o = static_cast<Operator *>(_obj);
+	each_column(_x, _ax, o->n, [o](const double *x, double *y) { return bsg_mvm(o->c, o->m, x, y); });
+}
+void SolveLU(void *_obj, CSVector &_x, CSVector &_lux) {
+	Operator *o = static_cast<Operator *>(_obj);
+	each_column(_x, _lux, o->n,
+	            [o](const double *x, double *y) { return bsg_solve_lu(o->c, o->f, 0, o->mode, o->nsweeps, x, y); });
+}
+void SolveL(void *_obj, CSVector &_x, CSVector &_lx) {
+	Operator *o = static_cast<Operator *>(_obj);
+	each_column(_x, _lx, o->n,
+	            [o](const double *x, double *y) { return bsg_solve_lu(o->c, o->f, 1, o->mode, o->nsweeps, x, y); });
+}
+void SolveU(void *_obj, CSVector &_x, CSVector &_ux) {
+	Operator *o = static_cast<Operator *>(_obj);
+	each_column(_x, _ux, o->n,
+	            [o](const double *x, double *y) { return bsg_solve_lu(o->c, o->f, 2, o->mode, o->nsweeps, x, y); });
+}
+
+} // namespace bsg_bslib
+
+extern "C" int bsg_bslib_operator_create(int n, const int *ia, const int *ja, const double *a, int symm_upper,
+                                         bsg_param *p, void **op) {
+	g_msg[0] = 0;
+	if (!op || !p) return BSG_ERR_ARG;
+	*op = nullptr;
+	Operator *o = new (std::nothrow) Operator();
+	if (!o) return BSG_ERR_NOMEM;
+	int rc = BSG_OK;
+	try {
+		o->c = context();
+	} catch (const char *) {
+		rc = g_code;
+	}
+	bsg_param q = *p;
+	q.ordtype = 0;
+	if (!rc) rc = bsg_mat_csr(o->c, n, ia, ja, a, symm_upper, &o->m);
+	if (!rc) rc = symm_upper ? bsg_fct_ich2(o->c, o->m, &q, &o->f) : bsg_fct_ilu2(o->c, o->m, &q, &o->f);
+	if (rc) {
+		std::snprintf(g_msg, sizeof g_msg, "%s", bsg_last_error());
+		bsg_fct_free(o->f);
+		bsg_mat_free(o->m);
+		delete o;
+		return rc;
+	}
+	o->n = n;
+	o->mode = q.trisolve;
+	o->nsweeps = q.nsweeps;
+	p->density = q.density;
+	p->density2 = q.density2;
+	p->timefct = q.timefct;
+	*op = o;
+	return BSG_OK;
+}
+
+extern "C" int bsg_bslib_operator_free(void *op) {
+	Operator *o = static_cast<Operator *>(op);
+	if (!o) return BSG_OK;
+	bsg_fct_free(o->f);
+	bsg_mat_free(o->m);
+	delete o;
+	return BSG_OK;
+}
+
+extern "C" void bsg_bslib_operator_fns(void *fns[4]) {
+	fns[0] = reinterpret_cast<void *>(static_cast<CMVM>(&bsg_bslib::MvmA));
+	fns[1] = reinterpret_cast<void *>(static_cast<CSOLVELU>(&bsg_bslib::SolveLU));
+	fns[2] = reinterpret_cast<void *>(static_cast<CSOLVEL>(&bsg_bslib::SolveL));
+	fns[3] = reinterpret_cast<void *>(static_cast<CSOLVEU>(&bsg_bslib::SolveU));
+}
 
 extern "C" const char *bsg_bslib_last_error(void) { return g_msg; }
 
@@ -243,12 +351,20 @@ extern "C" int bsg_bslib_abstract(int symm, void *gener, void *const fns[7], bsg
 	const bsg_param saved = g_ext;
 	g_ext = *p;
 	g_ext_set = true;
-	std::ofstream fout;
 	int rc = BSG_OK;
 	try {
-		solve(symm != 0, gener, cp, reinterpret_cast<CNSUP>(fns[0]), reinterpret_cast<CSPRNDS>(fns[1]),
-		      reinterpret_cast<CIAJA>(fns[2]), reinterpret_cast<CBLOCKROW>(fns[3]), reinterpret_cast<CRHS>(fns[4]),
-		      reinterpret_cast<CINIGUESS>(fns[5]), reinterpret_cast<CSTORESOL>(fns[6]));
+		std::ofstream nowhere;
+		const auto f0 = reinterpret_cast<CNSUP>(fns[0]);
+		const auto f1 = reinterpret_cast<CSPRNDS>(fns[1]);
+		const auto f2 = reinterpret_cast<CIAJA>(fns[2]);
+		const auto f3 = reinterpret_cast<CBLOCKROW>(fns[3]);
+		const auto f4 = reinterpret_cast<CRHS>(fns[4]);
+		const auto f5 = reinterpret_cast<CINIGUESS>(fns[5]);
+		const auto f6 = reinterpret_cast<CSTORESOL>(fns[6]);
+		if (symm == 2)
+			bsg_bslib::AbstractParSolver(gener, nullptr, nowhere, cp, f0, f1, f2, f3, f4, f5, f6);
+		else
+			solve(symm != 0, gener, cp, f0, f1, f2, f3, f4, f5, f6);
 		p->nitperf = cp.nitperf;
 		p->resfin = cp.resfin;
 		p->density = cp.density;

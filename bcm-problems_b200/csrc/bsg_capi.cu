@@ -729,6 +729,33 @@ static int drive(bsg_ctx *c, int n, const int *ia, const int *ja, const double *
 	return rc;
 }
 
+extern "C" int bsg_solve_lu(bsg_ctx *c, const bsg_fct *f, int which, int mode, int nsweeps, const double *x,
+                            double *y) {
+	if (!c || !f || !x || !y || which < 0 || which > 2 || mode < 0 || mode > 1)
+		return bsg_set_error(BSG_ERR_ARG, "bsg_solve_lu: bad argument");
+	const size_t n = (size_t)f->n * (f->d_bia ? 3 : 1);
+	cudaStream_t s = c->stream;
+	double *dx = nullptr, *dy = nullptr, *dt = nullptr, *work = nullptr;
+	int rc = BSG_OK;
+	if (cudaMallocAsync(&dx, sizeof(double) * (n ? n : 1), s) != cudaSuccess ||
+	    cudaMallocAsync(&dy, sizeof(double) * (n ? n : 1), s) != cudaSuccess ||
+	    cudaMallocAsync(&dt, sizeof(double) * (n ? n : 1), s) != cudaSuccess ||
+	    cudaMallocAsync(&work, sizeof(double) * (n ? n : 1), s) != cudaSuccess)
+		rc = bsg_set_error(BSG_ERR_NOMEM, "bsg_solve_lu: vectors");
+	if (!rc && cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+		rc = bsg_set_error(BSG_ERR_CUDA, "bsg_solve_lu: copy to the device failed");
+	// which 0: SolveL then SolveU (the preconditioner), 1: SolveL, 2: SolveU
+	if (!rc && which != 2) rc = bsg_trisolve_launch(c, f, 1, mode, nsweeps, dx, which == 0 ? dt : dy, work);
+	if (!rc && which != 1) rc = bsg_trisolve_launch(c, f, 0, mode, nsweeps, which == 0 ? dt : dx, dy, work);
+	if (!rc && cudaMemcpyAsync(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+		rc = bsg_set_error(BSG_ERR_CUDA, "bsg_solve_lu: copy of the result failed");
+	cudaStreamSynchronize(s);
+	for (double *q : {dx, dy, dt, work})
+		if (q) cudaFreeAsync(q, s);
+	if (!rc) rc = bsg_check_devstat(c);
+	return rc;
+}
+
 extern "C" int bsg_solve(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const double *b, double *x, bsg_param *p) {
 	if (!c || !m || !f || !p || !b || !x) return bsg_set_error(BSG_ERR_ARG, "bsg_solve: null argument");
 	const size_t n = (size_t)m->n * m->bs;

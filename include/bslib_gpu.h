@@ -42,7 +42,8 @@ extern "C" {
  * extensions of the GPU path that the reference does not have. */
 typedef struct bsg_param {
 	int msglev;       /* output level (0 quiet)                                   */
-	int fcttyp;       /* 1: IC(0)-like first order (not on GPU), else second order */
+	int fcttyp;       /* 1: IC(0) on A's pattern (CSMatrixR::Ich; refused on the GPU
+	                     with BSG_ERR_UNSUPPORTED), else second order            */
 	int ordtype;      /* ordering; only 0 (natural) is accepted on the GPU        */
 	double memory;    /* factor workspace, multiples of nnz(A) (|memory| used)    */
 	double tau1;      /* first-order threshold: |v| >= tau1 kept in U            */
@@ -50,7 +51,8 @@ typedef struct bsg_param {
 	double theta;     /* diagonal compensation factor for dropped entries        */
 	double sclmin;    /* minimal scaling value (ILU2)                            */
 	double pivmin;    /* minimal pivot (ILU2)                                    */
-	int ittype;       /* CG stop rule: 0 relative, 1 absolute (recursive resid.) */
+	int ittype;       /* CG stop rule on the recursive residual: 0 relative, 1
+	                     absolute, 2 max |r_i| <= |eps| (Bslib/cg.cpp:239-241)    */
 	int sttype;       /* GMRES / Lanczos stop rule: 0 absolute, 1 relative; 2 max-norm
 	                     of the residual (Lanczos; GMRES: relative)                */
 	int niter;        /* maximal number of iterations                            */
@@ -229,6 +231,11 @@ int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs
  * the two-sided Lanczos (CSVector::Lanczos) for a nonsymmetric point matrix,
  * GMRES(restart) for a nonsymmetric block matrix; 1 / 2: GMRES / FGMRES. */
 int bsg_solve(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *b, double *x, bsg_param *p);
+/* The preconditioner with host buffers: which 0 applies SolveL then SolveU
+ * (the CSOLVELU of Bslib/svector.h:40 that the callback Krylov loops call),
+ * 1 SolveL only, 2 SolveU only (CSMatrixR::SolveL / SolveU,
+ * Bslib/mvm.cpp:3042 / :3343); mode / nsweeps as bsg_solve_l_dev. */
+int bsg_solve_lu(bsg_ctx *ctx, const bsg_fct *f, int which, int mode, int nsweeps, const double *x, double *y);
 /* CSVector::SolveSymm(CSMatrixR&) (Bslib/solvers.cpp:4615): upper-stored SPD
  * CSR in, IC2 + PCG (or GMRES/FGMRES per p->krylov), solution out. */
 int bsg_solve_symm_csr(bsg_ctx *ctx, int n, const int *ia, const int *ja, const double *a, const double *b,

@@ -20,6 +20,8 @@
 #include <vector>
 #include "smatrix.h"
 #include "slvparam.h"
+#include "svector.h"
+#include "tree.h"
 
 namespace {
 
@@ -166,6 +168,67 @@ int ref_abstract(int symm, void *o, double tau1, double tau2, double theta, doub
 			out[0] = p.nitperf; out[1] = p.resfin; out[2] = p.density;
 			out[3] = std::chrono::duration<double>(t1 - t0).count();
 		}
+		return 0;
+	} catch (const char *e) {
+		std::cout.clear(cst);
+		std::strncpy(g_err, e ? e : "unknown", sizeof(g_err) - 1);
+		return -1;
+	}
+}
+
+// The reference's callback Krylov loops on one rank (a CTree of one
+// processor, as AbstractParSolver builds with nproc = 1): CSVector::Cg
+// (Bslib/cg.cpp:355) and CSVector::BlockGMRES (Bslib/gmres.cpp:337), with the
+// matrix and preconditioner operators given as CMVM / CSOLVELU function
+// pointers and their objects.  x: initial guess in, solution out.
+// stats[0..1] = iterations, wall seconds.
+int ref_cg_tree(int n, const double *b, double *x, void *obja, void *mvm, void *objlu, void *solvelu, int ittype,
+                double eps, int niter, double *stats) {
+	const std::ios::iostate cst = std::cout.rdstate();
+	try {
+		CTree tree(1, 2);
+		CSlvParam p;
+		p.msglev = 0; p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = 1;
+		CSVector vb(n), vx(n), sol(n);
+		std::memcpy(vb.GetVect(), b, sizeof(double) * n);
+		std::memcpy(vx.GetVect(), x, sizeof(double) * n);
+		std::ofstream fout("/dev/null");
+		fout.setstate(std::ios::badbit);
+		std::cout.setstate(std::ios::badbit);
+		auto t0 = std::chrono::steady_clock::now();
+		sol.Cg(fout, tree, obja, reinterpret_cast<CMVM>(mvm), objlu, reinterpret_cast<CSOLVELU>(solvelu), vx, vb, p);
+		auto t1 = std::chrono::steady_clock::now();
+		std::cout.clear(cst);
+		std::memcpy(x, sol.GetVect(), sizeof(double) * n);
+		if (stats) { stats[0] = p.nitperf; stats[1] = std::chrono::duration<double>(t1 - t0).count(); }
+		return 0;
+	} catch (const char *e) {
+		std::cout.clear(cst);
+		std::strncpy(g_err, e ? e : "unknown", sizeof(g_err) - 1);
+		return -1;
+	}
+}
+
+int ref_gmres_tree(int n, const double *b, double *x, void *obja, void *mvm, void *objlu, void *solvelu, int sttype,
+                   double eps, int niter, double *stats) {
+	const std::ios::iostate cst = std::cout.rdstate();
+	try {
+		CTree tree(1, 2);
+		CSlvParam p;
+		p.msglev = 0; p.sttype = sttype; p.eps = eps; p.niter = niter; p.ichk = 1; p.ooctyp = 0;
+		CSVector vb(n), vx(n), sol(n);
+		std::memcpy(vb.GetVect(), b, sizeof(double) * n);
+		std::memcpy(vx.GetVect(), x, sizeof(double) * n);
+		std::ofstream fout("/dev/null");
+		fout.setstate(std::ios::badbit);
+		std::cout.setstate(std::ios::badbit);
+		auto t0 = std::chrono::steady_clock::now();
+		sol.BlockGMRES(fout, p, tree, obja, reinterpret_cast<CMVM>(mvm), objlu, reinterpret_cast<CSOLVELU>(solvelu),
+		               vx, vb);
+		auto t1 = std::chrono::steady_clock::now();
+		std::cout.clear(cst);
+		std::memcpy(x, sol.GetVect(), sizeof(double) * n);
+		if (stats) { stats[0] = p.nitperf; stats[1] = std::chrono::duration<double>(t1 - t0).count(); }
 		return 0;
 	} catch (const char *e) {
 		std::cout.clear(cst);

@@ -427,3 +427,22 @@ class RefLib:
         r = subprocess.run([tool, text_path, bin_path], capture_output=True, text=True, timeout=120)
         if r.returncode != 0:
             raise RuntimeError(f"ref_convert failed: {r.stderr.strip()}")
+
+    def _krylov_tree(self, fn, n, b, x0, op, *args):
+        x = np.array(x0, dtype=np.float64, copy=True)
+        st = (C.c_double * 2)()
+        rc = fn(n, _d(b), x.ctypes.data_as(_dp), op.h, C.c_void_p(op.fns[0]), op.h, C.c_void_p(op.fns[1]), *args, st)
+        if rc != 0:
+            self.lib.ref_abstract_error.restype = C.c_char_p
+            raise RuntimeError(self.lib.ref_abstract_error().decode())
+        return x, dict(iters=int(st[0]), wall=st[1])
+
+    def cg_tree(self, n, b, x0, op, ittype=0, eps=1e-10, niter=1000):
+        """The reference's callback CSVector::Cg on a one-processor CTree, with
+        the matrix / preconditioner operators of `op` (.h object, .fns[0..1]
+        CMVM / CSOLVELU pointers)."""
+        return self._krylov_tree(self.lib.ref_cg_tree, n, b, x0, op, ittype, C.c_double(eps), niter)
+
+    def gmres_tree(self, n, b, x0, op, sttype=1, eps=1e-10, niter=300):
+        """The reference's callback CSVector::BlockGMRES on a one-processor CTree."""
+        return self._krylov_tree(self.lib.ref_gmres_tree, n, b, x0, op, sttype, C.c_double(eps), niter)

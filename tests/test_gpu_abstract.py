@@ -19,7 +19,11 @@ Cases: 3x3 Lame blocks, symmetric (block IC2 + PCG) with the relative and
 with the reference's default max-norm stop rule; variable block sizes
 (1, 2, 3 repeating) cut from a heat matrix; a nonsymmetric Lame variant
 through AbstractSolver (block ILU2 on the GPU, ILU2 + Lanczos in the
-reference); a nonzero initial guess; a matrix that is not positive definite.
+reference) and through AbstractParSolver on one process; a nonzero initial
+guess; a matrix that is not positive definite.  Last, the reference's own
+callback Krylov loops (CG and BlockGMRES on a one-processor CTree) run with
+the GPU's SpMV and preconditioner behind their CMVM / CSOLVELU callbacks, the
+role CParMvmA / CParSolveLU play in the reference's parallel driver.
 """
 import numpy as np
 import pytest
@@ -168,3 +172,76 @@ def test_not_positive_definite_raises(reflib):
     reflib.gen_free(hg)
     assert rc != bsg.OK
     assert bsg.bslib().bsg_bslib_last_error()
+
+
+def test_abstract_par_solver_single_rank(reflib):
+    """AbstractParSolver on one process: the GPU drop-in against the
+    reference's AbstractSolver on the same generator (the reference's
+    AbstractParSolver partitions with METIS even for one rank, which this
+    build does not have)."""
+    import bsg
+    s = P.lame3d(5, 0.3, 1.0, 9)
+    a = skewed(s)
+    sprnd = np.arange(s.n + 1, dtype=np.int32) * 3
+    b = s.rhs[0]
+    n = s.n * 3
+    hr = reflib.gen_create(sprnd, s.ia, s.ja, a, b, np.zeros(n), seed=21)
+    reflib.abstract(False, hr, ittype=1, sttype=1, eps=1e-10)
+    x_ref = reflib.gen_solution(hr, n)
+    reflib.gen_free(hr)
+    hg = reflib.gen_create(sprnd, s.ia, s.ja, a, b, np.zeros(n), seed=22)
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0, ittype=1, sttype=1,
+                          eps=1e-10, niter=3000)
+    rc = bsg.abstract_solve(2, hg, reflib.gen_fns(), p)
+    assert rc == bsg.OK, bsg.bslib().bsg_bslib_last_error()
+    x_gpu = reflib.gen_solution(hg, n)
+    assert list(reflib.gen_calls(hg)) == [1, 1, 1, s.n, s.n, s.n, s.n]
+    reflib.gen_free(hg)
+    assert relerr(x_gpu, x_ref) <= 1e-8
+
+
+def test_reference_cg_runs_on_gpu_operators(reflib):
+    """The reference's own callback CG loop (Bslib/cg.cpp:355, one-rank CTree)
+    with the GPU's SpMV and IC2 preconditioner behind CMVM / CSOLVELU, against
+    the reference's SolveSymm with its own operators: the same iteration
+    count +-1 and the same solution to 1e-8."""
+    import bsg
+    s = P.heat3d(12, 10, 8, sigma=1.0, seed=41)
+    u = s.upper()
+    b = s.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
+    op = bsg.GpuOperator(s.n, u.ia, u.ja, u.a, True, p)
+    try:
+        x, info = reflib.cg_tree(s.n, b, np.zeros(s.n), op, ittype=0, eps=1e-10, niter=1000)
+    finally:
+        op.free()
+    xr, ir = reflib.solve_symm(u.ia, u.ja, u.a, b, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=-1.0, ittype=0, eps=1e-10)
+    err = relerr(x, xr)
+    print(f"reference Cg on GPU operators: {info['iters']} it (reference operators {ir['iters']}), rel. error {err:.2e}")
+    assert abs(info["iters"] - ir["iters"]) <= 1
+    assert err <= 1e-8
+
+
+def test_reference_block_gmres_runs_on_gpu_operators(reflib):
+    """The reference's callback BlockGMRES (Bslib/gmres.cpp:337, one-rank
+    CTree) with the GPU's SpMV and ILU2 preconditioner, against the
+    reference's Solver (ILU2 + Lanczos) with its own operators."""
+    import bsg
+    s = P.heat3d(10, 9, 8, sigma=1.0, seed=43)
+    a = s.a.copy()
+    rows = np.repeat(np.arange(s.n), np.diff(s.ia))
+    off = s.ja != rows
+    a[off] *= 1.0 + 0.3 * np.sign(s.ja[off] - rows[off])
+    b = s.rhs[0]
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
+    op = bsg.GpuOperator(s.n, s.ia, s.ja, a, False, p)
+    try:
+        x, info = reflib.gmres_tree(s.n, b, np.zeros(s.n), op, sttype=1, eps=1e-10, niter=200)
+    finally:
+        op.free()
+    xr, ir = reflib.solver(s.ia, s.ja, a, b, tau1=1e-3, tau2=1e-3, sttype=1, eps=1e-10)
+    A = sp.csr_matrix((a, s.ja, s.ia), shape=(s.n, s.n))
+    err = relerr(x, xr)
+    print(f"reference BlockGMRES on GPU operators: {info['iters']} it, rel. error {err:.2e}")
+    assert np.linalg.norm(b - A @ x) <= 1e-9 * np.linalg.norm(b)
+    assert err <= 1e-8
