@@ -110,6 +110,7 @@ def lib():
         "bsg_read_vect_bin": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, dp, ip, ip]),
         "bsg_solve": (i_, [vp, vp, vp, dp, dp, C.POINTER(Param)]),
         "bsg_solve_lu": (i_, [vp, vp, i_, i_, i_, dp, dp]),
+        "bsg_set_spin_limit_ns": (i_, [vp, C.c_ulonglong]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)

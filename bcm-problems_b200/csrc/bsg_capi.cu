@@ -208,6 +208,24 @@ extern "C" int bsg_destroy(bsg_ctx *c) {
 	return BSG_OK;
 }
 
+int bsg_spin_limit_set_fact(unsigned long long ns);
+int bsg_spin_limit_set_trsv(unsigned long long ns);
+int bsg_spin_limit_set_unet(unsigned long long ns);
+
+extern "C" int bsg_set_spin_limit_ns(bsg_ctx *c, unsigned long long ns) {
+	if (!c) return bsg_set_error(BSG_ERR_ARG, "bsg_set_spin_limit_ns: null context");
+	if (ns < 1000ull || ns > 600000000000ull)
+		return bsg_set_error(BSG_ERR_ARG, "bsg_set_spin_limit_ns: the limit must lie in [1 us, 600 s]");
+	BSG_CUDA(cudaSetDevice(c->device));
+	BSG_CUDA(cudaStreamSynchronize(c->stream));
+	int rc = bsg_spin_limit_set_fact(ns);
+	if (!rc) rc = bsg_spin_limit_set_trsv(ns);
+	if (!rc) rc = bsg_spin_limit_set_unet(ns);
+	if (rc) return bsg_set_error(rc, "bsg_set_spin_limit_ns: cudaMemcpyToSymbol failed");
+	BSG_CUDA(cudaDeviceSynchronize());
+	return BSG_OK;
+}
+
 extern "C" int bsg_sync(bsg_ctx *c) {
 	if (!c) return bsg_set_error(BSG_ERR_ARG, "bsg_sync: null context");
 	BSG_CUDA(cudaStreamSynchronize(c->stream));

@@ -82,8 +82,16 @@ __device__ __forceinline__ void devstat_fail(bsg_devstat *st, int code, int wher
 
 // Spin-wait bound: every device wait on another warp's result gives up after
 // this many nanoseconds of globaltimer time, reports BSG_ERR_TIMEOUT and
-// returns.  Two seconds is far above any legitimate wait.
-#define BSG_SPIN_LIMIT_NS 2000000000ull
+// returns.  The default, two seconds, is far above any legitimate wait;
+// bsg_set_spin_limit_ns() changes it.  Every translation unit with waits
+// keeps its own copy in constant memory (static), set through
+// bsg_spin_limit_set_here() from that unit, for the current device.
+#define BSG_SPIN_LIMIT_DEFAULT_NS 2000000000ull
+static __constant__ unsigned long long c_bsg_spin_limit_ns = BSG_SPIN_LIMIT_DEFAULT_NS;
+#define BSG_SPIN_LIMIT_NS c_bsg_spin_limit_ns
+static inline __attribute__((unused)) cudaError_t bsg_spin_limit_set_here(unsigned long long ns) {
+	return cudaMemcpyToSymbol(c_bsg_spin_limit_ns, &ns, sizeof ns);
+}
 
 // ---- device-resident objects ---------------------------------------------
 struct bsg_ctx {

@@ -210,9 +210,19 @@ __device__ int wset_insert(WS &s, int k) {
 // Add a nonnegative compensation to row j's 64-bit fixed-point accumulator
 // (value * 2^scale_bits, truncated): integer addition makes the sum exact and
 // independent of the order of the adds, and a reduction without return value
-// costs no round trip.  scale_bits leaves room for 2^12 maximal terms.
-__device__ void acc_push(unsigned long long *acc, int j, double comp, double scale) {
-	atomicAdd(acc + j, (unsigned long long)(comp * scale));
+// costs no round trip.  The sum cannot wrap: a compensation is theta * |v|
+// with |v| < tau2, so below 2^51 after scaling (bsg_comp_scale), and only the
+// members of C(j) push to row j, at most CMAX_BIG = 2^13 of them (a row with
+// more fails with BSG_ERR_WORKSPACE), so the sum stays below 2^64.  A term
+// outside that bound (it cannot occur) is reported as BSG_ERR_WORKSPACE
+// rather than added.
+__device__ void acc_push(unsigned long long *acc, int j, double comp, double scale, bsg_devstat *st) {
+	const double t = comp * scale;
+	if (!(t < 0x1p51)) {
+		devstat_fail(st, BSG_ERR_WORKSPACE, j, 7);
+		return;
+	}
+	atomicAdd(acc + j, (unsigned long long)t);
 }
 __device__ double acc_value(const unsigned long long *acc, int j, double inv_scale) {
 	return __dmul_rn((double)__ldcg(acc + j), inv_scale);
@@ -804,7 +814,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	// ---- hand the dropped entries' compensations to their rows
 	for (int t = lane; t < nl; t += 32) {
 		const double v = s.pf_l[t];
-		if (v != 0.0) acc_push(A.acc, s.hkey[s.lsts[t]], v, A.acc_scale);
+		if (v != 0.0) acc_push(A.acc, s.hkey[s.lsts[t]], v, A.acc_scale, A.st);
 	}
 	if (lane == 0) A.lev[i] = levmax;
 	__threadfence();
@@ -1019,9 +1029,10 @@ inline int nb(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
 
 int bsg_fct_finish(bsg_ctx *c, bsg_fct *f);
 
-// Scale of the fixed-point compensation sums: a compensation is below
-// tau2 * theta < 2^e, so 2^(51 - e) leaves room for 2^12 maximal terms in 63
-// bits; the rule is exact (frexp) so the oracle derives the same scale.
+// Scale of the fixed-point compensation sums: a compensation is at most
+// tau2 * theta < 2^e, so 2^(51 - e) keeps each term below 2^51 and the sum of
+// the at most 2^13 terms a row receives below 2^64; the rule is exact (frexp)
+// so the oracle derives the same scale.
 void bsg_comp_scale(double tau2, double theta, double *scale, double *inv_scale) {
 	int e = -13;
 	double maxterm = tau2 * theta;
@@ -1204,4 +1215,9 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	if (rc) return rc;
 	*out = f;
 	return BSG_OK;
+}
+
+// this unit's copy of the spin-wait bound (bsg_set_spin_limit_ns)
+int bsg_spin_limit_set_fact(unsigned long long ns) {
+	return bsg_spin_limit_set_here(ns) == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 }

@@ -340,3 +340,8 @@ int bsg_trisolve_t_launch(bsg_ctx *c, bsg_fct *f, int which, int mode, int nswee
 	}
 	return trisolve_impl(c, f, t, mode, nsweeps, x, y, work);
 }
+
+// this unit's copy of the spin-wait bound (bsg_set_spin_limit_ns)
+int bsg_spin_limit_set_trsv(unsigned long long ns) {
+	return bsg_spin_limit_set_here(ns) == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}

@@ -1574,3 +1574,8 @@ int bsg_unet_apply(void *net, bsg_ctx *c, const double *v, double *z, double *wo
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
+
+// this unit's copy of the spin-wait bound (bsg_set_spin_limit_ns)
+int bsg_spin_limit_set_unet(unsigned long long ns) {
+	return bsg_spin_limit_set_here(ns) == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}

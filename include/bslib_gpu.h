@@ -100,6 +100,14 @@ typedef struct bsg_fct bsg_fct;
 int bsg_create(bsg_ctx **ctx, int device, void *stream);
 int bsg_destroy(bsg_ctx *ctx);
 int bsg_sync(bsg_ctx *ctx);
+/* Time limit of every device spin-wait (the sync-free triangular solves, the
+ * factorisation scheduler, the tensor-core pipeline of the learned stage), in
+ * nanoseconds of GPU time: a wait that reaches it gives up, the call returns
+ * BSG_ERR_TIMEOUT and the context stays usable.  Default 2 s; accepted range
+ * 1 us .. 600 s.  It holds for the context's device, for every context on it,
+ * from the next launch on; the call synchronises the context's stream first.
+ * No counterpart in the reference (its loops have no waits). */
+int bsg_set_spin_limit_ns(bsg_ctx *ctx, unsigned long long ns);
 
 /* ---- matrices (CSMatrixR / CSMatrixRS, Bslib/smatrix.h:540-546, :1040-1048) */
 /* Point CSR from host arrays.  symm_upper = 1: only the upper triangle is
