@@ -111,6 +111,7 @@ def lib():
         "bsg_solve": (i_, [vp, vp, vp, dp, dp, C.POINTER(Param)]),
         "bsg_solve_lu": (i_, [vp, vp, i_, i_, i_, dp, dp]),
         "bsg_set_spin_limit_ns": (i_, [vp, C.c_ulonglong]),
+        "bsg_block_lanczos_dev": (i_, [vp, vp, vp, i_, i_, vp, vp, C.POINTER(Param), dp]),
     }
     for name, (rt, at) in sig.items():
         f = getattr(L, name)
@@ -428,6 +429,16 @@ def lanczos(ctx, mat, fct, b, x, param):
     """Two-sided Lanczos (CSVector::Lanczos) on device tensors (x holds x0)."""
     _check(lib().bsg_lanczos_dev(ctx.h, mat.h, fct.h, _ptr(b), _ptr(x), C.byref(param)))
     return param
+
+
+def block_lanczos(ctx, mat, fct, ittype, B, X, param):
+    """Block Lanczos (ittype 2 central, 3 right, 4 left) on device tensors
+    B, X [nrhs, n] (X holds x0); returns the final relative true residuals."""
+    nrhs = B.shape[0]
+    res = np.zeros(nrhs)
+    _check(lib().bsg_block_lanczos_dev(ctx.h, mat.h, fct.h, ittype, nrhs, _ptr(B), _ptr(X), C.byref(param),
+                                       res.ctypes.data_as(C.POINTER(C.c_double))))
+    return res
 
 
 def gmres(ctx, mat, fct, b, x, param):

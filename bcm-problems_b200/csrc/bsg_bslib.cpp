@@ -176,7 +176,11 @@ void solve(bool symm, void *g, CSlvParam &param, CNSUP fnsup, CSPRNDS fsprnds, C
 	bsg_ctx *c = context();
 	bsg_mat *m = nullptr;
 	bsg_fct *f = nullptr;
-	int rc = bsg_mat_vbsr(c, s.nsup, s.sprnd.data(), s.ia.data(), s.ja.data(), s.a.data(), symm ? 1 : 0, &m);
+	// the block Lanczos variants of Solver(CSMatrixRS&) (ittype 2 / 3 / 4)
+	// run on the point form: the GPU's transposed solves are point solves
+	const bool point = !symm && q.krylov == 0 && q.ittype >= 2 && q.ittype <= 4;
+	int rc = bsg_mat_vbsr(c, s.nsup, s.sprnd.data(), s.ia.data(), s.ja.data(), s.a.data(),
+	                      (symm ? 1 : 0) | (point ? BSG_VBSR_POINT : 0), &m);
 	if (!rc) rc = symm ? bsg_fct_ich2(c, m, &q, &f) : bsg_fct_ilu2(c, m, &q, &f);
 	if (!rc) rc = bsg_solve(c, m, f, s.b.data(), s.x.data(), &q);
 	bsg_fct_free(f);

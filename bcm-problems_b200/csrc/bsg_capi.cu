@@ -402,6 +402,8 @@ extern "C" int bsg_mat_vbsr(bsg_ctx *c, int nsup, const int *sprnd, const int *i
                             int symm_upper, bsg_mat **out) {
 	if (!c || !out || !sprnd) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: null argument");
 	*out = nullptr;
+	const bool force_point = (symm_upper & BSG_VBSR_POINT) != 0;
+	symm_upper &= 1;
 	int rc = check_csr_host(nsup, ia, ja, 1);
 	if (rc) return rc;
 	if (sprnd[0] != 0) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_vbsr: sprnd[0] != 0");
@@ -420,7 +422,7 @@ extern "C" int bsg_mat_vbsr(bsg_ctx *c, int nsup, const int *sprnd, const int *i
 		if (rc) return rc;
 	}
 	if (all1) return bsg_mat_csr(c, nsup, ia, ja, a, symm_upper, out);
-	if (all3) return bsg_mat_bsr(c, nsup, 3, ia, ja, a, symm_upper, out);
+	if (all3 && !force_point) return bsg_mat_bsr(c, nsup, 3, ia, ja, a, symm_upper, out);
 	std::vector<int> pia, pja;
 	std::vector<double> pa;
 	rc = vbsr_to_point_host(nsup, sprnd, ia, ja, a, symm_upper, pia, pja, pa);
@@ -789,9 +791,12 @@ extern "C" int bsg_solve(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f, const d
 	    cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
 		rc = bsg_set_error(BSG_ERR_CUDA, "bsg_solve: copy to the device failed");
 	if (!rc) {
+		const bool point = m->bs == 1 && !f->d_bia;
 		if (p->krylov != 0) rc = bsg_gmres_dev(c, m, f, db, dx, p);
 		else if (m->symm) rc = bsg_pcg_dev(c, m, f, db, dx, p);              // CSVector::Cg
-		else if (m->bs == 1 && !f->d_bia) rc = bsg_lanczos_dev(c, m, f, db, dx, p); // CSVector::Lanczos
+		else if (point && p->ittype >= 2 && p->ittype <= 4)                   // block Lanczos variants
+			rc = bsg_block_lanczos_dev(c, m, f, p->ittype, 1, db, dx, p, nullptr);
+		else if (point) rc = bsg_lanczos_dev(c, m, f, db, dx, p);            // CSVector::Lanczos
 		else rc = bsg_gmres_dev(c, m, f, db, dx, p);
 	}
 	// the last iterate comes back also when the iteration limit was reached

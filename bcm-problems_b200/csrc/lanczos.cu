@@ -123,6 +123,9 @@ int mvm_t(bsg_ctx *c, bsg_mat *m, const double *x, double *y) {
 
 } // namespace
 
+// y = A^T x for a point matrix (the SELL copy of A^T is built on first use).
+int bsg_mvm_t_launch(bsg_ctx *c, bsg_mat *m, const double *x, double *y) { return mvm_t(c, m, x, y); }
+
 extern "C" int bsg_lanczos_dev(bsg_ctx *c, const bsg_mat *mc, const bsg_fct *fc, const double *d_b, double *d_x,
                                bsg_param *p) {
 	if (!c || !mc || !fc || !d_b || !d_x || !p) return bsg_set_error(BSG_ERR_ARG, "bsg_lanczos_dev: null argument");

@@ -132,7 +132,9 @@ int bsg_mat_bsr(bsg_ctx *ctx, int nsup, int bs, const int *ia, const int *ja, co
  * one another in `a`, each column-major, columns ascending in every block row
  * (symm_upper: upper blocks only, the diagonal block first).  All blocks 3x3:
  * the block path of bsg_mat_bsr; all 1x1: point CSR; otherwise the point
- * expansion (upper triangle of each diagonal block when symm_upper). */
+ * expansion (upper triangle of each diagonal block when symm_upper).
+ * symm_upper | BSG_VBSR_POINT: the point expansion whatever the sizes. */
+#define BSG_VBSR_POINT 2
 int bsg_mat_vbsr(bsg_ctx *ctx, int nsup, const int *sprnd, const int *ia, const int *ja, const double *a,
                  int symm_upper, bsg_mat **out);
 int bsg_mat_free(bsg_mat *m);
@@ -213,6 +215,21 @@ int bsg_gmres_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double
  * eps ||r0||, 2: max |r_i| <= eps).  Point matrices; x0 = d_x on entry. */
 int bsg_lanczos_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *d_b, double *d_x, bsg_param *p);
 
+/* Block Lanczos of the CSMatrixRS driver (CSVector::BlockLanczosCentral /
+ * BlockLanczosRight / BlockLanczosLeft, Bslib/lanczos.cpp:2467 / :932 /
+ * :1719; CSVector::Solver(CSMatrixRS&) runs them for ittype 2 / 3 / 4,
+ * Bslib/solvers.cpp:1798-1800): block Golub-Kahan bidiagonalisation of the
+ * preconditioned matrix (central L^{-1} A U^{-1}, right A (LU)^{-1}, left
+ * (LU)^{-1} A) with block Givens rotations, on nrhs <= 16 right-hand sides at
+ * once.  Point matrices with a point factor.  d_B, d_X: [nrhs][n], d_X holds
+ * x0.  Stops, tested every p->ichk steps as the reference tests, when every
+ * right-hand side has ||b_j - A x_j|| < eps ||b_j - A x0_j|| (right variant:
+ * or the preconditioned normal residual has fallen by eps).  res (host,
+ * nrhs, may be NULL): final ||b_j - A x_j|| / ||b_j||; p->resfin their
+ * maximum, p->nitperf the steps made. */
+int bsg_block_lanczos_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int ittype, int nrhs, const double *d_B,
+                          double *d_X, bsg_param *p, double *res);
+
 /* Batched PCG (CSVector::Cg's recurrence, Bslib/cg.cpp:31-350, which handles
  * one right-hand side, :375-377): nrhs right-hand sides times nseg diagonal
  * blocks ("segments") of A that no entry couples -- e.g. the load cases of
@@ -235,9 +252,12 @@ int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs
  * :4615, :1339, :1568) on a matrix and its factor, host buffers: x holds the
  * initial guess on entry (the drivers start from the vector itself) and the
  * solution on exit, also when the iteration limit stopped the loop
- * (BSG_ERR_NOCONV).  p->krylov 0: PCG (CSVector::Cg) for a symmetric matrix,
- * the two-sided Lanczos (CSVector::Lanczos) for a nonsymmetric point matrix,
- * GMRES(restart) for a nonsymmetric block matrix; 1 / 2: GMRES / FGMRES. */
+ * (BSG_ERR_NOCONV).  p->krylov 0: PCG (CSVector::Cg) for a symmetric matrix;
+ * for a nonsymmetric one the iteration of CSVector::Solver(CSMatrixRS&):
+ * p->ittype 2 / 3 / 4 the block Lanczos variants (bsg_block_lanczos_dev,
+ * point matrices), otherwise the two-sided Lanczos (CSVector::Lanczos) for a
+ * point matrix and GMRES(restart) for a 3x3 block matrix; krylov 1 / 2:
+ * GMRES / FGMRES. */
 int bsg_solve(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, const double *b, double *x, bsg_param *p);
 /* The preconditioner with host buffers: which 0 applies SolveL then SolveU
  * (the CSOLVELU of Bslib/svector.h:40 that the callback Krylov loops call),

@@ -442,4 +442,41 @@ int ref_read_system_bin(const char *path, int nvec, int *n_out, int **ia, int **
 	}
 }
 
+// Block Lanczos of the CSMatrixRS driver (CSVector::BlockLanczosCentral /
+// BlockLanczosRight / BlockLanczosLeft, Bslib/lanczos.cpp:2467 / :932 / :1719)
+// as CSVector::Solver(CSMatrixRS&) runs them (Bslib/solvers.cpp:1651-1800):
+// CombineLU + block ILU2 of a block matrix with uniform block size bs, then
+// the variant of ittype (2 central, 3 right, 4 left) on the nrhs columns of B
+// at once, x0 = 0.  stats: [0] = wall seconds.
+int ref_block_lanczos(int nsup, int bs, const int *ia, const int *ja, const double *a, int ittype, int nrhs,
+                      const double *B, double *X, double tau1, double tau2, double theta, double eps, int niter,
+                      int ichk, double *stats) {
+	QuietCout q;
+	try {
+		RSBuild m(nsup, bs, ia, ja, a);
+		CSlvParam p;
+		p.msglev = 0; p.tau1 = tau1; p.tau2 = tau2; p.theta = theta; p.memory = 20.0;
+		p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = ichk;
+		CSMatrixRS al, au, l, u, dummy;
+		m.CombineLU(al, au);
+		std::ofstream fout("/dev/null");
+		fout.setstate(std::ios::badbit);
+		dummy.Ilu2(fout, p, al, au, l, u);
+		const int n = nsup * bs;
+		CSVector vb(n, 1, nrhs), vx(n, 1, nrhs), sol(n, 1, nrhs);
+		std::memcpy(vb.GetVect(), B, sizeof(double) * n * nrhs);
+		vx.SetSVect(0.0);
+		double t0 = now_s();
+		if (ittype == 2) sol.BlockLanczosCentral(fout, &m, &l, &u, vx, vb, p);
+		else if (ittype == 3) sol.BlockLanczosRight(fout, &m, &l, &u, vx, vb, p);
+		else sol.BlockLanczosLeft(fout, &m, &l, &u, vx, vb, p);
+		double t1 = now_s();
+		std::memcpy(X, sol.GetVect(), sizeof(double) * n * nrhs);
+		if (stats) stats[0] = t1 - t0;
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
 } // extern "C"

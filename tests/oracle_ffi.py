@@ -446,3 +446,15 @@ class RefLib:
     def gmres_tree(self, n, b, x0, op, sttype=1, eps=1e-10, niter=300):
         """The reference's callback CSVector::BlockGMRES on a one-processor CTree."""
         return self._krylov_tree(self.lib.ref_gmres_tree, n, b, x0, op, sttype, C.c_double(eps), niter)
+
+    def block_lanczos(self, ia, ja, a, bs, ittype, B, tau1=1e-3, tau2=1e-3, theta=0.1, eps=1e-8, niter=1000, ichk=1):
+        """CombineLU + block ILU2 + CSVector::BlockLanczos{Central,Right,Left}
+        (ittype 2 / 3 / 4) on the columns of B (rows of the array), x0 = 0."""
+        nb = len(ia) - 1
+        B = np.ascontiguousarray(np.atleast_2d(B), dtype=np.float64)
+        X = np.zeros_like(B)
+        st = (C.c_double * 1)()
+        self._err(self.lib.ref_block_lanczos(nb, bs, _i(ia), _i(ja), _d(a), ittype, B.shape[0], _d(B), _d(X),
+                                             C.c_double(tau1), C.c_double(tau2), C.c_double(theta),
+                                             C.c_double(eps), niter, ichk, st))
+        return X

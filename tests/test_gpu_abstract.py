@@ -245,3 +245,21 @@ def test_reference_block_gmres_runs_on_gpu_operators(reflib):
     print(f"reference BlockGMRES on GPU operators: {info['iters']} it, rel. error {err:.2e}")
     assert np.linalg.norm(b - A @ x) <= 1e-9 * np.linalg.norm(b)
     assert err <= 1e-8
+
+
+@pytest.mark.parametrize("ittype", [2, 3, 4])
+def test_abstract_solver_block_lanczos(reflib, ittype):
+    """AbstractSolver with ittype 2 / 3 / 4 (the reference's default is 2):
+    the reference's block ILU2 + block Lanczos variant against the GPU's block
+    Lanczos on the point form of the same system."""
+    s = P.lame3d(5, 0.3, 1.0, 10)
+    a = skewed(s)
+    sprnd = np.arange(s.n + 1, dtype=np.int32) * 3
+    b = s.rhs[0]
+    x_ref, x_gpu, info, p = run_both(reflib, False, sprnd, s.ia, s.ja, a, b, np.zeros_like(b), ittype=ittype,
+                                     eps=1e-10)
+    A = sp.bsr_matrix((a.reshape(-1, 3, 3).transpose(0, 2, 1), s.ja, s.ia), shape=(s.n * 3, s.n * 3)).tocsr()
+    err = relerr(x_gpu, x_ref)
+    print(f"AbstractSolver ittype {ittype}: GPU {p.nitperf} steps, rel. error {err:.2e}")
+    assert np.linalg.norm(b - A @ x_gpu) <= 1e-9 * np.linalg.norm(b)
+    assert err <= 1e-7
