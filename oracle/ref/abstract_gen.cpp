@@ -182,13 +182,15 @@ int ref_abstract(int symm, void *o, double tau1, double tau2, double theta, doub
 // matrix and preconditioner operators given as CMVM / CSOLVELU function
 // pointers and their objects.  x: initial guess in, solution out.
 // stats[0..1] = iterations, wall seconds.
-int ref_cg_tree(int n, const double *b, double *x, void *obja, void *mvm, void *objlu, void *solvelu, int ittype,
+// The callback CG stops on sttype (0 absolute, 1 relative residual norm,
+// Bslib/cg.cpp:605-612), not on ittype.
+int ref_cg_tree(int n, const double *b, double *x, void *obja, void *mvm, void *objlu, void *solvelu, int sttype,
                 double eps, int niter, double *stats) {
 	const std::ios::iostate cst = std::cout.rdstate();
 	try {
 		CTree tree(1, 2);
 		CSlvParam p;
-		p.msglev = 0; p.ittype = ittype; p.eps = eps; p.niter = niter; p.ichk = 1;
+		p.msglev = 0; p.sttype = sttype; p.eps = eps; p.niter = niter; p.ichk = 1;
 		CSVector vb(n), vx(n), sol(n);
 		std::memcpy(vb.GetVect(), b, sizeof(double) * n);
 		std::memcpy(vx.GetVect(), x, sizeof(double) * n);

@@ -437,11 +437,11 @@ class RefLib:
             raise RuntimeError(self.lib.ref_abstract_error().decode())
         return x, dict(iters=int(st[0]), wall=st[1])
 
-    def cg_tree(self, n, b, x0, op, ittype=0, eps=1e-10, niter=1000):
+    def cg_tree(self, n, b, x0, op, sttype=1, eps=1e-10, niter=1000):
         """The reference's callback CSVector::Cg on a one-processor CTree, with
         the matrix / preconditioner operators of `op` (.h object, .fns[0..1]
-        CMVM / CSOLVELU pointers)."""
-        return self._krylov_tree(self.lib.ref_cg_tree, n, b, x0, op, ittype, C.c_double(eps), niter)
+        CMVM / CSOLVELU pointers); it stops on sttype (0 absolute, 1 relative)."""
+        return self._krylov_tree(self.lib.ref_cg_tree, n, b, x0, op, sttype, C.c_double(eps), niter)
 
     def gmres_tree(self, n, b, x0, op, sttype=1, eps=1e-10, niter=300):
         """The reference's callback CSVector::BlockGMRES on a one-processor CTree."""

@@ -212,13 +212,13 @@ def test_reference_cg_runs_on_gpu_operators(reflib):
     p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
     op = bsg.GpuOperator(s.n, u.ia, u.ja, u.a, True, p)
     try:
-        x, info = reflib.cg_tree(s.n, b, np.zeros(s.n), op, ittype=0, eps=1e-10, niter=1000)
+        x, info = reflib.cg_tree(s.n, b, np.zeros(s.n), op, sttype=1, eps=1e-10, niter=1000)
     finally:
         op.free()
     xr, ir = reflib.solve_symm(u.ia, u.ja, u.a, b, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=-1.0, ittype=0, eps=1e-10)
     err = relerr(x, xr)
     print(f"reference Cg on GPU operators: {info['iters']} it (reference operators {ir['iters']}), rel. error {err:.2e}")
-    assert abs(info["iters"] - ir["iters"]) <= 1
+    assert abs(info["iters"] - ir["iters"]) <= 2
     assert err <= 1e-8
 
 

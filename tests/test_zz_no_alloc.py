@@ -33,10 +33,11 @@ def _pool_marks(device=0):
 
 
 def _reset_high_mark(device=0):
+    from cuda.bindings import driver as dr
     from cuda.bindings import runtime as rt
     err, pool = rt.cudaDeviceGetDefaultMemPool(device)
     assert err == rt.cudaError_t.cudaSuccess
-    (err,) = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, rt.cuuint64_t(0))
+    (err,) = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemHigh, dr.cuuint64_t(0))
     assert err == rt.cudaError_t.cudaSuccess
 
 
