@@ -134,6 +134,15 @@ __global__ void k_bbeta(int nsys, double eps2, int niter, double *sc, int *si, i
 	d[SC_BETA] = beta;
 }
 
+// End of one pass of the loop body: continue while a system is active and
+// the pass limit is not reached; clear the active count for the next pass.
+__global__ void k_bcontinue(cudaGraphConditionalHandle h, int *cnt, int max_passes) {
+	const int passes = ++cnt[2];
+	const bool go = cnt[0] > 0 && passes < max_passes;
+	cnt[0] = 0;
+	cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 // system of element e of the [nrhs][n] vectors
 __device__ __forceinline__ int sys_of(long long e, long long n, int nseg, const int *segid) {
 	const int rhs = (int)(e / n);
@@ -488,32 +497,54 @@ extern "C" int bsg_pcg_batch_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f,
 		k_bbeta<<<sgrid, 256, 0, st>>>(nsys, eps2, p->niter, sc, si, cnt);
 		return 0;
 	};
-	cudaGraph_t graph = nullptr;
+	// The whole iteration loop is one graph: a conditional WHILE node whose
+	// body is K captured iterations followed by k_bcontinue, which decides on
+	// the device whether another pass runs.  The host launches the graph once
+	// per solve (and once more per true-residual restart) and reads nothing
+	// in between.
+	cudaGraph_t graph = nullptr, body = nullptr;
 	cudaGraphExec_t exec = nullptr;
+	cudaGraphConditionalHandle hcond = 0;
+	cudaGraphNode_t wnode = nullptr;
+	const int max_replays = (p->niter + K - 1) / K + 8;
 	const unsigned long long l0 = g_bsg_launches;
-	BCHK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-	for (int k = 0; k < K && !rc; k++) rc = iteration();
-	cudaError_t ce = cudaStreamEndCapture(st, &graph);
-	const unsigned long long per_graph = g_bsg_launches - l0;
+	cudaError_t ce = cudaGraphCreate(&graph, 0);
+	if (ce == cudaSuccess) ce = cudaGraphConditionalHandleCreate(&hcond, graph, 1, cudaGraphCondAssignDefault);
+	if (ce == cudaSuccess) {
+		cudaGraphNodeParams cp = {};
+		cp.type = cudaGraphNodeTypeConditional;
+		cp.conditional.handle = hcond;
+		cp.conditional.type = cudaGraphCondTypeWhile;
+		cp.conditional.size = 1;
+		ce = cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp);
+		if (ce == cudaSuccess) body = cp.conditional.phGraph_out[0];
+	}
+	if (ce == cudaSuccess) ce = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+	if (ce == cudaSuccess) {
+		for (int k = 0; k < K && !rc; k++) rc = iteration();
+		BSG_COUNT(1);
+		k_bcontinue<<<1, 1, 0, st>>>(hcond, cnt, max_replays);
+		cudaGraph_t captured = nullptr;
+		ce = cudaStreamEndCapture(st, &captured);
+	}
+	const unsigned long long per_pass = g_bsg_launches - l0;
 	g_bsg_launches = l0;
 	if (rc || ce != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
 		if (graph) cudaGraphDestroy(graph);
 		cudaEventDestroy(e0);
 		cudaEventDestroy(e1);
-		return restore(bsg_set_error(rc ? rc : BSG_ERR_CUDA, "batched PCG: graph capture failed"));
+		return restore(bsg_set_error(rc ? rc : BSG_ERR_CUDA, "batched PCG: graph construction failed"));
 	}
 	int *h_cnt = nullptr;
 	BCHK(cudaMallocHost(&h_cnt, sizeof(int) * 4));
 	int replays = 0, restarts = 0, status = BSG_OK;
-	const int max_replays = (p->niter + K - 1) / K + 8;
+	BCHK(cudaMemsetAsync(cnt, 0, sizeof(int) * 3, st));
 	for (;;) {
-		BCHK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
 		BCHK(cudaGraphLaunch(exec, st));
-		g_bsg_launches += per_graph;
-		replays++;
-		BCHK(cudaMemcpyAsync(h_cnt, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+		BCHK(cudaMemcpyAsync(h_cnt, cnt, sizeof(int) * 3, cudaMemcpyDeviceToHost, st));
 		BCHK(cudaStreamSynchronize(st));
-		if (h_cnt[0] > 0 && replays < max_replays) continue;
+		g_bsg_launches += per_pass * (unsigned long long)(h_cnt[2] - replays);
+		replays = h_cnt[2];
 		// all stopped: confirm on the FP64 true residuals, restart drifted systems
 		if ((rc = bsg_spmm_launch(m, nrhs, d_X, q, n, st))) break;
 		BSG_COUNT(1);

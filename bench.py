@@ -208,6 +208,173 @@ def run_reference(args, rank):
     return 0
 
 
+def run_config(k, args):
+    """One JSON line for benchmark configuration k (1..4) on one GPU; the
+    metric's workload (k = 5) is the default run.  Times are CUDA events:
+    configurations 1 and 4 time whole solves from the host system arrays
+    (set-up, factorisation, iteration); 2 and 3 time the set-up with the
+    block factorisation once (fct_ms) and each precision arm's iteration
+    (itr_ms) on that factor.  Solutions are compared with the reference
+    Bslib's own solve where that finishes in seconds on one core (1, and a
+    sample of the problems of 4), else with the all-FP64 GPU arm, as
+    configuration 2 asks."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    import bsg
+    import problems as P
+    from oracle_ffi import RefLib, REF_SO
+    dist = None
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        if k != 4:
+            raise SystemExit("--config with several GPUs: only configuration 4 (independent problems) shards")
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = bsg.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    s = P.config(k)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    have_ref = os.path.exists(REF_SO)
+    line = {"metric": f"ms to rel. residual, benchmark configuration {k}", "unit": "ms", "n_gpus": 1,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic"}
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    if k == 1:  # 32^3 heat, IC2 1e-3, PCG to 1e-10
+        u = s.upper()
+        arms = {}
+        for name, prm in (("fp64_pcg", dict(precision=0, trisolve=0)),
+                          ("fp64_pcg_sweeps", dict(precision=0, trisolve=1, nsweeps=6)),
+                          ("mixed_pcg", dict(precision=1, trisolve=1, nsweeps=6))):
+            def step():
+                p = bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0,
+                                      eps=1e-10, niter=3000, true_residual=1, **prm)
+                m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
+                f = bsg.Factor(ctx, m, "ich2", p)
+                x = torch.zeros(s.n, dtype=torch.float64, device="cuda")
+                bsg.pcg(ctx, m, f, d_b, x, p)
+                return p, x
+            d_b = torch.as_tensor(s.rhs[0], device="cuda")
+            for _ in range(3):
+                step()
+            t, (p, x) = timed(step)
+            arms[name] = dict(ms=round(t, 3), iterations=p.nitperf, true_residual=p.resfin, x=x.cpu().numpy())
+        if have_ref:
+            t0 = time.perf_counter()
+            xr, info = RefLib().solve_symm(u.ia, u.ja, u.a, s.rhs[0], fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1,
+                                           memory=-1.0, ittype=0, eps=1e-10, niter=3000)
+            line["cpu_baseline"] = {"value": round((time.perf_counter() - t0) * 1e3, 3), "unit": "ms", "cores": 1,
+                                    "kind": "reference", "iterations": info["iters"],
+                                    "sample": "the full system, one solve"}
+            for a in arms.values():
+                a["rel_err_vs_reference"] = rel(a["x"], xr)
+        line["config"] = {"workload": "heat3d 7-point 32^3, unit conductivity, seed 0; IC2 tau 1e-3; PCG to 1e-10",
+                          "n": s.n, "nnz": s.nnz}
+    elif k in (2, 3):  # block Lame: ILU2 + GMRES(50) (2) / 6 load cases, block IC2 + batched PCG (3)
+        kind = "ilu2" if k == 2 else "ich2"
+        src = s if k == 2 else s.upper()
+        p = bsg.default_param(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=1e-8,
+                              niter=3000, precision=0, trisolve=1, nsweeps=6, krylov=1 if k == 2 else 0,
+                              restart=50, sttype=1, true_residual=1)
+
+        def setup():
+            m = bsg.Matrix(ctx, src.n, src.ia, src.ja, src.a, bs=3, symm_upper=(k == 3))
+            return m, bsg.Factor(ctx, m, kind, p)
+        t_fct, (m, f) = timed(setup)
+        B = torch.as_tensor(s.rhs, device="cuda").contiguous()
+        arms = {}
+        for name in ("fp64", "fp32"):
+            if name == "fp32":
+                f.to_fp32()
+            q = bsg.default_param(**{fld: getattr(p, fld) for fld, _ in bsg.Param._fields_ if fld != "pad"})
+            X = torch.zeros_like(B)
+            if k == 2:
+                t, _ = timed(lambda: bsg.gmres(ctx, m, f, B[0], X[0], q))
+                its, res = [q.nitperf], [q.resfin]
+            else:
+                t, (its, res, _) = timed(lambda: bsg.pcg_batch(ctx, m, f, B, X, q))
+            arms[name] = dict(itr_ms=round(t, 3), iterations=[int(v) for v in its], true_residual=[float(r) for r in res],
+                              x=X.cpu().numpy())
+        for a in arms.values():
+            a["rel_err_vs_fp64"] = [rel(a["x"][j], arms["fp64"]["x"][j]) for j in range(B.shape[0])]
+        line["config"] = ({"workload": "Lame 3x3 BSR 64^3 nodes (786k DOF), lognormal E seed 1, z=0 clamped; block "
+                                       "ILU2 tau 1e-3, Jacobi(6) block sweeps, GMRES(50) to 1e-8",
+                           "nb": s.n, "nnzb": s.nnz} if k == 2 else
+                          {"workload": "periodic Lame cell 48^3 nodes, inclusions 30% contrast 100 seed 2, 6 load "
+                                       "cases; block IC2 tau 1e-3, Jacobi(6) block sweeps, batched PCG to 1e-8",
+                           "nb": s.n, "nnzb": s.nnz})
+        line["fct_ms"] = round(t_fct, 3)
+    elif k == 4:  # 256 uneven 2-D heat problems, batched IC2-PCG to 1e-8
+        # N ranks (torchrun): each takes whole problems, balanced by nonzeros
+        # (shard.py), solves them as one batch on its GPU; one all-gather of
+        # the per-problem iteration counts and residuals; the time is the max
+        # over ranks.  One rank: the whole batch.
+        import shard
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+        kw = dict(ordtype=0, fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=20.0, ittype=0, eps=1e-8,
+                  niter=3000, precision=1, trisolve=1, nsweeps=6)
+        own = shard.partition_segments(shard.segment_weights(s), world)[rank]
+        loc = shard.local_system(s, own)
+        solver = shard.gpu_batch_solver(ctx, kw)
+        solver(loc)  # warm-up (autotuning of the batch shapes)
+        if world > 1:
+            dist.barrier()
+        t, (x_loc, its, res) = timed(lambda: solver(loc))
+        if world > 1:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        out = shard.solve_segments_sharded(s, lambda _sys: (x_loc, its, res), rank, world, gather=True)
+        its, res = out["iterations"], out["residuals"]
+        arms = {"mixed_batched_pcg": dict(ms=round(t, 3), ranks=world, iterations_max=int(its.max()),
+                                          iterations_mean=float(its.mean()), true_residual_max=float(res.max()))}
+        line["scaling"] = "strong"
+        # this rank's solution in global order, for the reference comparison
+        x = np.zeros(s.n)
+        for g, (a0, a1) in zip(own, zip(loc.parts[:-1], loc.parts[1:])):
+            x[int(s.parts[g]):int(s.parts[g + 1])] = x_loc[int(a0):int(a1)]
+        if have_ref and rank == 0:  # a sample of rank 0's problems against the reference's own solve
+            import scipy.sparse as sp
+            A = s.to_scipy()
+            errs, tref = [], 0.0
+            ref = RefLib()
+            for g in own[::max(1, len(own) // 16)][:16]:
+                a, b = int(s.parts[g]), int(s.parts[g + 1])
+                sub = sp.triu(A[a:b, a:b]).tocsr()
+                sub.sort_indices()
+                t0 = time.perf_counter()
+                xr, _ = ref.solve_symm(sub.indptr.astype(np.int32), sub.indices.astype(np.int32), sub.data.copy(),
+                                       s.rhs[0][a:b], fcttyp=2, tau1=TAU, tau2=TAU, theta=0.1, memory=-1.0, ittype=0,
+                                       eps=1e-8, niter=3000)
+                tref += time.perf_counter() - t0
+                errs.append(rel(x[a:b], xr))
+            arms["mixed_batched_pcg"]["rel_err_vs_reference_max"] = max(errs)
+            line["cpu_baseline"] = {"value": round(tref * 1e3, 3), "unit": "ms", "cores": 1, "kind": "reference",
+                                    "sample": "16 of rank 0's problems, evenly spaced, one SolveSymm each"}
+        line["config"] = {"workload": "256 2-D heat problems, sides log-uniform [32,256], lognormal k seed 3; "
+                                      "FP32 IC2, Jacobi(6) sweeps, batched PCG to 1e-8", "n": s.n, "nnz": s.nnz}
+    else:
+        raise SystemExit("--config takes 1..4 (the metric's workload, 5, is the default run)")
+    for a in arms.values():
+        a.pop("x", None)
+    line["arms"] = arms
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -218,12 +385,18 @@ def main():
     ap.add_argument("--lean", action="store_true",
                     help="timed steps only (no other arms, e2e, kernel timing or CPU baseline): profiling runs")
     ap.add_argument("--grid", type=int, default=GRID, help="cells per side (profiling of smaller cases)")
+    ap.add_argument("--config", type=int, default=0,
+                    help="measure benchmark configuration 1..4 instead (one GPU, one JSON line)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.config:
+        import torch
+        torch.cuda.set_device(local)
+        return run_config(args.config, args)
     args.warmup = max(args.warmup, 3)
 
     import numpy as np

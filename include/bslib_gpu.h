@@ -237,13 +237,16 @@ int bsg_block_lanczos_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int 
  * matrix.  Each (right-hand side, segment) pair is its own system with its
  * own scalars and stopping test (ittype 0: ||r|| <= eps ||r0||), solved
  * together: one SpMM, one preconditioner pass per right-hand side and
- * segmented reductions per iteration, the iterations replayed from a CUDA
- * graph.  d_B, d_X: [nrhs][n] (n = point rows), d_X holds x0.  seg_off: host,
+ * segmented reductions per iteration.  The iteration loop is one CUDA graph
+ * launched once: a conditional while node whose body runs 8 iterations and
+ * decides on the device whether another pass is needed; the host reads the
+ * result only when every system has stopped (and once more per
+ * true-residual restart).  d_B, d_X: [nrhs][n] (n = point rows), d_X holds x0.  seg_off: host,
  * nseg + 1 point-row offsets (whole block rows; NULL when nseg == 1).
  * iters / res (host, nrhs * nseg, may be NULL): per-system iterations and
  * FP64 true relative residuals; p->nitperf / p->resfin get their maxima.
  * tuned (host, 4 ints, may be NULL): reduction chunk, SpMM group, iterations
- * per graph, graph replays. */
+ * per pass of the graph's loop body, passes made. */
 int bsg_pcg_batch_dev(bsg_ctx *ctx, const bsg_mat *m, const bsg_fct *f, int nrhs, int nseg, const int *seg_off,
                       const double *d_B, double *d_X, bsg_param *p, int *iters, double *res, int *tuned);
 
