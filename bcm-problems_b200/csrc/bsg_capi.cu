@@ -593,17 +593,21 @@ extern "C" int bsg_mvm(bsg_ctx *c, const bsg_mat *m, const double *x, double *y)
 
 // ---- factors --------------------------------------------------------------
 
+int bsg_ic0_run(bsg_ctx *c, bsg_mat *m, bsg_fct **out);
+
 static int fct_common(bsg_ctx *c, bsg_mat *m, bsg_param *p, int kind, bsg_fct **out) {
 	if (!c || !m || !p || !out) return bsg_set_error(BSG_ERR_ARG, "factorisation: null argument");
 	*out = nullptr;
 	if (p->ordtype != 0) return bsg_set_error(BSG_ERR_UNSUPPORTED, "only natural ordering (ordtype = 0) runs on the GPU");
-	if (kind == 0 && p->fcttyp == 1)
-		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) is not on the GPU path; use fcttyp = 2");
 	bsg_fct *f = nullptr;
 	// a 3x3 block matrix gets the reference's block factorisations
-	// (CSMatrixRS::Ilu2 / CSMatrixRS::Ich2)
+	// (CSMatrixRS::Ilu2 / CSMatrixRS::Ich2); fcttyp 1 of a symmetric point
+	// matrix is IC(0) (CSMatrixR::Ich, SolveSymm's fcttyp 1)
 	const bool block = m->bs == 3 && p->blockfct != 0;
-	int rc = block ? bsg_bfact_run(c, m, kind == 0, p, &f) : bsg_fact_run(c, m, kind, p, &f);
+	const bool ic0 = kind == 0 && p->fcttyp == 1;
+	if (ic0 && (block || m->bs != 1 || !m->symm))
+		return bsg_set_error(BSG_ERR_UNSUPPORTED, "fcttyp = 1 (IC(0)) needs a symmetric point matrix (upper input)");
+	int rc = ic0 ? bsg_ic0_run(c, m, &f) : block ? bsg_bfact_run(c, m, kind == 0, p, &f) : bsg_fact_run(c, m, kind, p, &f);
 	if (rc) return rc;
 	float ms = 0;
 	cudaEventElapsedTime(&ms, c->ev0, c->ev1);

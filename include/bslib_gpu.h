@@ -42,8 +42,9 @@ extern "C" {
  * extensions of the GPU path that the reference does not have. */
 typedef struct bsg_param {
 	int msglev;       /* output level (0 quiet)                                   */
-	int fcttyp;       /* 1: IC(0) on A's pattern (CSMatrixR::Ich; refused on the GPU
-	                     with BSG_ERR_UNSUPPORTED), else second order            */
+	int fcttyp;       /* bsg_fct_ich2 of a symmetric point matrix: 1 IC(0) on A's
+	                     pattern (CSMatrixR::Ich), else the second-order IC2;
+	                     block matrices and ILU2 always second order          */
 	int ordtype;      /* ordering; only 0 (natural) is accepted on the GPU        */
 	double memory;    /* factor workspace, multiples of nnz(A) (|memory| used)    */
 	double tau1;      /* first-order threshold: |v| >= tau1 kept in U            */

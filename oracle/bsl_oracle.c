@@ -650,3 +650,89 @@ int orc_lanczos(int n, const int *ia, const int *ja, const double *a, const int 
 	free(sol); free(r); free(good); free(sol1); free(D); free(D1); free(d); free(d1); free(img); free(p);
 	return k;
 }
+
+/* IC(0) on A's pattern: CSMatrixR::Ich (Bslib/ich2r.cpp:1821-1895).  The
+ * reference transposes the upper-stored A (rows of A^T: columns ascending,
+ * the diagonal last), computes for every row i and each off-diagonal column
+ * k, ascending,
+ *     l_ik = (a_ik - sum_m l_km l_im) * d_k      (merge over m < k)
+ * then the pivot a_ii - sum_k l_ik^2, clamped below at 1e-20, d_i = 1/sqrt,
+ * and transposes back.  Every term is a product then a subtraction (no fused
+ * multiply-add).  Output: U by rows on A's upper pattern (iu/ju copies of
+ * ia/ja), d_i in the diagonal slot, u(k,i) = l_ik.  Returns 0, or -1 for bad
+ * input (a row that does not start with its diagonal). */
+int orc_ich0(int n, const int *ia, const int *ja, const double *a, int **iu_out, int **ju_out, double **u_out) {
+	const int nz = ia[n];
+	/* rows of A^T: strict lower columns ascending, positions in the upper arrays */
+	int *tcnt = (int *)calloc((size_t)n + 1, sizeof(int));
+	int *tja = (int *)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+	int *tpos = (int *)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+	double *lv = (double *)malloc(sizeof(double) * (size_t)(nz > 0 ? nz : 1));
+	double *dinv = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+	int *iu = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+	int *ju = (int *)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+	double *u = (double *)malloc(sizeof(double) * (size_t)(nz > 0 ? nz : 1));
+	int rc = 0;
+	if (!tcnt || !tja || !tpos || !lv || !dinv || !iu || !ju || !u) { rc = -1; goto done; }
+	for (int i = 0; i < n; i++) {
+		if (ia[i + 1] <= ia[i] || ja[ia[i]] != i) { rc = -1; goto done; }
+		for (int k = ia[i] + 1; k < ia[i + 1]; k++) tcnt[ja[k] + 1]++;
+	}
+	for (int i = 0; i < n; i++) tcnt[i + 1] += tcnt[i];
+	{
+		int *fill = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+		if (!fill) { rc = -1; goto done; }
+		for (int i = 0; i < n; i++) fill[i] = tcnt[i];
+		/* rows of A visited in ascending order: each column list comes out ascending */
+		for (int k = 0; k < n; k++)
+			for (int p = ia[k] + 1; p < ia[k + 1]; p++) {
+				const int i = ja[p];
+				tja[fill[i]] = k;
+				tpos[fill[i]] = p;
+				fill[i]++;
+			}
+		free(fill);
+	}
+	for (int i = 0; i < n; i++) {
+		const int i1 = tcnt[i], i2 = tcnt[i + 1];
+		for (int j = i1; j < i2; j++) {
+			const int k = tja[j];
+			double r = a[tpos[j]];
+			int ik = tcnt[k], ik2 = tcnt[k + 1], q = i1;
+			while (ik < ik2 && q < j) {
+				if (tja[ik] < tja[q]) {
+					ik++;
+				} else if (tja[ik] > tja[q]) {
+					q++;
+				} else {
+					const double pr = lv[ik] * lv[q];
+					r = r - pr;
+					q++;
+					ik++;
+				}
+			}
+			lv[j] = r * dinv[k];
+		}
+		double r = a[ia[i]];
+		for (int j = i1; j < i2; j++) {
+			const double pr = lv[j] * lv[j];
+			r = r - pr;
+		}
+		if (r < 1.0e-20) r = 1.0e-20;
+		dinv[i] = 1.0 / sqrt(r);
+	}
+	for (int i = 0; i <= n; i++) iu[i] = ia[i];
+	for (int p = 0; p < nz; p++) ju[p] = ja[p];
+	for (int i = 0; i < n; i++) u[ia[i]] = dinv[i];
+	for (int i = 0; i < n; i++)
+		for (int j = tcnt[i]; j < tcnt[i + 1]; j++) u[tpos[j]] = lv[j];
+	*iu_out = iu;
+	*ju_out = ju;
+	*u_out = u;
+	iu = NULL;
+	ju = NULL;
+	u = NULL;
+done:
+	free(tcnt); free(tja); free(tpos); free(lv); free(dinv); free(iu); free(ju); free(u);
+	return rc;
+}

@@ -42,6 +42,10 @@ int orc_fact(int kind, int n, const int *ia, const int *ja, const double *al, co
              double tau2, double theta, double sclmin, double pivmin, int **iu, int **ju, double **lval,
              double **uval, double *stats);
 
+/* IC(0) on A's pattern (CSMatrixR::Ich): upper-stored A in, U by rows on
+ * the same pattern out (inverse pivots in the diagonal slots), malloc'ed. */
+int orc_ich0(int n, const int *ia, const int *ja, const double *a, int **iu, int **ju, double **u);
+
 /* Preconditioned CG with an upper-stored SPD matrix and an IC factor, the
  * reference's stopping rules (ittype 0: relative, 1: absolute on the
  * recursively updated residual).  Returns iterations; x holds the solution. */

@@ -50,6 +50,15 @@ double now_s() {
 	return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+// The reference prints to cout in places whatever msglev says, and formatting
+// numbers through its streams crashes inside a Python process: calls that
+// print keep cout in a failed state meanwhile.
+struct QuietCout {
+	std::ios::iostate st = std::cout.rdstate();
+	QuietCout() { std::cout.setstate(std::ios::badbit); }
+	~QuietCout() { std::cout.clear(st); }
+};
+
 // Error convention: the reference throws const char*; map it to a negative code
 // and keep the message for ref_last_error().
 thread_local char g_err[256];
@@ -180,6 +189,7 @@ int ref_ilu2(int n, const int *ia, const int *ja, const double *a, double tau1, 
 int ref_solve_symm(int n, const int *ia, const int *ja, const double *a, const double *b, double *x,
                    int fcttyp, double tau1, double tau2, double theta, double memory,
                    int ittype, double eps, int niter, int ichk, double *stats) {
+	QuietCout quiet; // CSMatrixR::Ich (fcttyp 1) prints its size and time
 	try {
 		CSMatrixR m = make_csr(n, ia, ja, a);
 		CSlvParam p;
@@ -398,11 +408,6 @@ int ref_solve_symm_block(int nsup, int bs, const int *ia, const int *ja, const d
 // Bslib/smatrixr.cpp:3984 / :3852; CSVector::WriteVectBin / ReadVectBin,
 // Bslib/svector.cpp:537 / :488; CSMatrixR::ConvertToBinary, :4010).  They print
 // to cout; the harness silences it around the calls.
-struct QuietCout {
-	std::ios::iostate st = std::cout.rdstate();
-	QuietCout() { std::cout.setstate(std::ios::badbit); }
-	~QuietCout() { std::cout.clear(st); }
-};
 
 int ref_write_mtr_bin(const char *path, int n, const int *ia, const int *ja, const double *a) {
 	QuietCout q;
@@ -473,6 +478,20 @@ int ref_block_lanczos(int nsup, int bs, const int *ia, const int *ja, const doub
 		double t1 = now_s();
 		std::memcpy(X, sol.GetVect(), sizeof(double) * n * nrhs);
 		if (stats) stats[0] = t1 - t0;
+		return 0;
+	} catch (const char *e) {
+		return fail(e);
+	}
+}
+
+// IC(0) of an upper-stored SPD matrix (CSMatrixR::Ich, Bslib/ich2r.cpp:1821):
+// U by rows, inverse pivots first.
+int ref_ich0(int n, const int *ia, const int *ja, const double *a, int **ia_u, int **ja_u, double **a_u) {
+	QuietCout q;
+	try {
+		CSMatrixR m = make_csr(n, ia, ja, a);
+		CSMatrixR u = m.Ich();
+		export_csr(u, ia_u, ja_u, a_u);
 		return 0;
 	} catch (const char *e) {
 		return fail(e);

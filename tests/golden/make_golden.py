@@ -53,6 +53,13 @@ def main():
         out[f"{tag}_density"] = np.array(st[:2])
         out[f"{tag}_solve_l"] = ref.solve_l(iu, ju, uu, x)
         out[f"{tag}_solve_u"] = ref.solve_u(iu, ju, uu, x)
+    iu, ju, uu = ref.ich0(u.ia, u.ja, u.a)
+    out["ic0_iu"], out["ic0_ju"], out["ic0_u"] = iu, ju, uu
+    # SolveSymm(CSMatrixR&) itself cannot run IC(0): it hands Cg the (empty)
+    # block factor whenever memory >= 0 and Ich fills only the plain one
+    # (Bslib/solvers.cpp:4690-4730), so Cg runs on the IC(0) factor directly
+    xs0, info0 = ref.cg(u.ia, u.ja, u.a, iu, ju, uu, s.rhs[0], ittype=0, eps=1e-10)
+    out["symm_ic0_x"], out["symm_ic0_iters"] = xs0, np.array(info0["iters"])
     an = nonsymmetric(s)
     out["ns_a"] = an
     for tag, t1, t2 in (("ilu2_a", 1e-3, 1e-3), ("ilu2_b", 1e-2, 1e-4)):

@@ -118,6 +118,18 @@ class Oracle:
             uv = lv
         return iu, ju, lv, uv, (st[0], st[1])
 
+    def ich0(self, ia, ja, a):
+        """IC(0) (CSMatrixR::Ich) of an upper-stored matrix: (iu, ju, u)."""
+        n = len(ia) - 1
+        piu, pju, pu = _ip(), _ip(), _dp()
+        keep = [np.ascontiguousarray(v) for v in (ia, ja, a)]
+        if self.lib.orc_ich0(n, _i(keep[0]), _i(keep[1]), _d(keep[2]), C.byref(piu), C.byref(pju), C.byref(pu)) != 0:
+            raise RuntimeError("orc_ich0 failed")
+        iu, ju, u, _ = _take_csr(self.lib, n, piu, pju, pu)
+        for p in (piu, pju, pu):
+            self.lib.orc_free(p)
+        return iu, ju, u
+
     def pcg(self, ia, ja, a, iu, ju, u, b, ittype=0, eps=1e-10, niter=1000):
         n = len(ia) - 1
         x = np.zeros(n)
@@ -231,6 +243,16 @@ class RefLib:
         y = np.zeros(n)
         self._err(self.lib.ref_solve_u(n, _i(iu), _i(ju), _d(u), _d(x), _d(y)))
         return y
+
+    def ich0(self, ia, ja, a):
+        """CSMatrixR::Ich (IC(0)) of an upper-stored matrix: (iu, ju, u)."""
+        n = len(ia) - 1
+        piu, pju, pu = _ip(), _ip(), _dp()
+        self._err(self.lib.ref_ich0(n, _i(ia), _i(ja), _d(a), C.byref(piu), C.byref(pju), C.byref(pu)))
+        iu, ju, u, _ = _take_csr(self.lib, n, piu, pju, pu)
+        for p in (piu, pju, pu):
+            self.lib.ref_free(p)
+        return iu, ju, u
 
     def ich2(self, ia, ja, a, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0):
         n = len(ia) - 1

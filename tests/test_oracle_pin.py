@@ -182,3 +182,21 @@ def test_live_reference_block_ich2_larger_cases(oracle, reflib):
         ia_f, ja_f, uf, _ = reflib.ich2_block(u.ia, u.ja, u.a, 3, tau1=t1, tau2=t2)
         o = oracle.ich2_block(u.ia, u.ja, u.a, 3, tau1=t1, tau2=t2)
         assert np.array_equal(o[0], ia_f) and np.array_equal(o[1], ja_f) and np.array_equal(o[2], uf)
+
+
+def test_ich0_matches_reference(oracle, gold):
+    """IC(0) (CSMatrixR::Ich): the oracle's factor is the reference's bit for
+    bit (the same products and subtractions, no fused multiply-add)."""
+    g = gold
+    iu, ju, u = oracle.ich0(g["ua_ia"], g["ua_ja"], g["ua_a"])
+    assert np.array_equal(iu, g["ic0_iu"]) and np.array_equal(ju, g["ic0_ju"])
+    assert np.array_equal(u, g["ic0_u"])
+
+
+def test_ich0_matches_live_reference_at_cfg1(oracle, reflib):
+    s = P.config(1)
+    u = s.upper()
+    a = oracle.ich0(u.ia, u.ja, u.a)
+    b = reflib.ich0(u.ia, u.ja, u.a)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
