@@ -389,7 +389,7 @@ class UNet:
 FACT_STAT_NAMES = ("tries", "parks", "cyc_pop", "cyc_close", "cyc_blocked", "cyc_tail", "cyc_upd", "cyc_fin",
                    "members", "mask", "rounds", "cyc_pf", "cyc_pa", "cyc_pb", "big_rows", "warps",
                    "cyc_pass_load", "cyc_pass_close", "cyc_to_publish", "cyc_post_publish", "batches", "closed",
-                   "unused22", "unused23")
+                   "cyc_tail_close", "cyc_fin_prepub")
 
 
 def fact_stats():

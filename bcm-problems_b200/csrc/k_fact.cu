@@ -106,7 +106,8 @@ struct FactArgs {
 // Scheduler / phase counters summed over all warps of the last factorisation.
 enum { FS_TRY = 0, FS_PARK, FS_CYC_POP, FS_CYC_CLOSE, FS_CYC_BLOCKED, FS_CYC_TAIL, FS_CYC_UPD, FS_CYC_FIN,
        FS_CONTRIB, FS_MASK, FS_ROUNDS, FS_CYC_PF, FS_CYC_PA, FS_CYC_PB, FS_BIG, FS_WARPS,
-       FS_CYC_PLOAD, FS_CYC_PCLOSE, FS_CYC_TOPUB, FS_CYC_POSTPUB, FS_BATCHES, FS_CLOSED, FACT_NSTAT = 24 };
+       FS_CYC_PLOAD, FS_CYC_PCLOSE, FS_CYC_TOPUB, FS_CYC_POSTPUB, FS_BATCHES, FS_CLOSED, FS_CYC_TCLOSE,
+       FS_CYC_FPRE, FACT_NSTAT = 24 };
 struct PhaseClock {
 	unsigned long long v[FACT_NSTAT];
 };
@@ -224,9 +225,6 @@ __device__ void acc_push(unsigned long long *acc, int j, double comp, double sca
 	}
 	atomicAdd(acc + j, (unsigned long long)t);
 }
-__device__ double acc_value(const unsigned long long *acc, int j, double inv_scale) {
-	return __dmul_rn((double)__ldcg(acc + j), inv_scale);
-}
 
 // The queue is a ring of qcap slots (a power of two, at least twice the
 // rows): a row is in the queue at most once at a time (queued on admission,
@@ -316,10 +314,12 @@ __device__ void park(const FactArgs &A, int i, int m) {
 // index and flag, or none: the member dropped i), a second inserts the
 // stored columns between the member and i (R x R skipped) into the member
 // set, new members taking slots by ballot.  Returns the number closed; the
-// smallest member still unfinished goes to *pmin.
+// smallest member still unfinished goes to pmin, the number of members the
+// pass discovered to added.
 template <class WS>
-__device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax, int &pmin, int &err) {
+__device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax, int &pmin, int &err, int &added) {
 	const int nW = min(s.sc[0], s.cmax);
+	added = 0;
 	const unsigned lt = (1u << lane) - 1;
 	int pm = 0x7fffffff;
 	if (lane == 0) s.sc[2] = 0;
@@ -420,6 +420,7 @@ __device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax
 			}
 			__syncwarp();
 			if (lane == 0) s.sc[0] = q0 + __popc(b);
+			added += __popc(b);
 			__syncwarp();
 		}
 		err = __reduce_min_sync(0xffffffffu, err);
@@ -627,20 +628,25 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	}
 
 	int levmax = 0;
+	unsigned long long accraw = 0;
+	bool waited = false;
 	long long tail0 = clock64(); // end of the last wait: the row's own latency starts here
 	for (;;) {
 		// ---- close the finished members, pass after pass, until a pass
 		//      closes none; the smallest member left is the bound
+		// (a pass that closed members but discovered none leaves nothing
+		// for another pass: every member is known, and the ones it found
+		// unfinished are waited for below)
 		int bound = i;
 		const long long k0 = clock64();
 		for (;;) {
 			pc.v[FS_ROUNDS]++;
-			int pmin = 0x7fffffff;
+			int pmin = 0x7fffffff, added = 0;
 			const long long q0 = clock64();
-			const int closed = close_pass(A, s, i, lane, levmax, pmin, err);
+			const int closed = close_pass(A, s, i, lane, levmax, pmin, err, added);
 			pc.v[FS_CYC_PCLOSE] += clock64() - q0;
 			if (err) break;
-			if (!closed) {
+			if (!closed || !added) {
 				bound = pmin == 0x7fffffff ? i : pmin;
 				break;
 			}
@@ -652,6 +658,11 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		}
 		const long long k1 = clock64();
 		pc.v[FS_CYC_CLOSE] += k1 - k0;
+		if (waited) pc.v[FS_CYC_TCLOSE] += k1 - k0;
+		// the compensations received so far (every member seen finished has
+		// pushed its own before publishing): loaded now, used after the last
+		// pass, so the load overlaps the updates
+		if (lane == 0) accraw = __ldcg(A.acc + i);
 		// ---- updates of the closed members below the bound
 		err = apply_members(A, s, bound, lane, pc);
 		const long long k2 = clock64();
@@ -668,6 +679,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		if (lane == 0) res = wait_row(A, bound);
 		res = __shfl_sync(0xffffffffu, res, 0);
 		tail0 = clock64();
+		waited = true;
 		pc.v[FS_CYC_BLOCKED] += tail0 - k2;
 		if (res == 0) return bound;
 		if (res < 0) {
@@ -678,7 +690,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	levmax = __reduce_max_sync(0xffffffffu, levmax);
 	pc.v[FS_CONTRIB] += min(s.sc[0], s.cmax);
 	{
-		const double comp = acc_value(A.acc, i, A.acc_inv_scale);
+		const double comp = __dmul_rn((double)__shfl_sync(0xffffffffu, accraw, 0), A.acc_inv_scale);
 		if (lane == 0) {
 			const int di0 = hfind_insert(s, i);
 			s.hl[di0] = __dadd_rn(s.hl[di0], comp);
@@ -754,6 +766,12 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		if (lane == 0) s.sc[2] = base + __popc(b);
 		__syncwarp();
 	}
+	// the stored length is known: reserve the pool space now, so the
+	// atomic's round trip overlaps the compensation sum and the pivot
+	const int len = s.sc[2] + 1;
+	const int alloc = (len + 3) & ~3;
+	long long off = 0;
+	if (lane == 0) off = (long long)atomicAdd(A.pool_len, (unsigned long long)alloc);
 	if (lane == 0) {
 		double dl = s.hl[di], du = s.hu[di];
 		for (int t = 0; t < nl; t++) {
@@ -786,10 +804,6 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	}
 
 	// ---- store the stored part: diagonal, then the kept columns ascending
-	const int len = nk + 1;
-	const int alloc = (len + 3) & ~3;
-	long long off = 0;
-	if (lane == 0) off = (long long)atomicAdd(A.pool_len, (unsigned long long)alloc);
 	off = __shfl_sync(0xffffffffu, off, 0);
 	if (off + alloc > A.pool_cap || len > 0xffff) {
 		if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 6);
@@ -823,6 +837,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	__syncwarp();
 	const long long cpub = clock64();
 	pc.v[FS_CYC_TOPUB] += cpub - tail0;
+	pc.v[FS_CYC_FPRE] += cpub - c3;
 
 	// ---- release the rows of A's row i, wake parked rows, count
 	for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) admit_step(A, A.ju[k], ADM_ONE_FIN);
@@ -1051,7 +1066,10 @@ static unsigned long long g_fact_stats[FACT_NSTAT];
 // updates, finish; [8] members of C(i),
 // [9] mask columns, [10] closure rounds, [11..13] SM cycles in prefetch,
 // slot resolution and fma phases, [14] rows retried in the global-memory
-// workspace, [15] warps launched.
+// workspace, [15] warps launched, [16..19] SM cycles loading / closing in
+// the passes, from the last wait to publishing, after publishing, [20]
+// update batches, [21] members applied, [22] SM cycles of the closure passes
+// after a wait, [23] of the finish before publishing.
 extern "C" int bsg_fact_stats(unsigned long long *out, int nout) {
 	if (!out && nout > 0) return bsg_set_error(BSG_ERR_ARG, "bsg_fact_stats: null output");
 	for (int k = 0; k < nout && k < FACT_NSTAT; k++) out[k] = g_fact_stats[k];
