@@ -772,14 +772,33 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	const int alloc = (len + 3) & ~3;
 	long long off = 0;
 	if (lane == 0) off = (long long)atomicAdd(A.pool_len, (unsigned long long)alloc);
+	// ---- hand the dropped entries' compensations to their rows now: the
+	//      reductions are done by the time this row publishes (rows read a
+	//      row's pushes only after acquiring its record)
+	for (int t = lane; t < nl; t += 32) {
+		const double v = s.pf_l[t];
+		if (v != 0.0) acc_push(A.acc, s.hkey[s.lsts[t]], v, A.acc_scale, A.st);
+	}
+	// ---- the row's own compensations into its diagonal, in ascending column
+	//      order; a kept column contributes +0.0, which leaves the (positive)
+	//      sum unchanged, so the adds need no branch and the loads run ahead
 	if (lane == 0) {
 		double dl = s.hl[di], du = s.hu[di];
-		for (int t = 0; t < nl; t++) {
-			const double v = s.pf_l[t];
-			if (v != 0.0) {
-				dl = __dadd_rn(dl, v);
-				du = __dadd_rn(du, v);
+		int t = 0;
+		for (; t + 8 <= nl; t += 8) {
+			double v[8];
+#pragma unroll
+			for (int q = 0; q < 8; q++) v[q] = s.pf_l[t + q];
+#pragma unroll
+			for (int q = 0; q < 8; q++) {
+				dl = __dadd_rn(dl, v[q]);
+				du = __dadd_rn(du, v[q]);
 			}
+		}
+		for (; t < nl; t++) {
+			const double v = s.pf_l[t];
+			dl = __dadd_rn(dl, v);
+			du = __dadd_rn(du, v);
 		}
 		s.hl[di] = dl;
 		s.hu[di] = du;
@@ -824,11 +843,6 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		A.pool_cf[off + 1 + t] = (unsigned)s.hkey[h] | (flag << 30);
 		A.pool_l[off + 1 + t] = l;
 		if (ilu) A.pool_u[off + 1 + t] = u;
-	}
-	// ---- hand the dropped entries' compensations to their rows
-	for (int t = lane; t < nl; t += 32) {
-		const double v = s.pf_l[t];
-		if (v != 0.0) acc_push(A.acc, s.hkey[s.lsts[t]], v, A.acc_scale, A.st);
 	}
 	if (lane == 0) A.lev[i] = levmax;
 	__threadfence();
