@@ -277,7 +277,12 @@ __device__ int q_pop(const FactArgs &A) {
 #define ADM_ONE_FIN 1u
 #define ADM_ONE_CLAIM (1u << 15)
 #define ADM_CLAIMED (1u << 31)
-__device__ __forceinline__ bool admissible(unsigned v) { return ((v >> 15) & 0x7fffu) == 0 && (v & 0x7fffu) <= 1; }
+#ifndef BSG_ADMIT_UNFINISHED
+#define BSG_ADMIT_UNFINISHED 1
+#endif
+__device__ __forceinline__ bool admissible(unsigned v) {
+	return ((v >> 15) & 0x7fffu) == 0 && (v & 0x7fffu) <= BSG_ADMIT_UNFINISHED;
+}
 __device__ void admit_step(const FactArgs &A, int j, unsigned delta) {
 	const unsigned old = atomicSub(reinterpret_cast<unsigned *>(A.nstat) + j, delta);
 	if (!admissible(old) && admissible(old - delta)) q_push(A, j);
