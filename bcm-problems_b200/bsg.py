@@ -215,6 +215,13 @@ class Matrix:
         _check(lib().bsg_mat_info(self.h, C.byref(n), C.byref(bs), C.byref(nnz)))
         return n.value, bs.value, nnz.value
 
+    def sell_stats(self):
+        """Sliced copy of a point matrix: stored entries (padding included)
+        and rows summed outside the slices (more than 256 entries)."""
+        out = (C.c_longlong * 9)()
+        _check(lib().bsg_sell_stats(self.h, None, out))
+        return dict(entries=out[0], long=out[6])
+
     def mvm(self, x, y):
         """y = A x, both CUDA float64 tensors of length n*bs."""
         _check(lib().bsg_mvm_dev(self.ctx.h, self.h, _ptr(x), _ptr(y)))
@@ -292,11 +299,13 @@ class Factor:
 
     def sell_stats(self):
         """Sliced copies of the factor: stored entries of the strict L / U
-        rows, tiles of their tiled FP32 form (0: untiled) and the most x
-        blocks one tile stages."""
-        out = (C.c_longlong * 6)()
+        rows, tiles of their tiled FP32 form (0: untiled), the most x
+        blocks one tile stages and the rows of L / U summed outside the
+        slices (more than 256 entries)."""
+        out = (C.c_longlong * 9)()
         _check(lib().bsg_sell_stats(None, self.h, out))
-        return dict(entries_l=out[1], entries_u=out[2], tiles_l=out[3], tiles_u=out[4], tile_blocks=out[5])
+        return dict(entries_l=out[1], entries_u=out[2], tiles_l=out[3], tiles_u=out[4], tile_blocks=out[5],
+                    long_l=out[7], long_u=out[8])
 
     def solve_l(self, x, y, mode=0, nsweeps=3):
         _check(lib().bsg_solve_l_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))

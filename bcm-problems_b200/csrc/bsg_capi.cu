@@ -32,7 +32,8 @@ extern "C" unsigned long long bsg_launch_count(void) { return g_bsg_launches; }
 // Stored entries (padding included) of the SELL copies: [0] the matrix,
 // [1] strict L rows, [2] strict U rows of the factor (0 where absent);
 // [3] / [4] tiles of the tiled L / U form (0: untiled), [5] most staged x
-// blocks (32 floats) of one tile over both.
+// blocks (32 floats) of one tile over both; [6] / [7] / [8] long rows of the
+// matrix / L / U (rows summed outside the slices).
 extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out) {
 	if (!out) return bsg_set_error(BSG_ERR_ARG, "bsg_sell_stats: null output");
 	out[0] = m ? m->sell.entries : 0;
@@ -41,6 +42,9 @@ extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out
 	out[3] = f ? f->sl.ntile : 0;
 	out[4] = f ? f->su.ntile : 0;
 	out[5] = f ? (f->sl.tmax > f->su.tmax ? f->sl.tmax : f->su.tmax) : 0;
+	out[6] = m ? m->sell.nlong : 0;
+	out[7] = f ? f->sl.nlong : 0;
+	out[8] = f ? f->su.nlong : 0;
 	return BSG_OK;
 }
 

@@ -127,6 +127,18 @@ struct bsg_sell {
 	int *tb_off = nullptr;
 	int *tb = nullptr;
 	unsigned *cpair = nullptr;
+	// Long rows (more than SELL_LONG entries; none in the tiled form) are left
+	// out of the slices -- their slots hold padding and bit l of lmask[slice]
+	// marks them -- and kept as CSR: rows lrow[0 .. nvlong) (more than
+	// SELL_VLONG entries) are summed by a whole block each, the rest of
+	// lrow[0 .. nlong) by one warp each, so no slice waits on one lane walking
+	// a row of thousands of entries.
+	int nlong = 0, nvlong = 0;
+	int *lrow = nullptr;
+	long long *loff = nullptr; // [nlong + 1]
+	int *lcol = nullptr;
+	void *lval = nullptr;      // float or double, as val
+	unsigned char *lmask = nullptr;
 };
 // sigma > 0: sort rows by length inside windows of sigma rows first;
 // tiled != 0 (FP32 only, sigma dividing 256): also build the tiled form when

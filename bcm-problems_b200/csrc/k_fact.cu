@@ -249,7 +249,10 @@ __device__ int q_pop(const FactArgs &A) {
 	int *slot = A.queue + (h & (unsigned long long)(A.qcap - 1));
 	int v = atomicExch(slot, -1);
 	if (v >= 0) return v;
+	// the limit runs from the last finished row: an empty queue while other
+	// warps still finish rows (a long chain of dependent rows) is progress
 	unsigned long long t0 = globaltimer_ns();
+	int seen = *(volatile int *)A.done_count;
 	for (unsigned it = 1;; it++) {
 		__nanosleep(64);
 		if (*(volatile int *)slot >= 0) {
@@ -257,9 +260,13 @@ __device__ int q_pop(const FactArgs &A) {
 			if (v >= 0) return v;
 		}
 		if ((it & 31) == 0) {
-			if (*(volatile int *)A.done_count >= A.n) return -1;
+			const int done = *(volatile int *)A.done_count;
+			if (done >= A.n) return -1;
 			if (*(volatile int *)&A.st->code != 0) return -1;
-			if (globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) {
+			if (done != seen) {
+				seen = done;
+				t0 = globaltimer_ns();
+			} else if (globaltimer_ns() - t0 > BSG_SPIN_LIMIT_NS) {
 				devstat_fail(A.st, BSG_ERR_TIMEOUT, (int)(h & 0x7fffffff));
 				return -1;
 			}

@@ -15,26 +15,151 @@
 // DRAM sector stays fully used.  Each lane keeps 8 entries in flight
 // (unrolled), enough bytes per SM to run at the HBM roofline: per entry 4 B
 // column + 4 B (FP32) or 8 B (FP64) value.
+//
+// Long rows.  A slice is as slow as its longest row walked by one lane, so
+// rows of more than SELL_LONG entries (the wrap-around fill of periodic
+// problems reaches thousands) leave the slices and are summed as CSR rows by
+// a warp, or by a block beyond SELL_VLONG entries, in the same kernel, ahead
+// of the slices.  Their sums run in another order than the sequential one.
 #include "bsg_internal.cuh"
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
+#include <cub/device/device_select.cuh>
 
 #define SELL_C 8
+#define SELL_LONG 256   // entries: longer rows leave the slices
+#define SELL_VLONG 4096 // entries: longer rows take a whole block
 
 namespace {
 
-__global__ void k_sell_width(int n, const int *rp, int skip, const int *perm, int even, long long *width) {
+// Slice widths; rows longer than longlen (> 0) count as empty, and bit l of
+// lmask[slice] marks slot l as such a row.
+__global__ void k_sell_width(int n, const int *rp, int skip, const int *perm, int even, int longlen,
+                             long long *width, unsigned char *lmask) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	const int slice = t / SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
 	const int r = t < n ? (perm ? perm[t] : t) : n; // one thread per row slot
 	int len = r < n ? rp[r + 1] - rp[r] - skip : 0;
 	if (len < 0) len = 0;
+	const bool lng = longlen > 0 && len > longlen;
+	if (lng) len = 0;
+	const unsigned bits = __ballot_sync(0xffffffffu, lng);
 #pragma unroll
 	for (int o = SELL_C / 2; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o, SELL_C));
 	if (even) len = (len + 1) & ~1;
-	if ((t % SELL_C) == 0 && slice < nsl) width[slice] = (long long)SELL_C * len;
+	if ((t % SELL_C) == 0 && slice < nsl) {
+		width[slice] = (long long)SELL_C * len;
+		if (lmask) lmask[slice] = (unsigned char)(bits >> (threadIdx.x & 31 & ~(SELL_C - 1)));
+	}
+}
+
+// class of every row: 2 more than SELL_VLONG entries, 1 more than SELL_LONG
+__global__ void k_long_flags(int n, const int *rp, int skip, unsigned char *fv, unsigned char *fl, int *iota) {
+	for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+		const int len = rp[r + 1] - rp[r] - skip;
+		fv[r] = len > SELL_VLONG;
+		fl[r] = len > SELL_LONG && len <= SELL_VLONG;
+		iota[r] = r;
+	}
+}
+
+__global__ void k_long_len(int nl, const int *lrow, const int *rp, int skip, long long *len) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nl; i += gridDim.x * blockDim.x)
+		len[i] = i < nl ? rp[lrow[i] + 1] - rp[lrow[i]] - skip : 0;
+}
+
+// one warp per long row: its entries in CSR order
+template <typename VT>
+__global__ void k_long_fill(int nl, const int *lrow, const long long *loff, const int *rp, const int *ci,
+                            const double *v, int skip, int *lcol, VT *lval) {
+	const int lane = threadIdx.x & 31;
+	for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nl; i += (gridDim.x * blockDim.x) >> 5) {
+		const int b = rp[lrow[i]] + skip;
+		const long long o = loff[i], len = loff[i + 1] - o;
+		for (long long k = lane; k < len; k += 32) {
+			lcol[o + k] = ci[b + k];
+			lval[o + k] = (VT)v[b + k];
+		}
+	}
+}
+
+template <typename VT>
+struct sell_long {
+	int nlong, nvlong;
+	const int *row;
+	const long long *off;
+	const int *col;
+	const VT *val;
+	const unsigned char *mask;
+};
+
+template <typename VT>
+sell_long<VT> long_of(const bsg_sell *m) {
+	return {m->nlong, m->nvlong, m->lrow, m->loff, m->lcol, (const VT *)m->lval, m->lmask};
+}
+
+// Sum of the products of entries [b, e) of a long row by one warp (BLOCK
+// false, tid = lane) or by a block of 256 threads (red: 8 doubles of shared
+// memory): thread t takes entries t, t + T, t + 2 T, ... in order, U loads in
+// flight, then a fixed tree.  Every thread of the warp / block gets the sum.
+template <typename VT, typename XT, int IN, bool BLOCK, int U>
+__device__ __forceinline__ double long_row_sum(long long b, long long e, int tid, const int *__restrict__ lcol,
+                                               const VT *__restrict__ lval, const XT *__restrict__ x,
+                                               const double *__restrict__ dinv_in, double *red) {
+	constexpr int T = BLOCK ? 256 : 32;
+	double sum = 0.0;
+	for (long long j = b + tid; j < e; j += (long long)U * T) {
+		int c[U];
+		double a[U], xv[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const long long q = j + (long long)u * T;
+			c[u] = q < e ? __ldcs(lcol + q) : -1;
+			a[u] = q < e ? (double)__ldcs(lval + q) : 0.0;
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			xv[u] = c[u] >= 0 ? (double)__ldg(x + c[u]) : 0.0;
+			if (IN == 1 && c[u] >= 0) xv[u] *= __ldg(dinv_in + c[u]);
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++)
+			if (c[u] >= 0) sum = fma(a[u], xv[u], sum);
+	}
+	sum = warp_sum(sum);
+	if (BLOCK) {
+		if ((tid & 31) == 0) red[tid >> 5] = sum;
+		__syncthreads();
+		double t = 0.0;
+#pragma unroll
+		for (int w = 0; w < 8; w++) t += red[w];
+		__syncthreads(); // red is free for the next row
+		sum = t;
+	}
+	return sum;
+}
+
+// The long rows of a product or pass (blockDim 256): out(r, sum) by thread 0
+// of the block or lane 0 of the warp that summed row r.
+template <typename VT, typename XT, int IN, typename F>
+__device__ __forceinline__ void long_rows(const sell_long<VT> &lg, const XT *__restrict__ x,
+                                          const double *__restrict__ dinv_in, F out) {
+	if (!lg.nlong) return;
+	__shared__ double red[8];
+	for (int i = blockIdx.x; i < lg.nvlong; i += gridDim.x) {
+		const double s = long_row_sum<VT, XT, IN, true, 4>(__ldg(lg.off + i), __ldg(lg.off + i + 1), threadIdx.x,
+		                                                   lg.col, lg.val, x, dinv_in, red);
+		if (threadIdx.x == 0) out(__ldg(lg.row + i), s);
+	}
+	const int lane = threadIdx.x & 31;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int i = lg.nvlong + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < lg.nlong; i += nwarps) {
+		const double s = long_row_sum<VT, XT, IN, false, 8>(__ldg(lg.off + i), __ldg(lg.off + i + 1), lane, lg.col,
+		                                                    lg.val, x, dinv_in, nullptr);
+		if (lane == 0) out(__ldg(lg.row + i), s);
+	}
 }
 
 // ---- tiled form ----------------------------------------------------------
@@ -230,7 +355,7 @@ __global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, c
 
 template <typename VT>
 __global__ void k_sell_fill(int n, const int *rp, const int *ci, const double *v, int skip, const int *perm,
-                            const long long *off, int *scol, VT *sval) {
+                            int longlen, const long long *off, int *scol, VT *sval) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
 	const int slice = t / SELL_C, l = t % SELL_C;
@@ -239,7 +364,8 @@ __global__ void k_sell_fill(int n, const int *rp, const int *ci, const double *v
 	const long long base = off[slice];
 	const int w = (int)((off[slice + 1] - base) / SELL_C);
 	const int b = r < n ? rp[r] + skip : 0;
-	const int len = r < n ? rp[r + 1] - b : 0;
+	int len = r < n ? rp[r + 1] - b : 0;
+	if (longlen > 0 && len > longlen) len = 0; // a long row: padding only
 	for (int k = 0; k < w; k++) {
 		const long long p = base + (long long)SELL_C * k + l;
 		if (k < len) {
@@ -261,8 +387,13 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
                                                     const int *__restrict__ scol, const VT *__restrict__ sval,
                                                     const double *__restrict__ xin, const double *__restrict__ dinv_in,
                                                     const double *__restrict__ xrhs,
-                                                    const double *__restrict__ dinv_out, double *__restrict__ y) {
+                                                    const double *__restrict__ dinv_out, double *__restrict__ y,
+                                                    sell_long<VT> lg) {
 	constexpr int SPW = 32 / SELL_C; // slices per warp
+	long_rows<VT, double, IN>(lg, xin, dinv_in, [&](int r, double sum) {
+		if (OUT == 0) y[r] = sum;
+		else y[r] = (xrhs[r] - sum) * dinv_out[r];
+	});
 	const int lane = threadIdx.x & 31;
 	const int grp = lane / SELL_C, l = lane % SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
@@ -272,6 +403,7 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
 		if (slice >= nsl) continue;
 		const long long base = __ldg(off + slice);
 		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
 		const int *cp = scol + base + l;
 		const VT *vp = sval + base + l;
 		double sum = 0.0;
@@ -300,7 +432,7 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
 			sum = fma(a, xv, sum);
 		}
 		const int t = slice * SELL_C + l;
-		if (t < n) {
+		if (t < n && !((lm >> l) & 1u)) {
 			const int r = perm ? __ldg(perm + t) : t;
 			if (OUT == 0) y[r] = sum;
 			else y[r] = (xrhs[r] - sum) * dinv_out[r];
@@ -318,8 +450,13 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
                                                       const int *__restrict__ scol, const float *__restrict__ sval,
                                                       const float *__restrict__ x32, const double *__restrict__ rhs,
                                                       const double *__restrict__ dinv, double *__restrict__ y,
-                                                      float *__restrict__ y32) {
+                                                      float *__restrict__ y32, sell_long<float> lg) {
 	constexpr int SPW = 32 / SELL_C;
+	long_rows<float, float, 0>(lg, x32, nullptr, [&](int r, double sum) {
+		const double v = (rhs[r] - sum) * dinv[r];
+		if (OUT64) y[r] = v;
+		else y32[r] = (float)v;
+	});
 	const int lane = threadIdx.x & 31;
 	const int grp = lane / SELL_C, l = lane % SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
@@ -329,6 +466,7 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
 		if (slice >= nsl) continue;
 		const long long base = __ldg(off + slice);
 		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
 		const int *cp = scol + base + l;
 		const float *vp = sval + base + l;
 		double sum = 0.0;
@@ -351,7 +489,7 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
 			sum = fma((double)__ldcs(vp + SELL_C * k), (double)__ldg(x32 + c), sum);
 		}
 		const int t = slice * SELL_C + l;
-		if (t < n) {
+		if (t < n && !((lm >> l) & 1u)) {
 			const int r = perm ? __ldg(perm + t) : t;
 			const double v = (rhs[r] - sum) * dinv[r];
 			if (OUT64) y[r] = v;
@@ -463,12 +601,84 @@ static int bsg_sell_tile(bsg_ctx *c, int n, const int *rp, const int *ci, int sk
 	return BSG_OK;
 }
 
+// The long rows of a CSR matrix into m->lrow / loff / lcol / lval: first the
+// rows of more than SELL_VLONG entries, then those of more than SELL_LONG,
+// each group in row order.
+template <typename VT>
+static int bsg_sell_long(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, bsg_sell *m) {
+	cudaStream_t s = c->stream;
+	unsigned char *fv, *fl;
+	int *iota, *sel, *num;
+	BSG_CUDA(cudaMallocAsync(&fv, n, s));
+	BSG_CUDA(cudaMallocAsync(&fl, n, s));
+	BSG_CUDA(cudaMallocAsync(&iota, sizeof(int) * n, s));
+	BSG_CUDA(cudaMallocAsync(&sel, sizeof(int) * 2 * (size_t)n, s));
+	BSG_CUDA(cudaMallocAsync(&num, sizeof(int) * 2, s));
+	const int g = nb(n, 256) < BSG_SMS * 8 ? nb(n, 256) : BSG_SMS * 8;
+	BSG_COUNT(1);
+	k_long_flags<<<g, 256, 0, s>>>(n, rp, skip, fv, fl, iota);
+	size_t tb = 0;
+	BSG_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, iota, fv, sel, num, n, s));
+	void *tmp;
+	BSG_CUDA(cudaMallocAsync(&tmp, tb > 0 ? tb : 1, s));
+	BSG_CUDA(cub::DeviceSelect::Flagged(tmp, tb, iota, fv, sel, num, n, s));
+	BSG_CUDA(cub::DeviceSelect::Flagged(tmp, tb, iota, fl, sel + n, num + 1, n, s));
+	int h[2] = {0, 0};
+	BSG_CUDA(cudaMemcpyAsync(h, num, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	cudaFreeAsync(tmp, s);
+	cudaFreeAsync(fv, s);
+	cudaFreeAsync(fl, s);
+	cudaFreeAsync(iota, s);
+	cudaFreeAsync(num, s);
+	const int nl = h[0] + h[1];
+	if (nl == 0) {
+		cudaFreeAsync(sel, s);
+		return BSG_OK;
+	}
+	m->nlong = nl;
+	m->nvlong = h[0];
+	BSG_CUDA(cudaMallocAsync(&m->lrow, sizeof(int) * nl, s));
+	if (h[0]) BSG_CUDA(cudaMemcpyAsync(m->lrow, sel, sizeof(int) * h[0], cudaMemcpyDeviceToDevice, s));
+	if (h[1]) BSG_CUDA(cudaMemcpyAsync(m->lrow + h[0], sel + n, sizeof(int) * h[1], cudaMemcpyDeviceToDevice, s));
+	cudaFreeAsync(sel, s);
+	long long *len;
+	BSG_CUDA(cudaMallocAsync(&len, sizeof(long long) * (nl + 1), s));
+	BSG_CUDA(cudaMallocAsync(&m->loff, sizeof(long long) * (nl + 1), s));
+	BSG_COUNT(1);
+	k_long_len<<<nb(nl + 1, 256), 256, 0, s>>>(nl, m->lrow, rp, skip, len);
+	size_t ts = 0;
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, ts, len, m->loff, nl + 1, s));
+	BSG_CUDA(cudaMallocAsync(&tmp, ts > 0 ? ts : 1, s));
+	BSG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, ts, len, m->loff, nl + 1, s));
+	long long total = 0;
+	BSG_CUDA(cudaMemcpyAsync(&total, m->loff + nl, sizeof(long long), cudaMemcpyDeviceToHost, s));
+	BSG_CUDA(cudaStreamSynchronize(s));
+	cudaFreeAsync(tmp, s);
+	cudaFreeAsync(len, s);
+	BSG_CUDA(cudaMallocAsync(&m->lcol, sizeof(int) * total, s));
+	BSG_CUDA(cudaMallocAsync(&m->lval, sizeof(VT) * total, s));
+	BSG_COUNT(1);
+	k_long_fill<VT><<<nb((long long)nl * 32, 256) < BSG_SMS * 8 ? nb((long long)nl * 32, 256) : BSG_SMS * 8, 256, 0,
+	                  s>>>(nl, m->lrow, m->loff, rp, ci, v, skip, m->lcol, (VT *)m->lval);
+	BSG_CUDA(cudaGetLastError());
+	m->entries += total;
+	return BSG_OK;
+}
+
 template <typename VT>
 int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const double *v, int skip, bsg_sell *out,
                      int sigma, int tiled) {
 	cudaStream_t s = c->stream;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
 	out->perm = nullptr;
+	out->entries = 0;
+	if (n > 0) {
+		int rc = bsg_sell_long<VT>(c, n, rp, ci, v, skip, out);
+		if (rc) return rc;
+	}
+	// the tiled form has no long rows
+	if (out->nlong) tiled = 0;
 	if (sigma > 0 && n > 0) {
 		// SELL-C-sigma: rows sorted by length inside windows of sigma rows
 		unsigned long long *keys, *k2;
@@ -488,12 +698,15 @@ int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const doub
 		BSG_CUDA(cub::DeviceRadixSort::SortPairs(d_t2, t2, keys, k2, vals, out->perm, n, 0, end_bit, s));
 		cudaFreeAsync(keys, s); cudaFreeAsync(k2, s); cudaFreeAsync(vals, s); cudaFreeAsync(d_t2, s);
 	}
+	const int longlen = out->nlong ? SELL_LONG : 0;
+	if (out->nlong) BSG_CUDA(cudaMallocAsync(&out->lmask, nsl > 0 ? nsl : 1, s));
 	long long *width;
 	BSG_CUDA(cudaMallocAsync(&width, sizeof(long long) * (nsl + 1), s));
 	BSG_CUDA(cudaMallocAsync(&out->off, sizeof(long long) * (nsl + 1), s));
 	BSG_CUDA(cudaMemsetAsync(width + nsl, 0, sizeof(long long), s));
 	BSG_COUNT(2);
-	k_sell_width<<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, skip, out->perm, tiled, width);
+	k_sell_width<<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, skip, out->perm, tiled, longlen, width,
+	                                                               out->lmask);
 	// off = exclusive scan of the slice sizes
 	size_t tmp = 0;
 	BSG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, width, out->off, nsl + 1, s));
@@ -504,11 +717,11 @@ int bsg_sell_build_t(bsg_ctx *c, int n, const int *rp, const int *ci, const doub
 	BSG_CUDA(cudaMemcpyAsync(&total, out->off + nsl, sizeof(long long), cudaMemcpyDeviceToHost, s));
 	BSG_CUDA(cudaStreamSynchronize(s));
 	out->n = n;
-	out->entries = total;
+	out->entries += total;
 	BSG_CUDA(cudaMallocAsync(&out->col, sizeof(int) * (total > 0 ? total : 1), s));
 	BSG_CUDA(cudaMallocAsync(&out->val, sizeof(VT) * (total > 0 ? total : 1), s));
 	out->fp32 = sizeof(VT) == 4;
-	k_sell_fill<VT><<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, ci, v, skip, out->perm, out->off,
+	k_sell_fill<VT><<<nb((long long)nsl * SELL_C, 256), 256, 0, s>>>(n, rp, ci, v, skip, out->perm, longlen, out->off,
 	                                                                out->col, (VT *)out->val);
 	BSG_CUDA(cudaGetLastError());
 	BSG_CUDA(cudaFreeAsync(width, s));
@@ -526,6 +739,17 @@ int bsg_sell_build(bsg_ctx *c, int n, const int *rp, const int *ci, const double
 
 void bsg_sell_free(bsg_sell *m, cudaStream_t s) {
 	bsg_sell_untile(m, s);
+	if (m->lrow) cudaFreeAsync(m->lrow, s);
+	if (m->loff) cudaFreeAsync(m->loff, s);
+	if (m->lcol) cudaFreeAsync(m->lcol, s);
+	if (m->lval) cudaFreeAsync(m->lval, s);
+	if (m->lmask) cudaFreeAsync(m->lmask, s);
+	m->lrow = nullptr;
+	m->loff = nullptr;
+	m->lcol = nullptr;
+	m->lval = nullptr;
+	m->lmask = nullptr;
+	m->nlong = m->nvlong = 0;
 	if (m->perm) cudaFreeAsync(m->perm, s);
 	m->perm = nullptr;
 	if (m->off) cudaFreeAsync(m->off, s);
@@ -548,10 +772,10 @@ int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y)
 	BSG_COUNT(1);
 	if (m->fp32)
 		k_sell_apply<float, 0, 0><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x,
-		                                                          nullptr, nullptr, nullptr, y);
+		                                                          nullptr, nullptr, nullptr, y, long_of<float>(m));
 	else
 		k_sell_apply<double, 0, 0><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const double *)m->val, x,
-		                                                           nullptr, nullptr, nullptr, y);
+		                                                           nullptr, nullptr, nullptr, y, long_of<double>(m));
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
@@ -563,12 +787,18 @@ int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const dou
 	const int g = sell_grid(m->n);
 	if (m->fp32) {
 		const float *v = (const float *)m->val;
-		if (scaled_in) k_sell_apply<float, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout);
-		else k_sell_apply<float, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout);
+		const sell_long<float> lg = long_of<float>(m);
+		if (scaled_in)
+			k_sell_apply<float, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout, lg);
+		else
+			k_sell_apply<float, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout, lg);
 	} else {
 		const double *v = (const double *)m->val;
-		if (scaled_in) k_sell_apply<double, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout);
-		else k_sell_apply<double, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout);
+		const sell_long<double> lg = long_of<double>(m);
+		if (scaled_in)
+			k_sell_apply<double, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout, lg);
+		else
+			k_sell_apply<double, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout, lg);
 	}
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
@@ -596,9 +826,9 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 				k_tsell_sweep32<0><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
 				                                                     m->tb, b, x, dinv, nullptr, a);
 		} else if (last) {
-			k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr);
+			k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr, long_of<float>(m));
 		} else {
-			k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a);
+			k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a, long_of<float>(m));
 		}
 		float *t = a; a = b; b = t;
 	}
@@ -615,7 +845,7 @@ int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, co
 		    m->n, m->ntile, m->perm, m->off, m->cpair, (const float *)m->val, m->tb_off, m->tb, x32, x, dinv, yout, nullptr);
 	else
 		k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x,
-		                                                  dinv, yout, nullptr);
+		                                                  dinv, yout, nullptr, long_of<float>(m));
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }

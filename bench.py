@@ -541,7 +541,7 @@ def main():
     L.bsg_fct_info(fh, C.byref(fn), C.byref(fnnz), None, None, None, None)
     nnz_strict = fnnz.value - n
     spmv_bytes = nnz.value * 12 + (n + 1) * 4 + 2 * n * 8
-    st = (C.c_longlong * 6)()
+    st = (C.c_longlong * 9)()
     bsg._check(L.bsg_sell_stats(None, fh, st))
     tiled = st[4] > 0  # the backward sweep timed below
     # algorithmic bytes of one triangular solve pass with an FP32 factor, the

@@ -344,8 +344,10 @@ int bsg_fact_stats(unsigned long long *out, int nout);
 /* Stored entries, padding included, of the sliced copies the bandwidth-bound
  * products read: out[0] matrix, out[1] strict L, out[2] strict U; out[3] /
  * out[4] tiles of the tiled FP32 L / U sweeps (0: untiled, columns gathered
- * from global memory), out[5] most 32-float x blocks one tile stages.
- * out holds 6 values. */
+ * from global memory), out[5] most 32-float x blocks one tile stages;
+ * out[6] / out[7] / out[8] rows of the matrix / L / U longer than 256
+ * entries, kept out of the slices and summed by a warp or block each.
+ * out holds 9 values. */
 int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out);
 
 #ifdef __cplusplus
