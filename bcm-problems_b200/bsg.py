@@ -100,6 +100,7 @@ def lib():
         "bsg_lanczos_dev": (i_, [vp, vp, vp, vp, vp, C.POINTER(Param)]),
         "bsg_solve_t_dev": (i_, [vp, vp, i_, i_, i_, vp, vp]),
         "bsg_sell_stats": (i_, [vp, vp, C.POINTER(C.c_longlong)]),
+        "bsg_solve_multi_dev": (i_, [vp, vp, i_, i_, i_, i_, vp, vp]),
         "bsg_fct_export_block": (i_, [vp, ip, ip, ip, ip, dp, dp]),
         "bsg_mat_vbsr": (i_, [vp, i_, ip, ip, ip, dp, i_, pp]),
         "bsg_read_mtr_bin": (i_, [C.c_char_p, C.POINTER(C.c_longlong), ip, ip, ip, ip, ip, ip, ip, dp]),
@@ -312,6 +313,11 @@ class Factor:
 
     def solve_u(self, x, y, mode=0, nsweeps=3):
         _check(lib().bsg_solve_u_dev(self.ctx.h, self.h, mode, nsweeps, _ptr(x), _ptr(y)))
+
+    def solve_multi(self, lower, X, Y, mode=0, nsweeps=3):
+        """Solves with L (lower) or U for the rows of X (nrhs, n) into Y."""
+        _check(lib().bsg_solve_multi_dev(self.ctx.h, self.h, int(lower), mode, nsweeps, X.shape[0], _ptr(X),
+                                         _ptr(Y)))
 
     def solve_ut(self, x, y, mode=0, nsweeps=3):
         """y = U^{-T} x (SolveL on U's storage)."""

@@ -26,8 +26,8 @@
 #include <vector>
 
 int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s);
-int bsg_precond_apply(bsg_ctx *c, const bsg_fct *f, const bsg_param *p, const double *r, double *z, double *tmp,
-                      double *work);
+int bsg_precond_apply_multi(bsg_ctx *c, const bsg_fct *f, const bsg_param *p, int nr, const double *r, double *z,
+                            double *tmp, double *work);
 
 namespace {
 
@@ -357,8 +357,8 @@ extern "C" int bsg_pcg_batch_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f,
 	if (!rc) rc = alloc((void **)&z, sizeof(double) * N);
 	if (!rc) rc = alloc((void **)&pp, sizeof(double) * N);
 	if (!rc) rc = alloc((void **)&q, sizeof(double) * N);
-	if (!rc) rc = alloc((void **)&t, sizeof(double) * n);
-	if (!rc) rc = alloc((void **)&w, sizeof(double) * n);
+	if (!rc) rc = alloc((void **)&t, sizeof(double) * N);
+	if (!rc) rc = alloc((void **)&w, sizeof(double) * N);
 	if (!rc) rc = alloc((void **)&sc, sizeof(double) * SC_N * nsys);
 	if (!rc) rc = alloc((void **)&si, sizeof(int) * SI_N * nsys);
 	if (!rc) rc = alloc((void **)&segid, sizeof(int) * n);
@@ -459,12 +459,9 @@ extern "C" int bsg_pcg_batch_dev(bsg_ctx *c, const bsg_mat *m, const bsg_fct *f,
 		k_bdots<1><<<dgrid, 256, 0, st>>>(ch.nchunk, ch.beg, ch.end, x0, y0, nullptr, nullptr, part);
 		k_bfinal<1><<<fgrid, 256, 0, st>>>(nsys, ch.first, part, sc, s0, s0);
 	};
+	// every right-hand side in one pass over the factor per sweep
 	auto precond_all = [&](const double *src, double *dst) {
-		for (int k = 0; k < nrhs; k++) {
-			int e = bsg_precond_apply(c, f, p, src + k * n, dst + k * n, t, w);
-			if (e) return e;
-		}
-		return 0;
+		return bsg_precond_apply_multi(c, f, p, nrhs, src, dst, t, w);
 	};
 
 	BCHK(cudaMemsetAsync(c->d_stat, 0, sizeof(bsg_devstat), st));

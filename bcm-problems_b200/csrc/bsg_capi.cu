@@ -33,18 +33,20 @@ extern "C" unsigned long long bsg_launch_count(void) { return g_bsg_launches; }
 // [1] strict L rows, [2] strict U rows of the factor (0 where absent);
 // [3] / [4] tiles of the tiled L / U form (0: untiled), [5] most staged x
 // blocks (32 floats) of one tile over both; [6] / [7] / [8] long rows of the
-// matrix / L / U (rows summed outside the slices).
+// matrix / L / U (rows summed outside the slices).  A block factor reports
+// its block SELL copies: 9 entries a block, long block rows.
 extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out) {
 	if (!out) return bsg_set_error(BSG_ERR_ARG, "bsg_sell_stats: null output");
 	out[0] = m ? m->sell.entries : 0;
-	out[1] = f ? f->sl.entries : 0;
-	out[2] = f ? f->su.entries : 0;
+	// a block factor's copies count 9 entries a block
+	out[1] = f ? (f->d_bia ? 9 * f->bsl.blocks : f->sl.entries) : 0;
+	out[2] = f ? (f->d_bia ? 9 * f->bsu.blocks : f->su.entries) : 0;
 	out[3] = f ? f->sl.ntile : 0;
 	out[4] = f ? f->su.ntile : 0;
 	out[5] = f ? (f->sl.tmax > f->su.tmax ? f->sl.tmax : f->su.tmax) : 0;
 	out[6] = m ? m->sell.nlong : 0;
-	out[7] = f ? f->sl.nlong : 0;
-	out[8] = f ? f->su.nlong : 0;
+	out[7] = f ? (f->d_bia ? f->bsl.nlong : f->sl.nlong) : 0;
+	out[8] = f ? (f->d_bia ? f->bsu.nlong : f->su.nlong) : 0;
 	return BSG_OK;
 }
 
@@ -679,6 +681,8 @@ extern "C" int bsg_fct_free(bsg_fct *f) {
 	bsg_sell_free(&f->su, s);
 	bsg_sell_free(&f->slt, s);
 	bsg_sell_free(&f->sut, s);
+	bsg_bsell_free(&f->bsl, s);
+	bsg_bsell_free(&f->bsu, s);
 	for (void *q : {(void *)f->d_utr_v, (void *)f->d_utr_f, (void *)f->d_l_f})
 		if (q) cudaFreeAsync(q, s);
 	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);
@@ -724,6 +728,17 @@ extern "C" int bsg_solve_u_dev(bsg_ctx *c, const bsg_fct *f, int mode, int nswee
 	return rc;
 }
 
+extern "C" int bsg_solve_multi_dev(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nrhs,
+                                   const double *x, double *y) {
+	if (!c || !f || !x || !y || x == y || nrhs < 1)
+		return bsg_set_error(BSG_ERR_ARG, "bsg_solve_multi_dev: bad argument");
+	double *work = nullptr;
+	if (mode == 1 && nsweeps > 1) BSG_CUDA(cudaMallocAsync(&work, sizeof(double) * f->n * (size_t)nrhs, c->stream));
+	int rc = bsg_trisolve_multi(c, f, lower ? 1 : 0, mode, nsweeps, nrhs, x, y, work);
+	if (work) cudaFreeAsync(work, c->stream);
+	if (!rc) rc = bsg_check_devstat(c);
+	return rc;
+}
 
 // ---- host-buffer drivers ----------------------------------------------------
 

@@ -153,6 +153,43 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
                       float *work32, double *yout);
 int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, const double *dinv, const float *x32,
                           double *yout);
+// The same for nr vectors at stride n, the matrix read once per 8 vectors;
+// every vector gets the bits of a single-vector call.  work32: 2 n nr floats.
+int bsg_sell_sweep_multi(cudaStream_t s, const bsg_sell *m, int nr, const double *x, const double *dinv,
+                         const double *yin, int scaled_in, double *yout);
+int bsg_sell_sweeps32_multi(cudaStream_t s, const bsg_sell *m, int nr, const double *x, const double *dinv,
+                            int nsweeps, float *work32, double *yout);
+
+// Block SELL of 3 x 3 blocks (k_bsell.cu): slices of 8 block rows, block k
+// of slot l at off_s + 8 k + l (column: block column), its 9 values row-major
+// in planes: value p at 9 off_s + 72 k + 8 p + l.  Block rows of more than
+// 64 blocks are kept out of the slices as block CSR (lrow / loff / lcol /
+// lval, 9 values a block), summed by a warp each, or by a block of 256
+// threads beyond 1024 blocks (the first nvlong of them).
+struct bsg_bsell {
+	int nb = 0;
+	int fp32 = 0;
+	long long blocks = 0;     // stored blocks, padding and long rows included
+	long long *off = nullptr; // slice offsets in blocks [nslices + 1]
+	int *col = nullptr;
+	void *val = nullptr;      // float or double
+	int nlong = 0, nvlong = 0;
+	int *lrow = nullptr;
+	long long *loff = nullptr;
+	int *lcol = nullptr;
+	void *lval = nullptr;
+	unsigned char *lmask = nullptr;
+};
+// From the point CSR of a strict block part (every block's 9 entries stored,
+// blocks in column order in each point row).
+int bsg_bsell_build(bsg_ctx *c, int nb, const int *rp, const int *ci, const double *v, int fp32, bsg_bsell *out);
+void bsg_bsell_free(bsg_bsell *m, cudaStream_t s);
+// Block Jacobi sweeps for nr vectors at stride 3 nb: y0 = D x, then
+// nsweeps - 1 passes y <- D (x - N y) (D: nb column-major 3 x 3 blocks), one
+// kernel a pass, the factor read once per 8 vectors; work: 3 nb nr doubles
+// (nsweeps > 1).  Every vector gets the bits of a single-vector call.
+int bsg_bsell_sweeps(cudaStream_t s, const bsg_bsell *m, const double *d, int nsweeps, int nr, const double *x,
+                     double *y, double *work);
 
 struct bsg_mat {
 	bsg_ctx *ctx;
@@ -208,6 +245,7 @@ struct bsg_fct {
 	int *d_bia, *d_bja;
 	double *d_bl, *d_bu;
 	double *d_bdl, *d_bdu, *d_ones;
+	bsg_bsell bsl, bsu;           // block SELL copies of the strict L / U block rows (sweeps)
 };
 
 // ---- launch accounting ------------------------------------------------------
@@ -234,3 +272,9 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct *
 int bsg_bfact_make_fp32(bsg_fct *f);
 int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                          double *work);
+// nr triangular solves with one factor, vectors at stride n (work: n nr
+// doubles); sweeps read the factor once for up to 8 vectors.
+int bsg_trisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nr, const double *x,
+                       double *y, double *work);
+int bsg_btrisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nr, const double *x,
+                        double *y, double *work);

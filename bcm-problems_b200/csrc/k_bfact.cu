@@ -612,17 +612,6 @@ __global__ void k_bdiag_pack(int nb, const int *fi, const double *fl, const doub
 		}
 }
 // y = D t per block (D column-major), t and y may alias
-__global__ void k_bdiag_apply(int nb, const double *d, const double *t, double *y) {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= nb) return;
-	const double *b = d + (size_t)i * 9;
-	const double t0 = t[3 * i], t1 = t[3 * i + 1], t2 = t[3 * i + 2];
-	for (int r = 0; r < 3; r++) y[3 * i + r] = b[r] * t0 + b[r + 3] * t1 + b[r + 6] * t2;
-}
-__global__ void k_fill_d(long long n, double *x, double v) {
-	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-		x[i] = v;
-}
 // Exact block solve, one warp walking the block rows in dependency order
 // (lower: ascending, upper: descending): y_i = D_i (x_i - N_i y) with N's
 // point rows 3 i .. 3 i + 2 gathered by the lanes.  Latency-bound: the
@@ -877,12 +866,10 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct *
 	f->nnz_strict = (int)nstrict;
 	FCUDA(cudaMallocAsync(&f->d_bdl, sizeof(double) * 9 * (size_t)nb, st));
 	FCUDA(cudaMallocAsync(&f->d_bdu, sizeof(double) * 9 * (size_t)nb, st));
-	FCUDA(cudaMallocAsync(&f->d_ones, sizeof(double) * n, st));
-	BSG_COUNT(2);
+	BSG_COUNT(1);
 	k_bdiag_pack<<<nb_(nb, 256), 256, 0, st>>>(nb, f->d_bia, f->d_bl, f->d_bu, f->d_bdl, f->d_bdu);
-	k_fill_d<<<nb_(n, 256) < BSG_SMS * 8 ? nb_(n, 256) : BSG_SMS * 8, 256, 0, st>>>(n, f->d_ones, 1.0);
-	int rc3 = bsg_sell_build(c, n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 0, &f->sl, 0);
-	if (!rc3) rc3 = bsg_sell_build(c, n, f->d_ur_i, f->d_ur_j, f->d_ur_v, 0, 0, &f->su, 0);
+	int rc3 = bsg_bsell_build(c, nb, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, &f->bsl);
+	if (!rc3) rc3 = bsg_bsell_build(c, nb, f->d_ur_i, f->d_ur_j, f->d_ur_v, 0, &f->bsu);
 	if (rc3) return fail(rc3);
 	FCUDA(cudaStreamSynchronize(st));
 #undef FCUDA
@@ -893,10 +880,10 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct *
 // FP32 values for the sweeps' strict parts (block diagonals stay FP64)
 int bsg_bfact_make_fp32(bsg_fct *f) {
 	cudaStream_t s = f->ctx->stream;
-	bsg_sell_free(&f->sl, s);
-	bsg_sell_free(&f->su, s);
-	int rc = bsg_sell_build(f->ctx, f->n, f->d_lr_i, f->d_lr_j, f->d_lr_v, 0, 1, &f->sl, 0);
-	if (!rc) rc = bsg_sell_build(f->ctx, f->n, f->d_ur_i, f->d_ur_j, f->d_ur_v, 0, 1, &f->su, 0);
+	bsg_bsell_free(&f->bsl, s);
+	bsg_bsell_free(&f->bsu, s);
+	int rc = bsg_bsell_build(f->ctx, f->nb, f->d_lr_i, f->d_lr_j, f->d_lr_v, 1, &f->bsl);
+	if (!rc) rc = bsg_bsell_build(f->ctx, f->nb, f->d_ur_i, f->d_ur_j, f->d_ur_v, 1, &f->bsu);
 	if (rc) return rc;
 	f->fp32 = 1;
 	return BSG_OK;
@@ -904,7 +891,7 @@ int bsg_bfact_make_fp32(bsg_fct *f) {
 
 // Block triangular solve (lower: SolveL, else SolveU).  mode 0: exact (one
 // warp, rows in order); mode 1: nsweeps Jacobi iterates y <- D (x - N y)
-// from y = D x, work = n doubles.
+// from y = D x on the block SELL copies, work = n doubles.
 int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, const double *x, double *y,
                          double *work) {
 	cudaStream_t s = c->stream;
@@ -918,15 +905,24 @@ int bsg_btrisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int 
 		return BSG_OK;
 	}
 	if (nsweeps < 1) return bsg_set_error(BSG_ERR_ARG, "block sweeps: nsweeps >= 1");
-	if (nsweeps > 1 && !work) return bsg_set_error(BSG_ERR_ARG, "block sweeps: work vector missing");
-	BSG_COUNT(1);
-	k_bdiag_apply<<<nb_(nb, 256), 256, 0, s>>>(nb, d, x, y);
-	for (int k = 1; k < nsweeps; k++) {
-		int rc = bsg_sell_sweep(s, lower ? &f->sl : &f->su, x, f->d_ones, y, 0, work); // work = x - N y
-		if (rc) return rc;
-		BSG_COUNT(1);
-		k_bdiag_apply<<<nb_(nb, 256), 256, 0, s>>>(nb, d, work, y);
+	return bsg_bsell_sweeps(s, lower ? &f->bsl : &f->bsu, d, nsweeps, 1, x, y, work);
+}
+
+// nr block triangular solves, vectors at stride n = 3 nb (work: n nr
+// doubles).  Sweeps read the block SELL copy once per 8 vectors and give
+// every vector the bits of its own solve; exact solves run one at a time.
+int bsg_btrisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nr, const double *x,
+                        double *y, double *work) {
+	const int n = f->n;
+	if (mode == 0 || nr == 1) {
+		for (int q = 0; q < nr; q++) {
+			const size_t o = (size_t)q * n;
+			int rc = bsg_btrisolve_launch(c, f, lower, mode, nsweeps, x + o, y + o, work ? work + o : nullptr);
+			if (rc) return rc;
+		}
+		return BSG_OK;
 	}
-	BSG_CUDA(cudaGetLastError());
-	return BSG_OK;
+	if (nsweeps < 1) return bsg_set_error(BSG_ERR_ARG, "block sweeps: nsweeps >= 1");
+	return bsg_bsell_sweeps(c->stream, lower ? &f->bsl : &f->bsu, lower ? f->d_bdl : f->d_bdu, nsweeps, nr, x, y,
+	                        work);
 }

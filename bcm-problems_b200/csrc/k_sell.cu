@@ -498,6 +498,207 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
 	}
 }
 
+// ---- several vectors ------------------------------------------------------
+// The products of k_sell_apply / k_sell_sweep32 for nr <= NRM vectors at
+// stride ld (vector q at x + q ld), the matrix read once: every lane keeps
+// NRM sums.  Per vector the products are summed in the single-vector
+// kernels' order (entry by entry per lane, then the same trees for long
+// rows), so each vector's result is bit-identical to a single-vector call.
+
+template <typename VT, typename XT, int IN, bool BLOCK, int NRM>
+__device__ __forceinline__ void long_row_sum_m(long long b, long long e, int tid, int nr, long long ld,
+                                               const int *__restrict__ lcol, const VT *__restrict__ lval,
+                                               const XT *__restrict__ x, const double *__restrict__ dinv_in,
+                                               double (*red)[8], double *sum) {
+	constexpr int T = BLOCK ? 256 : 32;
+#pragma unroll
+	for (int q = 0; q < NRM; q++) sum[q] = 0.0;
+#pragma unroll 2
+	for (long long j = b + tid; j < e; j += T) {
+		const int c = __ldcs(lcol + j);
+		const double a = (double)__ldcs(lval + j);
+		const double di = IN == 1 ? __ldg(dinv_in + c) : 1.0;
+#pragma unroll
+		for (int q = 0; q < NRM; q++)
+			if (q < nr) {
+				double xv = (double)__ldg(x + q * ld + c);
+				if (IN == 1) xv *= di;
+				sum[q] = fma(a, xv, sum[q]);
+			}
+	}
+#pragma unroll
+	for (int q = 0; q < NRM; q++) sum[q] = warp_sum(sum[q]);
+	if (BLOCK) {
+		if ((tid & 31) == 0)
+#pragma unroll
+			for (int q = 0; q < NRM; q++) red[q][tid >> 5] = sum[q];
+		__syncthreads();
+#pragma unroll
+		for (int q = 0; q < NRM; q++) {
+			double t = 0.0;
+#pragma unroll
+			for (int w = 0; w < 8; w++) t += red[q][w];
+			sum[q] = t;
+		}
+		__syncthreads();
+	}
+}
+
+template <typename VT, typename XT, int IN, int NRM, typename F>
+__device__ __forceinline__ void long_rows_m(const sell_long<VT> &lg, int nr, long long ld, const XT *__restrict__ x,
+                                            const double *__restrict__ dinv_in, F out) {
+	if (!lg.nlong) return;
+	__shared__ double red[NRM][8];
+	double sum[NRM];
+	for (int i = blockIdx.x; i < lg.nvlong; i += gridDim.x) {
+		long_row_sum_m<VT, XT, IN, true, NRM>(__ldg(lg.off + i), __ldg(lg.off + i + 1), threadIdx.x, nr, ld, lg.col,
+		                                      lg.val, x, dinv_in, red, sum);
+		if (threadIdx.x == 0) {
+			const int r = __ldg(lg.row + i);
+#pragma unroll
+			for (int q = 0; q < NRM; q++)
+				if (q < nr) out(r, q, sum[q]);
+		}
+	}
+	const int lane = threadIdx.x & 31;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int i = lg.nvlong + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < lg.nlong; i += nwarps) {
+		long_row_sum_m<VT, XT, IN, false, NRM>(__ldg(lg.off + i), __ldg(lg.off + i + 1), lane, nr, ld, lg.col, lg.val,
+		                                       x, dinv_in, nullptr, sum);
+		if (lane == 0) {
+			const int r = __ldg(lg.row + i);
+#pragma unroll
+			for (int q = 0; q < NRM; q++)
+				if (q < nr) out(r, q, sum[q]);
+		}
+	}
+}
+
+// Slice part of the several-vector kernels: the NRM sums of slot l of a slice.
+template <typename VT, typename XT, int IN, int NRM>
+__device__ __forceinline__ void slice_sums_m(int w, const int *__restrict__ cp, const VT *__restrict__ vp, int nr,
+                                             long long ld, const XT *__restrict__ x,
+                                             const double *__restrict__ dinv_in, double *sum) {
+#pragma unroll
+	for (int q = 0; q < NRM; q++) sum[q] = 0.0;
+	int k = 0;
+	for (; k + 4 <= w; k += 4) {
+		int c[4];
+		double a[4];
+#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			c[u] = __ldcs(cp + SELL_C * (k + u));
+			a[u] = (double)__ldcs(vp + SELL_C * (k + u));
+		}
+#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			const double di = IN == 1 ? __ldg(dinv_in + c[u]) : 1.0;
+#pragma unroll
+			for (int q = 0; q < NRM; q++)
+				if (q < nr) {
+					double xv = (double)__ldg(x + q * ld + c[u]);
+					if (IN == 1) xv *= di;
+					sum[q] = fma(a[u], xv, sum[q]);
+				}
+		}
+	}
+	for (; k < w; k++) {
+		const int c = __ldcs(cp + SELL_C * k);
+		const double a = (double)__ldcs(vp + SELL_C * k);
+		const double di = IN == 1 ? __ldg(dinv_in + c) : 1.0;
+#pragma unroll
+		for (int q = 0; q < NRM; q++)
+			if (q < nr) {
+				double xv = (double)__ldg(x + q * ld + c);
+				if (IN == 1) xv *= di;
+				sum[q] = fma(a, xv, sum[q]);
+			}
+	}
+}
+
+// k_sell_apply for nr vectors (the pivots dinv_in / dinv_out are shared)
+template <typename VT, int IN, int OUT, int NRM>
+__global__ void __launch_bounds__(256) k_sell_apply_m(int n, int nr, long long ld, const int *__restrict__ perm,
+                                                      const long long *__restrict__ off,
+                                                      const int *__restrict__ scol, const VT *__restrict__ sval,
+                                                      const double *__restrict__ xin,
+                                                      const double *__restrict__ dinv_in,
+                                                      const double *__restrict__ xrhs,
+                                                      const double *__restrict__ dinv_out, double *__restrict__ y,
+                                                      sell_long<VT> lg) {
+	constexpr int SPW = 32 / SELL_C;
+	auto out = [&](int r, int q, double sum) {
+		if (OUT == 0) y[q * ld + r] = sum;
+		else y[q * ld + r] = (xrhs[q * ld + r] - sum) * dinv_out[r];
+	};
+	long_rows_m<VT, double, IN, NRM>(lg, nr, ld, xin, dinv_in, out);
+	const int lane = threadIdx.x & 31;
+	const int grp = lane / SELL_C, l = lane % SELL_C;
+	const int nsl = (n + SELL_C - 1) / SELL_C;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * SPW; s0 < nsl; s0 += nwarps * SPW) {
+		const int slice = s0 + grp;
+		if (slice >= nsl) continue;
+		const long long base = __ldg(off + slice);
+		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
+		double sum[NRM];
+		slice_sums_m<VT, double, IN, NRM>(w, scol + base + l, sval + base + l, nr, ld, xin, dinv_in, sum);
+		const int t = slice * SELL_C + l;
+		if (t < n && !((lm >> l) & 1u)) {
+			const int r = perm ? __ldg(perm + t) : t;
+#pragma unroll
+			for (int q = 0; q < NRM; q++)
+				if (q < nr) out(r, q, sum[q]);
+		}
+	}
+}
+
+// k_sell_sweep32 for nr vectors: FP32 iterates x32 + q ld in, out to
+// y + q ld (OUT64) or y32 + q ld
+template <int OUT64, int NRM>
+__global__ void __launch_bounds__(256) k_sell_sweep32_m(int n, int nr, long long ld, const int *__restrict__ perm,
+                                                        const long long *__restrict__ off,
+                                                        const int *__restrict__ scol, const float *__restrict__ sval,
+                                                        const float *__restrict__ x32, const double *__restrict__ rhs,
+                                                        const double *__restrict__ dinv, double *__restrict__ y,
+                                                        float *__restrict__ y32, sell_long<float> lg) {
+	constexpr int SPW = 32 / SELL_C;
+	auto out = [&](int r, int q, double sum) {
+		const double v = (rhs[q * ld + r] - sum) * dinv[r];
+		if (OUT64) y[q * ld + r] = v;
+		else y32[q * ld + r] = (float)v;
+	};
+	long_rows_m<float, float, 0, NRM>(lg, nr, ld, x32, nullptr, out);
+	const int lane = threadIdx.x & 31;
+	const int grp = lane / SELL_C, l = lane % SELL_C;
+	const int nsl = (n + SELL_C - 1) / SELL_C;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * SPW; s0 < nsl; s0 += nwarps * SPW) {
+		const int slice = s0 + grp;
+		if (slice >= nsl) continue;
+		const long long base = __ldg(off + slice);
+		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
+		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
+		double sum[NRM];
+		slice_sums_m<float, float, 0, NRM>(w, scol + base + l, sval + base + l, nr, ld, x32, nullptr, sum);
+		const int t = slice * SELL_C + l;
+		if (t < n && !((lm >> l) & 1u)) {
+			const int r = perm ? __ldg(perm + t) : t;
+#pragma unroll
+			for (int q = 0; q < NRM; q++)
+				if (q < nr) out(r, q, sum[q]);
+		}
+	}
+}
+
+// x32 + q n = (x + q n) * dinv rounded to FP32, q < nr
+__global__ void k_scale32_m(int n, int nr, const double *x, const double *dinv, float *x32) {
+	const long long N = (long long)n * nr;
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+		x32[i] = (float)(x[i] * dinv[i % n]);
+}
+
 // x32 = x * dinv rounded to FP32 (the first Jacobi iterate)
 __global__ void k_scale32(int n, const double *x, const double *dinv, float *x32) {
 	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -852,3 +1053,85 @@ int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, co
 
 // Stored entries (with padding) of a SELL matrix: the bytes a product reads.
 long long bsg_sell_entries(const bsg_sell *m) { return m->entries; }
+
+// ---- several vectors: launchers -------------------------------------------
+// Vectors at stride n (vector q at x + q n), nr >= 1; the matrix is read once
+// per group of up to 8 vectors.
+
+// One Jacobi pass for nr vectors: yout = (x - N yin) * dinv; scaled_in: yin
+// = x * dinv.
+int bsg_sell_sweep_multi(cudaStream_t s, const bsg_sell *m, int nr, const double *x, const double *dinv,
+                         const double *yin, int scaled_in, double *yout) {
+	const int n = m->n, g = sell_grid(n);
+	const long long ld = n;
+	for (int q0 = 0; q0 < nr; q0 += 8) {
+		const int k = nr - q0 < 8 ? nr - q0 : 8;
+		const long long o = (long long)q0 * n;
+		const double *xi = scaled_in ? x + o : yin + o;
+		BSG_COUNT(1);
+#define BSG_SW(VT, NRM)                                                                                                \
+	do {                                                                                                               \
+		const VT *v = (const VT *)m->val;                                                                              \
+		if (scaled_in)                                                                                                 \
+			k_sell_apply_m<VT, 1, 1, NRM><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, xi, dinv, x + o, dinv, \
+			                                                 yout + o, long_of<VT>(m));                                  \
+		else                                                                                                           \
+			k_sell_apply_m<VT, 0, 1, NRM><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, xi, nullptr, x + o,    \
+			                                                 dinv, yout + o, long_of<VT>(m));                            \
+	} while (0)
+		if (m->fp32) {
+			if (k <= 4) BSG_SW(float, 4);
+			else BSG_SW(float, 8);
+		} else {
+			if (k <= 4) BSG_SW(double, 4);
+			else BSG_SW(double, 8);
+		}
+#undef BSG_SW
+	}
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}
+
+// bsg_sell_sweeps32 for nr vectors; work32 holds 2 n nr floats.  The tiled
+// form is not used (its staging is per vector).
+int bsg_sell_sweeps32_multi(cudaStream_t s, const bsg_sell *m, int nr, const double *x, const double *dinv,
+                            int nsweeps, float *work32, double *yout) {
+	if (!m->fp32 || nsweeps < 2) return BSG_ERR_ARG;
+	const int n = m->n, g = sell_grid(n);
+	const long long ld = n;
+	float *a = work32, *b = work32 + (size_t)n * nr;
+	BSG_COUNT(1);
+	{
+		const long long N = (long long)n * nr;
+		const int gs = nb(N, 256) < BSG_SMS * 16 ? nb(N, 256) : BSG_SMS * 16;
+		k_scale32_m<<<gs, 256, 0, s>>>(n, nr, x, dinv, b);
+	}
+	const float *v = (const float *)m->val;
+	const sell_long<float> lg = long_of<float>(m);
+	for (int pass = 0; pass < nsweeps - 1; pass++) {
+		const bool last = pass == nsweeps - 2;
+		for (int q0 = 0; q0 < nr; q0 += 8) {
+			const int k = nr - q0 < 8 ? nr - q0 : 8;
+			const long long o = (long long)q0 * n;
+			BSG_COUNT(1);
+			if (last) {
+				if (k <= 4)
+					k_sell_sweep32_m<1, 4><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					                                         yout + o, nullptr, lg);
+				else
+					k_sell_sweep32_m<1, 8><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					                                         yout + o, nullptr, lg);
+			} else {
+				if (k <= 4)
+					k_sell_sweep32_m<0, 4><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					                                         nullptr, a + o, lg);
+				else
+					k_sell_sweep32_m<0, 8><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					                                         nullptr, a + o, lg);
+			}
+		}
+		float *t = a; a = b; b = t;
+	}
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}

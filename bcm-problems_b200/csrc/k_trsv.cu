@@ -291,6 +291,40 @@ int bsg_trisolve_launch(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 	return trisolve_impl(c, f, t, mode, nsweeps, x, y, work);
 }
 
+// nr solves with one factor, vectors at stride n; work holds n nr doubles
+// (needed for sweeps).  Sweeps read the untiled sliced copy once per 8
+// vectors and give every vector the bits of a single solve (the tiled FP32
+// sweeps sum in the same order); exact solves run one vector at a time.
+int bsg_trisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nr, const double *x,
+                       double *y, double *work) {
+	if (f->d_bia) return bsg_btrisolve_multi(c, f, lower, mode, nsweeps, nr, x, y, work);
+	const int n = f->n;
+	if (nr > 1 && mode != 0 && nsweeps >= 2) {
+		if (!work) return bsg_set_error(BSG_ERR_ARG, "sweeps of several vectors: work vector missing");
+		const bsg_sell *sl = lower ? &f->sl : &f->su;
+		const double *dinv = lower ? f->d_dinv_l : f->d_dinv_u;
+		if (f->fp32) return bsg_sell_sweeps32_multi(c->stream, sl, nr, x, dinv, nsweeps, reinterpret_cast<float *>(work), y);
+		// FP64: nsweeps - 1 passes, ping-pong so that the last lands in y
+		const int passes = nsweeps - 1;
+		double *bufs[2] = {y, work};
+		int cur = (passes + 1) % 2;
+		const double *yin = nullptr;
+		for (int p = 0; p < passes; p++) {
+			int rc = bsg_sell_sweep_multi(c->stream, sl, nr, x, dinv, yin, p == 0, bufs[cur]);
+			if (rc) return rc;
+			yin = bufs[cur];
+			cur ^= 1;
+		}
+		return BSG_OK;
+	}
+	for (int q = 0; q < nr; q++) {
+		const size_t o = (size_t)q * n;
+		int rc = bsg_trisolve_launch(c, f, lower, mode, nsweeps, x + o, y + o, work ? work + o : nullptr);
+		if (rc) return rc;
+	}
+	return BSG_OK;
+}
+
 // The transposed forms of an ILU2 factor: U^T rows are the L-row pattern
 // with U's values (the transposition that built the L rows, applied to U),
 // L^T rows are U's own pattern with L's values.  IC2 factors need none

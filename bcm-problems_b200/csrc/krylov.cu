@@ -80,6 +80,14 @@ int bsg_precond_apply(bsg_ctx *c, const bsg_fct *f, const bsg_param *p, const do
 	return bsg_trisolve_launch(c, f, 0, mode, p->nsweeps, tmp, z, work);
 }
 
+// bsg_precond_apply for nr vectors at stride n (tmp, work: n nr doubles)
+int bsg_precond_apply_multi(bsg_ctx *c, const bsg_fct *f, const bsg_param *p, int nr, const double *r, double *z,
+                            double *tmp, double *work) {
+	int rc = bsg_trisolve_multi(c, f, 1, p->trisolve, p->nsweeps, nr, r, tmp, work);
+	if (rc) return rc;
+	return bsg_trisolve_multi(c, f, 0, p->trisolve, p->nsweeps, nr, tmp, z, work);
+}
+
 int bsg_check_devstat(bsg_ctx *c);
 
 // FP64 true residual ||b - A x|| / ||b|| (one host sync).

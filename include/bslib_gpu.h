@@ -181,6 +181,13 @@ int bsg_fct_free(bsg_fct *f);
  * sweeps (approximate, fully parallel).  `work` may be NULL for mode 0. */
 int bsg_solve_l_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
 int bsg_solve_u_dev(bsg_ctx *ctx, const bsg_fct *f, int mode, int nsweeps, const double *d_x, double *d_y);
+/* nrhs solves with L (lower != 0) or U, vectors at stride n in d_x / d_y.
+ * Sweeps (mode 1) read the factor once for up to 8 vectors, and every vector
+ * gets the bits of its own bsg_solve_l_dev / bsg_solve_u_dev; exact solves
+ * run one vector at a time.  The batched PCG applies its preconditioner to
+ * all right-hand sides this way. */
+int bsg_solve_multi_dev(bsg_ctx *ctx, const bsg_fct *f, int lower, int mode, int nsweeps, int nrhs,
+                        const double *d_x, double *d_y);
 /* Transposed solves: which 0 with U^T (SolveL applied to U's storage), 1 with
  * L^T (SolveU applied to L's storage) -- the transposed preconditioner of
  * Bslib/lanczos.cpp:266-270; same modes.  The transposed forms of an ILU2
@@ -346,7 +353,10 @@ int bsg_fact_stats(unsigned long long *out, int nout);
  * out[4] tiles of the tiled FP32 L / U sweeps (0: untiled, columns gathered
  * from global memory), out[5] most 32-float x blocks one tile stages;
  * out[6] / out[7] / out[8] rows of the matrix / L / U longer than 256
- * entries, kept out of the slices and summed by a warp or block each.
+ * entries, kept out of the slices and summed by a warp or block each.  For
+ * a 3x3 block factor out[1] / out[2] count 9 entries per stored block of
+ * its block-sliced copies and out[7] / out[8] block rows of more than 64
+ * blocks.
  * out holds 9 values. */
 int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out);
 
