@@ -29,7 +29,8 @@
 // globaltimer.
 //
 // Storage.  A finished row keeps only its stored part: the diagonal (inverse
-// pivot) and the U / R entries sorted by column, in a pool, published by one
+// pivot; the column field of that entry holds the row's forward-solve depth)
+// and the U / R entries sorted by column, in a pool, published by one
 // 64-bit release store of (done | offset | length).  Dropped entries are not
 // kept: their theta compensations are pushed at once into a per-row 64-bit
 // fixed-point accumulator (scale set by tau2 * theta, bsg_comp_scale), whose
@@ -59,13 +60,20 @@
 #define FACT_WARPS 4
 #define CMAX 128   // members of C(i)
 #define HCAP 256   // distinct mask columns per row (power of two)
-#define PFCAP 512  // prefetched contributor entries per row
+#ifndef PFCAP
+#define PFCAP 256  // prefetched contributor entries per row
+#endif
 // capacities of the global-memory workspaces that take the rows that do not
 // fit the shared one (about 0.7 MB each), and how many there are
 #define BIG_SLOTS 64
 #define CMAX_BIG 8192
 #define HCAP_BIG 8192
 #define PFCAP_BIG 8192
+// members within MWIN rows below the row are kept in a bitmap (one shared
+// atomic per test-and-set), farther ones in the hash
+#ifndef MWIN
+#define MWIN 16384
+#endif
 #define W_EMPTY (-1)
 #define W_CLOSED (-2)
 
@@ -99,7 +107,7 @@ struct FactArgs {
 	int *done_count;
 	bsg_devstat *st;
 	unsigned long long *stats; // FACT_NSTAT counters (see bsg_fact_stats)
-	unsigned char *big_ws;     // BIG_SLOTS workspaces of GlobWS::bytes
+	unsigned char *big_ws;     // BIG_SLOTS workspaces of GlobWS<>::bytes
 	int *big_owner;            // 1 while a warp holds that workspace
 };
 
@@ -117,8 +125,11 @@ struct PhaseClock {
 // tried again by the same warp in a larger workspace in global memory
 // (GlobWS), so any row up to the big capacities factors.  Both expose the
 // same members; sc[] = {members, mask columns, kept columns, blocking row}.
+// IC2 (ILU false) keeps one value per column: its shared workspace has no
+// U-side arrays, so more warps fit on an SM.
+template <bool ILU>
 struct SmemWS {
-	static constexpr bool big = false;
+	static constexpr bool big = false, ilu = ILU;
 	static constexpr int cmax = CMAX, hcap = HCAP, pfcap = PFCAP;
 	int W[CMAX];           // members (discovery order, then sorted)
 	int Wp[CMAX];          // pool index of column i in that row (stored members)
@@ -128,28 +139,31 @@ struct SmemWS {
 	unsigned char Wfs[CMAX];
 	int Wb[CMAX + 1];      // prefetch segment bases (sorted order)
 	unsigned char Wst[CMAX]; // member state: 0 not closed, 1 closed, 2 applied
-	int wset[CMAX * 2];    // membership hash of W (keys)
+	int Wlv[CMAX];         // forward-solve depth of a closed member
+	int wset[CMAX * 2];    // membership hash of W (keys), members below i - MWIN
+	unsigned wbits[MWIN > 0 ? MWIN / 32 : 1]; // membership bitmap: bit i - 1 - k for member k
 	int hkey[HCAP];        // column accumulator
-	double hl[HCAP], hu[HCAP];
+	double hl[HCAP], hu[ILU ? HCAP : 1];
 	int lst[HCAP];         // extracted slots, then sorted
 	int lsts[HCAP];
 	int lkey[HCAP];        // columns of the extracted slots
 	unsigned pf_cf[PFCAP]; // prefetched contributor segments
 	short pf_slot[PFCAP];
-	double pf_l[PFCAP], pf_u[PFCAP];
+	double pf_l[PFCAP], pf_u[ILU ? PFCAP : 1];
 	int sc[4];
 };
 
+template <bool ILU>
 struct GlobWS {
-	static constexpr bool big = true;
+	static constexpr bool big = true, ilu = ILU;
 	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG;
 	static constexpr size_t bytes = 8 * (2 * (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
-	                                4 * (6 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
+	                                4 * (7 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
 	                                     4 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
-	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG;
+	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG + MWIN / 8;
 	double *hl, *hu, *pf_l, *pf_u;
-	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wb, *wset, *hkey, *lst, *lsts, *lkey, *sc;
-	unsigned *pf_cf;
+	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wlv, *Wb, *wset, *hkey, *lst, *lsts, *lkey, *sc;
+	unsigned *pf_cf, *wbits;
 	short *pf_slot;
 	unsigned char *Wf, *Wfs, *Wst;
 	__device__ explicit GlobWS(unsigned char *p) {
@@ -157,16 +171,39 @@ struct GlobWS {
 		pf_l = hu + HCAP_BIG; pf_u = pf_l + PFCAP_BIG;
 		W = reinterpret_cast<int *>(pf_u + PFCAP_BIG);
 		Wp = W + CMAX_BIG; We = Wp + CMAX_BIG; Ws = We + CMAX_BIG; Wps = Ws + CMAX_BIG; Wes = Wps + CMAX_BIG;
-		Wb = Wes + CMAX_BIG; wset = Wb + CMAX_BIG + 4;
+		Wlv = Wes + CMAX_BIG; Wb = Wlv + CMAX_BIG; wset = Wb + CMAX_BIG + 4;
 		hkey = wset + 2 * CMAX_BIG; lst = hkey + HCAP_BIG; lsts = lst + HCAP_BIG; lkey = lsts + HCAP_BIG;
 		pf_cf = reinterpret_cast<unsigned *>(lkey + HCAP_BIG);
 		sc = reinterpret_cast<int *>(pf_cf + PFCAP_BIG);
 		pf_slot = reinterpret_cast<short *>(sc + 4);
 		Wf = reinterpret_cast<unsigned char *>(pf_slot + PFCAP_BIG); Wfs = Wf + CMAX_BIG; Wst = Wfs + CMAX_BIG;
+		wbits = reinterpret_cast<unsigned *>(Wst + CMAX_BIG);
 	}
 };
 
 __device__ __forceinline__ unsigned hash_u(int k) { return (unsigned)k * 2654435761u; }
+
+// Exclusive prefix sum of v over the warp; total gets the sum.
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
+	int x = v;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		const int y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= o) x += y;
+	}
+	total = __shfl_sync(0xffffffffu, x, 31);
+	return x - v;
+}
+
+// Index of the last segment base <= k in b[0 .. n) (b ascending, b[0] <= k).
+__device__ __forceinline__ int seg_owner(const int *b, int n, int k) {
+	int lo = 0, hi = n - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (b[mid] <= k) lo = mid; else hi = mid - 1;
+	}
+	return lo;
+}
 
 // Find or insert column c; returns slot or -1 if full.
 template <class WS>
@@ -179,7 +216,7 @@ __device__ int hfind_insert(WS &s, int c) {
 			int old = atomicCAS(&s.hkey[h], -1, c);
 			if (old == -1) {
 				s.hl[h] = 0.0;
-				s.hu[h] = 0.0;
+				if (WS::ilu) s.hu[h] = 0.0;
 				return (int)h;
 			}
 			if (old == c) return (int)h;
@@ -189,11 +226,17 @@ __device__ int hfind_insert(WS &s, int c) {
 	return -1;
 }
 
-// Insert row k into the member set; 1 if new, 0 if present, -1 if full.
-// Most candidates are already members: probe with plain reads, CAS only
-// into an empty slot.
+// Insert row k into the member set of row i; 1 if new, 0 if present, -1
+// if full.  Near rows: one bit each.  Far rows: a hash; most candidates are
+// already members, so probe with plain reads and CAS only into an empty slot.
 template <class WS>
-__device__ int wset_insert(WS &s, int k) {
+__device__ int wset_insert(WS &s, int i, int k) {
+	const int d = i - 1 - k;
+	if (d < MWIN) {
+		const unsigned bit = 1u << (d & 31);
+		if (s.wbits[d >> 5] & bit) return 0;
+		return (atomicOr(&s.wbits[d >> 5], bit) & bit) ? 0 : 1;
+	}
 	unsigned h = hash_u(k) & (2 * s.cmax - 1);
 	for (int probe = 0; probe < 2 * s.cmax; probe++) {
 		int cur = s.wset[h];
@@ -276,13 +319,15 @@ __device__ int q_pop(const FactArgs &A) {
 
 // Admission.  nstat[j] packs the static contributors of row j (the rows k
 // < j with A(k,j) != 0) that are unfinished (bits 0..14) and unclaimed (bits
-// 15..29); bit 31 marks j claimed once.  Row j enters the queue when all of
-// them are claimed and at most one is unfinished: it then starts while its
-// last predecessor is being computed and waits for it.  Both counts only
-// fall, so exactly one decrement makes the condition true, and that one
-// queues the row.
+// 15..29); bit 30 marks j queued once, bit 31 claimed once.  Row j enters the
+// queue when all of them are claimed and at most one is unfinished: it then
+// starts while its last predecessor is being computed and waits for it.  A
+// row that another row waits for is queued earlier (promoted) if nobody has
+// queued it yet.  Bit 30 makes the first of the two the only one: a row is
+// queued once this way, and again only when a row it parked on finishes.
 #define ADM_ONE_FIN 1u
 #define ADM_ONE_CLAIM (1u << 15)
+#define ADM_QUEUED (1u << 30)
 #define ADM_CLAIMED (1u << 31)
 #ifndef BSG_ADMIT_UNFINISHED
 #define BSG_ADMIT_UNFINISHED 1
@@ -290,9 +335,12 @@ __device__ int q_pop(const FactArgs &A) {
 __device__ __forceinline__ bool admissible(unsigned v) {
 	return ((v >> 15) & 0x7fffu) == 0 && (v & 0x7fffu) <= BSG_ADMIT_UNFINISHED;
 }
+__device__ void enqueue_once(const FactArgs &A, int j) {
+	if (!(atomicOr(reinterpret_cast<unsigned *>(A.nstat) + j, ADM_QUEUED) & ADM_QUEUED)) q_push(A, j);
+}
 __device__ void admit_step(const FactArgs &A, int j, unsigned delta) {
 	const unsigned old = atomicSub(reinterpret_cast<unsigned *>(A.nstat) + j, delta);
-	if (!admissible(old) && admissible(old - delta)) q_push(A, j);
+	if (!admissible(old) && admissible(old - delta)) enqueue_once(A, j);
 }
 
 // Wait (lane 0) for row m while a warp is computing it: 1 once m is
@@ -309,6 +357,22 @@ __device__ int wait_row(const FactArgs &A, int m) {
 	}
 }
 
+// Row m, which row i needs, is unfinished and nobody computes it (lane 0):
+// queue it if it never was, then give an idle warp up to PROMOTE_WAIT_NS to
+// take it.  1: m finished meanwhile; 2: a warp computes m now; 0: neither
+// (the caller parks).
+#define PROMOTE_WAIT_NS 20000ull
+__device__ int promote(const FactArgs &A, int m) {
+	enqueue_once(A, m);
+	const unsigned long long t0 = globaltimer_ns();
+	for (;;) {
+		if (ld_acquire_u64(A.rec + m) & REC_DONE) return 1;
+		if (*(volatile int *)(A.inprog + m) != 0) return 2;
+		if (*(volatile int *)&A.st->code != 0 || globaltimer_ns() - t0 > PROMOTE_WAIT_NS) return 0;
+		__nanosleep(64);
+	}
+}
+
 // Park row i on unfinished row m (lane 0).
 __device__ void park(const FactArgs &A, int i, int m) {
 	for (;;) {
@@ -322,20 +386,20 @@ __device__ void park(const FactArgs &A, int i, int m) {
 
 // One closure pass, warp-cooperative: every unclosed member that is finished
 // gets closed.  The rows of those members are flattened into 16-byte chunks
-// spread over the lanes: a first sweep finds column i in each row (its pool
-// index and flag, or none: the member dropped i), a second inserts the
-// stored columns between the member and i (R x R skipped) into the member
-// set, new members taking slots by ballot.  Returns the number closed; the
-// smallest member still unfinished goes to pmin, the number of members the
-// pass discovered to added.
+// spread over the lanes and loaded once: column i is found in each row (its
+// pool index and flag, or none: the member dropped i), entry 0 carries the
+// member's forward-solve depth, and the stored columns between the member
+// and i (R x R skipped) are inserted into the member set, new members taking
+// slots by a prefix sum.  Returns the number closed; the smallest member
+// still unfinished goes to pmin, the number of members the pass discovered
+// to added.
 template <class WS>
 __device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax, int &pmin, int &err, int &added) {
 	const int nW = min(s.sc[0], s.cmax);
 	added = 0;
 	const unsigned lt = (1u << lane) - 1;
 	int pm = 0x7fffffff;
-	if (lane == 0) s.sc[2] = 0;
-	__syncwarp();
+	int nd = 0;
 	// finished unclosed members: W index, pool offset, length (scratch in Ws/Wps/Wes)
 	for (int base = 0; base < nW; base += 32) {
 		const int t = base + lane;
@@ -348,93 +412,117 @@ __device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax
 		const bool done = m >= 0 && (rec & REC_DONE);
 		if (m >= 0 && !done) pm = min(pm, m);
 		const unsigned b = __ballot_sync(0xffffffffu, done);
-		const int q0 = s.sc[2];
 		if (done) {
-			const int q = q0 + __popc(b & lt);
+			const int q = nd + __popc(b & lt);
 			s.Ws[q] = t;
 			s.Wps[q] = (int)REC_OFF(rec);
 			s.Wes[q] = REC_LEN(rec);
 			s.Wf[t] = (unsigned char)F_D; // until column i is found
 		}
-		__syncwarp();
-		if (lane == 0) s.sc[2] = q0 + __popc(b);
-		__syncwarp();
+		nd += __popc(b);
 	}
 	pmin = __reduce_min_sync(0xffffffffu, pm);
-	const int nd = s.sc[2];
 	if (nd == 0) return 0;
-	// chunk bases of the flattened rows
-	if (lane == 0) {
-		int acc = 0;
-		for (int d = 0; d < nd; d++) {
-			s.Wb[d] = acc;
-			acc += (s.Wes[d] + 3) >> 2;
-		}
-		s.Wb[nd] = acc;
-	}
 	__syncwarp();
-	const int T = s.Wb[nd];
-	// sweep 1: column i in each row
-	for (int k0 = 0; k0 < T; k0 += 32) {
-		const int k = k0 + lane;
-		if (k < T) {
-			int lo = 0, hi = nd - 1;
-			while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= k) lo = mid; else hi = mid - 1; }
-			const int ch = k - s.Wb[lo], len = s.Wes[lo];
-			const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
-			const unsigned e4[4] = {v.x, v.y, v.z, v.w};
+	// chunk bases of the flattened rows
+	int T = 0;
+	for (int d0 = 0; d0 < nd; d0 += 32) {
+		const int d = d0 + lane;
+		int tot;
+		const int ex = warp_excl_scan(d < nd ? (s.Wes[d] + 3) >> 2 : 0, lane, tot);
+		if (d < nd) s.Wb[d] = T + ex;
+		T += tot;
+	}
+	if (lane == 0) s.Wb[nd] = T;
+	__syncwarp();
+	// load every chunk once (the first NREG rounds stay in registers): column
+	// i and the depth
+	constexpr int NREG = 4;
+	uint4 reg[NREG];
+	int rown[NREG];
 #pragma unroll
-			for (int c = 0; c < 4; c++) {
-				const int e = 4 * ch + c;
-				if (e >= 1 && e < len && CF_COL(e4[c]) == i) {
-					const int t = s.Ws[lo];
-					s.Wp[t] = s.Wps[lo] + e;
-					s.Wf[t] = (unsigned char)CF_FLAG(e4[c]);
-				}
+	for (int r = 0; r < NREG; r++) {
+		reg[r] = make_uint4(0u, 0u, 0u, 0u);
+		rown[r] = 0;
+	}
+	for (int k0 = 0, r = 0; k0 < T; k0 += 32, r++) {
+		const int k = k0 + lane;
+		if (k >= T) continue;
+		const int lo = seg_owner(s.Wb, nd, k);
+		const int ch = k - s.Wb[lo], len = s.Wes[lo];
+		const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
+		const unsigned e4[4] = {v.x, v.y, v.z, v.w};
+		const int t = s.Ws[lo];
+		if (ch == 0) s.Wlv[t] = CF_COL(e4[0]);
+#pragma unroll
+		for (int c = 0; c < 4; c++) {
+			const int e = 4 * ch + c;
+			if (e >= 1 && e < len && CF_COL(e4[c]) == i) {
+				s.Wp[t] = s.Wps[lo] + e;
+				s.Wf[t] = (unsigned char)CF_FLAG(e4[c]);
 			}
 		}
+#pragma unroll
+		for (int q = 0; q < NREG; q++)
+			if (q == r) {
+				reg[q] = v;
+				rown[q] = lo;
+			}
 	}
 	__syncwarp();
-	// sweep 2: the stored columns between the member and i become members
-	for (int k0 = 0; k0 < T && !err; k0 += 32) {
+	// the stored columns between the member and i become members
+	for (int k0 = 0, r = 0; k0 < T && !err; k0 += 32, r++) {
 		const int k = k0 + lane;
 		unsigned e4[4] = {0u, 0u, 0u, 0u};
 		int pos = 0, ch = 0;
 		unsigned fi = F_D;
 		if (k < T) {
-			int lo = 0, hi = nd - 1;
-			while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= k) lo = mid; else hi = mid - 1; }
+			int lo = 0;
+			uint4 v = make_uint4(0u, 0u, 0u, 0u);
+			if (r < NREG) {
+#pragma unroll
+				for (int q = 0; q < NREG; q++)
+					if (q == r) {
+						v = reg[q];
+						lo = rown[q];
+					}
+			} else {
+				lo = seg_owner(s.Wb, nd, k);
+			}
 			ch = k - s.Wb[lo];
 			const int t = s.Ws[lo];
 			fi = s.Wf[t];
 			if (fi != F_D) {
 				pos = s.Wp[t] - s.Wps[lo];
 				if (4 * ch < pos) {
-					const uint4 v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
+					if (r >= NREG) v = __ldcg(reinterpret_cast<const uint4 *>(A.pool_cf + s.Wps[lo]) + ch);
 					e4[0] = v.x; e4[1] = v.y; e4[2] = v.z; e4[3] = v.w;
 				}
 			}
 		}
+		unsigned fresh = 0; // bit c: entry c is a new member
 #pragma unroll
 		for (int c = 0; c < 4; c++) {
 			const int e = 4 * ch + c;
-			const bool cand = e >= 1 && e < pos && !(fi == F_R && CF_FLAG(e4[c]) == F_R);
-			int isnew = 0;
-			if (cand) {
-				isnew = wset_insert(s, CF_COL(e4[c]));
+			if (e >= 1 && e < pos && !(fi == F_R && CF_FLAG(e4[c]) == F_R)) {
+				const int isnew = wset_insert(s, i, CF_COL(e4[c]));
 				if (isnew < 0) err = BSG_ERR_WORKSPACE;
+				else if (isnew) fresh |= 1u << c;
 			}
-			const unsigned b = __ballot_sync(0xffffffffu, isnew == 1);
-			const int q0 = s.sc[0];
-			if (isnew == 1) {
-				const int slot = q0 + __popc(b & lt);
+		}
+		int tot;
+		const int ex = warp_excl_scan(__popc(fresh), lane, tot);
+		const int q0 = s.sc[0];
+#pragma unroll
+		for (int c = 0; c < 4; c++)
+			if (fresh & (1u << c)) {
+				const int slot = q0 + ex + __popc(fresh & ((1u << c) - 1));
 				if (slot < s.cmax) { s.W[slot] = CF_COL(e4[c]); s.Wst[slot] = 0; } else err = BSG_ERR_WORKSPACE;
 			}
-			__syncwarp();
-			if (lane == 0) s.sc[0] = q0 + __popc(b);
-			added += __popc(b);
-			__syncwarp();
-		}
+		__syncwarp();
+		if (lane == 0) s.sc[0] = q0 + tot;
+		added += tot;
+		__syncwarp();
 		err = __reduce_min_sync(0xffffffffu, err);
 	}
 	// closed: pool end, state, forward-solve depth through U members
@@ -442,7 +530,7 @@ __device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax
 		const int t = s.Ws[d];
 		s.We[t] = s.Wps[d] + s.Wes[d];
 		s.Wst[t] = 1;
-		if (s.Wf[t] == F_U) levmax = max(levmax, __ldcg(A.lev + s.W[t]) + 1);
+		if (s.Wf[t] == F_U) levmax = max(levmax, s.Wlv[t] + 1);
 	}
 	__syncwarp();
 	return nd;
@@ -454,7 +542,7 @@ __device__ int close_pass(const FactArgs &A, WS &s, int i, int lane, int &levmax
 // a BSG_ERR_* code (uniform over the warp).
 template <class WS>
 __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, PhaseClock &pc) {
-	const bool ilu = A.kind == 1;
+	constexpr bool ilu = WS::ilu;
 	const int nW = min(s.sc[0], s.cmax);
 	// compact the selected members (closed, below the bound) in index order
 	if (lane == 0) s.sc[2] = 0;
@@ -483,15 +571,18 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 	}
 	__syncwarp();
 	// segment bases: stored member t contributes its entries [pos, end)
-	if (lane == 0) {
-		int b = 0;
-		for (int t = 0; t < nb; t++) {
-			s.Wb[t] = b;
-			if (s.Wfs[t] != F_D) b += s.Wes[t] - s.Wps[t];
+	{
+		int run = 0;
+		for (int t0 = 0; t0 < nb; t0 += 32) {
+			const int t = t0 + lane;
+			int tot;
+			const int ex = warp_excl_scan(t < nb && s.Wfs[t] != F_D ? s.Wes[t] - s.Wps[t] : 0, lane, tot);
+			if (t < nb) s.Wb[t] = run + ex;
+			run += tot;
 		}
-		s.Wb[nb] = b;
+		if (lane == 0) s.Wb[nb] = run;
+		__syncwarp();
 	}
-	__syncwarp();
 	int err = 0;
 	for (int t0 = 0; t0 < nb && !err;) {
 		int t1 = t0;
@@ -509,8 +600,7 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 				c4[r] = 0; l4[r] = 0; u4[r] = 0;
 				if (f < npf) {
 					// owner: the last member with Wb <= entry (dropped members have empty segments)
-					int lo = t0, hi = t1 - 1;
-					while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= gb + f) lo = mid; else hi = mid - 1; }
+					const int lo = t0 + seg_owner(s.Wb + t0, t1 - t0, gb + f);
 					const long long g = (long long)s.Wps[lo] + (gb + f - s.Wb[lo]);
 					c4[r] = __ldcg(A.pool_cf + g);
 					l4[r] = __ldcg(A.pool_l + g);
@@ -520,7 +610,11 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 #pragma unroll
 			for (int r = 0; r < 4; r++) {
 				const int f = f0 + r * 32 + lane;
-				if (f < npf) { s.pf_cf[f] = c4[r]; s.pf_l[f] = l4[r]; s.pf_u[f] = u4[r]; }
+				if (f < npf) {
+					s.pf_cf[f] = c4[r];
+					s.pf_l[f] = l4[r];
+					if (ilu) s.pf_u[f] = u4[r];
+				}
 			}
 		}
 		__syncwarp();
@@ -528,8 +622,7 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 		pc.v[FS_CYC_PF] += g1 - g0;
 		// phase A: accumulator slot of every entry, in parallel (R x R gets none)
 		for (int f = lane; f < npf; f += 32) {
-			int lo = t0, hi = t1 - 1;
-			while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (s.Wb[mid] <= gb + f) lo = mid; else hi = mid - 1; }
+			const int lo = t0 + seg_owner(s.Wb + t0, t1 - t0, gb + f);
 			const unsigned cf = s.pf_cf[f];
 			short sl = -1;
 			if (!(s.Wfs[lo] == F_R && CF_FLAG(cf) == F_R)) {
@@ -555,9 +648,7 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 					s.hl[sl] = fma(-uel, s.pf_l[b + e], s.hl[sl]);
 					s.hu[sl] = fma(-lel, s.pf_u[b + e], s.hu[sl]);
 				} else {
-					double v = fma(-lel, s.pf_l[b + e], s.hl[sl]);
-					s.hl[sl] = v;
-					s.hu[sl] = v;
+					s.hl[sl] = fma(-lel, s.pf_l[b + e], s.hl[sl]);
 				}
 			}
 			__syncwarp();
@@ -582,9 +673,10 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 // are left.
 template <class WS>
 __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc) {
-	const bool ilu = A.kind == 1;
+	constexpr bool ilu = WS::ilu;
 	const long long c0 = clock64();
 	for (int t = lane; t < 2 * s.cmax; t += 32) s.wset[t] = -1;
+	for (int t = lane; t < MWIN / 32; t += 32) s.wbits[t] = 0u; // (no bitmap: MWIN 0)
 	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
 	if (lane == 0) s.sc[0] = 0;
 	__syncwarp();
@@ -600,7 +692,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		int k = A.jt[t];
 		s.W[t - tb] = k;
 		s.Wst[t - tb] = 0;
-		wset_insert(s, k);
+		wset_insert(s, i, k);
 	}
 	if (lane == 0) s.sc[0] = te - tb;
 	__syncwarp();
@@ -612,7 +704,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	if (lane == 0) {
 		int slot = hfind_insert(s, i);
 		s.hl[slot] = A.diag0[i];
-		s.hu[slot] = A.diag0[i];
+		if (ilu) s.hu[slot] = A.diag0[i];
 	}
 	__syncwarp();
 	{
@@ -625,9 +717,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 				s.hl[sl] = __dmul_rn(__dmul_rn(A.al[k], si_u), A.scll[j]);
 				s.hu[sl] = __dmul_rn(__dmul_rn(A.au[k], si_l), A.sclu[j]);
 			} else {
-				double v = __dmul_rn(__dmul_rn(A.al[k], si_l), A.scll[j]);
-				s.hl[sl] = v;
-				s.hu[sl] = v;
+				s.hl[sl] = __dmul_rn(__dmul_rn(A.al[k], si_l), A.scll[j]);
 			}
 		}
 		err = __reduce_min_sync(0xffffffffu, err);
@@ -688,7 +778,10 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		// ---- wait for the smallest unfinished member while a warp computes
 		//      it; park when nobody does
 		int res = 0;
-		if (lane == 0) res = wait_row(A, bound);
+		if (lane == 0) {
+			res = wait_row(A, bound);
+			if (res == 0 && promote(A, bound)) res = wait_row(A, bound);
+		}
 		res = __shfl_sync(0xffffffffu, res, 0);
 		tail0 = clock64();
 		waited = true;
@@ -706,7 +799,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		if (lane == 0) {
 			const int di0 = hfind_insert(s, i);
 			s.hl[di0] = __dadd_rn(s.hl[di0], comp);
-			s.hu[di0] = __dadd_rn(s.hu[di0], comp);
+			if (ilu) s.hu[di0] = __dadd_rn(s.hu[di0], comp);
 		}
 		__syncwarp();
 	}
@@ -795,7 +888,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	//      order; a kept column contributes +0.0, which leaves the (positive)
 	//      sum unchanged, so the adds need no branch and the loads run ahead
 	if (lane == 0) {
-		double dl = s.hl[di], du = s.hu[di];
+		double dl = s.hl[di], du = ilu ? s.hu[di] : 0.0;
 		int t = 0;
 		for (; t + 8 <= nl; t += 8) {
 			double v[8];
@@ -804,16 +897,16 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 #pragma unroll
 			for (int q = 0; q < 8; q++) {
 				dl = __dadd_rn(dl, v[q]);
-				du = __dadd_rn(du, v[q]);
+				if (ilu) du = __dadd_rn(du, v[q]);
 			}
 		}
 		for (; t < nl; t++) {
 			const double v = s.pf_l[t];
 			dl = __dadd_rn(dl, v);
-			du = __dadd_rn(du, v);
+			if (ilu) du = __dadd_rn(du, v);
 		}
 		s.hl[di] = dl;
-		s.hu[di] = du;
+		if (ilu) s.hu[di] = du;
 	}
 	__syncwarp();
 	const int nk = s.sc[2];
@@ -841,13 +934,14 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		return -2;
 	}
 	if (lane == 0) {
-		A.pool_cf[off] = (unsigned)i | (F_U << 30);
+		// entry 0 is the diagonal; its column field carries the row's depth
+		A.pool_cf[off] = (unsigned)levmax | (F_U << 30);
 		A.pool_l[off] = deleml;
 		if (ilu) A.pool_u[off] = delemu;
 	}
 	for (int t = lane; t < nk; t += 32) {
 		const int h = s.lst[t];
-		double l = s.hl[h], u = s.hu[h];
+		double l = s.hl[h], u = ilu ? s.hu[h] : l;
 		if (ilu) { l = __dmul_rn(l, delemu); u = __dmul_rn(u, deleml); } else { l = __dmul_rn(l, deleml); u = l; }
 		double w = fabs(l);
 		if (ilu) w = fmax(w, fabs(u));
@@ -886,10 +980,11 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	return -1;
 }
 
+template <bool ILU>
 __global__ void __launch_bounds__(FACT_WARPS * 32, 2) k_fact_rows(FactArgs A) {
 	extern __shared__ unsigned char smem_raw[];
 	const int warp = threadIdx.x >> 5;
-	SmemWS &s = reinterpret_cast<SmemWS *>(smem_raw)[warp];
+	SmemWS<ILU> &s = reinterpret_cast<SmemWS<ILU> *>(smem_raw)[warp];
 	const int lane = threadIdx.x & 31;
 	PhaseClock pc;
 #pragma unroll
@@ -939,7 +1034,7 @@ __global__ void __launch_bounds__(FACT_WARPS * 32, 2) k_fact_rows(FactArgs A) {
 				continue;
 			}
 			__threadfence();
-			GlobWS g(A.big_ws + (size_t)slot * GlobWS::bytes);
+			GlobWS<ILU> g(A.big_ws + (size_t)slot * GlobWS<ILU>::bytes);
 			r = try_row(A, g, i, lane, pc);
 			__syncwarp();
 			if (lane == 0) {
@@ -975,7 +1070,7 @@ __global__ void k_fact_init(int n, const int *it, int *nstat, int *whead, unsign
 		devstat_fail(st, BSG_ERR_WORKSPACE, i, 8);
 		cnt = 0;
 	}
-	nstat[i] = (cnt << 15) | cnt;
+	nstat[i] = (cnt << 15) | cnt | (cnt == 0 ? ADM_QUEUED : 0u); // k_fact_seed queues those
 	inprog[i] = 0;
 	whead[i] = W_EMPTY;
 	rec[i] = 0;
@@ -1044,7 +1139,7 @@ __global__ void k_emit_u(int n, int kind, const unsigned long long *rec, const u
 	for (long long e = off; e < off + len; e++) {
 		unsigned x = cf[e];
 		if (CF_FLAG(x) != F_U) continue;
-		int j = CF_COL(x);
+		int j = e == off ? i : CF_COL(x); // entry 0: the diagonal (its column field holds the depth)
 		ju[z] = j;
 		if (j == i) {
 			l[z] = __dmul_rn(pl[e], scll[i]);
@@ -1164,20 +1259,21 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
 	BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
 	k_fact_seed<<<nb(n, 256), 256, 0, st>>>(A);
-	size_t smem = sizeof(SmemWS) * FACT_WARPS;
-	BSG_CUDA(cudaFuncSetAttribute(k_fact_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	void (*kern)(FactArgs) = kind == 1 ? k_fact_rows<true> : k_fact_rows<false>;
+	const size_t smem = (kind == 1 ? sizeof(SmemWS<true>) : sizeof(SmemWS<false>)) * FACT_WARPS;
+	BSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	int per_sm = 0;
-	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fact_rows, FACT_WARPS * 32, smem));
+	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FACT_WARPS * 32, smem));
 	if (per_sm < 1) per_sm = 1;
 	int grid = per_sm * BSG_SMS;
 	int need = (n + FACT_WARPS - 1) / FACT_WARPS;
 	if (grid > need) grid = need;
 	if (grid < 1) grid = 1;
-	if (cudaMallocAsync(&A.big_ws, GlobWS::bytes * (size_t)BIG_SLOTS, st) != cudaSuccess)
+	if (cudaMallocAsync(&A.big_ws, GlobWS<true>::bytes * (size_t)BIG_SLOTS, st) != cudaSuccess)
 		return bsg_set_error(BSG_ERR_NOMEM, "factor row workspace");
 	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * BIG_SLOTS, st));
 	BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * BIG_SLOTS, st));
-	k_fact_rows<<<grid, FACT_WARPS * 32, smem, st>>>(A);
+	kern<<<grid, FACT_WARPS * 32, smem, st>>>(A);
 	BSG_CUDA(cudaGetLastError());
 	int rc = bsg_check_devstat(c);
 	cudaMemcpyAsync(g_fact_stats, A.stats, sizeof(g_fact_stats), cudaMemcpyDeviceToHost, st);
