@@ -57,7 +57,12 @@
 #define CF_COL(x) ((int)((x) & 0x3fffffffu))
 #define CF_FLAG(x) ((x) >> 30)
 
+#ifndef FACT_WARPS
 #define FACT_WARPS 4
+#endif
+#ifndef FACT_MINB
+#define FACT_MINB 2 // blocks per SM the registers must allow
+#endif
 #define CMAX 128   // members of C(i)
 #define HCAP 256   // distinct mask columns per row (power of two)
 #ifndef PFCAP
@@ -73,6 +78,9 @@
 // atomic per test-and-set), farther ones in the hash
 #ifndef MWIN
 #define MWIN 16384
+#endif
+#ifndef WSETCAP
+#define WSETCAP 128 // far members (hash slots, a power of two)
 #endif
 #define W_EMPTY (-1)
 #define W_CLOSED (-2)
@@ -130,7 +138,7 @@ struct PhaseClock {
 template <bool ILU>
 struct SmemWS {
 	static constexpr bool big = false, ilu = ILU;
-	static constexpr int cmax = CMAX, hcap = HCAP, pfcap = PFCAP;
+	static constexpr int cmax = CMAX, hcap = HCAP, pfcap = PFCAP, wcap = WSETCAP;
 	int W[CMAX];           // members (discovery order, then sorted)
 	int Wp[CMAX];          // pool index of column i in that row (stored members)
 	int We[CMAX];          // pool end of that row
@@ -139,16 +147,24 @@ struct SmemWS {
 	unsigned char Wfs[CMAX];
 	int Wb[CMAX + 1];      // prefetch segment bases (sorted order)
 	unsigned char Wst[CMAX]; // member state: 0 not closed, 1 closed, 2 applied
-	int Wlv[CMAX];         // forward-solve depth of a closed member
-	int wset[CMAX * 2];    // membership hash of W (keys), members below i - MWIN
+	int wset[WSETCAP];     // membership hash of W (keys), members below i - MWIN
 	unsigned wbits[MWIN > 0 ? MWIN / 32 : 1]; // membership bitmap: bit i - 1 - k for member k
 	int hkey[HCAP];        // column accumulator
 	double hl[HCAP], hu[ILU ? HCAP : 1];
-	int lst[HCAP];         // extracted slots, then sorted
-	int lsts[HCAP];
-	int lkey[HCAP];        // columns of the extracted slots
-	unsigned pf_cf[PFCAP]; // prefetched contributor segments
-	short pf_slot[PFCAP];
+	int lsts[HCAP];        // selected members (updates); sorted slots (finish)
+	// the updates' prefetch buffers and the finish's slot lists are never
+	// live at once; Wlv (depth of a closed member) lives in a closure pass
+	union {
+		struct {
+			unsigned pf_cf[PFCAP]; // prefetched contributor segments
+			short pf_slot[PFCAP];
+		};
+		struct {
+			int lst[HCAP];         // extracted slots, then sorted
+			int lkey[HCAP];        // columns of the extracted slots
+		};
+		int Wlv[CMAX];
+	};
 	double pf_l[PFCAP], pf_u[ILU ? PFCAP : 1];
 	int sc[4];
 };
@@ -156,7 +172,7 @@ struct SmemWS {
 template <bool ILU>
 struct GlobWS {
 	static constexpr bool big = true, ilu = ILU;
-	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG;
+	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG, wcap = 2 * CMAX_BIG;
 	static constexpr size_t bytes = 8 * (2 * (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
 	                                4 * (7 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
 	                                     4 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
@@ -237,8 +253,8 @@ __device__ int wset_insert(WS &s, int i, int k) {
 		if (s.wbits[d >> 5] & bit) return 0;
 		return (atomicOr(&s.wbits[d >> 5], bit) & bit) ? 0 : 1;
 	}
-	unsigned h = hash_u(k) & (2 * s.cmax - 1);
-	for (int probe = 0; probe < 2 * s.cmax; probe++) {
+	unsigned h = hash_u(k) & (s.wcap - 1);
+	for (int probe = 0; probe < s.wcap; probe++) {
 		int cur = s.wset[h];
 		if (cur == k) return 0;
 		if (cur == -1) {
@@ -246,7 +262,7 @@ __device__ int wset_insert(WS &s, int i, int k) {
 			if (old == -1) return 1;
 			if (old == k) return 0;
 		}
-		h = (h + 1) & (2 * s.cmax - 1);
+		h = (h + 1) & (s.wcap - 1);
 	}
 	return -1;
 }
@@ -675,7 +691,7 @@ template <class WS>
 __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc) {
 	constexpr bool ilu = WS::ilu;
 	const long long c0 = clock64();
-	for (int t = lane; t < 2 * s.cmax; t += 32) s.wset[t] = -1;
+	for (int t = lane; t < s.wcap; t += 32) s.wset[t] = -1;
 	for (int t = lane; t < MWIN / 32; t += 32) s.wbits[t] = 0u; // (no bitmap: MWIN 0)
 	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
 	if (lane == 0) s.sc[0] = 0;
@@ -981,7 +997,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 }
 
 template <bool ILU>
-__global__ void __launch_bounds__(FACT_WARPS * 32, 2) k_fact_rows(FactArgs A) {
+__global__ void __launch_bounds__(FACT_WARPS * 32, FACT_MINB) k_fact_rows(FactArgs A) {
 	extern __shared__ unsigned char smem_raw[];
 	const int warp = threadIdx.x >> 5;
 	SmemWS<ILU> &s = reinterpret_cast<SmemWS<ILU> *>(smem_raw)[warp];

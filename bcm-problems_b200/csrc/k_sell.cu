@@ -380,8 +380,9 @@ __global__ void k_sell_fill(int n, const int *rp, const int *ci, const double *v
 
 // y = A x (OUT 0) or y = (x - N yin) * dinv (OUT 1); IN 1 forms
 // yin[c] = x[c] * dinv[c] on the fly (the first two Jacobi iterates in one
-// pass).
-template <typename VT, int IN, int OUT>
+// pass).  LG: the matrix has long rows (without, the kernel keeps the
+// registers, and so the occupancy, of the plain slice loop).
+template <typename VT, int IN, int OUT, bool LG>
 __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict__ perm,
                                                     const long long *__restrict__ off,
                                                     const int *__restrict__ scol, const VT *__restrict__ sval,
@@ -390,10 +391,11 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
                                                     const double *__restrict__ dinv_out, double *__restrict__ y,
                                                     sell_long<VT> lg) {
 	constexpr int SPW = 32 / SELL_C; // slices per warp
-	long_rows<VT, double, IN>(lg, xin, dinv_in, [&](int r, double sum) {
-		if (OUT == 0) y[r] = sum;
-		else y[r] = (xrhs[r] - sum) * dinv_out[r];
-	});
+	if (LG)
+		long_rows<VT, double, IN>(lg, xin, dinv_in, [&](int r, double sum) {
+			if (OUT == 0) y[r] = sum;
+			else y[r] = (xrhs[r] - sum) * dinv_out[r];
+		});
 	const int lane = threadIdx.x & 31;
 	const int grp = lane / SELL_C, l = lane % SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
 		if (slice >= nsl) continue;
 		const long long base = __ldg(off + slice);
 		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
-		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
+		const unsigned lm = LG && lg.mask ? __ldg(lg.mask + slice) : 0u;
 		const int *cp = scol + base + l;
 		const VT *vp = sval + base + l;
 		double sum = 0.0;
@@ -444,7 +446,7 @@ __global__ void __launch_bounds__(256) k_sell_apply(int n, const int *__restrict
 // * dinv, written as FP64 (the last pass, OUT64 1) or as the FP32 iterate the
 // next pass gathers (OUT64 0).  Gathering 4-byte iterates halves the
 // sector traffic of the gathers; the products and sums stay FP64.
-template <int OUT64>
+template <int OUT64, bool LG>
 __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restrict__ perm,
                                                       const long long *__restrict__ off,
                                                       const int *__restrict__ scol, const float *__restrict__ sval,
@@ -452,11 +454,12 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
                                                       const double *__restrict__ dinv, double *__restrict__ y,
                                                       float *__restrict__ y32, sell_long<float> lg) {
 	constexpr int SPW = 32 / SELL_C;
-	long_rows<float, float, 0>(lg, x32, nullptr, [&](int r, double sum) {
-		const double v = (rhs[r] - sum) * dinv[r];
-		if (OUT64) y[r] = v;
-		else y32[r] = (float)v;
-	});
+	if (LG)
+		long_rows<float, float, 0>(lg, x32, nullptr, [&](int r, double sum) {
+			const double v = (rhs[r] - sum) * dinv[r];
+			if (OUT64) y[r] = v;
+			else y32[r] = (float)v;
+		});
 	const int lane = threadIdx.x & 31;
 	const int grp = lane / SELL_C, l = lane % SELL_C;
 	const int nsl = (n + SELL_C - 1) / SELL_C;
@@ -466,7 +469,7 @@ __global__ void __launch_bounds__(256) k_sell_sweep32(int n, const int *__restri
 		if (slice >= nsl) continue;
 		const long long base = __ldg(off + slice);
 		const int w = (int)((__ldg(off + slice + 1) - base) / SELL_C);
-		const unsigned lm = lg.mask ? __ldg(lg.mask + slice) : 0u;
+		const unsigned lm = LG && lg.mask ? __ldg(lg.mask + slice) : 0u;
 		const int *cp = scol + base + l;
 		const float *vp = sval + base + l;
 		double sum = 0.0;
@@ -971,12 +974,16 @@ static int sell_grid(int n) {
 // y = A x
 int bsg_sell_spmv(cudaStream_t s, const bsg_sell *m, const double *x, double *y) {
 	BSG_COUNT(1);
-	if (m->fp32)
-		k_sell_apply<float, 0, 0><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x,
-		                                                          nullptr, nullptr, nullptr, y, long_of<float>(m));
-	else
-		k_sell_apply<double, 0, 0><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const double *)m->val, x,
-		                                                           nullptr, nullptr, nullptr, y, long_of<double>(m));
+	const int g = sell_grid(m->n);
+#define BSG_SPMV(VT, LG)                                                                                               \
+	k_sell_apply<VT, 0, 0, LG><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const VT *)m->val, x, nullptr, nullptr, \
+	                                             nullptr, y, long_of<VT>(m))
+	if (m->fp32) {
+		if (m->nlong) BSG_SPMV(float, true); else BSG_SPMV(float, false);
+	} else {
+		if (m->nlong) BSG_SPMV(double, true); else BSG_SPMV(double, false);
+	}
+#undef BSG_SPMV
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
@@ -986,21 +993,18 @@ int bsg_sell_sweep(cudaStream_t s, const bsg_sell *m, const double *x, const dou
                    int scaled_in, double *yout) {
 	BSG_COUNT(1);
 	const int g = sell_grid(m->n);
+#define BSG_SW(VT, IN, LG)                                                                                             \
+	k_sell_apply<VT, IN, 1, LG><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const VT *)m->val,                     \
+	                                              IN ? x : yin, IN ? dinv : nullptr, x, dinv, yout, long_of<VT>(m))
+	const bool lg = m->nlong > 0;
 	if (m->fp32) {
-		const float *v = (const float *)m->val;
-		const sell_long<float> lg = long_of<float>(m);
-		if (scaled_in)
-			k_sell_apply<float, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout, lg);
-		else
-			k_sell_apply<float, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout, lg);
+		if (scaled_in) { if (lg) BSG_SW(float, 1, true); else BSG_SW(float, 1, false); }
+		else { if (lg) BSG_SW(float, 0, true); else BSG_SW(float, 0, false); }
 	} else {
-		const double *v = (const double *)m->val;
-		const sell_long<double> lg = long_of<double>(m);
-		if (scaled_in)
-			k_sell_apply<double, 1, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, x, dinv, x, dinv, yout, lg);
-		else
-			k_sell_apply<double, 0, 1><<<g, 256, 0, s>>>(m->n, m->perm, m->off, m->col, v, yin, nullptr, x, dinv, yout, lg);
+		if (scaled_in) { if (lg) BSG_SW(double, 1, true); else BSG_SW(double, 1, false); }
+		else { if (lg) BSG_SW(double, 0, true); else BSG_SW(double, 0, false); }
 	}
+#undef BSG_SW
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
@@ -1027,9 +1031,19 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 				k_tsell_sweep32<0><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
 				                                                     m->tb, b, x, dinv, nullptr, a);
 		} else if (last) {
-			k_sell_sweep32<1><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr, long_of<float>(m));
+			if (m->nlong)
+				k_sell_sweep32<1, true><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr,
+				                                          long_of<float>(m));
+			else
+				k_sell_sweep32<1, false><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr,
+				                                           long_of<float>(m));
 		} else {
-			k_sell_sweep32<0><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a, long_of<float>(m));
+			if (m->nlong)
+				k_sell_sweep32<0, true><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a,
+				                                          long_of<float>(m));
+			else
+				k_sell_sweep32<0, false><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, nullptr, a,
+				                                           long_of<float>(m));
 		}
 		float *t = a; a = b; b = t;
 	}
@@ -1044,9 +1058,12 @@ int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, co
 	if (m->ntile)
 		k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, (size_t)m->tmax * 32 * sizeof(float), s>>>(
 		    m->n, m->ntile, m->perm, m->off, m->cpair, (const float *)m->val, m->tb_off, m->tb, x32, x, dinv, yout, nullptr);
+	else if (m->nlong)
+		k_sell_sweep32<1, true><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val,
+		                                                        x32, x, dinv, yout, nullptr, long_of<float>(m));
 	else
-		k_sell_sweep32<1><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val, x32, x,
-		                                                  dinv, yout, nullptr, long_of<float>(m));
+		k_sell_sweep32<1, false><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val,
+		                                                         x32, x, dinv, yout, nullptr, long_of<float>(m));
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
