@@ -278,3 +278,11 @@ int bsg_trisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int ns
                        double *y, double *work);
 int bsg_btrisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int nsweeps, int nr, const double *x,
                         double *y, double *work);
+// Strict upper part of a CSR pattern transposed: for every column, the rows
+// above it that hold an entry there (k_format.cu).
+int bsg_strict_transpose(bsg_ctx *c, int n, const int *ia, const int *ja, int nnz, int **it_o, int **jt_o,
+                         int **perm_o, int *nnz_o);
+// Block IC2 / ILU2 rows with the dynamic schedule (k_fact.cu).
+int bsg_bfact_dyn(bsg_ctx *c, int nb, int sym, const bsg_param *p, const int *bia, const int *bja, int nnzb,
+                  const double *bal, const double *bau, const double *scll, const double *sclu, const double *diagg,
+                  int **ig_o, int **jg_o, double **gl_o, double **gu_o, unsigned long long *nstored);

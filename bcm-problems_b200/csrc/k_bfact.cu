@@ -9,127 +9,26 @@
 // Blocks are column-major 3 x 3 (entry (r, c) at r + 3 c), as CSMatrixRS
 // keeps them.
 //
-// Schedule.  Block rows of a natural-order 3-D elasticity matrix form a
-// dependency chain (every block row couples to the previous one), so rows
-// are factored in order by one persistent CTA that spreads each row's work
-// over its 512 threads:
-//   1. the members of the row -- earlier rows that stored an element in this
-//      column -- come from per-column lists that every stored element
-//      appended to (the reference walks linked lists instead, :1578-1617);
-//   2. the scaled row of A goes into dense per-column accumulators;
-//   3. every (member, element) pair registers its column, then subtracts its
-//      two 3 x 3 products (L and U side) with atomics;
-//   4. one thread per touched column filters it, adding the compensation to
-//      the pivot block and to that column's future diagonal block;
-//   5. one thread takes the SVD of the pivot block; the kept blocks are
-//      scaled, ranked by column, stored as U (max-norm >= tau1) or R, and
-//      appended to their columns' member lists.
-// The updates are summed in arrival order, and the SVD is this file's own,
-// so the factor agrees with the reference to rounding, not bit for bit; a
-// singular vector's sign cancels in L U, but for (nearly) repeated singular
-// values the reference's vectors and these differ by a rotation, which can
-// move a block across a threshold.
+// Rows.  The block rows are factored by the point factorisation's kernel in
+// its block mode (k_fact.cu, bsg_bfact_dyn): a warp per block row on the
+// dynamic schedule (closure of the members over finished rows, admission,
+// waiting, parking); the members' updates are applied in ascending member
+// order, the compensations of dropped blocks reach the dropped column's
+// pivot block through exact fixed-point sums, so the factor does not depend
+// on the schedule.  This file builds the scaled CombineLU block matrix
+// before, and the reference layout and the solve-ready forms after.  The SVD
+// is this file's own, so the factor agrees with the reference to rounding,
+// not bit for bit; a singular vector's sign cancels in L U, but for (nearly)
+// repeated singular values the reference's vectors and these differ by a
+// rotation, which can move a block across a threshold.
 #include "bsg_internal.cuh"
+#include "bsg_blk3.cuh"
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 namespace {
 
-constexpr int BT = 512;       // threads of the row kernel
-constexpr int LMAX = 4096;    // distinct columns one row may touch
-constexpr int MMAX = 4096;    // members of one row
-constexpr int CH = 32;        // entries per member-list chunk
-
 inline int nb_(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
-
-// ---- 3 x 3 helpers (column-major) -----------------------------------------
-// out = p q with p given by strides: p(r, k) at p[r * pr + k * pc]; q(k, c)
-// at q[k * qr + c * qc]; sums in k order from zero
-__device__ __forceinline__ void mm3(const double *p, int pr, int pc, const double *q, int qr, int qc, double *out) {
-#pragma unroll
-	for (int r = 0; r < 3; r++)
-#pragma unroll
-		for (int c = 0; c < 3; c++) {
-			double s = 0.0;
-#pragma unroll
-			for (int k = 0; k < 3; k++) s += p[r * pr + k * pc] * q[k * qr + c * qc];
-			out[r + 3 * c] = s;
-		}
-}
-
-// A = U diag(s) V^T of a 3 x 3 matrix (column-major), s descending, U and V
-// orthogonal: one-sided Jacobi (Hestenes), rotating column pairs of W = A V
-// until they are orthogonal; U = the normalised columns of W, completed to an
-// orthonormal basis (Gram-Schmidt of unit vectors) where a singular value
-// vanishes.
-__device__ void svd3(const double *a, double *u, double *s, double *v) {
-	double w[9], vw[9];
-	for (int k = 0; k < 9; k++) {
-		w[k] = a[k];
-		vw[k] = (k % 4) == 0 ? 1.0 : 0.0;
-	}
-	for (int sweep = 0; sweep < 30; sweep++) {
-		double off = 0.0;
-		for (int pq = 0; pq < 3; pq++) {
-			const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
-			double al = 0.0, be = 0.0, ga = 0.0;
-			for (int r = 0; r < 3; r++) {
-				al += w[r + 3 * p] * w[r + 3 * p];
-				be += w[r + 3 * q] * w[r + 3 * q];
-				ga += w[r + 3 * p] * w[r + 3 * q];
-			}
-			const double nrm = sqrt(al * be);
-			if (nrm == 0.0 || fabs(ga) <= 1e-16 * nrm) continue;
-			off = fmax(off, fabs(ga) / nrm);
-			const double zeta = (be - al) / (2.0 * ga);
-			const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-			const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
-			for (int r = 0; r < 3; r++) {
-				const double wp = w[r + 3 * p], wq = w[r + 3 * q];
-				w[r + 3 * p] = cs * wp - sn * wq;
-				w[r + 3 * q] = sn * wp + cs * wq;
-				const double vp = vw[r + 3 * p], vq = vw[r + 3 * q];
-				vw[r + 3 * p] = cs * vp - sn * vq;
-				vw[r + 3 * q] = sn * vp + cs * vq;
-			}
-		}
-		if (off <= 1e-15) break;
-	}
-	double sv[3];
-	for (int c = 0; c < 3; c++) sv[c] = sqrt(w[3 * c] * w[3 * c] + w[1 + 3 * c] * w[1 + 3 * c] + w[2 + 3 * c] * w[2 + 3 * c]);
-	int o[3] = {0, 1, 2}; // descending order
-	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
-	if (sv[o[1]] < sv[o[2]]) { const int t = o[1]; o[1] = o[2]; o[2] = t; }
-	if (sv[o[0]] < sv[o[1]]) { const int t = o[0]; o[0] = o[1]; o[1] = t; }
-	const double smax = sv[o[0]];
-	int good[3];
-	for (int c = 0; c < 3; c++) {
-		const int k = o[c];
-		s[c] = sv[k];
-		good[c] = sv[k] > 1e-300 && sv[k] > 1e-14 * smax;
-		for (int r = 0; r < 3; r++) {
-			u[r + 3 * c] = good[c] ? w[r + 3 * k] / sv[k] : 0.0;
-			v[r + 3 * c] = vw[r + 3 * k];
-		}
-	}
-	for (int c = 0; c < 3; c++) {
-		if (good[c]) continue;
-		for (int e = 0; e < 3; e++) {
-			double x[3] = {e == 0 ? 1.0 : 0.0, e == 1 ? 1.0 : 0.0, e == 2 ? 1.0 : 0.0};
-			for (int d = 0; d < 3; d++) {
-				if (d == c || !good[d]) continue;
-				const double pr = u[3 * d] * x[0] + u[1 + 3 * d] * x[1] + u[2 + 3 * d] * x[2];
-				for (int r = 0; r < 3; r++) x[r] -= pr * u[r + 3 * d];
-			}
-			const double nx = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-			if (nx > 0.5) {
-				for (int r = 0; r < 3; r++) u[r + 3 * c] = x[r] / nx;
-				good[c] = 1;
-				break;
-			}
-		}
-	}
-}
 
 // ---- CombineLU of a block matrix on the device ----------------------------
 // keys (row, col) of the union pattern: upper blocks (j >= i) at (i, j),
@@ -215,315 +114,6 @@ __global__ void k_bscale(int nb, int sym, const int *bia, const double *au, doub
 	double t[9];
 	mm3(sl, 1, 3, d, 1, 3, t);                 // scll D
 	mm3(t, 1, 3, su, 3, 1, diagg + (size_t)i * 9); // ... sclu^T
-}
-
-// ---- the row kernel ---------------------------------------------------------
-struct BArgs {
-	int nb;
-	const int *bia, *bja;     // CombineLU pattern (diagonal block first)
-	const double *al, *au;    // transposed lower / upper blocks
-	const double *scll, *sclu;
-	double *diagg;            // scaled diagonal blocks, plus compensations
-	double *fml, *fmu;        // dense accumulators, 9 per block column
-	int *imask;               // row that last registered a column
-	int *ig, *jg;             // stored rows: pivot, then +col (U) / -col (R)
-	double *gl, *gu;
-	long long cap;            // stored blocks available
-	int *mhead, *mtail, *mcnt; // per-column member lists (chunks)
-	int *chk, *chq, *chnext;  // chunk entries: member row, stored position; next chunk
-	int *pool;                // chunks in use
-	int pool_cap;
-	double tau1, tau2, theta, pivmin;
-	int sym;                  // block IC2: eigendecomposition pivots, L = U^T
-	unsigned long long *nstored; // [0] U blocks, [1] R blocks
-	bsg_devstat *st;
-};
-
-__device__ int upper_index(const int *pre, int n, int w) { // largest m with pre[m] <= w
-	int lo = 0, hi = n - 1;
-	while (lo < hi) {
-		const int mid = (lo + hi + 1) >> 1;
-		if (pre[mid] <= w) lo = mid;
-		else hi = mid - 1;
-	}
-	return lo;
-}
-
-// loads of data this kernel writes: L2 only (atomics update L2, not L1)
-__device__ __forceinline__ void ld9(const double *p, double *o) {
-#pragma unroll
-	for (int k = 0; k < 9; k++) o[k] = __ldcg(p + k);
-}
-
-// shared memory of the row kernel, carved from the dynamic allocation
-constexpr size_t BSMEM = sizeof(int) * (3 * MMAX + 1 + 3 * LMAX) + MMAX;
-
-__global__ void __launch_bounds__(BT, 1) k_bilu2_rows(BArgs A) {
-	extern __shared__ __align__(16) int bsm[];
-	int *mk = bsm, *mq = mk + MMAX, *mpre = mq + MMAX, *lst = mpre + MMAX + 1, *keep = lst + LMAX,
-	    *rank_ = keep + LMAX;
-	unsigned char *mr = reinterpret_cast<unsigned char *>(rank_ + LMAX);
-	__shared__ double dsum[BT / 32][3];
-	__shared__ double dl[9], du[9];
-	__shared__ int nm, nl, nk, W, base, fail, failrow;
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	if (tid == 0) {
-		base = 0;
-		fail = 0;
-		A.ig[0] = 0;
-	}
-	__syncthreads();
-	for (int irow = 0; irow < A.nb; irow++) {
-		// ---- members of the row (warp 0) and the scaled row of A (the rest)
-		if (tid == 0) {
-			nm = __ldcg(A.mcnt + irow);
-			nl = 0;
-			if (nm > MMAX) fail = 1;
-		}
-		__syncthreads();
-		if (fail) break;
-		if (warp == 0) {
-			int c = __ldcg(A.mhead + irow), o = 0;
-			while (c >= 0 && o < nm) {
-				if (o + lane < nm) {
-					mk[o + lane] = __ldcg(A.chk + (size_t)c * CH + lane);
-					mq[o + lane] = __ldcg(A.chq + (size_t)c * CH + lane);
-				}
-				o += CH;
-				c = __ldcg(A.chnext + c);
-			}
-		} else {
-			const double *sli = A.scll + (size_t)irow * 9, *sui = A.sclu + (size_t)irow * 9;
-			for (int p = A.bia[irow] + tid - 32; p < A.bia[irow + 1]; p += BT - 32) {
-				const int j = A.bja[p];
-				double t[9];
-				if (j == irow) {
-					double dg[9];
-					ld9(A.diagg + (size_t)j * 9, dg);
-					for (int k = 0; k < 9; k++) A.fml[(size_t)j * 9 + k] = A.fmu[(size_t)j * 9 + k] = dg[k];
-				} else {
-					mm3(sli, 1, 3, A.au + (size_t)p * 9, 1, 3, t);
-					mm3(t, 1, 3, A.sclu + (size_t)j * 9, 3, 1, A.fmu + (size_t)j * 9);
-					if (!A.sym) { // the symmetric form keeps one mask (L = U^T)
-						mm3(sui, 1, 3, A.al + (size_t)p * 9, 1, 3, t);
-						mm3(t, 1, 3, A.scll + (size_t)j * 9, 3, 1, A.fml + (size_t)j * 9);
-					}
-				}
-				atomicExch(A.imask + j, irow);
-				const int slot = atomicAdd(&nl, 1);
-				if (slot < LMAX) lst[slot] = j;
-			}
-		}
-		__syncthreads();
-		// ---- member segments [q, end of the member's row) and their prefix (warp 0)
-		for (int m = tid; m < nm; m += BT) {
-			const int k = mk[m], q = mq[m];
-			mpre[m + 1] = __ldcg(A.ig + k + 1) - q;
-			mr[m] = __ldcg(A.jg + q) < 0;
-		}
-		__syncthreads();
-		if (warp == 0) {
-			int carry = 0;
-			if (lane == 0) mpre[0] = 0;
-			for (int o = 0; o < nm; o += 32) {
-				int v = o + lane < nm ? mpre[o + lane + 1] : 0;
-				for (int d = 1; d < 32; d <<= 1) {
-					const int y = __shfl_up_sync(0xffffffffu, v, d);
-					if (lane >= d) v += y;
-				}
-				if (o + lane < nm) mpre[o + lane + 1] = v + carry;
-				carry += __shfl_sync(0xffffffffu, v, 31);
-			}
-			if (lane == 0) W = carry;
-		}
-		__syncthreads();
-		// ---- register the members' columns (first registration zeroes them)
-		for (int w = tid; w < W; w += BT) {
-			const int m = upper_index(mpre, nm, w);
-			const int e = mq[m] + (w - mpre[m]);
-			int c = __ldcg(A.jg + e);
-			if (mr[m] && c < 0) continue;
-			c = c < 0 ? -c : c;
-			if (atomicExch(A.imask + c, irow) != irow) {
-				for (int k = 0; k < 9; k++) A.fml[(size_t)c * 9 + k] = A.fmu[(size_t)c * 9 + k] = 0.0;
-				const int slot = atomicAdd(&nl, 1);
-				if (slot < LMAX) lst[slot] = c;
-			}
-		}
-		__syncthreads();
-		if (nl > LMAX) {
-			if (tid == 0) fail = 2;
-			break;
-		}
-		// ---- updates: fmu[c] -= Lki^T Ukc, fml[c] -= Uki^T Lkc
-		for (int w = tid; w < W; w += BT) {
-			const int m = upper_index(mpre, nm, w);
-			const int q = mq[m], e = q + (w - mpre[m]);
-			int c = __ldcg(A.jg + e);
-			if (mr[m] && c < 0) continue;
-			c = c < 0 ? -c : c;
-			double lel[9], uel[9], gu[9], gl[9], tu[9], tl[9];
-			ld9(A.gl + (size_t)q * 9, lel);
-			ld9(A.gu + (size_t)q * 9, uel);
-			ld9(A.gu + (size_t)e * 9, gu);
-			ld9(A.gl + (size_t)e * 9, gl);
-			mm3(lel, 3, 1, gu, 1, 3, tu); // lel^T gu
-			for (int k = 0; k < 9; k++) atomicAdd(A.fmu + (size_t)c * 9 + k, -tu[k]);
-			if (!A.sym) {
-				mm3(uel, 3, 1, gl, 1, 3, tl); // uel^T gl
-				for (int k = 0; k < 9; k++) atomicAdd(A.fml + (size_t)c * 9 + k, -tl[k]);
-			}
-		}
-		__syncthreads();
-		// ---- filter: keep max-norm >= tau2, else compensate both diagonals
-		double ds0 = 0.0, ds1 = 0.0, ds2 = 0.0;
-		for (int t = tid; t < nl; t += BT) {
-			const int c = lst[t];
-			keep[t] = 0;
-			if (c == irow) continue;
-			double fl[9], fu[9];
-			ld9((A.sym ? A.fmu : A.fml) + (size_t)c * 9, fl);
-			ld9(A.fmu + (size_t)c * 9, fu);
-			double mx = 0.0;
-			for (int k = 0; k < 9; k++) mx = fmax(mx, fmax(fabs(fl[k]), fabs(fu[k])));
-			if (mx >= A.tau2) {
-				keep[t] = 1;
-			} else {
-				double dg[9];
-				ld9(A.diagg + (size_t)c * 9, dg);
-				for (int r = 0; r < 3; r++)
-					for (int cc = 0; cc < 3; cc++) {
-						const double v = A.theta * fmax(fabs(fl[r + 3 * cc]), fabs(fu[r + 3 * cc]));
-						if (r == 0) ds0 += v;
-						else if (r == 1) ds1 += v;
-						else ds2 += v;
-						dg[4 * cc] += v;
-					}
-				for (int cc = 0; cc < 3; cc++) A.diagg[(size_t)c * 9 + 4 * cc] = dg[4 * cc];
-			}
-		}
-		ds0 = warp_sum(ds0);
-		ds1 = warp_sum(ds1);
-		ds2 = warp_sum(ds2);
-		if (lane == 0) {
-			dsum[warp][0] = ds0;
-			dsum[warp][1] = ds1;
-			dsum[warp][2] = ds2;
-		}
-		__syncthreads();
-		// ---- pivot block (thread 0)
-		if (tid == 0) {
-			double fd[9];
-			ld9(A.fmu + (size_t)irow * 9, fd);
-			for (int r = 0; r < 3; r++) {
-				double sm = 0.0;
-				for (int w2 = 0; w2 < BT / 32; w2++) sm += dsum[w2][r];
-				fd[4 * r] += sm;
-			}
-			double u[9], v[9], sv[3];
-			svd3(fd, u, sv, v);
-			if (A.sym) { // Ich2PivScaleRow (Bslib/ich2rs.cpp:532-647): eigenpairs, no clamp
-				for (int k = 0; k < 3; k++) {
-					if (u[3 * k] * v[3 * k] + u[1 + 3 * k] * v[1 + 3 * k] + u[2 + 3 * k] * v[2 + 3 * k] < 0.0 && sv[k] > 0.0) {
-						fail = 5;
-						failrow = irow;
-					}
-					for (int r = 0; r < 3; r++) u[r + 3 * k] = v[r + 3 * k];
-					sv[k] = 1.0 / sqrt(sv[k]);
-				}
-			} else {
-				for (int k = 0; k < 3; k++) sv[k] = 1.0 / sqrt(sv[k] < A.pivmin ? A.pivmin : sv[k]);
-			}
-			for (int r = 0; r < 3; r++)
-				for (int c = 0; c < 3; c++) {
-					dl[r + 3 * c] = u[c + 3 * r] * sv[r]; // diag(s^-1/2) U^T
-					du[r + 3 * c] = v[c + 3 * r] * sv[r]; // diag(s^-1/2) V^T
-				}
-			int K = 0;
-			for (int t = 0; t < nl; t++) K += keep[t];
-			nk = K;
-		}
-		__syncthreads();
-		if (fail) break;
-		if ((long long)base + 1 + nk > A.cap) {
-			if (tid == 0) fail = 3;
-			break;
-		}
-		for (int t = tid; t < nl; t += BT) { // rank = kept blocks of smaller column
-			if (!keep[t]) continue;
-			const int c = lst[t];
-			int r = 0;
-			for (int t2 = 0; t2 < nl; t2++) r += keep[t2] && lst[t2] < c;
-			rank_[t] = r;
-		}
-		if (tid == 0) { // the pivot block: gl = dl^T, gu = du^T
-			A.jg[base] = irow;
-			for (int r = 0; r < 3; r++)
-				for (int c = 0; c < 3; c++) {
-					A.gl[(size_t)base * 9 + r + 3 * c] = dl[c + 3 * r];
-					A.gu[(size_t)base * 9 + r + 3 * c] = du[c + 3 * r];
-				}
-		}
-		__syncthreads();
-		// ---- scale, store, and append to the columns' member lists
-		unsigned long long nu = 0, nr = 0;
-		for (int t = tid; t < nl; t += BT) {
-			if (!keep[t]) continue;
-			const int c = lst[t];
-			const int pos = base + 1 + rank_[t];
-			double fl[9], fu[9], tl[9], tu[9];
-			ld9(A.fmu + (size_t)c * 9, fu);
-			mm3(dl, 1, 3, fu, 1, 3, tu);
-			if (A.sym) {
-				for (int k = 0; k < 9; k++) tl[k] = tu[k];
-			} else {
-				ld9(A.fml + (size_t)c * 9, fl);
-				mm3(du, 1, 3, fl, 1, 3, tl);
-			}
-			double mx = 0.0;
-			for (int k = 0; k < 9; k++) {
-				A.gl[(size_t)pos * 9 + k] = tl[k];
-				A.gu[(size_t)pos * 9 + k] = tu[k];
-				mx = fmax(mx, fmax(fabs(tl[k]), fabs(tu[k])));
-			}
-			const int isu = mx >= A.tau1;
-			A.jg[pos] = isu ? c : -c;
-			nu += isu;
-			nr += !isu;
-			// member entry (irow, pos) for column c: only this thread owns c now
-			const int n0 = __ldcg(A.mcnt + c);
-			int ch = __ldcg(A.mtail + c);
-			if ((n0 % CH) == 0) {
-				const int nc = atomicAdd(A.pool, 1);
-				if (nc >= A.pool_cap) {
-					fail = 4;
-					continue;
-				}
-				A.chnext[nc] = -1;
-				if (ch >= 0) A.chnext[ch] = nc;
-				else A.mhead[c] = nc;
-				A.mtail[c] = nc;
-				ch = nc;
-			}
-			A.chk[(size_t)ch * CH + (n0 % CH)] = irow;
-			A.chq[(size_t)ch * CH + (n0 % CH)] = pos;
-			A.mcnt[c] = n0 + 1;
-		}
-		if (nu) atomicAdd(A.nstored, nu);
-		if (nr) atomicAdd(A.nstored + 1, nr);
-		__syncthreads();
-		if (tid == 0) {
-			base += 1 + nk;
-			A.ig[irow + 1] = base;
-			atomicAdd(A.nstored, 1ull); // the pivot block
-		}
-		__syncthreads();
-		if (fail) break;
-	}
-	if (tid == 0 && fail) {
-		if (fail == 5) devstat_fail(A.st, BSG_ERR_PIVOT, failrow, 2);
-		else devstat_fail(A.st, BSG_ERR_WORKSPACE, 0, 100 + fail);
-	}
 }
 
 // ---- final: the U part scaled back (Ich2StoreScaleU) ----------------------
@@ -748,42 +338,18 @@ int bsg_bfact_run(bsg_ctx *c, bsg_mat *m, int sym, const bsg_param *p, bsg_fct *
 	BALLOC(diagg, double, (long long)nb * 9);
 	BSG_COUNT(1);
 	k_bscale<<<nb_(nb, 128), 128, 0, st>>>(nb, sym, bia, bau, p->sclmin, scll, sclu, sinvl, sinvu, diagg, c->d_stat);
-	// ---- row kernel workspace
-	const double mem = fabs(p->memory) > 1.0 ? fabs(p->memory) : 1.0;
-	const long long cap = (long long)(mem * (double)nnzb) + nb + 16;
-	if (cap > 0x7fffffffLL) return bsg_set_error(BSG_ERR_ARG, "block factorisation: workspace above 2^31 blocks");
-	const int pool_cap = (int)(nb + cap / CH + 16);
-	BALLOC(fml, double, (long long)nb * 9);
-	BALLOC(fmu, double, (long long)nb * 9);
-	BALLOC(imask, int, nb);
-	BALLOC(ig, int, nb + 1);
-	BALLOC(jg, int, cap);
-	BALLOC(gl, double, cap * 9);
-	BALLOC(gu, double, cap * 9);
-	BALLOC(mhead, int, nb);
-	BALLOC(mtail, int, nb);
-	BALLOC(mcnt, int, nb);
-	BALLOC(chk, int, (long long)pool_cap * CH);
-	BALLOC(chq, int, (long long)pool_cap * CH);
-	BALLOC(chnext, int, pool_cap);
-	BALLOC(pool, int, 1);
+	// ---- the rows, a warp each, on the dynamic schedule of the point factorisation
 	BALLOC(nstored, unsigned long long, 2);
-	BSG_CUDA(cudaMemsetAsync(imask, 0xff, sizeof(int) * nb, st));
-	BSG_CUDA(cudaMemsetAsync(mhead, 0xff, sizeof(int) * nb, st));
-	BSG_CUDA(cudaMemsetAsync(mtail, 0xff, sizeof(int) * nb, st));
-	BSG_CUDA(cudaMemsetAsync(mcnt, 0, sizeof(int) * nb, st));
-	BSG_CUDA(cudaMemsetAsync(pool, 0, sizeof(int), st));
-	BSG_CUDA(cudaMemsetAsync(nstored, 0, sizeof(unsigned long long) * 2, st));
-	BArgs A;
-	A.nb = nb; A.bia = bia; A.bja = bja; A.al = bal; A.au = bau; A.scll = scll; A.sclu = sclu; A.diagg = diagg;
-	A.fml = fml; A.fmu = fmu; A.imask = imask; A.ig = ig; A.jg = jg; A.gl = gl; A.gu = gu; A.cap = cap;
-	A.mhead = mhead; A.mtail = mtail; A.mcnt = mcnt; A.chk = chk; A.chq = chq; A.chnext = chnext; A.pool = pool;
-	A.pool_cap = pool_cap; A.tau1 = p->tau1; A.tau2 = p->tau2; A.theta = p->theta; A.pivmin = p->pivmin;
-	A.nstored = nstored; A.st = c->d_stat; A.sym = sym;
-	BSG_CUDA(cudaFuncSetAttribute(k_bilu2_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BSMEM));
-	BSG_COUNT(1);
-	k_bilu2_rows<<<1, BT, BSMEM, st>>>(A);
-	BSG_CUDA(cudaGetLastError());
+	int *ig = nullptr, *jg = nullptr;
+	double *gl = nullptr, *gu = nullptr;
+	{
+		const int rcd = bsg_bfact_dyn(c, nb, sym, p, bia, bja, nnzb, bal, bau, scll, sclu, diagg, &ig, &jg, &gl, &gu,
+		                              nstored);
+		if (rcd) return rcd;
+	}
+	DevVec ig_h, jg_h, gl_h, gu_h;
+	ig_h.p = ig; jg_h.p = jg; gl_h.p = gl; gu_h.p = gu;
+	ig_h.s = jg_h.s = gl_h.s = gu_h.s = st;
 	int rc = bsg_check_devstat(c);
 	if (rc) return rc;
 	// ---- U part scaled back

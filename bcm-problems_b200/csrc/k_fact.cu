@@ -48,6 +48,7 @@
 // Bslib/ich2r.cpp:910-954) and each row's depth in the forward-solve
 // dependency graph (the level schedule of the triangular solves).
 #include "bsg_internal.cuh"
+#include "bsg_blk3.cuh"
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 
@@ -82,6 +83,12 @@
 #ifndef WSETCAP
 #define WSETCAP 128 // far members (hash slots, a power of two)
 #endif
+// block rows (3 x 3 blocks): mask columns of the shared workspace, member
+// bitmap window
+#define HCAP_BLK 256
+#define CMAX_BLK 256
+#define MWIN_BLK 8192
+#define FACT_WARPS_BLK 2 // warps of a CTA in block mode (larger workspaces)
 #define W_EMPTY (-1)
 #define W_CLOSED (-2)
 
@@ -134,56 +141,61 @@ struct PhaseClock {
 // (GlobWS), so any row up to the big capacities factors.  Both expose the
 // same members; sc[] = {members, mask columns, kept columns, blocking row}.
 // IC2 (ILU false) keeps one value per column: its shared workspace has no
-// U-side arrays, so more warps fit on an SM.
-template <bool ILU>
+// U-side arrays, so more warps fit on an SM.  Block rows (BLK) keep 9
+// values per column (U side; ILU: then the L side at 9 (hcap + slot)) in hl
+// and read their members' blocks straight from the pool.
+template <bool ILU, bool BLK = false>
 struct SmemWS {
-	static constexpr bool big = false, ilu = ILU;
-	static constexpr int cmax = CMAX, hcap = HCAP, pfcap = PFCAP, wcap = WSETCAP;
-	int W[CMAX];           // members (discovery order, then sorted)
-	int Wp[CMAX];          // pool index of column i in that row (stored members)
-	int We[CMAX];          // pool end of that row
-	unsigned char Wf[CMAX];
-	int Ws[CMAX], Wps[CMAX], Wes[CMAX];
-	unsigned char Wfs[CMAX];
-	int Wb[CMAX + 1];      // prefetch segment bases (sorted order)
-	unsigned char Wst[CMAX]; // member state: 0 not closed, 1 closed, 2 applied
-	int wset[WSETCAP];     // membership hash of W (keys), members below i - MWIN
-	unsigned wbits[MWIN > 0 ? MWIN / 32 : 1]; // membership bitmap: bit i - 1 - k for member k
-	int hkey[HCAP];        // column accumulator
-	double hl[HCAP], hu[ILU ? HCAP : 1];
-	int lsts[HCAP];        // selected members (updates); sorted slots (finish)
+	static constexpr bool big = false, ilu = ILU, blk = BLK;
+	static constexpr int cmax = BLK ? CMAX_BLK : CMAX, hcap = BLK ? HCAP_BLK : HCAP, pfcap = PFCAP,
+	                     wcap = WSETCAP, mwin = BLK ? MWIN_BLK : MWIN;
+	int W[cmax];           // members (discovery order, then sorted)
+	int Wp[cmax];          // pool index of column i in that row (stored members)
+	int We[cmax];          // pool end of that row
+	unsigned char Wf[cmax];
+	int Ws[cmax], Wps[cmax], Wes[cmax];
+	unsigned char Wfs[cmax];
+	int Wb[cmax + 1];      // prefetch segment bases (sorted order)
+	unsigned char Wst[cmax]; // member state: 0 not closed, 1 closed, 2 applied
+	int wset[WSETCAP];     // membership hash of W (keys), members below i - mwin
+	unsigned wbits[mwin > 0 ? mwin / 32 : 1]; // membership bitmap: bit i - 1 - k for member k
+	int hkey[hcap];        // column accumulator
+	double hl[BLK ? hcap * (ILU ? 18 : 9) : HCAP], hu[ILU && !BLK ? HCAP : 1];
+	int lsts[hcap];        // selected members (updates); sorted slots (finish)
 	// the updates' prefetch buffers and the finish's slot lists are never
 	// live at once; Wlv (depth of a closed member) lives in a closure pass
 	union {
 		struct {
-			unsigned pf_cf[PFCAP]; // prefetched contributor segments
-			short pf_slot[PFCAP];
+			unsigned pf_cf[BLK ? 1 : PFCAP]; // prefetched contributor segments
+			short pf_slot[BLK ? 1 : PFCAP];
 		};
 		struct {
-			int lst[HCAP];         // extracted slots, then sorted
-			int lkey[HCAP];        // columns of the extracted slots
+			int lst[hcap];         // extracted slots, then sorted
+			int lkey[hcap];        // columns of the extracted slots
 		};
-		int Wlv[CMAX];
+		int Wlv[cmax];
 	};
-	double pf_l[PFCAP], pf_u[ILU ? PFCAP : 1];
+	double pf_l[BLK ? 1 : PFCAP], pf_u[ILU && !BLK ? PFCAP : 1];
 	int sc[4];
 };
 
-template <bool ILU>
+template <bool ILU, bool BLK = false>
 struct GlobWS {
-	static constexpr bool big = true, ilu = ILU;
-	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG, wcap = 2 * CMAX_BIG;
-	static constexpr size_t bytes = 8 * (2 * (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
+	static constexpr bool big = true, ilu = ILU, blk = BLK;
+	static constexpr int cmax = CMAX_BIG, hcap = HCAP_BIG, pfcap = PFCAP_BIG, wcap = 2 * CMAX_BIG,
+	                     mwin = BLK ? MWIN_BLK : MWIN;
+	static constexpr size_t nval = BLK ? 18 * (size_t)HCAP_BIG : (size_t)HCAP_BIG; // hl doubles
+	static constexpr size_t bytes = 8 * (nval + (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
 	                                4 * (7 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
 	                                     4 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
-	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG + MWIN / 8;
+	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG + mwin / 8;
 	double *hl, *hu, *pf_l, *pf_u;
 	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wlv, *Wb, *wset, *hkey, *lst, *lsts, *lkey, *sc;
 	unsigned *pf_cf, *wbits;
 	short *pf_slot;
 	unsigned char *Wf, *Wfs, *Wst;
 	__device__ explicit GlobWS(unsigned char *p) {
-		hl = reinterpret_cast<double *>(p); hu = hl + HCAP_BIG;
+		hl = reinterpret_cast<double *>(p); hu = hl + nval;
 		pf_l = hu + HCAP_BIG; pf_u = pf_l + PFCAP_BIG;
 		W = reinterpret_cast<int *>(pf_u + PFCAP_BIG);
 		Wp = W + CMAX_BIG; We = Wp + CMAX_BIG; Ws = We + CMAX_BIG; Wps = Ws + CMAX_BIG; Wes = Wps + CMAX_BIG;
@@ -231,8 +243,16 @@ __device__ int hfind_insert(WS &s, int c) {
 		if (k == -1) {
 			int old = atomicCAS(&s.hkey[h], -1, c);
 			if (old == -1) {
-				s.hl[h] = 0.0;
-				if (WS::ilu) s.hu[h] = 0.0;
+				if (WS::blk) {
+#pragma unroll
+					for (int k = 0; k < 9; k++) s.hl[9 * h + k] = 0.0;
+					if (WS::ilu)
+#pragma unroll
+						for (int k = 0; k < 9; k++) s.hl[9 * (s.hcap + h) + k] = 0.0;
+				} else {
+					s.hl[h] = 0.0;
+					if (WS::ilu) s.hu[h] = 0.0;
+				}
 				return (int)h;
 			}
 			if (old == c) return (int)h;
@@ -248,7 +268,7 @@ __device__ int hfind_insert(WS &s, int c) {
 template <class WS>
 __device__ int wset_insert(WS &s, int i, int k) {
 	const int d = i - 1 - k;
-	if (d < MWIN) {
+	if (d < WS::mwin) {
 		const unsigned bit = 1u << (d & 31);
 		if (s.wbits[d >> 5] & bit) return 0;
 		return (atomicOr(&s.wbits[d >> 5], bit) & bit) ? 0 : 1;
@@ -676,6 +696,328 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 	return __reduce_min_sync(0xffffffffu, err);
 }
 
+
+// After row i is published: release the rows of A's row i, wake the rows
+// parked on i, count.
+__device__ void after_publish(const FactArgs &A, int i, int lane) {
+	for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) admit_step(A, A.ju[k], ADM_ONE_FIN);
+	if (lane == 0) {
+		__threadfence();
+		int w = atomicExch(A.whead + i, W_CLOSED);
+		while (w >= 0) {
+			int nx = *(volatile int *)(A.wnext + w);
+			q_push(A, w);
+			w = nx;
+		}
+	}
+	__syncwarp();
+	if (lane == 0) atomicAdd(A.done_count, 1);
+}
+
+// ---- block rows (CSMatrixRS::Ich2 / Ilu2, 3 x 3 column-major blocks) -------
+// A's blocks, the scalings and the scaled diagonal blocks are 9 doubles
+// each (al / au / scll / sclu / diag0); a pool entry holds a block column
+// (cf) and 9 doubles in pool_l (the L side; IC2: the only side) and, for
+// ILU2, pool_u.  Entry 0 of a row is the pivot scaling (pool_l = dl^T,
+// pool_u = du^T) with the row's depth in its column field.
+
+template <class WS>
+__device__ __forceinline__ double *bv_u(WS &s, int h) { return s.hl + 9 * h; }
+template <class WS>
+__device__ __forceinline__ double *bv_l(WS &s, int h) { return s.hl + 9 * (s.hcap + h); }
+
+// The scaled block row of A (Ilu2 / Ich2 init: scll_i A_ij scll_j^T, the
+// diagonal block with its scaling done).
+template <class WS>
+__device__ int init_blk(const FactArgs &A, WS &s, int i, int lane) {
+	int err = 0;
+	if (lane == 0) {
+		const int h = hfind_insert(s, i);
+		double *u = bv_u(s, h);
+#pragma unroll
+		for (int k = 0; k < 9; k++) u[k] = __ldg(A.diag0 + 9 * (size_t)i + k);
+		if (WS::ilu) {
+			double *l = bv_l(s, h);
+#pragma unroll
+			for (int k = 0; k < 9; k++) l[k] = u[k];
+		}
+	}
+	__syncwarp();
+	const double *sli = A.scll + 9 * (size_t)i, *sui = A.sclu + 9 * (size_t)i;
+	for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) {
+		const int j = A.ju[k];
+		const int h = hfind_insert(s, j);
+		if (h < 0) {
+			err = BSG_ERR_WORKSPACE;
+			continue;
+		}
+		double t[9];
+		mm3(sli, 1, 3, A.au + 9 * (size_t)k, 1, 3, t);
+		mm3(t, 1, 3, A.sclu + 9 * (size_t)j, 3, 1, bv_u(s, h));
+		if (WS::ilu) {
+			mm3(sui, 1, 3, A.al + 9 * (size_t)k, 1, 3, t);
+			mm3(t, 1, 3, A.scll + 9 * (size_t)j, 3, 1, bv_l(s, h));
+		}
+	}
+	err = __reduce_min_sync(0xffffffffu, err);
+	__syncwarp();
+	return err;
+}
+
+// The updates of the closed members below `bound`, ascending: member k with
+// its block at column i (L: gl, U: gu) updates every block e of its row from
+// column i on: f_u(c) -= gl^T gu_e, f_l(c) -= gu^T gl_e (R x R skipped).
+// The lanes take the blocks of one member (distinct columns), the members
+// go in order, so the sums do not depend on the schedule.
+template <class WS>
+__device__ int apply_blk(const FactArgs &A, WS &s, int bound, int lane, PhaseClock &pc) {
+	constexpr bool ilu = WS::ilu;
+	const int nW = min(s.sc[0], s.cmax);
+	if (lane == 0) s.sc[2] = 0;
+	__syncwarp();
+	for (int base = 0; base < nW; base += 32) {
+		const int t = base + lane;
+		const bool sel = t < nW && s.Wst[t] == 1 && s.W[t] < bound;
+		const unsigned b = __ballot_sync(0xffffffffu, sel);
+		const int pos0 = s.sc[2];
+		if (sel) s.lsts[pos0 + __popc(b & ((1u << lane) - 1))] = t;
+		__syncwarp();
+		if (lane == 0) s.sc[2] = pos0 + __popc(b);
+		__syncwarp();
+	}
+	const int nb = s.sc[2];
+	if (nb == 0) return 0;
+	pc.v[FS_BATCHES]++;
+	pc.v[FS_CLOSED] += nb;
+	for (int q = lane; q < nb; q += 32) {
+		const int t = s.lsts[q], k = s.W[t];
+		int r = 0;
+		for (int u = 0; u < nb; u++) r += s.W[s.lsts[u]] < k;
+		s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
+		s.Wst[t] = 2;
+	}
+	__syncwarp();
+	const double *pg_l = A.pool_l, *pg_u = ilu ? A.pool_u : A.pool_l;
+	int err = 0;
+	for (int t = 0; t < nb && !err; t++) {
+		if (s.Wfs[t] == F_D) continue;
+		const long long q = s.Wps[t], end = s.Wes[t];
+		const bool rr = s.Wfs[t] == F_R;
+		double lel[9], uel[9];
+#pragma unroll
+		for (int k = 0; k < 9; k++) {
+			lel[k] = __ldcg(pg_l + 9 * q + k);
+			uel[k] = ilu ? __ldcg(pg_u + 9 * q + k) : 0.0;
+		}
+		for (long long e = q + lane; e < end; e += 32) {
+			const unsigned cf = __ldcg(A.pool_cf + e);
+			if (rr && CF_FLAG(cf) == F_R) continue;
+			double gu[9], gl[9];
+#pragma unroll
+			for (int k = 0; k < 9; k++) {
+				gu[k] = __ldcg(pg_u + 9 * e + k);
+				gl[k] = ilu ? __ldcg(pg_l + 9 * e + k) : 0.0;
+			}
+			const int h = hfind_insert(s, CF_COL(cf));
+			if (h < 0) {
+				err = BSG_ERR_WORKSPACE;
+				continue;
+			}
+			double tu[9];
+			mm3(lel, 3, 1, gu, 1, 3, tu); // gl_q^T gu_e
+			double *u = bv_u(s, h);
+#pragma unroll
+			for (int k = 0; k < 9; k++) u[k] -= tu[k];
+			if (ilu) {
+				double tl[9];
+				mm3(uel, 3, 1, gl, 1, 3, tl); // gu_q^T gl_e
+				double *l = bv_l(s, h);
+#pragma unroll
+				for (int k = 0; k < 9; k++) l[k] -= tl[k];
+			}
+		}
+		__syncwarp();
+		err = __reduce_min_sync(0xffffffffu, err);
+	}
+	return err;
+}
+
+// Finish of a block row (Ilu2FiltrRow / Ilu2PivScaleRow, Bslib/ilu2rs.cpp:
+// 616-852; Ich2 forms, Bslib/ich2rs.cpp:532-647): blocks of max-norm below
+// tau2 are dropped, theta times their entries going to this row's pivot
+// block (row sums) and to the dropped column's diagonal block (column sums,
+// through its fixed-point accumulators); the pivot block with the
+// compensations received from other rows takes its SVD (IC2: eigenpairs,
+// a negative eigenvalue is a pivot error); the kept blocks are scaled and
+// stored as U (max-norm >= tau1) or R in ascending column order.
+template <class WS>
+__device__ int finish_blk(const FactArgs &A, WS &s, int i, int lane, int levmax, unsigned long long accraw,
+                          PhaseClock &pc, long long tail0) {
+	constexpr bool ilu = WS::ilu;
+	// the three received compensations (lanes 0..2)
+	const double comp = __dmul_rn((double)accraw, A.acc_inv_scale);
+	// ---- the off-diagonal mask columns, ascending
+	if (lane == 0) s.sc[1] = 0;
+	__syncwarp();
+	for (int h = lane; h < s.hcap; h += 32) {
+		const int c = s.hkey[h];
+		const bool take = c >= 0 && c != i;
+		const unsigned b = __ballot_sync(0xffffffffu, take);
+		const int base = s.sc[1];
+		if (take) {
+			const int q = base + __popc(b & ((1u << lane) - 1));
+			s.lst[q] = h;
+			s.lkey[q] = c;
+		}
+		__syncwarp();
+		if (lane == 0) s.sc[1] = base + __popc(b);
+		__syncwarp();
+	}
+	const int nl = s.sc[1];
+	for (int t0 = 0; t0 < nl; t0 += 32) {
+		const int t = t0 + lane;
+		const int key = t < nl ? s.lkey[t] : 0x7fffffff;
+		int rnk = 0;
+		for (int u = 0; u < nl; u++) rnk += s.lkey[u] < key;
+		if (t < nl) s.lsts[rnk] = s.lst[t];
+	}
+	__syncwarp();
+	const int di = hfind_insert(s, i);
+	// ---- filter (ascending columns; kept slots compacted into lst)
+	double rs0 = 0.0, rs1 = 0.0, rs2 = 0.0;
+	if (lane == 0) s.sc[2] = 0;
+	__syncwarp();
+	for (int t0 = 0; t0 < nl; t0 += 32) {
+		const int t = t0 + lane;
+		bool keep = false;
+		if (t < nl) {
+			const int h = s.lsts[t];
+			const double *u = bv_u(s, h), *l = ilu ? bv_l(s, h) : u;
+			double a[9], mx = 0.0;
+#pragma unroll
+			for (int k = 0; k < 9; k++) {
+				a[k] = fmax(fabs(l[k]), fabs(u[k]));
+				mx = fmax(mx, a[k]);
+			}
+			keep = mx >= A.tau2;
+			if (!keep) {
+				double cs0 = 0.0, cs1 = 0.0, cs2 = 0.0;
+#pragma unroll
+				for (int r = 0; r < 3; r++) {
+					const double v0 = A.theta * a[r], v1 = A.theta * a[r + 3], v2 = A.theta * a[r + 6];
+					const double rsum = v0 + v1 + v2;
+					if (r == 0) rs0 += rsum; else if (r == 1) rs1 += rsum; else rs2 += rsum;
+					cs0 += v0;
+					cs1 += v1;
+					cs2 += v2;
+				}
+				const int c = s.hkey[h];
+				acc_push(A.acc, 3 * c, cs0, A.acc_scale, A.st);
+				acc_push(A.acc, 3 * c + 1, cs1, A.acc_scale, A.st);
+				acc_push(A.acc, 3 * c + 2, cs2, A.acc_scale, A.st);
+			}
+		}
+		const unsigned b = __ballot_sync(0xffffffffu, keep);
+		const int base = s.sc[2];
+		if (keep) s.lst[base + __popc(b & ((1u << lane) - 1))] = s.lsts[t];
+		__syncwarp();
+		if (lane == 0) s.sc[2] = base + __popc(b);
+		__syncwarp();
+	}
+	rs0 = warp_sum(rs0);
+	rs1 = warp_sum(rs1);
+	rs2 = warp_sum(rs2);
+	const double c0 = __shfl_sync(0xffffffffu, comp, 0), c1 = __shfl_sync(0xffffffffu, comp, 1),
+	             c2 = __shfl_sync(0xffffffffu, comp, 2);
+	const int nk = s.sc[2];
+	const int len = nk + 1;
+	const int alloc = (len + 3) & ~3;
+	long long off = 0;
+	if (lane == 0) off = (long long)atomicAdd(A.pool_len, (unsigned long long)alloc);
+	// ---- pivot (lane 0): dl = diag(s^-1/2) U^T, du = diag(s^-1/2) V^T into
+	//      the diagonal slot (its values are not needed after this)
+	int bad = 0;
+	if (lane == 0) {
+		double fd[9];
+		double *u = bv_u(s, di);
+#pragma unroll
+		for (int k = 0; k < 9; k++) fd[k] = u[k];
+		fd[0] = (fd[0] + rs0) + c0;
+		fd[4] = (fd[4] + rs1) + c1;
+		fd[8] = (fd[8] + rs2) + c2;
+		double uu[9], vv[9], sv[3];
+		svd3(fd, uu, sv, vv);
+		if (!ilu) {
+			for (int k = 0; k < 3; k++) {
+				if (uu[3 * k] * vv[3 * k] + uu[1 + 3 * k] * vv[1 + 3 * k] + uu[2 + 3 * k] * vv[2 + 3 * k] < 0.0 &&
+				    sv[k] > 0.0)
+					bad = 1;
+				for (int r = 0; r < 3; r++) uu[r + 3 * k] = vv[r + 3 * k];
+				sv[k] = 1.0 / sqrt(sv[k]);
+			}
+		} else {
+			for (int k = 0; k < 3; k++) sv[k] = 1.0 / sqrt(sv[k] < A.pivmin ? A.pivmin : sv[k]);
+		}
+		double *dl = bv_u(s, di), *du = ilu ? bv_l(s, di) : dl;
+		for (int r = 0; r < 3; r++)
+			for (int c = 0; c < 3; c++) {
+				dl[r + 3 * c] = uu[c + 3 * r] * sv[r];
+				if (ilu) du[r + 3 * c] = vv[c + 3 * r] * sv[r];
+			}
+	}
+	bad = __shfl_sync(0xffffffffu, bad, 0);
+	if (bad) {
+		if (lane == 0) devstat_fail(A.st, BSG_ERR_PIVOT, i);
+		return -2;
+	}
+	off = __shfl_sync(0xffffffffu, off, 0);
+	if (off + alloc > A.pool_cap || len > 0xffff) {
+		if (lane == 0) devstat_fail(A.st, BSG_ERR_WORKSPACE, i, 6);
+		return -2;
+	}
+	__syncwarp();
+	const double *dl = bv_u(s, di), *du = ilu ? bv_l(s, di) : dl;
+	// ---- store: the pivot scaling, then the kept blocks scaled
+	if (lane < 9) {
+		const int r = lane % 3, c = lane / 3;
+		if (lane == 0) A.pool_cf[off] = (unsigned)levmax | (F_U << 30);
+		A.pool_l[9 * off + lane] = dl[c + 3 * r];
+		if (ilu) A.pool_u[9 * off + lane] = du[c + 3 * r];
+	}
+	for (int t = lane; t < nk; t += 32) {
+		const int h = s.lst[t];
+		const double *u = bv_u(s, h), *l = ilu ? bv_l(s, h) : u;
+		double tu[9], tl[9];
+		mm3(dl, 1, 3, u, 1, 3, tu);
+		if (ilu) mm3(du, 1, 3, l, 1, 3, tl);
+		double mx = 0.0;
+#pragma unroll
+		for (int k = 0; k < 9; k++) {
+			if (!ilu) tl[k] = tu[k];
+			mx = fmax(mx, fmax(fabs(tl[k]), fabs(tu[k])));
+		}
+		const unsigned flag = mx >= A.tau1 ? F_U : F_R;
+		const long long e = off + 1 + t;
+		A.pool_cf[e] = (unsigned)s.hkey[h] | (flag << 30);
+#pragma unroll
+		for (int k = 0; k < 9; k++) {
+			A.pool_l[9 * e + k] = tl[k];
+			if (ilu) A.pool_u[9 * e + k] = tu[k];
+		}
+	}
+	if (lane == 0) A.lev[i] = levmax;
+	__threadfence();
+	__syncwarp();
+	if (lane == 0) st_release_u64(A.rec + i, REC_DONE | ((unsigned long long)off << 32) | (unsigned long long)len);
+	__syncwarp();
+	const long long cpub = clock64();
+	pc.v[FS_CYC_TOPUB] += cpub - tail0;
+	after_publish(A, i, lane);
+	pc.v[FS_CYC_TAIL] += clock64() - tail0;
+	pc.v[FS_MASK] += nl;
+	return -1;
+}
+
 // Factor row i.  Returns -1 when done, the unfinished row it waits for
 // (>= 0), -2 on error (reported through the status word), or -3 when the
 // row does not fit a shared-memory workspace (nothing was published yet, so
@@ -692,7 +1034,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	constexpr bool ilu = WS::ilu;
 	const long long c0 = clock64();
 	for (int t = lane; t < s.wcap; t += 32) s.wset[t] = -1;
-	for (int t = lane; t < MWIN / 32; t += 32) s.wbits[t] = 0u; // (no bitmap: MWIN 0)
+	for (int t = lane; t < WS::mwin / 32; t += 32) s.wbits[t] = 0u; // (no bitmap: mwin 0)
 	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
 	if (lane == 0) s.sc[0] = 0;
 	__syncwarp();
@@ -717,6 +1059,14 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	//      received from rows that dropped column i join the diagonal last
 	int err = 0;
 	const int ab = A.iu[i], ae = A.iu[i + 1];
+	if constexpr (WS::blk) {
+		err = init_blk(A, s, i, lane);
+		if (err) {
+			if (!WS::big) return -3;
+			if (lane == 0) devstat_fail(A.st, err, i, 4);
+			return -2;
+		}
+	} else {
 	if (lane == 0) {
 		int slot = hfind_insert(s, i);
 		s.hl[slot] = A.diag0[i];
@@ -743,6 +1093,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		if (!WS::big) return -3;
 		if (lane == 0) devstat_fail(A.st, err, i, 4);
 		return -2;
+	}
 	}
 
 	int levmax = 0;
@@ -780,9 +1131,10 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		// the compensations received so far (every member seen finished has
 		// pushed its own before publishing): loaded now, used after the last
 		// pass, so the load overlaps the updates
-		if (lane == 0) accraw = __ldcg(A.acc + i);
+		if (lane < (WS::blk ? 3 : 1)) accraw = __ldcg(A.acc + (WS::blk ? 3 * (size_t)i + lane : (size_t)i));
 		// ---- updates of the closed members below the bound
-		err = apply_members(A, s, bound, lane, pc);
+		if constexpr (WS::blk) err = apply_blk(A, s, bound, lane, pc);
+		else err = apply_members(A, s, bound, lane, pc);
 		const long long k2 = clock64();
 		pc.v[FS_CYC_UPD] += k2 - k1;
 		if (err) {
@@ -810,6 +1162,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	}
 	levmax = __reduce_max_sync(0xffffffffu, levmax);
 	pc.v[FS_CONTRIB] += min(s.sc[0], s.cmax);
+	if constexpr (WS::blk) return finish_blk(A, s, i, lane, levmax, accraw, pc, tail0);
 	{
 		const double comp = __dmul_rn((double)__shfl_sync(0xffffffffu, accraw, 0), A.acc_inv_scale);
 		if (lane == 0) {
@@ -975,19 +1328,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	pc.v[FS_CYC_TOPUB] += cpub - tail0;
 	pc.v[FS_CYC_FPRE] += cpub - c3;
 
-	// ---- release the rows of A's row i, wake parked rows, count
-	for (int k = A.iu[i] + 1 + lane; k < A.iu[i + 1]; k += 32) admit_step(A, A.ju[k], ADM_ONE_FIN);
-	if (lane == 0) {
-		__threadfence();
-		int w = atomicExch(A.whead + i, W_CLOSED);
-		while (w >= 0) {
-			int nx = *(volatile int *)(A.wnext + w);
-			q_push(A, w);
-			w = nx;
-		}
-	}
-	__syncwarp();
-	if (lane == 0) atomicAdd(A.done_count, 1);
+	after_publish(A, i, lane);
 	const long long c4 = clock64();
 	pc.v[FS_CYC_POSTPUB] += c4 - cpub;
 	pc.v[FS_CYC_FIN] += c4 - c3;
@@ -996,11 +1337,12 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	return -1;
 }
 
-template <bool ILU>
-__global__ void __launch_bounds__(FACT_WARPS * 32, FACT_MINB) k_fact_rows(FactArgs A) {
+template <bool ILU, bool BLK>
+__global__ void __launch_bounds__((BLK ? FACT_WARPS_BLK : FACT_WARPS) * 32, FACT_MINB) k_fact_rows(FactArgs A) {
+	constexpr int fw = BLK ? FACT_WARPS_BLK : FACT_WARPS;
 	extern __shared__ unsigned char smem_raw[];
 	const int warp = threadIdx.x >> 5;
-	SmemWS<ILU> &s = reinterpret_cast<SmemWS<ILU> *>(smem_raw)[warp];
+	SmemWS<ILU, BLK> &s = reinterpret_cast<SmemWS<ILU, BLK> *>(smem_raw)[warp];
 	const int lane = threadIdx.x & 31;
 	PhaseClock pc;
 #pragma unroll
@@ -1033,7 +1375,7 @@ __global__ void __launch_bounds__(FACT_WARPS * 32, FACT_MINB) k_fact_rows(FactAr
 			pc.v[FS_BIG]++;
 			int slot = -1;
 			if (lane == 0) {
-				const int start = (int)((blockIdx.x * FACT_WARPS + warp) % BIG_SLOTS);
+				const int start = (int)((blockIdx.x * fw + warp) % BIG_SLOTS);
 				for (int k = 0; k < BIG_SLOTS && slot < 0; k++) {
 					const int q = (start + k) % BIG_SLOTS;
 					if (atomicCAS(A.big_owner + q, 0, 1) == 0) slot = q;
@@ -1050,7 +1392,7 @@ __global__ void __launch_bounds__(FACT_WARPS * 32, FACT_MINB) k_fact_rows(FactAr
 				continue;
 			}
 			__threadfence();
-			GlobWS<ILU> g(A.big_ws + (size_t)slot * GlobWS<ILU>::bytes);
+			GlobWS<ILU, BLK> g(A.big_ws + (size_t)slot * GlobWS<ILU, BLK>::bytes);
 			r = try_row(A, g, i, lane, pc);
 			__syncwarp();
 			if (lane == 0) {
@@ -1175,7 +1517,38 @@ __global__ void k_level_keys(int n, const int *lev, unsigned long long *keys, in
 	vals[i] = i;
 }
 
+// block rows: stored blocks per row, then the rows in order (pivot scaling
+// first: column i; U blocks +column, R blocks -column), counts of U / R
+__global__ void k_blk_len(int nb, const unsigned long long *rec, int *cnt) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < nb) cnt[i] = REC_LEN(rec[i]);
+}
+__global__ void k_blk_emit(int nb, int ilu, const unsigned long long *rec, const unsigned *cf, const double *pl,
+                           const double *pu, const int *ig, int *jg, double *gl, double *gu, unsigned long long *nst) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nb) return;
+	const long long off = REC_OFF(rec[i]);
+	const int len = REC_LEN(rec[i]);
+	const long long o = ig[i];
+	unsigned long long nu = 0, nr = 0;
+	for (int e = 0; e < len; e++) {
+		const unsigned x = cf[off + e];
+		const bool u = e == 0 || CF_FLAG(x) == F_U;
+		const int col = e == 0 ? i : CF_COL(x);
+		jg[o + e] = u ? col : -col;
+		nu += u;
+		nr += !u;
+		for (int k = 0; k < 9; k++) {
+			gl[9 * (o + e) + k] = pl[9 * (off + e) + k];
+			gu[9 * (o + e) + k] = ilu ? pu[9 * (off + e) + k] : pl[9 * (off + e) + k];
+		}
+	}
+	atomicAdd(nst, nu);
+	atomicAdd(nst + 1, nr);
+}
+
 inline int nb(long long n, int t) { return n > 0 ? (int)((n + t - 1) / t) : 1; }
+inline int nb_blocks(long long n) { return nb(n, 256); }
 
 } // namespace
 
@@ -1275,7 +1648,7 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
 	BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
 	k_fact_seed<<<nb(n, 256), 256, 0, st>>>(A);
-	void (*kern)(FactArgs) = kind == 1 ? k_fact_rows<true> : k_fact_rows<false>;
+	void (*kern)(FactArgs) = kind == 1 ? k_fact_rows<true, false> : k_fact_rows<false, false>;
 	const size_t smem = (kind == 1 ? sizeof(SmemWS<true>) : sizeof(SmemWS<false>)) * FACT_WARPS;
 	BSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	int per_sm = 0;
@@ -1376,4 +1749,166 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 // this unit's copy of the spin-wait bound (bsg_set_spin_limit_ns)
 int bsg_spin_limit_set_fact(unsigned long long ns) {
 	return bsg_spin_limit_set_here(ns) == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
+}
+
+// Block IC2 (sym) / ILU2 of 3 x 3 block rows with the dynamic schedule of
+// the point factorisation: a warp per block row, the closure over finished
+// rows, admission, waiting, parking and promotion unchanged; the row's
+// arithmetic on blocks (init_blk / apply_blk / finish_blk).  Input: the
+// CombineLU block pattern (diagonal first) with its scaled values and
+// scalings (9 doubles each, column-major).  Output: the stored rows in row
+// order (ig[nb + 1]; jg: +column U, -column R, the pivot scaling first;
+// gl / gu: 9 doubles a block), allocated here, and the U / R counts.
+int bsg_bfact_dyn(bsg_ctx *c, int nb, int sym, const bsg_param *p, const int *bia, const int *bja, int nnzb,
+                  const double *bal, const double *bau, const double *scll, const double *sclu, const double *diagg,
+                  int **ig_o, int **jg_o, double **gl_o, double **gu_o, unsigned long long *nstored) {
+	const int kind = sym ? 0 : 1;
+	cudaStream_t st = c->stream;
+	int *it = nullptr, *jt = nullptr, nt = 0;
+	int rc = bsg_strict_transpose(c, nb, bia, bja, nnzb, &it, &jt, nullptr, &nt);
+	if (rc) return rc;
+	double mem = p->memory < 0 ? -p->memory : p->memory;
+	if (mem < 8.0) mem = 8.0;
+	long long qcap = 1;
+	while (qcap < 2LL * nb + 65536) qcap <<= 1;
+	double *pl = nullptr, *pu = nullptr;
+	unsigned *cf = nullptr;
+	unsigned long long *rec, *acc, *pool_len, *qhead, *qtail;
+	int *lev, *nstat, *whead, *wnext, *queue, *done_count, *inprog;
+	BSG_CUDA(cudaMallocAsync(&rec, sizeof(unsigned long long) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&acc, sizeof(unsigned long long) * 3 * (size_t)nb, st));
+	BSG_CUDA(cudaMallocAsync(&lev, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&nstat, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&whead, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&wnext, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&inprog, sizeof(int) * nb, st));
+	BSG_CUDA(cudaMallocAsync(&queue, sizeof(int) * qcap, st));
+	BSG_CUDA(cudaMallocAsync(&done_count, sizeof(int), st));
+	BSG_CUDA(cudaMallocAsync(&pool_len, sizeof(unsigned long long), st));
+	BSG_CUDA(cudaMallocAsync(&qhead, sizeof(unsigned long long), st));
+	BSG_CUDA(cudaMallocAsync(&qtail, sizeof(unsigned long long), st));
+	void (*kern)(FactArgs) = kind == 1 ? k_fact_rows<true, true> : k_fact_rows<false, true>;
+	const size_t smem = (kind == 1 ? sizeof(SmemWS<true, true>) : sizeof(SmemWS<false, true>)) * FACT_WARPS_BLK;
+	const size_t big = kind == 1 ? GlobWS<true, true>::bytes : GlobWS<false, true>::bytes;
+	BSG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	int per_sm = 0;
+	BSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FACT_WARPS_BLK * 32, smem));
+	if (per_sm < 1) per_sm = 1;
+	int grid = per_sm * BSG_SMS;
+	const int need = (nb + FACT_WARPS_BLK - 1) / FACT_WARPS_BLK;
+	if (grid > need) grid = need;
+	if (grid < 1) grid = 1;
+	FactArgs A;
+	A.n = nb; A.kind = kind;
+	A.iu = bia; A.ju = bja; A.al = bal; A.au = bau;
+	A.it = it; A.jt = jt;
+	A.scll = scll; A.sclu = sclu; A.diag0 = diagg;
+	A.tau1 = p->tau1; A.tau2 = p->tau2; A.theta = p->theta; A.pivmin = p->pivmin;
+	A.pool_len = pool_len;
+	A.rec = rec; A.acc = acc; A.lev = lev;
+	// a compensation column sum has three terms below tau2 * theta each
+	bsg_comp_scale(3.0 * p->tau2, p->theta, &A.acc_scale, &A.acc_inv_scale);
+	A.nstat = nstat; A.whead = whead; A.wnext = wnext; A.inprog = inprog; A.queue = queue; A.qcap = qcap;
+	A.qhead = qhead; A.qtail = qtail; A.done_count = done_count; A.st = c->d_stat;
+	if (cudaMallocAsync(&A.big_ws, big * (size_t)BIG_SLOTS, st) != cudaSuccess)
+		return bsg_set_error(BSG_ERR_NOMEM, "block factor row workspace");
+	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * BIG_SLOTS, st));
+	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
+	// The pool first holds 8 blocks per block of A (block IC2 / ILU2 keep
+	// about 4); a factor that needs more is computed again with the pool
+	// the memory parameter allows.
+	for (double memu = mem < 8.0 ? mem : 8.0;; memu = mem) {
+		long long cap = (long long)(memu * (double)nnzb) + 8LL * nb + 1024;
+		if (cap > 0x7ffffff0LL) cap = 0x7ffffff0LL;
+		if (cudaMallocAsync(&cf, sizeof(unsigned) * cap, st) != cudaSuccess ||
+		    cudaMallocAsync(&pl, sizeof(double) * 9 * cap, st) != cudaSuccess ||
+		    (kind == 1 && cudaMallocAsync(&pu, sizeof(double) * 9 * cap, st) != cudaSuccess))
+			return bsg_set_error(BSG_ERR_NOMEM, "block factor pool");
+		A.pool_cf = cf; A.pool_l = pl; A.pool_u = pu; A.pool_cap = cap;
+		BSG_CUDA(cudaMemsetAsync(c->d_stat, 0, sizeof(bsg_devstat), st));
+		BSG_CUDA(cudaMemsetAsync(pool_len, 0, sizeof(unsigned long long), st));
+		BSG_CUDA(cudaMemsetAsync(qhead, 0, sizeof(unsigned long long), st));
+		BSG_CUDA(cudaMemsetAsync(qtail, 0, sizeof(unsigned long long), st));
+		BSG_CUDA(cudaMemsetAsync(done_count, 0, sizeof(int), st));
+		BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * BIG_SLOTS, st));
+		BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
+		BSG_COUNT(4);
+		k_fact_init<<<nb_blocks(nb), 256, 0, st>>>(nb, it, nstat, whead, rec, acc, lev, inprog, c->d_stat);
+		BSG_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * 3 * (size_t)nb, st));
+		k_fill_int<<<BSG_SMS * 4, 256, 0, st>>>(qcap, queue, -1);
+		k_fact_seed<<<nb_blocks(nb), 256, 0, st>>>(A);
+		kern<<<grid, FACT_WARPS_BLK * 32, smem, st>>>(A);
+		BSG_CUDA(cudaGetLastError());
+		bsg_devstat h;
+		BSG_CUDA(cudaMemcpyAsync(&h, c->d_stat, sizeof(h), cudaMemcpyDeviceToHost, st));
+		BSG_CUDA(cudaStreamSynchronize(st));
+		if (h.code == BSG_ERR_WORKSPACE && h.pad[0] == 6 && memu < mem) { // the pool was too small
+			cudaFreeAsync(cf, st);
+			cudaFreeAsync(pl, st);
+			if (pu) cudaFreeAsync(pu, st);
+			cf = nullptr; pl = pu = nullptr;
+			continue;
+		}
+		break;
+	}
+	rc = bsg_check_devstat(c);
+	cudaMemcpyAsync(g_fact_stats, A.stats, sizeof(g_fact_stats), cudaMemcpyDeviceToHost, st);
+	cudaStreamSynchronize(st);
+	g_fact_stats[FS_WARPS] = (unsigned long long)grid * FACT_WARPS_BLK;
+	cudaFreeAsync(A.stats, st);
+	cudaFreeAsync(A.big_ws, st);
+	cudaFreeAsync(A.big_owner, st);
+	if (!rc) {
+		int ndone = 0;
+		BSG_CUDA(cudaMemcpy(&ndone, done_count, sizeof(int), cudaMemcpyDeviceToHost));
+		if (ndone != nb) rc = bsg_set_error(BSG_ERR_TIMEOUT, "block factorisation scheduler stopped early");
+	}
+	int *cnt = nullptr, *ig = nullptr;
+	if (!rc && (cudaMallocAsync(&cnt, sizeof(int) * (nb + 1), st) != cudaSuccess ||
+	            cudaMallocAsync(&ig, sizeof(int) * (nb + 1), st) != cudaSuccess))
+		rc = bsg_set_error(BSG_ERR_NOMEM, "block factor rows");
+	long long total = 0;
+	if (!rc) {
+		BSG_COUNT(1);
+		cudaMemsetAsync(cnt + nb, 0, sizeof(int), st);
+		k_blk_len<<<nb_blocks(nb), 256, 0, st>>>(nb, rec, cnt);
+		size_t tmp = 0;
+		cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, ig, nb + 1, st);
+		void *d_tmp = nullptr;
+		if (cudaMallocAsync(&d_tmp, tmp + 1, st) != cudaSuccess) rc = bsg_set_error(BSG_ERR_NOMEM, "scan");
+		else {
+			cub::DeviceScan::ExclusiveSum(d_tmp, tmp, cnt, ig, nb + 1, st);
+			int t = 0;
+			cudaMemcpyAsync(&t, ig + nb, sizeof(int), cudaMemcpyDeviceToHost, st);
+			cudaStreamSynchronize(st);
+			total = t;
+			cudaFreeAsync(d_tmp, st);
+		}
+	}
+	int *jg = nullptr;
+	double *gl = nullptr, *gu = nullptr;
+	if (!rc && (cudaMallocAsync(&jg, sizeof(int) * (total > 0 ? total : 1), st) != cudaSuccess ||
+	            cudaMallocAsync(&gl, sizeof(double) * 9 * (total > 0 ? total : 1), st) != cudaSuccess ||
+	            cudaMallocAsync(&gu, sizeof(double) * 9 * (total > 0 ? total : 1), st) != cudaSuccess))
+		rc = bsg_set_error(BSG_ERR_NOMEM, "block factor rows");
+	if (!rc) {
+		BSG_COUNT(1);
+		cudaMemsetAsync(nstored, 0, sizeof(unsigned long long) * 2, st);
+		k_blk_emit<<<nb_blocks(nb), 256, 0, st>>>(nb, kind, rec, cf, pl, pu, ig, jg, gl, gu, nstored);
+		if (cudaGetLastError() != cudaSuccess) rc = bsg_set_error(BSG_ERR_CUDA, "block factor rows");
+	}
+	for (void *q : {(void *)it, (void *)jt, (void *)cf, (void *)pl, (void *)pu, (void *)rec, (void *)acc, (void *)lev,
+	                (void *)nstat, (void *)whead, (void *)wnext, (void *)inprog, (void *)queue, (void *)done_count,
+	                (void *)pool_len, (void *)qhead, (void *)qtail, (void *)cnt})
+		if (q) cudaFreeAsync(q, st);
+	if (rc) {
+		for (void *q : {(void *)ig, (void *)jg, (void *)gl, (void *)gu})
+			if (q) cudaFreeAsync(q, st);
+		return rc;
+	}
+	*ig_o = ig;
+	*jg_o = jg;
+	*gl_o = gl;
+	*gu_o = gu;
+	return BSG_OK;
 }
