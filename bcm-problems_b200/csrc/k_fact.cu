@@ -177,6 +177,7 @@ struct SmemWS {
 	};
 	double pf_l[BLK ? 1 : PFCAP], pf_u[ILU && !BLK ? PFCAP : 1];
 	int sc[4];
+	int slots[1];          // (the global workspace lists its slots; this one scans them)
 };
 
 template <bool ILU, bool BLK = false>
@@ -188,10 +189,11 @@ struct GlobWS {
 	static constexpr size_t bytes = 8 * (nval + (size_t)HCAP_BIG + 2 * (size_t)PFCAP_BIG) +
 	                                4 * (7 * (size_t)CMAX_BIG + (CMAX_BIG + 4) + 2 * (size_t)CMAX_BIG +
 	                                     4 * (size_t)HCAP_BIG + PFCAP_BIG + 4) +
-	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG + mwin / 8;
+	                                2 * (size_t)PFCAP_BIG + 3 * (size_t)CMAX_BIG + mwin / 8 + 4 * (size_t)HCAP_BIG;
 	double *hl, *hu, *pf_l, *pf_u;
 	int *W, *Wp, *We, *Ws, *Wps, *Wes, *Wlv, *Wb, *wset, *hkey, *lst, *lsts, *lkey, *sc;
 	unsigned *pf_cf, *wbits;
+	int *slots;            // the accumulator slots in use, in insertion order
 	short *pf_slot;
 	unsigned char *Wf, *Wfs, *Wst;
 	__device__ explicit GlobWS(unsigned char *p) {
@@ -206,6 +208,7 @@ struct GlobWS {
 		pf_slot = reinterpret_cast<short *>(sc + 4);
 		Wf = reinterpret_cast<unsigned char *>(pf_slot + PFCAP_BIG); Wfs = Wf + CMAX_BIG; Wst = Wfs + CMAX_BIG;
 		wbits = reinterpret_cast<unsigned *>(Wst + CMAX_BIG);
+		slots = reinterpret_cast<int *>(wbits + mwin / 32);
 	}
 };
 
@@ -243,6 +246,7 @@ __device__ int hfind_insert(WS &s, int c) {
 		if (k == -1) {
 			int old = atomicCAS(&s.hkey[h], -1, c);
 			if (old == -1) {
+				if (WS::big) s.slots[atomicAdd(&s.sc[3], 1)] = (int)h;
 				if (WS::blk) {
 #pragma unroll
 					for (int k = 0; k < 9; k++) s.hl[9 * h + k] = 0.0;
@@ -856,42 +860,23 @@ __device__ int finish_blk(const FactArgs &A, WS &s, int i, int lane, int levmax,
 	constexpr bool ilu = WS::ilu;
 	// the three received compensations (lanes 0..2)
 	const double comp = __dmul_rn((double)accraw, A.acc_inv_scale);
-	// ---- the off-diagonal mask columns, ascending
-	if (lane == 0) s.sc[1] = 0;
-	__syncwarp();
-	for (int h = lane; h < s.hcap; h += 32) {
-		const int c = s.hkey[h];
-		const bool take = c >= 0 && c != i;
-		const unsigned b = __ballot_sync(0xffffffffu, take);
-		const int base = s.sc[1];
-		if (take) {
-			const int q = base + __popc(b & ((1u << lane) - 1));
-			s.lst[q] = h;
-			s.lkey[q] = c;
-		}
-		__syncwarp();
-		if (lane == 0) s.sc[1] = base + __popc(b);
-		__syncwarp();
-	}
-	const int nl = s.sc[1];
-	for (int t0 = 0; t0 < nl; t0 += 32) {
-		const int t = t0 + lane;
-		const int key = t < nl ? s.lkey[t] : 0x7fffffff;
-		int rnk = 0;
-		for (int u = 0; u < nl; u++) rnk += s.lkey[u] < key;
-		if (t < nl) s.lsts[rnk] = s.lst[t];
-	}
-	__syncwarp();
-	const int di = hfind_insert(s, i);
-	// ---- filter (ascending columns; kept slots compacted into lst)
-	double rs0 = 0.0, rs1 = 0.0, rs2 = 0.0;
+	// ---- filter, in slot order: blocks of max-norm below tau2 are dropped,
+	//      theta times their entries going to this row's pivot block (row
+	//      sums, added exactly in fixed point, so their order does not
+	//      matter) and to the dropped column's pivot block; the kept ones
+	//      are listed in lsts / lkey
+	unsigned long long rq0 = 0, rq1 = 0, rq2 = 0;
+	int nl = 0;
 	if (lane == 0) s.sc[2] = 0;
 	__syncwarp();
-	for (int t0 = 0; t0 < nl; t0 += 32) {
-		const int t = t0 + lane;
+	const int hscan = WS::big ? s.sc[3] : s.hcap; // slots to look at
+	for (int q0 = 0; q0 < hscan; q0 += 32) { // whole warp in every round (ballots)
+		const int q = q0 + lane;
+		const int h = q < hscan ? (WS::big ? s.slots[q] : q) : -1;
+		const int c = h >= 0 ? s.hkey[h] : -1;
+		const bool take = c >= 0 && c != i;
 		bool keep = false;
-		if (t < nl) {
-			const int h = s.lsts[t];
+		if (take) {
 			const double *u = bv_u(s, h), *l = ilu ? bv_l(s, h) : u;
 			double a[9], mx = 0.0;
 #pragma unroll
@@ -905,31 +890,64 @@ __device__ int finish_blk(const FactArgs &A, WS &s, int i, int lane, int levmax,
 #pragma unroll
 				for (int r = 0; r < 3; r++) {
 					const double v0 = A.theta * a[r], v1 = A.theta * a[r + 3], v2 = A.theta * a[r + 6];
-					const double rsum = v0 + v1 + v2;
-					if (r == 0) rs0 += rsum; else if (r == 1) rs1 += rsum; else rs2 += rsum;
+					const unsigned long long rsum = (unsigned long long)((v0 + v1 + v2) * A.acc_scale);
+					if (r == 0) rq0 += rsum; else if (r == 1) rq1 += rsum; else rq2 += rsum;
 					cs0 += v0;
 					cs1 += v1;
 					cs2 += v2;
 				}
-				const int c = s.hkey[h];
 				acc_push(A.acc, 3 * c, cs0, A.acc_scale, A.st);
 				acc_push(A.acc, 3 * c + 1, cs1, A.acc_scale, A.st);
 				acc_push(A.acc, 3 * c + 2, cs2, A.acc_scale, A.st);
 			}
 		}
+		nl += __popc(__ballot_sync(0xffffffffu, take));
 		const unsigned b = __ballot_sync(0xffffffffu, keep);
 		const int base = s.sc[2];
-		if (keep) s.lst[base + __popc(b & ((1u << lane) - 1))] = s.lsts[t];
+		if (keep) {
+			const int at = base + __popc(b & ((1u << lane) - 1));
+			s.lsts[at] = h;
+			s.lkey[at] = c;
+		}
 		__syncwarp();
 		if (lane == 0) s.sc[2] = base + __popc(b);
 		__syncwarp();
 	}
-	rs0 = warp_sum(rs0);
-	rs1 = warp_sum(rs1);
-	rs2 = warp_sum(rs2);
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		rq0 += __shfl_xor_sync(0xffffffffu, rq0, o);
+		rq1 += __shfl_xor_sync(0xffffffffu, rq1, o);
+		rq2 += __shfl_xor_sync(0xffffffffu, rq2, o);
+	}
+	const double rs0 = __dmul_rn((double)rq0, A.acc_inv_scale), rs1 = __dmul_rn((double)rq1, A.acc_inv_scale),
+	             rs2 = __dmul_rn((double)rq2, A.acc_inv_scale);
+	const int nk = s.sc[2];
+	// ---- the kept columns ascending (rank sort, 8 keys a lane, one broadcast
+	//      key a step): lst
+	for (int t0 = 0; t0 < nk; t0 += 256) {
+		int key[8], rnk[8];
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int t = t0 + q * 32 + lane;
+			key[q] = t < nk ? s.lkey[t] : 0x7fffffff;
+			rnk[q] = 0;
+		}
+#pragma unroll 4
+		for (int u = 0; u < nk; u++) {
+			const int x = s.lkey[u];
+#pragma unroll
+			for (int q = 0; q < 8; q++) rnk[q] += x < key[q];
+		}
+#pragma unroll
+		for (int q = 0; q < 8; q++) {
+			const int t = t0 + q * 32 + lane;
+			if (t < nk) s.lst[rnk[q]] = s.lsts[t];
+		}
+	}
+	__syncwarp();
+	const int di = hfind_insert(s, i);
 	const double c0 = __shfl_sync(0xffffffffu, comp, 0), c1 = __shfl_sync(0xffffffffu, comp, 1),
 	             c2 = __shfl_sync(0xffffffffu, comp, 2);
-	const int nk = s.sc[2];
 	const int len = nk + 1;
 	const int alloc = (len + 3) & ~3;
 	long long off = 0;
@@ -1034,6 +1052,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	constexpr bool ilu = WS::ilu;
 	const long long c0 = clock64();
 	for (int t = lane; t < s.wcap; t += 32) s.wset[t] = -1;
+	if (lane == 0) s.sc[3] = 0;
 	for (int t = lane; t < WS::mwin / 32; t += 32) s.wbits[t] = 0u; // (no bitmap: mwin 0)
 	for (int t = lane; t < s.hcap; t += 32) s.hkey[t] = -1;
 	if (lane == 0) s.sc[0] = 0;
@@ -1178,15 +1197,18 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 	// ---- extract the off-diagonal mask columns and sort them ascending
 	if (lane == 0) s.sc[1] = 0;
 	__syncwarp();
-	for (int h = lane; h < s.hcap; h += 32) {
-		int c = s.hkey[h];
+	const int hscan = WS::big ? s.sc[3] : s.hcap; // slots to look at
+	for (int q0 = 0; q0 < hscan; q0 += 32) { // whole warp in every round (ballots)
+		const int q = q0 + lane;
+		const int h = q < hscan ? (WS::big ? s.slots[q] : q) : -1;
+		int c = h >= 0 ? s.hkey[h] : -1;
 		bool take = c >= 0 && c != i;
 		unsigned b = __ballot_sync(0xffffffffu, take);
 		int base = s.sc[1];
 		if (take) {
-			const int q = base + __popc(b & ((1u << lane) - 1));
-			s.lst[q] = h;
-			s.lkey[q] = c;
+			const int at = base + __popc(b & ((1u << lane) - 1));
+			s.lst[at] = h;
+			s.lkey[at] = c;
 		}
 		__syncwarp();
 		if (lane == 0) s.sc[1] = base + __popc(b);
