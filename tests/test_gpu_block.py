@@ -186,3 +186,22 @@ def test_block_ich2_negative_pivot_is_reported(ctx):
     assert e.value.code == bsg.ERR_PIVOT
     m, f, p = _gpu_ich2(ctx, s)  # the next factorisation works
     assert p.density > 1.0
+
+
+@pytest.mark.parametrize("case,kind", [("lame7", "ilu2"), ("periodic8", "ich2")])
+def test_block_factor_does_not_depend_on_the_schedule(ctx, case, kind):
+    """The block rows run on a dynamic schedule (a warp per row, rows
+    admitted as their members finish), but updates are applied in ascending
+    member order and compensations are summed exactly, so two factorisations
+    of the same matrix are bit-identical."""
+    import bsg
+    s = CASES[case]()
+    p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, theta=0.1, memory=20.0)
+    m = bsg.Matrix.from_system(ctx, s, symm_upper=kind == "ich2")
+    g = []
+    for _ in range(2):
+        f = bsg.Factor(ctx, m, kind, p)
+        g.append(f.export_block())
+        f.free()
+    for a, b in zip(g[0], g[1]):
+        assert np.array_equal(a, b)
