@@ -124,6 +124,8 @@ struct FactArgs {
 	unsigned long long *stats; // FACT_NSTAT counters (see bsg_fact_stats)
 	unsigned char *big_ws;     // BIG_SLOTS workspaces of GlobWS<>::bytes
 	int *big_owner;            // 1 while a warp holds that workspace
+	int *nhold;                // warps holding their row for a member nobody computes
+	int hold_max;              // at most this many (half the warps)
 };
 
 // Scheduler / phase counters summed over all warps of the last factorisation.
@@ -411,6 +413,32 @@ __device__ int promote(const FactArgs &A, int m) {
 		if (*(volatile int *)&A.st->code != 0 || globaltimer_ns() - t0 > PROMOTE_WAIT_NS) return 0;
 		__nanosleep(64);
 	}
+}
+
+// Hold row i (lane 0) for member m that no warp computes right now (m is
+// queued, or parked on a member of its own): spin until m is finished, for
+// at most HOLD_NS, instead of parking, which would recompute row i from the
+// start once m finishes.  At most hold_max warps hold at once, so the other
+// half keep serving the queue and m is computed without this warp.  1: m
+// finished; 0: the caller parks; -1: another warp failed.
+#define HOLD_NS 1000000ull
+__device__ int hold_for(const FactArgs &A, int m) {
+	if (atomicAdd(A.nhold, 1) >= A.hold_max) {
+		atomicSub(A.nhold, 1);
+		return 0;
+	}
+	const unsigned long long t0 = globaltimer_ns();
+	int res = 0;
+	for (unsigned it = 0;; it++) {
+		if (ld_acquire_u64(A.rec + m) & REC_DONE) { res = 1; break; }
+		if ((it & 15) == 15) {
+			if (*(volatile int *)&A.st->code != 0) { res = -1; break; }
+			if (globaltimer_ns() - t0 > HOLD_NS) break;
+		}
+		__nanosleep(128);
+	}
+	atomicSub(A.nhold, 1);
+	return res;
 }
 
 // Park row i on unfinished row m (lane 0).
@@ -1168,6 +1196,7 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		if (lane == 0) {
 			res = wait_row(A, bound);
 			if (res == 0 && promote(A, bound)) res = wait_row(A, bound);
+			if (res == 0) res = hold_for(A, bound);
 		}
 		res = __shfl_sync(0xffffffffu, res, 0);
 		tail0 = clock64();
@@ -1682,8 +1711,10 @@ int bsg_fact_run(bsg_ctx *c, bsg_mat *m, int kind, const bsg_param *p, bsg_fct *
 	if (grid < 1) grid = 1;
 	if (cudaMallocAsync(&A.big_ws, GlobWS<true>::bytes * (size_t)BIG_SLOTS, st) != cudaSuccess)
 		return bsg_set_error(BSG_ERR_NOMEM, "factor row workspace");
-	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * BIG_SLOTS, st));
-	BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * BIG_SLOTS, st));
+	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * (BIG_SLOTS + 1), st));
+	BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * (BIG_SLOTS + 1), st));
+	A.nhold = A.big_owner + BIG_SLOTS;
+	A.hold_max = grid * FACT_WARPS / 2;
 	kern<<<grid, FACT_WARPS * 32, smem, st>>>(A);
 	BSG_CUDA(cudaGetLastError());
 	int rc = bsg_check_devstat(c);
@@ -1834,7 +1865,9 @@ int bsg_bfact_dyn(bsg_ctx *c, int nb, int sym, const bsg_param *p, const int *bi
 	A.qhead = qhead; A.qtail = qtail; A.done_count = done_count; A.st = c->d_stat;
 	if (cudaMallocAsync(&A.big_ws, big * (size_t)BIG_SLOTS, st) != cudaSuccess)
 		return bsg_set_error(BSG_ERR_NOMEM, "block factor row workspace");
-	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * BIG_SLOTS, st));
+	BSG_CUDA(cudaMallocAsync(&A.big_owner, sizeof(int) * (BIG_SLOTS + 1), st));
+	A.nhold = A.big_owner + BIG_SLOTS;
+	A.hold_max = grid * FACT_WARPS_BLK / 2;
 	BSG_CUDA(cudaMallocAsync(&A.stats, sizeof(unsigned long long) * FACT_NSTAT, st));
 	// The pool first holds 8 blocks per block of A (block IC2 / ILU2 keep
 	// about 4); a factor that needs more is computed again with the pool
@@ -1852,7 +1885,7 @@ int bsg_bfact_dyn(bsg_ctx *c, int nb, int sym, const bsg_param *p, const int *bi
 		BSG_CUDA(cudaMemsetAsync(qhead, 0, sizeof(unsigned long long), st));
 		BSG_CUDA(cudaMemsetAsync(qtail, 0, sizeof(unsigned long long), st));
 		BSG_CUDA(cudaMemsetAsync(done_count, 0, sizeof(int), st));
-		BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * BIG_SLOTS, st));
+		BSG_CUDA(cudaMemsetAsync(A.big_owner, 0, sizeof(int) * (BIG_SLOTS + 1), st));
 		BSG_CUDA(cudaMemsetAsync(A.stats, 0, sizeof(unsigned long long) * FACT_NSTAT, st));
 		BSG_COUNT(4);
 		k_fact_init<<<nb_blocks(nb), 256, 0, st>>>(nb, it, nstat, whead, rec, acc, lev, inprog, c->d_stat);
