@@ -295,7 +295,10 @@ __global__ void __launch_bounds__(SELL_TILE) k_tile_blocks(int n, const int *rp,
 // tile, stage its x blocks in shared memory, then every thread forms one
 // row slot's sum from 4-byte values and 2-byte local columns.  The products
 // are summed in the same order as k_sell_sweep32, so the results agree bit
-// for bit.
+// for bit.  The staging is double-buffered: the next tile's x blocks are
+// copied with asynchronous 16-byte copies (cp.async, columns past n
+// zero-filled) while the current tile computes, so each tile costs one
+// barrier and the copies' latency hides behind the value stream.
 template <int OUT64>
 __global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, const int *__restrict__ perm,
                                                              const long long *__restrict__ off,
@@ -305,17 +308,31 @@ __global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, c
                                                              const int *__restrict__ tb, const float *__restrict__ x32,
                                                              const double *__restrict__ rhs,
                                                              const double *__restrict__ dinv, double *__restrict__ y,
-                                                             float *__restrict__ y32) {
-	extern __shared__ float sx[];
+                                                             float *__restrict__ y32, int tstride) {
+	extern __shared__ __align__(16) float sx[]; // two buffers of tmax x 32 floats
 	const int nsl = (n + SELL_C - 1) / SELL_C;
-	for (int tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-		const int b0 = __ldg(tb_off + tile), nbk = __ldg(tb_off + tile + 1) - b0;
-		__syncthreads(); // the previous tile's gathers are done
-		for (int i = threadIdx.x; i < nbk * 32; i += SELL_TILE) {
-			const int c = __ldg(tb + b0 + (i >> 5)) * 32 + (i & 31);
-			sx[i] = c < n ? __ldg(x32 + c) : 0.f;
+	// the x blocks of a tile into one buffer, 16 bytes a copy
+	auto stage = [&](int tile, float *buf) {
+		const int b0 = __ldg(tb_off + tile), npc = (__ldg(tb_off + tile + 1) - b0) * 8;
+		for (int q = threadIdx.x; q < npc; q += SELL_TILE) {
+			const int c = __ldg(tb + b0 + (q >> 3)) * 32 + (q & 7) * 4; // first column of the piece
+			const int left = n - c;
+			const unsigned bytes = left >= 4 ? 16u : (left > 0 ? 4u * (unsigned)left : 0u);
+			const float *src = bytes ? x32 + c : x32; // nothing is read when bytes is 0
+			const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + 4 * q);
+			asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 		}
+		asm volatile("cp.async.commit_group;" ::: "memory");
+	};
+	int tile = blockIdx.x;
+	if (tile < ntile) stage(tile, sx);
+	for (int it = 0; tile < ntile; it++, tile += gridDim.x) {
+		float *cur = sx + (it & 1) * tstride;
+		asm volatile("cp.async.wait_group 0;" ::: "memory");
+		// this tile's copies are visible to all; every thread is done with the
+		// tile before, whose buffer the next copies overwrite
 		__syncthreads();
+		if (tile + (int)gridDim.x < ntile) stage(tile + gridDim.x, sx + ((it + 1) & 1) * tstride);
 		const int t = tile * SELL_TILE + threadIdx.x;
 		const int slice = t / SELL_C, l = t % SELL_C;
 		if (slice < nsl) {
@@ -334,14 +351,14 @@ __global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, c
 				for (int u = 0; u < 8; u++) a[u] = __ldcs(vp + SELL_C * (k + u));
 #pragma unroll
 				for (int u = 0; u < 4; u++) {
-					sum = fma((double)a[2 * u], (double)sx[cc[u] & 0xffffu], sum);
-					sum = fma((double)a[2 * u + 1], (double)sx[cc[u] >> 16], sum);
+					sum = fma((double)a[2 * u], (double)cur[cc[u] & 0xffffu], sum);
+					sum = fma((double)a[2 * u + 1], (double)cur[cc[u] >> 16], sum);
 				}
 			}
 			for (; k < w; k += 2) {
 				const unsigned cc = __ldcs(cp + SELL_C * (k / 2));
-				sum = fma((double)__ldcs(vp + SELL_C * k), (double)sx[cc & 0xffffu], sum);
-				sum = fma((double)__ldcs(vp + SELL_C * (k + 1)), (double)sx[cc >> 16], sum);
+				sum = fma((double)__ldcs(vp + SELL_C * k), (double)cur[cc & 0xffffu], sum);
+				sum = fma((double)__ldcs(vp + SELL_C * (k + 1)), (double)cur[cc >> 16], sum);
 			}
 			if (t < n) {
 				const int r = perm ? __ldg(perm + t) : t;
@@ -791,8 +808,8 @@ static int bsg_sell_tile(bsg_ctx *c, int n, const int *rp, const int *ci, int sk
 	// the limit covers every tiled form: the L and U copies of one factor
 	// (and other factors) stage different amounts, and the attribute is per
 	// kernel, not per launch
-	const size_t smem = (size_t)m->tmax * 32 * sizeof(float);
-	const int smem_cap = TB_MAX * 32 * (int)sizeof(float);
+	const size_t smem = 2 * (size_t)m->tmax * 32 * sizeof(float); // two staging buffers
+	const int smem_cap = 2 * TB_MAX * 32 * (int)sizeof(float);
 	BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
 	BSG_CUDA(cudaFuncSetAttribute(k_tsell_sweep32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
 	int per_sm = 0;
@@ -1020,16 +1037,17 @@ int bsg_sell_sweeps32(cudaStream_t s, const bsg_sell *m, const double *x, const 
 	float *a = work32, *b = work32 + n;
 	BSG_COUNT(nsweeps);
 	k_scale32<<<nb(n, 256) < BSG_SMS * 16 ? nb(n, 256) : BSG_SMS * 16, 256, 0, s>>>(n, x, dinv, b);
-	const size_t smem = (size_t)m->tmax * 32 * sizeof(float);
+	const size_t smem = 2 * (size_t)m->tmax * 32 * sizeof(float);
+	const int tstride = m->tmax * 32;
 	for (int pass = 0; pass < nsweeps - 1; pass++) {
 		const bool last = pass == nsweeps - 2;
 		if (m->ntile) {
 			if (last)
 				k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
-				                                                     m->tb, b, x, dinv, yout, nullptr);
+				                                                     m->tb, b, x, dinv, yout, nullptr, tstride);
 			else
 				k_tsell_sweep32<0><<<m->tgrid, SELL_TILE, smem, s>>>(n, m->ntile, m->perm, m->off, m->cpair, v, m->tb_off,
-				                                                     m->tb, b, x, dinv, nullptr, a);
+				                                                     m->tb, b, x, dinv, nullptr, a, tstride);
 		} else if (last) {
 			if (m->nlong)
 				k_sell_sweep32<1, true><<<g, 256, 0, s>>>(n, m->perm, m->off, m->col, v, b, x, dinv, yout, nullptr,
@@ -1056,8 +1074,9 @@ int bsg_sell_sweep32_pass(cudaStream_t s, const bsg_sell *m, const double *x, co
                           double *yout) {
 	BSG_COUNT(1);
 	if (m->ntile)
-		k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, (size_t)m->tmax * 32 * sizeof(float), s>>>(
-		    m->n, m->ntile, m->perm, m->off, m->cpair, (const float *)m->val, m->tb_off, m->tb, x32, x, dinv, yout, nullptr);
+		k_tsell_sweep32<1><<<m->tgrid, SELL_TILE, 2 * (size_t)m->tmax * 32 * sizeof(float), s>>>(
+		    m->n, m->ntile, m->perm, m->off, m->cpair, (const float *)m->val, m->tb_off, m->tb, x32, x, dinv, yout, nullptr,
+		    m->tmax * 32);
 	else if (m->nlong)
 		k_sell_sweep32<1, true><<<sell_grid(m->n), 256, 0, s>>>(m->n, m->perm, m->off, m->col, (const float *)m->val,
 		                                                        x32, x, dinv, yout, nullptr, long_of<float>(m));
