@@ -398,16 +398,32 @@ bs_long<VT> bs_long_of(const bsg_bsell *m) {
 	return {m->nlong, m->nvlong, m->lrow, m->loff, m->lcol, (const VT *)m->lval, m->lmask};
 }
 
+// CTAs of a kernel that are resident at once (one wave): the sliced loops
+// stride over the grid, so a grid beyond it only adds a partial second wave
+template <typename VT, int NRM>
+int bs_wave() {
+	static int cap = 0;
+	if (!cap) {
+		int per_sm = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bsell_sweep<VT, NRM>, 256, 0);
+		cap = (per_sm > 0 ? per_sm : 1) * BSG_SMS;
+	}
+	return cap;
+}
+
 template <typename VT>
 void bs_pass(cudaStream_t s, const bsg_bsell *m, int g, int k, long long ld, const double *d, const double *x,
              const double *yin, double *yout) {
 	const VT *v = (const VT *)m->val;
 	if (k == 1)
-		k_bsell_sweep<VT, 1><<<g, 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout, bs_long_of<VT>(m));
+		k_bsell_sweep<VT, 1><<<min(g, bs_wave<VT, 1>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
+		                                                            bs_long_of<VT>(m));
 	else if (k <= 4)
-		k_bsell_sweep<VT, 4><<<g, 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout, bs_long_of<VT>(m));
+		k_bsell_sweep<VT, 4><<<min(g, bs_wave<VT, 4>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
+		                                                            bs_long_of<VT>(m));
 	else
-		k_bsell_sweep<VT, 8><<<g, 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout, bs_long_of<VT>(m));
+		k_bsell_sweep<VT, 8><<<min(g, bs_wave<VT, 8>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
+		                                                            bs_long_of<VT>(m));
 }
 
 } // namespace

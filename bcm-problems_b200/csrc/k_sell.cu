@@ -311,16 +311,24 @@ __global__ void __launch_bounds__(SELL_TILE) k_tsell_sweep32(int n, int ntile, c
                                                              float *__restrict__ y32, int tstride) {
 	extern __shared__ __align__(16) float sx[]; // two buffers of tmax x 32 floats
 	const int nsl = (n + SELL_C - 1) / SELL_C;
-	// the x blocks of a tile into one buffer, 16 bytes a copy
+	// the x blocks of a tile into one buffer, 16 bytes a copy; an iterate
+	// that does not start on a 16-byte boundary (the second half of an
+	// odd-length ping-pong pair) is staged with plain loads instead
+	const bool async16 = (reinterpret_cast<unsigned long long>(x32) & 15ull) == 0;
 	auto stage = [&](int tile, float *buf) {
 		const int b0 = __ldg(tb_off + tile), npc = (__ldg(tb_off + tile + 1) - b0) * 8;
 		for (int q = threadIdx.x; q < npc; q += SELL_TILE) {
 			const int c = __ldg(tb + b0 + (q >> 3)) * 32 + (q & 7) * 4; // first column of the piece
 			const int left = n - c;
-			const unsigned bytes = left >= 4 ? 16u : (left > 0 ? 4u * (unsigned)left : 0u);
-			const float *src = bytes ? x32 + c : x32; // nothing is read when bytes is 0
-			const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + 4 * q);
-			asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+			if (async16) {
+				const unsigned bytes = left >= 4 ? 16u : (left > 0 ? 4u * (unsigned)left : 0u);
+				const float *src = bytes ? x32 + c : x32; // nothing is read when bytes is 0
+				const unsigned dst = (unsigned)__cvta_generic_to_shared(buf + 4 * q);
+				asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+			} else {
+#pragma unroll
+				for (int e = 0; e < 4; e++) buf[4 * q + e] = e < left ? __ldg(x32 + c + e) : 0.f;
+			}
 		}
 		asm volatile("cp.async.commit_group;" ::: "memory");
 	};
@@ -981,6 +989,16 @@ void bsg_sell_free(bsg_sell *m, cudaStream_t s) {
 	m->val = nullptr;
 }
 
+// CTAs of 256 threads of a kernel that are resident at once: the sliced
+// loops stride over the grid, so more would only add a partial second wave
+template <typename K>
+static int wave_cap(K kern, int g) {
+	int per_sm = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+	const int cap = (per_sm > 0 ? per_sm : 1) * BSG_SMS;
+	return g < cap ? g : cap;
+}
+
 static int sell_grid(int n) {
 	int warps = (n + 31) / 32;
 	int blocks = (warps + 7) / 8;
@@ -1109,11 +1127,11 @@ int bsg_sell_sweep_multi(cudaStream_t s, const bsg_sell *m, int nr, const double
 	do {                                                                                                               \
 		const VT *v = (const VT *)m->val;                                                                              \
 		if (scaled_in)                                                                                                 \
-			k_sell_apply_m<VT, 1, 1, NRM><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, xi, dinv, x + o, dinv, \
-			                                                 yout + o, long_of<VT>(m));                                  \
+			k_sell_apply_m<VT, 1, 1, NRM><<<wave_cap(k_sell_apply_m<VT, 1, 1, NRM>, g), 256, 0, s>>>(                    \
+			    n, k, ld, m->perm, m->off, m->col, v, xi, dinv, x + o, dinv, yout + o, long_of<VT>(m));                  \
 		else                                                                                                           \
-			k_sell_apply_m<VT, 0, 1, NRM><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, xi, nullptr, x + o,    \
-			                                                 dinv, yout + o, long_of<VT>(m));                            \
+			k_sell_apply_m<VT, 0, 1, NRM><<<wave_cap(k_sell_apply_m<VT, 0, 1, NRM>, g), 256, 0, s>>>(                    \
+			    n, k, ld, m->perm, m->off, m->col, v, xi, nullptr, x + o, dinv, yout + o, long_of<VT>(m));               \
 	} while (0)
 		if (m->fp32) {
 			if (k <= 4) BSG_SW(float, 4);
@@ -1152,17 +1170,17 @@ int bsg_sell_sweeps32_multi(cudaStream_t s, const bsg_sell *m, int nr, const dou
 			BSG_COUNT(1);
 			if (last) {
 				if (k <= 4)
-					k_sell_sweep32_m<1, 4><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					k_sell_sweep32_m<1, 4><<<wave_cap(k_sell_sweep32_m<1, 4>, g), 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
 					                                         yout + o, nullptr, lg);
 				else
-					k_sell_sweep32_m<1, 8><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					k_sell_sweep32_m<1, 8><<<wave_cap(k_sell_sweep32_m<1, 8>, g), 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
 					                                         yout + o, nullptr, lg);
 			} else {
 				if (k <= 4)
-					k_sell_sweep32_m<0, 4><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					k_sell_sweep32_m<0, 4><<<wave_cap(k_sell_sweep32_m<0, 4>, g), 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
 					                                         nullptr, a + o, lg);
 				else
-					k_sell_sweep32_m<0, 8><<<g, 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
+					k_sell_sweep32_m<0, 8><<<wave_cap(k_sell_sweep32_m<0, 8>, g), 256, 0, s>>>(n, k, ld, m->perm, m->off, m->col, v, b + o, x + o, dinv,
 					                                         nullptr, a + o, lg);
 			}
 		}

@@ -257,19 +257,22 @@ def _random_graph(n, deg, seed):
     return P.System(n, 1, ia, np.concatenate(ja).astype(np.int32), np.concatenate(a), np.zeros((1, n)), None)
 
 
-@pytest.mark.parametrize("case", ["heat", "random"])
+@pytest.mark.parametrize("case", ["heat", "heat_odd", "random"])
 def test_fp32_sweeps_match_restated_recurrence(ctx, heat, case):
     """The FP32-factor sweeps (tiled, with x staged in shared memory, for the
-    stencil factor; gathered from global memory where a tile would stage too
-    many x blocks, for the random graph) equal the restated recurrence."""
+    stencil factors; gathered from global memory where a tile would stage too
+    many x blocks, for the random graph) equal the restated recurrence.  An
+    odd row count puts the second FP32 iterate of the ping-pong pair off a
+    16-byte boundary (staged with plain loads then)."""
     import bsg
     import torch
-    s = heat if case == "heat" else _random_graph(60000, 4, 21)
+    s = {"heat": lambda: heat, "heat_odd": lambda: P.heat3d(13, 11, 9, sigma=1.0, seed=5),
+         "random": lambda: _random_graph(60000, 4, 21)}[case]()
     p = bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, memory=20.0, precision=1)
     m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
     f = bsg.Factor(ctx, m, "ich2", p)
     st = f.sell_stats()
-    if case == "heat":
+    if case != "random":
         assert st["tiles_l"] > 0 and st["tiles_u"] > 0
     else:
         assert st["tiles_l"] == 0 and st["tiles_u"] == 0
