@@ -57,16 +57,19 @@ extern "C" int bsg_sell_stats(const bsg_mat *m, const bsg_fct *f, long long *out
 extern "C" int bsg_time_kernel(bsg_ctx *c, int kind, const bsg_mat *m, const bsg_fct *f, int mode, int nsweeps,
                                int reps, double *ms_per_launch) {
 	if (!c || reps < 1 || !ms_per_launch) return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: bad argument");
-	if ((kind == 0 && !m) || (kind != 0 && !f)) return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: missing object");
-	const size_t N = kind == 0 ? (size_t)m->n * m->bs : (size_t)f->n;
+	if (((kind == 0 || kind == 3) && !m) || ((kind == 1 || kind == 2) && !f) || kind < 0 || kind > 3)
+		return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: missing object");
+	if (kind == 3 && (nsweeps < 1 || nsweeps > 64)) return bsg_set_error(BSG_ERR_ARG, "bsg_time_kernel: nrhs 1..64");
+	const int nv = kind == 3 ? nsweeps : 1; // vectors
+	const size_t N = kind == 0 || kind == 3 ? (size_t)m->n * m->bs : (size_t)f->n;
 	double *x, *y, *w;
-	BSG_CUDA(cudaMallocAsync(&x, sizeof(double) * N, c->stream));
-	BSG_CUDA(cudaMallocAsync(&y, sizeof(double) * N, c->stream));
+	BSG_CUDA(cudaMallocAsync(&x, sizeof(double) * N * nv, c->stream));
+	BSG_CUDA(cudaMallocAsync(&y, sizeof(double) * N * nv, c->stream));
 	BSG_CUDA(cudaMallocAsync(&w, sizeof(double) * N, c->stream));
-	int rc = bsg_fill_launch(c->stream, (long long)N, x, 1.0);
+	int rc = bsg_fill_launch(c->stream, (long long)(N * nv), x, 1.0);
 	if (!rc) rc = bsg_fill_launch(c->stream, (long long)N, w, 0.5);
 	auto launch = [&]() {
-		if (kind == 0) return bsg_spmm_launch(m, 1, x, y, (long long)N, c->stream);
+		if (kind == 0 || kind == 3) return bsg_spmm_launch(m, nv, x, y, (long long)N, c->stream);
 		if (mode == 1) return bsg_trisolve_sweep_launch(c, f, kind == 1, x, w, y); // one full sweep
 		return bsg_trisolve_launch(c, f, kind == 1, mode, nsweeps, x, y, w);
 	};
@@ -683,6 +686,7 @@ extern "C" int bsg_fct_free(bsg_fct *f) {
 	bsg_sell_free(&f->sut, s);
 	bsg_bsell_free(&f->bsl, s);
 	bsg_bsell_free(&f->bsu, s);
+	if (f->d_swscr) cudaFreeAsync(f->d_swscr, s);
 	for (void *q : {(void *)f->d_utr_v, (void *)f->d_utr_f, (void *)f->d_l_f})
 		if (q) cudaFreeAsync(q, s);
 	if (f->d_l && f->d_l != f->d_u) cudaFreeAsync(f->d_l, s);

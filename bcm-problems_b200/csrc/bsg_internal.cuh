@@ -187,9 +187,12 @@ void bsg_bsell_free(bsg_bsell *m, cudaStream_t s);
 // Block Jacobi sweeps for nr vectors at stride 3 nb: y0 = D x, then
 // nsweeps - 1 passes y <- D (x - N y) (D: nb column-major 3 x 3 blocks), one
 // kernel a pass, the factor read once per 8 vectors; work: 3 nb nr doubles
-// (nsweeps > 1).  Every vector gets the bits of a single-vector call.
+// (nsweeps > 1).  With scr (bsg_bsell_scratch(nb, nr) doubles, 16-byte
+// aligned) several vectors keep their intermediate iterates interleaved there
+// and work is not used.  Every vector gets the bits of a single-vector call.
 int bsg_bsell_sweeps(cudaStream_t s, const bsg_bsell *m, const double *d, int nsweeps, int nr, const double *x,
-                     double *y, double *work);
+                     double *y, double *work, double *scr = nullptr);
+size_t bsg_bsell_scratch(int nb, int nr);
 
 struct bsg_mat {
 	bsg_ctx *ctx;
@@ -246,6 +249,10 @@ struct bsg_fct {
 	double *d_bl, *d_bu;
 	double *d_bdl, *d_bdu, *d_ones;
 	bsg_bsell bsl, bsu;           // block SELL copies of the strict L / U block rows (sweeps)
+	// two interleaved iterates of the several-vector block sweeps, grown on
+	// first use outside graph capture
+	double *d_swscr;
+	size_t swscr_n;
 };
 
 // ---- launch accounting ------------------------------------------------------

@@ -489,6 +489,20 @@ int bsg_btrisolve_multi(bsg_ctx *c, const bsg_fct *f, int lower, int mode, int n
 		return BSG_OK;
 	}
 	if (nsweeps < 1) return bsg_set_error(BSG_ERR_ARG, "block sweeps: nsweeps >= 1");
+	// the interleaved iterates' scratch, kept with the factor; grown only
+	// outside stream capture (inside, the sweeps go through y and work)
+	const size_t need = nsweeps > 1 ? bsg_bsell_scratch(f->nb, nr) : 0;
+	bsg_fct *fm = const_cast<bsg_fct *>(f);
+	if (need > f->swscr_n) {
+		cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+		if (cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+			if (fm->d_swscr) cudaFreeAsync(fm->d_swscr, c->stream);
+			fm->d_swscr = nullptr;
+			fm->swscr_n = 0;
+			if (cudaMallocAsync(&fm->d_swscr, sizeof(double) * need, c->stream) == cudaSuccess) fm->swscr_n = need;
+			else fm->d_swscr = nullptr;
+		}
+	}
 	return bsg_bsell_sweeps(c->stream, lower ? &f->bsl : &f->bsu, lower ? f->d_bdl : f->d_bdu, nsweeps, nr, x, y,
-	                        work);
+	                        work, need > 0 && need <= f->swscr_n ? fm->d_swscr : nullptr);
 }

@@ -134,38 +134,64 @@ struct bs_long {
 	const unsigned char *mask;
 };
 
-// y_i = D_i (x_i - s) for vector q (D_i column-major)
-__device__ __forceinline__ void bs_out(int i, long long o, const double *__restrict__ d, const double *__restrict__ x,
-                                       const double *s, double *__restrict__ y) {
+// y_i = D_i (x_i - s) for one vector, x_i at ox and y_i at oy (D_i column-major)
+__device__ __forceinline__ void bs_out(int i, long long ox, long long oy, const double *__restrict__ d,
+                                       const double *__restrict__ x, const double *s, double *__restrict__ y) {
 	const double *b = d + 9 * (size_t)i;
-	const double t0 = x[o] - s[0], t1 = x[o + 1] - s[1], t2 = x[o + 2] - s[2];
+	const double t0 = x[ox] - s[0], t1 = x[ox + 1] - s[1], t2 = x[ox + 2] - s[2];
 #pragma unroll
-	for (int r = 0; r < 3; r++) y[o + r] = fma(__ldg(b + r + 6), t2, fma(__ldg(b + r + 3), t1, __ldg(b + r) * t0));
+	for (int r = 0; r < 3; r++) y[oy + r] = fma(__ldg(b + r + 6), t2, fma(__ldg(b + r + 3), t1, __ldg(b + r) * t0));
 }
 
-// s[q][r] += the products of block (J, a) with vector q
-template <int NRM, typename VT>
-__device__ __forceinline__ void bs_block(int J, const VT *a, int nr, long long ld, const double *__restrict__ y,
-                                         double (*s)[3]) {
+// s[r] += row r of block a times (x0, x1, x2), entries in column order
+template <typename VT>
+__device__ __forceinline__ void bs_acc(const VT *a, double x0, double x1, double x2, double *s) {
 #pragma unroll
-	for (int q = 0; q < NRM; q++)
-		if (q < nr) {
-			const double *yq = y + q * ld + 3 * (long long)J;
-			const double x0 = __ldg(yq), x1 = __ldg(yq + 1), x2 = __ldg(yq + 2);
+	for (int r = 0; r < 3; r++) {
+		s[r] = fma((double)a[3 * r], x0, s[r]);
+		s[r] = fma((double)a[3 * r + 1], x1, s[r]);
+		s[r] = fma((double)a[3 * r + 2], x2, s[r]);
+	}
+}
+
+// s[q][r] += the products of block (J, a) with vector q.  Vectors either at
+// stride ld (entry (J, q, r) at q ld + 3 J + r) or, with IL, interleaved by
+// block row (entry at J ri + 3 q + r; ri even and the base 16-byte aligned),
+// where a block's nr vectors are 3 nr contiguous doubles read as pairs.
+template <int NRM, bool IL, typename VT>
+__device__ __forceinline__ void bs_block(int J, const VT *a, int nr, long long ld, int ri,
+                                         const double *__restrict__ y, double (*s)[3]) {
+	if constexpr (IL) {
+		static_assert(NRM % 2 == 0, "interleaved vectors in pairs");
+		const double *yj = y + (long long)J * ri;
 #pragma unroll
-			for (int r = 0; r < 3; r++) {
-				s[q][r] = fma((double)a[3 * r], x0, s[q][r]);
-				s[q][r] = fma((double)a[3 * r + 1], x1, s[q][r]);
-				s[q][r] = fma((double)a[3 * r + 2], x2, s[q][r]);
+		for (int q = 0; q < NRM; q += 2) {
+			if (q + 1 < nr) {
+				const double2 p0 = __ldg(reinterpret_cast<const double2 *>(yj + 3 * q));
+				const double2 p1 = __ldg(reinterpret_cast<const double2 *>(yj + 3 * q + 2));
+				const double2 p2 = __ldg(reinterpret_cast<const double2 *>(yj + 3 * q + 4));
+				bs_acc(a, p0.x, p0.y, p1.x, s[q]);
+				bs_acc(a, p1.y, p2.x, p2.y, s[q + 1]);
+			} else if (q < nr) { // the last of an odd count
+				const double2 p0 = __ldg(reinterpret_cast<const double2 *>(yj + 3 * q));
+				bs_acc(a, p0.x, p0.y, __ldg(yj + 3 * q + 2), s[q]);
 			}
 		}
+	} else {
+#pragma unroll
+		for (int q = 0; q < NRM; q++)
+			if (q < nr) {
+				const double *yq = y + q * ld + 3 * (long long)J;
+				bs_acc(a, __ldg(yq), __ldg(yq + 1), __ldg(yq + 2), s[q]);
+			}
+	}
 }
 
 // Sums of a long block row's blocks [b, e) (b, e multiples of 32) by a warp
 // (tid = lane) or a block of 256 threads: thread t takes blocks t, t + T, ...
 // in order, then a fixed tree; every thread gets the sums.
-template <typename VT, bool BLOCK, int NRM>
-__device__ __forceinline__ void bs_long_sum(long long b, long long e, int tid, int nr, long long ld,
+template <typename VT, bool BLOCK, int NRM, bool IL>
+__device__ __forceinline__ void bs_long_sum(long long b, long long e, int tid, int nr, long long ld, int ri,
                                             const int *__restrict__ lcol, const VT *__restrict__ lval,
                                             const double *__restrict__ y, double (*red)[8], double (*s)[3]) {
 	constexpr int T = BLOCK ? 256 : 32;
@@ -178,7 +204,7 @@ __device__ __forceinline__ void bs_long_sum(long long b, long long e, int tid, i
 		VT a[9];
 #pragma unroll
 		for (int p = 0; p < 9; p++) a[p] = __ldcs(vp + 32 * p);
-		bs_block<NRM>(J, a, nr, ld, y, s);
+		bs_block<NRM, IL>(J, a, nr, ld, ri, y, s);
 	}
 #pragma unroll
 	for (int q = 0; q < NRM; q++)
@@ -204,38 +230,39 @@ __device__ __forceinline__ void bs_long_sum(long long b, long long e, int tid, i
 	}
 }
 
-// One pass yout = D (x - N yin) for nr <= NRM vectors at stride ld.
-template <typename VT, int NRM>
-__global__ void __launch_bounds__(256) k_bsell_sweep(int nb, int nr, long long ld, const long long *__restrict__ off,
-                                                     const int *__restrict__ col, const VT *__restrict__ val,
-                                                     const double *__restrict__ d, const double *__restrict__ x,
-                                                     const double *__restrict__ yin, double *__restrict__ yout,
-                                                     bs_long<VT> lg) {
+// One pass yout = D (x - N yin) for nr <= NRM vectors; x at stride ld, yin
+// and yout at stride ld or (LIN / LOUT) interleaved with row strides ri / ro.
+template <typename VT, int NRM, bool LIN, bool LOUT>
+// (256, 1): no register cap, so that the U blocks' values of the FP64
+// single-vector pass are all in flight (122 registers; 40 under the default
+// cap ran a third slower)
+__global__ void __launch_bounds__(256, 1) k_bsell_sweep(int nb, int nr, long long ld, int ri, int ro,
+                                                     const long long *__restrict__ off, const int *__restrict__ col,
+                                                     const VT *__restrict__ val, const double *__restrict__ d,
+                                                     const double *__restrict__ x, const double *__restrict__ yin,
+                                                     double *__restrict__ yout, bs_long<VT> lg) {
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nwarps = (gridDim.x * blockDim.x) >> 5;
 	double s[NRM][3];
+	auto out = [&](int r) {
+#pragma unroll
+		for (int q = 0; q < NRM; q++)
+			if (q < nr)
+				bs_out(r, q * ld + 3 * (long long)r, LOUT ? (long long)r * ro + 3 * q : q * ld + 3 * (long long)r, d, x,
+				       s[q], yout);
+	};
 	if (lg.nlong) {
 		__shared__ double red[3 * NRM][8];
 		for (int i = blockIdx.x; i < lg.nvlong; i += gridDim.x) {
-			bs_long_sum<VT, true, NRM>(__ldg(lg.off + i), __ldg(lg.off + i + 1), threadIdx.x, nr, ld, lg.col, lg.val, yin,
-			                           red, s);
-			if (threadIdx.x == 0) {
-				const int r = __ldg(lg.row + i);
-#pragma unroll
-				for (int q = 0; q < NRM; q++)
-					if (q < nr) bs_out(r, q * ld + 3 * (long long)r, d, x, s[q], yout);
-			}
+			bs_long_sum<VT, true, NRM, LIN>(__ldg(lg.off + i), __ldg(lg.off + i + 1), threadIdx.x, nr, ld, ri, lg.col,
+			                                lg.val, yin, red, s);
+			if (threadIdx.x == 0) out(__ldg(lg.row + i));
 		}
 		for (int i = lg.nvlong + gw; i < lg.nlong; i += nwarps) {
-			bs_long_sum<VT, false, NRM>(__ldg(lg.off + i), __ldg(lg.off + i + 1), lane, nr, ld, lg.col, lg.val, yin,
-			                            nullptr, s);
-			if (lane == 0) {
-				const int r = __ldg(lg.row + i);
-#pragma unroll
-				for (int q = 0; q < NRM; q++)
-					if (q < nr) bs_out(r, q * ld + 3 * (long long)r, d, x, s[q], yout);
-			}
+			bs_long_sum<VT, false, NRM, LIN>(__ldg(lg.off + i), __ldg(lg.off + i + 1), lane, nr, ld, ri, lg.col, lg.val,
+			                                 yin, nullptr, s);
+			if (lane == 0) out(__ldg(lg.row + i));
 		}
 	}
 	constexpr int SPW = 32 / BS_C;
@@ -264,32 +291,30 @@ __global__ void __launch_bounds__(256) k_bsell_sweep(int nb, int nr, long long l
 				for (int p = 0; p < 9; p++) a[u][p] = __ldcs(vp + 72LL * (k + u) + BS_C * p);
 			}
 #pragma unroll
-			for (int u = 0; u < U; u++) bs_block<NRM>(J[u], a[u], nr, ld, yin, s);
+			for (int u = 0; u < U; u++) bs_block<NRM, LIN>(J[u], a[u], nr, ld, ri, yin, s);
 		}
 		for (; k < w; k++) {
 			const int J = __ldcs(cp + BS_C * k);
 			VT a[9];
 #pragma unroll
 			for (int p = 0; p < 9; p++) a[p] = __ldcs(vp + 72LL * k + BS_C * p);
-			bs_block<NRM>(J, a, nr, ld, yin, s);
+			bs_block<NRM, LIN>(J, a, nr, ld, ri, yin, s);
 		}
 		const int i = slice * BS_C + l;
-		if (i < nb && !((lm >> l) & 1u)) {
-#pragma unroll
-			for (int q = 0; q < NRM; q++)
-				if (q < nr) bs_out(i, q * ld + 3 * (long long)i, d, x, s[q], yout);
-		}
+		if (i < nb && !((lm >> l) & 1u)) out(i);
 	}
 }
 
-// y = D x for nr vectors at stride 3 nb (the first Jacobi iterate)
-__global__ void k_bs_diag(int nb, int nr, const double *__restrict__ d, const double *__restrict__ x,
+// y = D x for nr vectors, x at stride 3 nb, y at stride 3 nb or (ro > 0)
+// interleaved with row stride ro (the first Jacobi iterate)
+__global__ void k_bs_diag(int nb, int nr, int ro, const double *__restrict__ d, const double *__restrict__ x,
                           double *__restrict__ y) {
 	const long long N = (long long)nb * nr;
 	const double zero[3] = {0.0, 0.0, 0.0};
 	for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < N; e += (long long)gridDim.x * blockDim.x) {
 		const int i = (int)(e % nb);
-		bs_out(i, 3 * (e / nb) * nb + 3 * i, d, x, zero, y);
+		const long long q = e / nb, ox = 3 * q * nb + 3 * i;
+		bs_out(i, ox, ro > 0 ? (long long)i * ro + 3 * q : ox, d, x, zero, y);
 	}
 }
 
@@ -400,30 +425,35 @@ bs_long<VT> bs_long_of(const bsg_bsell *m) {
 
 // CTAs of a kernel that are resident at once (one wave): the sliced loops
 // stride over the grid, so a grid beyond it only adds a partial second wave
-template <typename VT, int NRM>
-int bs_wave() {
-	static int cap = 0;
+template <typename VT, int NRM, bool LIN, bool LOUT>
+void bs_launch(cudaStream_t s, const bsg_bsell *m, int g, int k, long long ld, int ri, int ro, const double *d,
+               const double *x, const double *yin, double *yout) {
+	static int cap = 0; // resident blocks of this instantiation on all SMs
 	if (!cap) {
 		int per_sm = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bsell_sweep<VT, NRM>, 256, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bsell_sweep<VT, NRM, LIN, LOUT>, 256, 0);
 		cap = (per_sm > 0 ? per_sm : 1) * BSG_SMS;
 	}
-	return cap;
+	k_bsell_sweep<VT, NRM, LIN, LOUT><<<min(g, cap), 256, 0, s>>>(m->nb, k, ld, ri, ro, m->off, m->col,
+	                                                             (const VT *)m->val, d, x, yin, yout, bs_long_of<VT>(m));
 }
 
+// One pass over k vectors of a group; lin / lout pick the interleaved layouts
+// (several vectors only).
 template <typename VT>
-void bs_pass(cudaStream_t s, const bsg_bsell *m, int g, int k, long long ld, const double *d, const double *x,
-             const double *yin, double *yout) {
-	const VT *v = (const VT *)m->val;
-	if (k == 1)
-		k_bsell_sweep<VT, 1><<<min(g, bs_wave<VT, 1>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
-		                                                            bs_long_of<VT>(m));
-	else if (k <= 4)
-		k_bsell_sweep<VT, 4><<<min(g, bs_wave<VT, 4>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
-		                                                            bs_long_of<VT>(m));
-	else
-		k_bsell_sweep<VT, 8><<<min(g, bs_wave<VT, 8>()), 256, 0, s>>>(m->nb, k, ld, m->off, m->col, v, d, x, yin, yout,
-		                                                            bs_long_of<VT>(m));
+void bs_pass(cudaStream_t s, const bsg_bsell *m, int g, int k, long long ld, int ri, int ro, bool lin, bool lout,
+             const double *d, const double *x, const double *yin, double *yout) {
+	if (k == 1) bs_launch<VT, 1, false, false>(s, m, g, k, ld, 0, 0, d, x, yin, yout);
+	else if (lin && lout) {
+		if (k <= 4) bs_launch<VT, 4, true, true>(s, m, g, k, ld, ri, ro, d, x, yin, yout);
+		else bs_launch<VT, 8, true, true>(s, m, g, k, ld, ri, ro, d, x, yin, yout);
+	} else if (lin) {
+		if (k <= 4) bs_launch<VT, 4, true, false>(s, m, g, k, ld, ri, 0, d, x, yin, yout);
+		else bs_launch<VT, 8, true, false>(s, m, g, k, ld, ri, 0, d, x, yin, yout);
+	} else {
+		if (k <= 4) bs_launch<VT, 4, false, false>(s, m, g, k, ld, 0, 0, d, x, yin, yout);
+		else bs_launch<VT, 8, false, false>(s, m, g, k, ld, 0, 0, d, x, yin, yout);
+	}
 }
 
 } // namespace
@@ -439,26 +469,39 @@ void bsg_bsell_free(bsg_bsell *m, cudaStream_t s) {
 	*m = bsg_bsell();
 }
 
+size_t bsg_bsell_scratch(int nb, int nr) { return 2 * (size_t)nb * (size_t)(3 * nr + (nr & 1)); }
+
 int bsg_bsell_sweeps(cudaStream_t s, const bsg_bsell *m, const double *d, int nsweeps, int nr, const double *x,
-                     double *y, double *work) {
+                     double *y, double *work, double *scr) {
 	const int passes = nsweeps - 1;
-	if (passes > 0 && !work) return bsg_set_error(BSG_ERR_ARG, "block sweeps: work vector missing");
 	const int nb = m->nb;
 	const long long ld = 3LL * nb;
-	// the iterates alternate between y and work, the last one lands in y
-	double *bufs[2] = {y, work};
-	int a = passes & 1;
+	// Several vectors with scratch: the intermediate iterates alternate
+	// between the two halves of scr, interleaved by block row (row stride
+	// 3 nr rounded up to even), so that a block's gathers are 16-byte loads of
+	// contiguous doubles; the last pass writes y at stride ld.  Otherwise the
+	// iterates alternate between y and work at stride ld, the last one
+	// landing in y.
+	const bool il = passes > 0 && nr > 1 && scr && (reinterpret_cast<uintptr_t>(scr) & 15) == 0;
+	if (passes > 0 && !il && !work) return bsg_set_error(BSG_ERR_ARG, "block sweeps: work vector missing");
+	const int R = il ? 3 * nr + (nr & 1) : 0;
+	double *bufs[2];
+	if (il) bufs[0] = scr, bufs[1] = scr + (size_t)nb * R;
+	else bufs[0] = y, bufs[1] = work;
+	int a = il ? 0 : passes & 1;
 	BSG_COUNT(1);
-	k_bs_diag<<<capped((long long)nb * nr, 256), 256, 0, s>>>(nb, nr, d, x, bufs[a]);
+	k_bs_diag<<<capped((long long)nb * nr, 256), 256, 0, s>>>(nb, nr, R, d, x, bufs[a]);
 	const int nsl = (nb + BS_C - 1) / BS_C;
 	const int g = capped(nbk(nsl, 4), 8); // 4 slices a warp, 8 warps a block
 	for (int p = 0; p < passes; p++) {
+		const bool lout = il && p + 1 < passes;
+		double *out = il && !lout ? y : bufs[a ^ 1];
 		for (int q0 = 0; q0 < nr; q0 += 8) {
 			const int k = nr - q0 < 8 ? nr - q0 : 8;
-			const long long o = (long long)q0 * ld;
+			const long long ox = (long long)q0 * ld, oi = il ? 3LL * q0 : ox, oo = lout ? 3LL * q0 : ox;
 			BSG_COUNT(1);
-			if (m->fp32) bs_pass<float>(s, m, g, k, ld, d, x + o, bufs[a] + o, bufs[a ^ 1] + o);
-			else bs_pass<double>(s, m, g, k, ld, d, x + o, bufs[a] + o, bufs[a ^ 1] + o);
+			if (m->fp32) bs_pass<float>(s, m, g, k, ld, R, R, il, lout, d, x + ox, bufs[a] + oi, out + oo);
+			else bs_pass<double>(s, m, g, k, ld, R, R, il, lout, d, x + ox, bufs[a] + oi, out + oo);
 		}
 		a ^= 1;
 	}

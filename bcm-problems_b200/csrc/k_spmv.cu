@@ -9,9 +9,9 @@
 //     length); consecutive rows of a warp read one contiguous stretch of
 //     ja/a, so the stream loads are fully coalesced; x is gathered through
 //     the read-only path and stays in L2 (<= 16.8 MB at n = 2.1M).
-//   * 3x3 block CSR: one warp per block row walks the row's contiguous
-//     9*nblocks values element by element (coalesced), accumulating the three
-//     output rows, then three warp reductions.
+//   * 3x3 block CSR: one warp per block row; 27 lanes at fixed (block, row,
+//     column) positions read the row's values 27 at a time (coalesced), then
+//     two shuffle rounds give the three output rows.
 //   * multi-RHS: the same sweeps carry K right-hand sides so the matrix is
 //     read once for all of them.
 #include "bsg_internal.cuh"
@@ -85,45 +85,72 @@ __global__ void __launch_bounds__(256) k_spmm_csr(int n, const int *__restrict__
 }
 
 // 3x3 block rows, device blocks row-major (element (r,c) at 9*blk + 3*r + c).
+// A warp takes a block row.  Lanes 0..26 hold fixed positions lane = 9 t + 3 r
+// + c (block t of three, row r, column c) and step through the row three
+// blocks at a time, so each step reads 27 contiguous values and gathers three
+// 24-byte pieces of x; U steps' loads are issued before their products.  The
+// sums over c and then over t are two shuffle rounds, and lanes 0, 3, 6 hold
+// the three output rows.  nr <= K vectors at stride ld share each value load;
+// each vector's sums are formed in the same order whatever K is.
 template <int K>
-__global__ void __launch_bounds__(256) k_spmv_bsr3(int nb, const int *__restrict__ ia, const int *__restrict__ ja,
-                                                   const double *__restrict__ a, const double *__restrict__ X,
-                                                   double *__restrict__ Y, long long ld) {
+__global__ void __launch_bounds__(256, K > 4 ? 4 : (K > 2 ? 5 : 8)) k_spmv_bsr3(int nb, int nr, const int *__restrict__ ia,
+                                                   const int *__restrict__ ja, const double *__restrict__ a,
+                                                   const double *__restrict__ X, double *__restrict__ Y,
+                                                   long long ld) {
 	const int lane = threadIdx.x & 31;
+	const int t = lane / 9, w = lane - 9 * (lane / 9), c = w % 3;
 	const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	constexpr int U = 4;
 	for (int br = warp; br < nb; br += nwarps) {
-		const int b = ia[br], e = ia[br + 1];
-		const int nv = (e - b) * 9;
-		const double *av = a + (size_t)b * 9;
-		double s0[K], s1[K], s2[K];
+		const int b = __ldg(ia + br), e = lane < 27 ? __ldg(ia + br + 1) : b;
+		double s[K];
 #pragma unroll
-		for (int r = 0; r < K; r++) s0[r] = s1[r] = s2[r] = 0.0;
-		for (int t = lane; t < nv; t += 32) {
-			int blk = t / 9;
-			int w = t - 9 * blk;
-			int rr = w / 3;
-			int cc = w - 3 * rr;
-			double v = ld_stream(av + t);
-			int col = 3 * __ldg(ja + b + blk) + cc;
+		for (int q = 0; q < K; q++) s[q] = 0.0;
+		int j = b + t;
+		for (; j + 3 * (U - 1) < e; j += 3 * U) {
+			double v[U];
+			int J[U];
 #pragma unroll
-			for (int r = 0; r < K; r++) {
-				double p = v * __ldg(X + r * ld + col);
-				s0[r] += rr == 0 ? p : 0.0;
-				s1[r] += rr == 1 ? p : 0.0;
-				s2[r] += rr == 2 ? p : 0.0;
+			for (int u = 0; u < U; u++) {
+				v[u] = ld_stream(a + 9LL * (j + 3 * u) + w);
+				J[u] = __ldg(ja + j + 3 * u);
 			}
+#pragma unroll
+			for (int u = 0; u < U; u++)
+#pragma unroll
+				for (int q = 0; q < K; q++)
+					if (q < nr) s[q] = fma(v[u], __ldg(X + q * ld + 3LL * J[u] + c), s[q]);
+		}
+		for (; j < e; j += 3) {
+			const double v = ld_stream(a + 9LL * j + w);
+			const long long J = 3LL * __ldg(ja + j) + c;
+#pragma unroll
+			for (int q = 0; q < K; q++)
+				if (q < nr) s[q] = fma(v, __ldg(X + q * ld + J), s[q]);
 		}
 #pragma unroll
-		for (int r = 0; r < K; r++) {
-			double t0 = warp_sum(s0[r]), t1 = warp_sum(s1[r]), t2 = warp_sum(s2[r]);
-			if (lane == 0) {
-				Y[r * ld + 3 * br + 0] = t0;
-				Y[r * ld + 3 * br + 1] = t1;
-				Y[r * ld + 3 * br + 2] = t2;
-			}
+		for (int q = 0; q < K; q++) {
+			if (q >= nr) break;
+			double v = s[q] + __shfl_down_sync(0xffffffffu, s[q], 1);
+			v += __shfl_down_sync(0xffffffffu, s[q], 2);
+			double u = v + __shfl_down_sync(0xffffffffu, v, 9);
+			u += __shfl_down_sync(0xffffffffu, v, 18);
+			if (lane < 9 && c == 0) Y[q * ld + 3LL * br + w / 3] = u;
 		}
 	}
+}
+
+template <int K>
+int bsr3_grid(int nb) {
+	static int cap = 0;
+	if (!cap) {
+		int per_sm = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_bsr3<K>, 256, 0);
+		cap = (per_sm > 0 ? per_sm : 1) * BSG_SMS;
+	}
+	const int g = (nb + 7) / 8; // a warp per block row, 8 warps a block
+	return g < 1 ? 1 : (g < cap ? g : cap);
 }
 
 int grid_for(int warps_needed) {
@@ -143,15 +170,15 @@ int bsg_choose_group(double mean_row) {
 
 int bsg_spmm_launch(const bsg_mat *m, int nrhs, const double *X, double *Y, long long ld, cudaStream_t s) {
 	if (m->bs == 3) {
-		int g = grid_for(m->n);
-		for (int r0 = 0; r0 < nrhs;) {
+		for (int r0 = 0; r0 < nrhs; r0 += 8) {
 			BSG_COUNT(1);
-			int k = nrhs - r0;
+			const int k = nrhs - r0 < 8 ? nrhs - r0 : 8;
 			const double *Xr = X + r0 * ld;
 			double *Yr = Y + r0 * ld;
-			if (k >= 4) { k_spmv_bsr3<4><<<g, 256, 0, s>>>(m->n, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld); r0 += 4; }
-			else if (k >= 2) { k_spmv_bsr3<2><<<g, 256, 0, s>>>(m->n, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld); r0 += 2; }
-			else { k_spmv_bsr3<1><<<g, 256, 0, s>>>(m->n, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld); r0 += 1; }
+			if (k == 1) k_spmv_bsr3<1><<<bsr3_grid<1>(m->n), 256, 0, s>>>(m->n, k, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld);
+			else if (k == 2) k_spmv_bsr3<2><<<bsr3_grid<2>(m->n), 256, 0, s>>>(m->n, k, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld);
+			else if (k <= 4) k_spmv_bsr3<4><<<bsr3_grid<4>(m->n), 256, 0, s>>>(m->n, k, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld);
+			else k_spmv_bsr3<8><<<bsr3_grid<8>(m->n), 256, 0, s>>>(m->n, k, m->d_ia, m->d_ja, m->d_a, Xr, Yr, ld);
 		}
 		return cudaGetLastError() == cudaSuccess ? BSG_OK : BSG_ERR_CUDA;
 	}

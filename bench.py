@@ -313,6 +313,23 @@ def run_config(k, args):
                                        "cases; block IC2 tau 1e-3, Jacobi(6) block sweeps, batched PCG to 1e-8",
                            "nb": s.n, "nnzb": s.nnz})
         line["fct_ms"] = round(t_fct, 3)
+        # block product roofline: each stored 3x3 block (72 B FP64 values, 4 B
+        # column), row pointers, and per vector one read of x and one write of y
+        nb_, bs_, nnzb = C.c_int(), C.c_int(), C.c_int()
+        bsg.lib().bsg_mat_info(m.h, C.byref(nb_), C.byref(bs_), C.byref(nnzb))
+        tk = bsg.lib().bsg_time_kernel
+        tk.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+        peak, peak_kind = peaks()
+        prod = {}
+        for nv in ((1,) if k == 2 else (1, B.shape[0])):
+            t_ = C.c_double()
+            bsg._check(tk(ctx.h, 3, m.h, None, 0, nv, 50, C.byref(t_)))
+            by = nnzb.value * 76 + (nb_.value + 1) * 4 + nv * nb_.value * 48
+            gbs = by / (t_.value * 1e-3) / 1e9
+            prod[f"vectors_{nv}"] = {"kernel": "k_spmv_bsr3", "ms": round(t_.value, 4), "bytes": by,
+                                     "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                                     "frac": round(gbs / peak, 3), "peak_kind": peak_kind}
+        line["block_product_roofline"] = prod
     elif k == 4:  # 256 uneven 2-D heat problems, batched IC2-PCG to 1e-8
         # N ranks (torchrun): each takes whole problems, balanced by nonzeros
         # (shard.py), solves them as one batch on its GPU; one all-gather of

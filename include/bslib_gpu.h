@@ -342,7 +342,8 @@ int bsg_unet_zero_grads(bsg_unet *u);
 /* Number of kernels this library has launched in the process so far. */
 unsigned long long bsg_launch_count(void);
 /* Average device time of `reps` launches of one kernel (kind 0: SpMV of m;
- * 1 / 2: forward / backward solve with f in `mode`/`nsweeps`), CUDA events. */
+ * 1 / 2: forward / backward solve with f in `mode`/`nsweeps`; 3: product of
+ * m with `nsweeps` vectors at once, 1..64), CUDA events. */
 int bsg_time_kernel(bsg_ctx *ctx, int kind, const bsg_mat *m, const bsg_fct *f, int mode, int nsweeps, int reps,
                     double *ms_per_launch);
 /* Scheduler counters of the last factorisation (see k_fact.cu); the first

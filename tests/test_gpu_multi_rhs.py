@@ -36,10 +36,12 @@ def test_multi_vector_sweeps_equal_single(ctx, case, precision):
     rng = np.random.default_rng(17)
     X = torch.as_tensor(rng.standard_normal((11, n)), device="cuda")
     y = torch.empty(n, dtype=torch.float64, device="cuda")
-    for nr in (3, 6, 11):  # one group of <= 4, one of <= 8, two groups
+    # one group of <= 4 or <= 8 vectors, two groups; even counts keep the
+    # block iterates interleaved between passes
+    for nr in (3, 4, 6, 10, 11):
         Y = torch.full((nr, n), np.nan, dtype=torch.float64, device="cuda")
         for lower in (True, False):
-            for sw in (2, 6):
+            for sw in (2, 3, 6):
                 f.solve_multi(lower, X[:nr].contiguous(), Y, mode=1, nsweeps=sw)
                 for q in range(nr):
                     (f.solve_l if lower else f.solve_u)(X[q].contiguous(), y, mode=1, nsweeps=sw)

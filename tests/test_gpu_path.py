@@ -82,6 +82,17 @@ def test_spmv_bsr3(ctx, oracle):
     ms.mvm(_t(x), y)
     assert np.abs(y.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
     del u
+    # several vectors in one pass over the blocks (groups of 1, 2, 4, 8, and
+    # two groups): each vector bit for bit its own product
+    X = np.random.default_rng(4).standard_normal((11, s.n * 3))
+    for nr in (2, 3, 6, 11):
+        Y = torch.full((nr, s.n * 3), np.nan, dtype=torch.float64, device="cuda")
+        m.mvm_multi(_t(X[:nr]), Y)
+        for q in range(nr):
+            m.mvm(_t(X[q]), y)
+            assert torch.equal(Y[q], y), (nr, q)
+            r = oracle.bsr_mvm(s.ia, s.ja, s.a, X[q], 3)
+            assert np.abs(y.cpu().numpy() - r).max() <= 1e-13 * np.abs(r).max()
 
 
 def _factor_match(gpu, ora):
