@@ -85,6 +85,8 @@ int orc_ilu2_block_jacobi(int nb, int bs, const int *is, const int *js, const do
                           double **l, double **u, double *stats);
 int orc_ich2_block(int nb, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
                    double theta, int **ia_f, int **ja_f, double **uo, double *stats);
+int orc_ich2_block_jacobi(int nb, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
+                          double theta, int **ia_f, int **ja_f, double **uo, double *stats);
 void orc_solve_l_block(int nb, int bs, const int *ia, const int *ja, const double *a, const double *x, double *y);
 void orc_solve_u_block(int nb, int bs, const int *ia, const int *ja, const double *a, const double *x, double *y);
 

@@ -172,7 +172,24 @@ static void svd3_jacobi(const double *a, double *s, double *u, double *vt) {
 	}
 }
 
-static int g_svd_jacobi = 0; /* orc_ilu2_block_jacobi sets it for one call */
+static int g_svd_jacobi = 0; /* orc_ilu2_block_jacobi / orc_ich2_block_jacobi set it for one call */
+
+/* Eigenpairs of a symmetric 3 x 3 block as the GPU path takes them: the
+ * Jacobi SVD above, the right singular vectors as eigenvectors (q column-
+ * major, descending) and the singular values as eigenvalues; a pair whose
+ * left and right vectors point opposite ways (u_k . v_k < 0, s_k > 0) is a
+ * negative eigenvalue (-2). */
+static int sym_eig3_jacobi(const double *a, double *eig, double *q) {
+	double a0[9], s[3], u[9], vt[9];
+	memcpy(a0, a, sizeof a0);
+	svd3_jacobi(a0, s, u, vt);
+	for (int k = 0; k < 3; k++) {
+		if (u[3 * k] * vt[k] + u[1 + 3 * k] * vt[k + 3] + u[2 + 3 * k] * vt[k + 6] < 0.0 && s[k] > 0.0) return -2;
+		eig[k] = s[k];
+		for (int r = 0; r < 3; r++) q[r + 3 * k] = vt[k + 3 * r];
+	}
+	return 0;
+}
 
 /* The SVD of one B x B block as the reference takes it: dgesvd for B > 1,
  * the sign split for B == 1 (Bslib/ilu2rs.cpp:118-140, :717-740).  a is
@@ -572,9 +589,13 @@ int orc_ich2_block(int nb, int bs, const int *ia, const int *ja, const double *a
 		const double *d = a + (size_t)ia[i] * b2;
 		double *sl = scl + (size_t)i * b2, *si = sinv + (size_t)i * b2;
 		int info = 0;
-		memcpy(aloc, d, sizeof(double) * b2);
-		dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
-		if (info) return -3;
+		if (bs == 3 && g_svd_jacobi) {
+			if (sym_eig3_jacobi(d, eig, aloc)) return -2;
+		} else {
+			memcpy(aloc, d, sizeof(double) * b2);
+			dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
+			if (info) return -3;
+		}
 		for (int k = 0; k < bs; k++)
 			if (eig[k] < 0.0) return -2;
 		for (int k = 0; k < bs; k++) eig[k] = sqrt(eig[k]);
@@ -679,14 +700,18 @@ int orc_ich2_block(int nb, int bs, const int *ia, const int *ja, const double *a
 		nlist1 = nlist2;
 		{ /* Ich2PivScaleRow */
 			int info = 0;
-			memcpy(aloc, fdi, sizeof(double) * b2);
-			dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
-			if (info) return -3;
-			for (int r = 0; r < bs; r++) /* eigenpairs in descending order */
-				for (int c = 0; c < bs; c++) delem[(bs - r - 1) * bs + c] = aloc[r * bs + c];
-			memcpy(aloc, delem, sizeof(double) * b2);
-			for (int k = 0; k < bs; k++) work[bs - k - 1] = eig[k];
-			for (int k = 0; k < bs; k++) eig[k] = work[k];
+			if (bs == 3 && g_svd_jacobi) { /* descending already */
+				if (sym_eig3_jacobi(fdi, eig, aloc)) return -2;
+			} else {
+				memcpy(aloc, fdi, sizeof(double) * b2);
+				dsyev_("V", "U", &bs, aloc, &bs, eig, work, &lwork, &info);
+				if (info) return -3;
+				for (int r = 0; r < bs; r++) /* eigenpairs in descending order */
+					for (int c = 0; c < bs; c++) delem[(bs - r - 1) * bs + c] = aloc[r * bs + c];
+				memcpy(aloc, delem, sizeof(double) * b2);
+				for (int k = 0; k < bs; k++) work[bs - k - 1] = eig[k];
+				for (int k = 0; k < bs; k++) eig[k] = work[k];
+			}
 			for (int k = 0; k < bs; k++) {
 				if (eig[k] < 0.0) return -2;
 				eig[k] = sqrt(eig[k]);
@@ -769,4 +794,15 @@ int orc_ich2_block(int nb, int bs, const int *ia, const int *ja, const double *a
 	free(scl); free(sinv); free(diagg); free(fm); free(imask); free(lstloc); free(lstupd); free(indlst);
 	free(iv); free(madj); free(ibegm); free(ig); free(jg); free(addrg); free(g);
 	return 0;
+}
+
+/* orc_ich2_block with the GPU path's Jacobi eigenpairs (sym_eig3_jacobi) in
+ * place of dsyev (3 x 3 blocks): the oracle that the GPU block IC2 factor is
+ * checked against value by value. */
+int orc_ich2_block_jacobi(int nb, int bs, const int *ia, const int *ja, const double *a, double tau1, double tau2,
+                          double theta, int **ia_f, int **ja_f, double **uo, double *stats) {
+	g_svd_jacobi = 1;
+	const int rc = orc_ich2_block(nb, bs, ia, ja, a, tau1, tau2, theta, ia_f, ja_f, uo, stats);
+	g_svd_jacobi = 0;
+	return rc;
 }

@@ -186,12 +186,14 @@ class Oracle:
             self.lib.orc_free(p)
         return ia_f, ja_f, l, u, (st[0], st[1])
 
-    def ich2_block(self, ia, ja, a, bs, tau1=1e-3, tau2=1e-3, theta=0.1):
-        """Block IC2 of an upper-stored symmetric block matrix: (ia, ja, u, (density, density2))."""
+    def ich2_block(self, ia, ja, a, bs, tau1=1e-3, tau2=1e-3, theta=0.1, jacobi_eig=False):
+        """Block IC2 of an upper-stored symmetric block matrix: (ia, ja, u, (density, density2)).
+        jacobi_eig: the GPU path's Jacobi eigenpairs instead of LAPACK's dsyev."""
         nb = len(ia) - 1
         pia, pja, pu = _ip(), _ip(), _dp()
         st = (C.c_double * 3)()
-        rc = self.lib.orc_ich2_block(nb, bs, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
+        f = self.lib.orc_ich2_block_jacobi if jacobi_eig else self.lib.orc_ich2_block
+        rc = f(nb, bs, _i(ia), _i(ja), _d(a), C.c_double(tau1), C.c_double(tau2),
                                      C.c_double(theta), C.byref(pia), C.byref(pja), C.byref(pu), st)
         if rc == -2:
             raise ArithmeticError("negative pivot in block IC2")

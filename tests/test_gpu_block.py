@@ -1,5 +1,5 @@
-"""Block ILU2 on the GPU (k_bfact.cu) against the block oracle
-(oracle/bsl_oracle_block.c).
+"""Block ILU2 and block IC2 on the GPU (k_fact.cu block mode, k_bfact.cu)
+against the block oracle (oracle/bsl_oracle_block.c).
 
 The reference scales and pivots with the SVDs of 3x3 blocks (LAPACK dgesvd);
 the GPU takes its own one-sided Jacobi SVD.  An SVD is unique only up to the
@@ -12,10 +12,10 @@ tau2, and the factors then drift apart at the threshold level.  The oracle
 shows the same effect: the LAPACK and the Jacobi variant of the reference's
 own algorithm differ by up to ~5e-3 in M^-1 on these matrices.  So:
 
-* against the oracle with the Jacobi SVD, on a matrix whose pivot blocks are
-  well separated (the nonsymmetric case), the GPU factor gives the same
-  preconditioner to 1e-10 and the same pattern in every row -- the GPU kernel
-  computes the reference's algorithm;
+* against the oracle with the Jacobi SVD (ILU2) or the Jacobi eigenpairs
+  (IC2), on matrices whose pivot blocks are well separated, the GPU factor
+  gives the same preconditioner to 1e-10 and the same pattern in every row --
+  the GPU kernel computes the reference's algorithm;
 * on all cases, the preconditioner agrees with the reference's (LAPACK) one
   to 2e-2 and the density to 1 %;
 * the GPU's own block solves equal the oracle's on the same factor (1e-13),
@@ -144,6 +144,27 @@ def _gpu_ich2(ctx, s, **kw):
     m = bsg.Matrix.from_system(ctx, s, symm_upper=True)
     f = bsg.Factor(ctx, m, "ich2", p)
     return m, f, p
+
+
+def test_block_ich2_equals_jacobi_oracle(ctx, oracle):
+    """Block IC2 against the oracle that takes the GPU's Jacobi eigenpairs
+    (the right singular vectors of the Jacobi SVD) in place of dsyev, on a
+    symmetric matrix whose pivot blocks keep well separated eigenvalues --
+    there the dsyev and the Jacobi oracle agree to rounding, so no rotation
+    can move a block across tau1 / tau2.  The GPU factor has the same pattern
+    in every row, the same density and the same preconditioner to 1e-10: the
+    GPU kernel computes the reference's algorithm."""
+    s = P.lame3d(6, sigma=1.0, seed=43)
+    m, f, p = _gpu_ich2(ctx, s)
+    ia, ja, l, u = f.export_block()
+    uu = s.upper()
+    o = oracle.ich2_block(uu.ia, uu.ja, uu.a, 3, tau1=1e-3, tau2=1e-3, theta=0.1, jacobi_eig=True)
+    r = oracle.ich2_block(uu.ia, uu.ja, uu.a, 3, tau1=1e-3, tau2=1e-3, theta=0.1)
+    assert _same_rows(r, o, s.n) == s.n  # the case is well separated
+    assert _precond_diff(oracle, (r[0], r[1], r[2], r[2]), (o[0], o[1], o[2], o[2]), s.n) <= 1e-12
+    assert _same_rows((ia, ja), o, s.n) == s.n
+    assert abs(p.density - o[3][0]) <= 1e-12
+    assert _precond_diff(oracle, (ia, ja, u, u), (o[0], o[1], o[2], o[2]), s.n) <= 1e-10
 
 
 @pytest.mark.parametrize("case", ["lame7", "periodic8"])
