@@ -293,6 +293,30 @@ __device__ int wset_insert(WS &s, int i, int k) {
 	return -1;
 }
 
+// Ranks of keys t0 + 32 q + lane (q < NQ) among the nl distinct keys, by one
+// broadcast key per step; entry t goes to position rank(t) of out.
+template <int NQ>
+__device__ __forceinline__ void rank_sort(const int *key_of, const int *val, int *out, int nl, int t0, int lane) {
+	int key[NQ], rnk[NQ];
+#pragma unroll
+	for (int q = 0; q < NQ; q++) {
+		const int t = t0 + q * 32 + lane;
+		key[q] = t < nl ? key_of[t] : 0x7fffffff;
+		rnk[q] = 0;
+	}
+#pragma unroll 4
+	for (int u = 0; u < nl; u++) {
+		const int x = key_of[u];
+#pragma unroll
+		for (int q = 0; q < NQ; q++) rnk[q] += x < key[q];
+	}
+#pragma unroll
+	for (int q = 0; q < NQ; q++) {
+		const int t = t0 + q * 32 + lane;
+		if (t < nl) out[rnk[q]] = val[t];
+	}
+}
+
 // Add a nonnegative compensation to row j's 64-bit fixed-point accumulator
 // (value * 2^scale_bits, truncated): integer addition makes the sum exact and
 // independent of the order of the adds, and a reduction without return value
@@ -629,13 +653,25 @@ __device__ int apply_members(const FactArgs &A, WS &s, int bound, int lane, Phas
 	if (nb == 0) return 0;
 	pc.v[FS_BATCHES]++;
 	pc.v[FS_CLOSED] += nb;
-	// rank sort by row index (rows are distinct); mark applied
-	for (int q = lane; q < nb; q += 32) {
-		const int t = s.lsts[q], k = s.W[t];
+	// rank sort by row index (rows are distinct); mark applied.  Up to 32
+	// members: the keys stay in registers and are broadcast by shuffles
+	if (nb <= 32) {
+		const int t = lane < nb ? s.lsts[lane] : 0;
+		const int k = lane < nb ? s.W[t] : 0x7fffffff;
 		int r = 0;
-		for (int u = 0; u < nb; u++) r += s.W[s.lsts[u]] < k;
-		s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
-		s.Wst[t] = 2;
+		for (int u = 0; u < nb; u++) r += __shfl_sync(0xffffffffu, k, u) < k;
+		if (lane < nb) {
+			s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
+			s.Wst[t] = 2;
+		}
+	} else {
+		for (int q = lane; q < nb; q += 32) {
+			const int t = s.lsts[q], k = s.W[t];
+			int r = 0;
+			for (int u = 0; u < nb; u++) r += s.W[s.lsts[u]] < k;
+			s.Ws[r] = k; s.Wps[r] = s.Wp[t]; s.Wes[r] = s.We[t]; s.Wfs[r] = s.Wf[t];
+			s.Wst[t] = 2;
+		}
 	}
 	__syncwarp();
 	// segment bases: stored member t contributes its entries [pos, end)
@@ -950,28 +986,12 @@ __device__ int finish_blk(const FactArgs &A, WS &s, int i, int lane, int levmax,
 	const double rs0 = __dmul_rn((double)rq0, A.acc_inv_scale), rs1 = __dmul_rn((double)rq1, A.acc_inv_scale),
 	             rs2 = __dmul_rn((double)rq2, A.acc_inv_scale);
 	const int nk = s.sc[2];
-	// ---- the kept columns ascending (rank sort, 8 keys a lane, one broadcast
-	//      key a step): lst
-	for (int t0 = 0; t0 < nk; t0 += 256) {
-		int key[8], rnk[8];
-#pragma unroll
-		for (int q = 0; q < 8; q++) {
-			const int t = t0 + q * 32 + lane;
-			key[q] = t < nk ? s.lkey[t] : 0x7fffffff;
-			rnk[q] = 0;
-		}
-#pragma unroll 4
-		for (int u = 0; u < nk; u++) {
-			const int x = s.lkey[u];
-#pragma unroll
-			for (int q = 0; q < 8; q++) rnk[q] += x < key[q];
-		}
-#pragma unroll
-		for (int q = 0; q < 8; q++) {
-			const int t = t0 + q * 32 + lane;
-			if (t < nk) s.lst[rnk[q]] = s.lsts[t];
-		}
-	}
+	// ---- the kept columns ascending (rank sort): lst
+	if (nk <= 32) rank_sort<1>(s.lkey, s.lsts, s.lst, nk, 0, lane);
+	else if (nk <= 64) rank_sort<2>(s.lkey, s.lsts, s.lst, nk, 0, lane);
+	else if (nk <= 128) rank_sort<4>(s.lkey, s.lsts, s.lst, nk, 0, lane);
+	else
+		for (int t0 = 0; t0 < nk; t0 += 256) rank_sort<8>(s.lkey, s.lsts, s.lst, nk, t0, lane);
 	__syncwarp();
 	const int di = hfind_insert(s, i);
 	const double c0 = __shfl_sync(0xffffffffu, comp, 0), c1 = __shfl_sync(0xffffffffu, comp, 1),
@@ -1244,27 +1264,13 @@ __device__ int try_row(const FactArgs &A, WS &s, int i, int lane, PhaseClock &pc
 		__syncwarp();
 	}
 	const int nl = s.sc[1];
-	// rank sort (columns are distinct): each lane ranks its keys against one
-	// broadcast key per step
-	for (int t0 = 0; t0 < nl; t0 += 256) {
-		int key[8], rnk[8];
-#pragma unroll
-		for (int q = 0; q < 8; q++) {
-			const int t = t0 + q * 32 + lane;
-			key[q] = t < nl ? s.lkey[t] : 0x7fffffff;
-			rnk[q] = 0;
-		}
-		for (int u = 0; u < nl; u++) {
-			const int x = s.lkey[u];
-#pragma unroll
-			for (int q = 0; q < 8; q++) rnk[q] += x < key[q];
-		}
-#pragma unroll
-		for (int q = 0; q < 8; q++) {
-			const int t = t0 + q * 32 + lane;
-			if (t < nl) s.lsts[rnk[q]] = s.lst[t];
-		}
-	}
+	// rank sort (columns are distinct): each lane ranks its keys (as few per
+	// lane as the row needs) against one broadcast key per step
+	if (nl <= 32) rank_sort<1>(s.lkey, s.lst, s.lsts, nl, 0, lane);
+	else if (nl <= 64) rank_sort<2>(s.lkey, s.lst, s.lsts, nl, 0, lane);
+	else if (nl <= 128) rank_sort<4>(s.lkey, s.lst, s.lsts, nl, 0, lane);
+	else
+		for (int t0 = 0; t0 < nl; t0 += 256) rank_sort<8>(s.lkey, s.lst, s.lsts, nl, t0, lane);
 	__syncwarp();
 	const int di = hfind_insert(s, i); // existing slot of the diagonal
 
