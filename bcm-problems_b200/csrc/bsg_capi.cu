@@ -9,6 +9,15 @@
 #include <vector>
 #include <algorithm>
 
+// The host entry points' CSR checks on device copies, with their messages and
+// order (k_format.cu): stage 0 the row pointers (ia[0] == 0 checked by the
+// caller), stage 1 the columns, and with upper the upper-storage rule.
+int bsg_check_csr_dev(bsg_ctx *c, int n, int nz, const int *d_ia, const int *d_ja, int stage, int upper);
+// Device 3x3 block CSR from device input with column-major blocks, expanded
+// from the upper triangle when upper; takes over or frees its inputs
+// (k_format.cu).
+int bsg_bsr3_from_input(bsg_ctx *c, int nb, int *ia, int *ja, double *a, int nz, int upper, int **ia_o, int **ja_o,
+                        double **a_o, int *nnz_o);
 int bsg_expand_symmetric(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz_up, int **ia_o,
                          int **ja_o, double **a_o, int *nnz_o);
 int bsg_combine_lu(bsg_ctx *c, int n, const int *ia, const int *ja, const double *a, int nnz, int **iu_o,
@@ -304,11 +313,11 @@ static int mat_csr_common(bsg_ctx *c, int n, const int *ia, const int *ja, const
 	if (!c || !out) return bsg_set_error(BSG_ERR_ARG, "bsg_mat_csr: null argument");
 	*out = nullptr;
 	int nz = 0;
-	if (host) {
-		int rc = check_csr_host(n, ia, ja, 1);
-		if (!rc && symm_upper) rc = check_upper_host(n, ia, ja);
-		if (rc) return rc;
+	if (host) { // the O(1) checks here, the rest on the device copies below
+		if (n < 0 || !ia) return bsg_set_error(BSG_ERR_ARG, "bad CSR: n < 0 or ia == NULL");
+		if (ia[0] != 0) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia[0] != 0");
 		nz = ia[n];
+		if (nz < 0) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia not monotone");
 	} else {
 		BSG_CUDA(cudaMemcpy(&nz, ia + n, sizeof(int), cudaMemcpyDeviceToHost));
 	}
@@ -327,11 +336,22 @@ static int mat_csr_common(bsg_ctx *c, int n, const int *ia, const int *ja, const
 	BSG_CUDA(cudaMallocAsync(&d_ja, sizeof(int) * (nz > 0 ? nz : 1), s));
 	BSG_CUDA(cudaMallocAsync(&d_a, sizeof(double) * (nz > 0 ? nz : 1), s));
 	BSG_CUDA(cudaMemcpyAsync(d_ia, ia, sizeof(int) * (n + 1), kind, s));
-	if (nz > 0) {
+	int rc = BSG_OK;
+	// host input: the row pointers are checked before the columns are read
+	if (host) rc = bsg_check_csr_dev(c, n, nz, d_ia, nullptr, 0, 0);
+	if (!rc && host && nz > 0 && !ja) rc = bsg_set_error(BSG_ERR_ARG, "bad CSR: ja == NULL");
+	if (!rc && nz > 0) {
 		BSG_CUDA(cudaMemcpyAsync(d_ja, ja, sizeof(int) * nz, kind, s));
 		BSG_CUDA(cudaMemcpyAsync(d_a, a, sizeof(double) * nz, kind, s));
 	}
-	int rc;
+	if (!rc && host) rc = bsg_check_csr_dev(c, n, nz, d_ia, d_ja, 1, symm_upper);
+	if (rc) {
+		cudaFreeAsync(d_ia, s);
+		cudaFreeAsync(d_ja, s);
+		cudaFreeAsync(d_a, s);
+		delete m;
+		return rc;
+	}
 	if (symm_upper) {
 		rc = bsg_expand_symmetric(c, n, d_ia, d_ja, d_a, nz, &m->d_ia, &m->d_ja, &m->d_a, &m->nnz);
 		if (!rc) rc = mat_finish_point(m, d_ia, d_ja, d_a, nz, true);
@@ -465,62 +485,43 @@ extern "C" int bsg_mat_bsr(bsg_ctx *c, int nsup, int bs, const int *ia, const in
 		}
 		return bsg_mat_vbsr(c, nsup, sprnd.data(), ia, sja.data(), sa.data(), symm_upper, out);
 	}
-	int rc = check_csr_host(nsup, ia, ja, bs);
-	if (!rc && symm_upper) rc = check_upper_host(nsup, ia, ja);
-	if (rc) return rc;
+	// the O(1) checks here, the rest on device copies; the symmetric expansion
+	// and the row-major blocks on the device
+	if (nsup < 0 || !ia) return bsg_set_error(BSG_ERR_ARG, "bad CSR: n < 0 or ia == NULL");
+	if (ia[0] != 0) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia[0] != 0");
 	const int nz = ia[nsup];
-	// host: expand symmetric blocks (A(j,i) = A(i,j)^T) and go row-major
-	std::vector<int> fia, fja;
-	std::vector<double> fa;
-	if (symm_upper) {
-		std::vector<int> cnt(nsup + 1, 0);
-		for (int i = 0; i < nsup; i++)
-			for (int k = ia[i]; k < ia[i + 1]; k++) {
-				cnt[i + 1]++;
-				if (ja[k] != i) cnt[ja[k] + 1]++;
-			}
-		for (int i = 0; i < nsup; i++) cnt[i + 1] += cnt[i];
-		fia = cnt;
-		fja.resize(cnt[nsup]);
-		fa.resize((size_t)cnt[nsup] * 9);
-		std::vector<int> pos(cnt.begin(), cnt.end() - 1);
-		for (int i = 0; i < nsup; i++)
-			for (int k = ia[i]; k < ia[i + 1]; k++) {
-				int j = ja[k];
-				const double *blk = a + (size_t)k * 9; // column-major (r,c) at 3c+r
-				int p = pos[i]++;
-				fja[p] = j;
-				for (int r = 0; r < 3; r++)
-					for (int cc = 0; cc < 3; cc++) fa[(size_t)p * 9 + 3 * r + cc] = blk[3 * cc + r];
-				if (j != i) {
-					int q = pos[j]++;
-					fja[q] = i;
-					for (int r = 0; r < 3; r++)
-						for (int cc = 0; cc < 3; cc++) fa[(size_t)q * 9 + 3 * r + cc] = blk[3 * r + cc];
-				}
-			}
-	} else {
-		fia.assign(ia, ia + nsup + 1);
-		fja.assign(ja, ja + nz);
-		fa.resize((size_t)nz * 9);
-		for (int k = 0; k < nz; k++)
-			for (int r = 0; r < 3; r++)
-				for (int cc = 0; cc < 3; cc++) fa[(size_t)k * 9 + 3 * r + cc] = a[(size_t)k * 9 + 3 * cc + r];
-	}
-	bsg_mat *m = new (std::nothrow) bsg_mat();
-	if (!m) return bsg_set_error(BSG_ERR_NOMEM, "bsg_mat_bsr");
-	m->ctx = c;
-	m->n = nsup;
-	m->bs = 3;
-	m->symm = symm_upper ? 1 : 0;
-	m->nnz = (int)fja.size();
+	if (nz < 0) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia not monotone");
+	BSG_CUDA(cudaSetDevice(c->device));
 	cudaStream_t s = c->stream;
-	BSG_CUDA(cudaMallocAsync(&m->d_ia, sizeof(int) * (nsup + 1), s));
-	BSG_CUDA(cudaMallocAsync(&m->d_ja, sizeof(int) * (m->nnz > 0 ? m->nnz : 1), s));
-	BSG_CUDA(cudaMallocAsync(&m->d_a, sizeof(double) * 9 * (m->nnz > 0 ? m->nnz : 1), s));
-	BSG_CUDA(cudaMemcpyAsync(m->d_ia, fia.data(), sizeof(int) * (nsup + 1), cudaMemcpyHostToDevice, s));
-	BSG_CUDA(cudaMemcpyAsync(m->d_ja, fja.data(), sizeof(int) * m->nnz, cudaMemcpyHostToDevice, s));
-	BSG_CUDA(cudaMemcpyAsync(m->d_a, fa.data(), sizeof(double) * 9 * m->nnz, cudaMemcpyHostToDevice, s));
+	int *d_ia = nullptr, *d_ja = nullptr;
+	double *d_a = nullptr;
+	BSG_CUDA(cudaMallocAsync(&d_ia, sizeof(int) * (nsup + 1), s));
+	BSG_CUDA(cudaMallocAsync(&d_ja, sizeof(int) * (nz > 0 ? nz : 1), s));
+	BSG_CUDA(cudaMallocAsync(&d_a, sizeof(double) * 9 * (size_t)(nz > 0 ? nz : 1), s));
+	BSG_CUDA(cudaMemcpyAsync(d_ia, ia, sizeof(int) * (nsup + 1), cudaMemcpyHostToDevice, s));
+	int rc = bsg_check_csr_dev(c, nsup, nz, d_ia, nullptr, 0, 0);
+	if (!rc && nz > 0 && (!ja || !a)) rc = bsg_set_error(BSG_ERR_ARG, "bad CSR: ja == NULL");
+	if (!rc && nz > 0) {
+		BSG_CUDA(cudaMemcpyAsync(d_ja, ja, sizeof(int) * nz, cudaMemcpyHostToDevice, s));
+		BSG_CUDA(cudaMemcpyAsync(d_a, a, sizeof(double) * 9 * (size_t)nz, cudaMemcpyHostToDevice, s));
+	}
+	if (!rc) rc = bsg_check_csr_dev(c, nsup, nz, d_ia, d_ja, 1, symm_upper);
+	bsg_mat *m = rc ? nullptr : new (std::nothrow) bsg_mat();
+	if (!rc && !m) rc = bsg_set_error(BSG_ERR_NOMEM, "bsg_mat_bsr");
+	if (!rc) {
+		m->ctx = c;
+		m->n = nsup;
+		m->bs = 3;
+		m->symm = symm_upper ? 1 : 0;
+		rc = bsg_bsr3_from_input(c, nsup, d_ia, d_ja, d_a, nz, symm_upper, &m->d_ia, &m->d_ja, &m->d_a, &m->nnz);
+		if (!rc) d_ia = d_ja = nullptr, d_a = nullptr; // taken over or freed
+	}
+	for (void *q : {(void *)d_ia, (void *)d_ja, (void *)d_a})
+		if (q) cudaFreeAsync(q, s);
+	if (rc) {
+		if (m) bsg_mat_free(m);
+		return rc;
+	}
 	m->group = 32;
 	// the factorisations of a block matrix work on its point expansion: keep
 	// the point CombineLU split and its static contributor lists

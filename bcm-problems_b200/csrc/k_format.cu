@@ -325,3 +325,130 @@ int bsg_transpose_full(bsg_ctx *c, int n, const int *ia, const int *ja, const do
 	BSG_CUDA(cudaFreeAsync(vals, c->stream));
 	return BSG_OK;
 }
+
+// ---- validation of a CSR pattern copied to the device ----------------------
+// The checks of the host-buffer entry points, run where the arrays are:
+// res[0] gets bit 0 for a decreasing row pointer, bit 1 for a column out of
+// [0, n); res[1] / res[2] the first row that lacks its leading diagonal / has
+// an entry below it (upper storage).
+namespace {
+__global__ void k_csr_rows_ok(int n, const int *__restrict__ ia, int *res) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		if (ia[i + 1] < ia[i]) atomicOr(res, 1);
+}
+__global__ void k_csr_cols_ok(int n, int nz, const int *__restrict__ ia, const int *__restrict__ ja, int upper,
+                              int *res) {
+	const int t0 = blockIdx.x * blockDim.x + threadIdx.x, T = gridDim.x * blockDim.x;
+	for (int k = t0; k < nz; k += T) {
+		const int c = ja[k];
+		if (c < 0 || c >= n) atomicOr(res, 2);
+	}
+	if (upper)
+		for (int i = t0; i < n; i += T) {
+			const int a = ia[i], b = ia[i + 1];
+			if (a == b || ja[a] != i) atomicMin(res + 1, i);
+			for (int k = a; k < b; k++)
+				if (ja[k] < i) {
+					atomicMin(res + 2, i);
+					break;
+				}
+		}
+}
+} // namespace
+
+int bsg_check_csr_dev(bsg_ctx *c, int n, int nz, const int *d_ia, const int *d_ja, int stage, int upper) {
+	cudaStream_t s = c->stream;
+	int *d_res;
+	const int init[3] = {0, 0x7fffffff, 0x7fffffff};
+	BSG_CUDA(cudaMallocAsync(&d_res, sizeof(init), s));
+	BSG_CUDA(cudaMemcpyAsync(d_res, init, sizeof(init), cudaMemcpyHostToDevice, s));
+	BSG_COUNT(1);
+	const long long work = stage == 0 ? n : (nz > n ? nz : n);
+	const int g = (int)((work + 255) / 256 < BSG_SMS * 8 ? (work + 255) / 256 : BSG_SMS * 8);
+	if (stage == 0) k_csr_rows_ok<<<g > 0 ? g : 1, 256, 0, s>>>(n, d_ia, d_res);
+	else k_csr_cols_ok<<<g > 0 ? g : 1, 256, 0, s>>>(n, nz, d_ia, d_ja, upper, d_res);
+	int res[3];
+	const cudaError_t e = cudaMemcpyAsync(res, d_res, sizeof(res), cudaMemcpyDeviceToHost, s);
+	cudaStreamSynchronize(s);
+	cudaFreeAsync(d_res, s);
+	BSG_CUDA(e);
+	BSG_CUDA(cudaGetLastError());
+	if (res[0] & 1) return bsg_set_error(BSG_ERR_ARG, "bad CSR: ia not monotone");
+	if (res[0] & 2) return bsg_set_error(BSG_ERR_ARG, "bad CSR: column index out of range");
+	if (res[1] != 0x7fffffff && res[1] <= res[2])
+		return bsg_set_error(BSG_ERR_ARG, "symmetric input: every row must start with its diagonal");
+	if (res[2] != 0x7fffffff) return bsg_set_error(BSG_ERR_ARG, "symmetric input: entry below the diagonal");
+	return BSG_OK;
+}
+
+// ---- 3x3 block CSR from column-major input blocks ---------------------------
+namespace {
+__global__ void k_iota_d(int n, double *v) {
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) v[k] = (double)k;
+}
+// block k transposed in place: column-major (r, c) at 3 c + r to row-major
+__global__ void k_bsr3_rowmajor(int nz, double *a) {
+	for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nz; k += (long long)gridDim.x * blockDim.x) {
+		double *b = a + 9 * k;
+		const double t1 = b[1], t2 = b[2], t5 = b[5];
+		b[1] = b[3];
+		b[2] = b[6];
+		b[5] = b[7];
+		b[3] = t1;
+		b[6] = t2;
+		b[7] = t5;
+	}
+}
+// full block row i from the upper input: A(i, j) = A_up(i, j) (j >= i), or
+// A_up(j, i)^T (j < i); src[p] is the input block of entry p
+__global__ void k_bsr3_fill_sym(int nb, const int *__restrict__ fia, const int *__restrict__ fja,
+                                const double *__restrict__ src, const double *__restrict__ in, double *__restrict__ out) {
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+		for (int p = fia[i]; p < fia[i + 1]; p++) {
+			const double *b = in + 9 * (long long)src[p];
+			double *o = out + 9 * (long long)p;
+			if (fja[p] >= i)
+				for (int r = 0; r < 3; r++)
+					for (int c = 0; c < 3; c++) o[3 * r + c] = b[3 * c + r];
+			else
+				for (int w = 0; w < 9; w++) o[w] = b[w];
+		}
+}
+} // namespace
+
+// Device 3x3 block CSR (blocks row-major) from device input with column-major
+// blocks: as given (blocks transposed in place; ia, ja and a are taken over:
+// *ia_o = ia, *ja_o = ja, *a_o = a), or (upper) expanded to both triangles
+// with columns ascending in every row (*ia_o, *ja_o, *a_o allocated; ia, ja
+// and a freed).  On failure the inputs stay the caller's.
+int bsg_bsr3_from_input(bsg_ctx *c, int nb, int *ia, int *ja, double *a, int nz, int upper, int **ia_o, int **ja_o,
+                        double **a_o, int *nnz_o) {
+	cudaStream_t s = c->stream;
+	const int cap = BSG_SMS * 8;
+	if (!upper) {
+		BSG_COUNT(1);
+		k_bsr3_rowmajor<<<nblk(nz, 256) < cap ? nblk(nz, 256) : cap, 256, 0, s>>>(nz, a);
+		BSG_CUDA(cudaGetLastError());
+		*ia_o = ia;
+		*ja_o = ja;
+		*a_o = a;
+		*nnz_o = nz;
+		return BSG_OK;
+	}
+	double *idx, *src;
+	BSG_CUDA(cudaMallocAsync(&idx, sizeof(double) * (nz > 0 ? nz : 1), s));
+	BSG_COUNT(1);
+	k_iota_d<<<nblk(nz, 256) < cap ? nblk(nz, 256) : cap, 256, 0, s>>>(nz, idx);
+	int rc = bsg_expand_symmetric(c, nb, ia, ja, idx, nz, ia_o, ja_o, &src, nnz_o);
+	cudaFreeAsync(idx, s);
+	if (rc) return rc;
+	BSG_CUDA(cudaMallocAsync(a_o, sizeof(double) * 9 * (size_t)(*nnz_o > 0 ? *nnz_o : 1), s));
+	BSG_COUNT(1);
+	k_bsr3_fill_sym<<<nblk(nb, 256), 256, 0, s>>>(nb, *ia_o, *ja_o, src, a, *a_o);
+	cudaFreeAsync(src, s);
+	cudaFreeAsync(ia, s);
+	cudaFreeAsync(ja, s);
+	cudaFreeAsync(a, s);
+	BSG_CUDA(cudaGetLastError());
+	return BSG_OK;
+}

@@ -369,13 +369,35 @@ def test_nonpositive_pivot_reports_reference_error(ctx):
 
 
 def test_bad_csr_rejected(ctx):
+    """Host-buffer input is checked (on device copies) with the messages and
+    in the order of the checks: row pointers, then columns, then the upper
+    storage rule, the first failing row deciding between its two messages."""
     import bsg
-    with pytest.raises(bsg.BsgError) as e:
-        bsg.Matrix(ctx, 2, np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32), np.ones(2))
-    assert e.value.code == bsg.ERR_ARG
-    with pytest.raises(bsg.BsgError) as e:
-        bsg.Matrix(ctx, 2, np.array([0, 1, 2], np.int32), np.array([0, 5], np.int32), np.ones(2))
-    assert e.value.code == bsg.ERR_ARG
+
+    def bad(n, ia, ja, upper=False, bs=1):
+        with pytest.raises(bsg.BsgError) as e:
+            bsg.Matrix(ctx, n, np.array(ia, np.int32), np.array(ja, np.int32), np.ones(bs * bs * len(ja)), bs=bs,
+                       symm_upper=upper)
+        assert e.value.code == bsg.ERR_ARG
+        return str(e.value)
+
+    assert "ia not monotone" in bad(2, [0, 2, 1], [0, 1])
+    assert "ia not monotone" in bad(2, [0, 1, -1], [0])
+    assert "ia[0] != 0" in bad(2, [1, 2, 3], [0, 1])
+    assert "out of range" in bad(2, [0, 1, 2], [0, 5])
+    assert "out of range" in bad(3, [0, 1, 2, 3], [0, 7, 1], upper=True)  # before the upper rule
+    assert "start with its diagonal" in bad(2, [0, 1, 2], [1, 1], upper=True)
+    assert "below the diagonal" in bad(2, [0, 1, 3], [0, 1, 0], upper=True)
+    # the first failing row decides: row 1 below / row 2 without its diagonal
+    assert "below the diagonal" in bad(3, [0, 1, 3, 4], [0, 1, 0, 1], upper=True)
+    assert "start with its diagonal" in bad(3, [0, 1, 2, 4], [0, 2, 2, 1], upper=True)
+    # 3x3 blocks: the same checks on the block pattern
+    assert "ia not monotone" in bad(2, [0, 2, 1], [0, 1], bs=3)
+    assert "out of range" in bad(2, [0, 1, 2], [0, 2], bs=3)
+    assert "start with its diagonal" in bad(2, [0, 2, 3], [1, 0, 1], upper=True, bs=3)
+    # the context stays usable
+    m = bsg.Matrix(ctx, 2, np.array([0, 1, 2], np.int32), np.array([0, 1], np.int32), np.ones(2), symm_upper=True)
+    assert m.info()[0] == 2
 
 
 @pytest.mark.parametrize("precision,trisolve", [(0, 0), (1, 1)])
