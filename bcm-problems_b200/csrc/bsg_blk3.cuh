@@ -30,7 +30,7 @@ __device__ void svd3(const double *a, double *u, double *s, double *v) {
 		vw[k] = (k % 4) == 0 ? 1.0 : 0.0;
 	}
 	for (int sweep = 0; sweep < 30; sweep++) {
-		double off = 0.0;
+		double off2 = 0.0; // largest ga^2 / (al be) of the sweep
 		for (int pq = 0; pq < 3; pq++) {
 			const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
 			double al = 0.0, be = 0.0, ga = 0.0;
@@ -39,9 +39,11 @@ __device__ void svd3(const double *a, double *u, double *s, double *v) {
 				be += w[r + 3 * q] * w[r + 3 * q];
 				ga += w[r + 3 * p] * w[r + 3 * q];
 			}
-			const double nrm = sqrt(al * be);
-			if (nrm == 0.0 || fabs(ga) <= 1e-16 * nrm) continue;
-			off = fmax(off, fabs(ga) / nrm);
+			// columns already orthogonal to 1e-16 relative: no rotation (the
+			// test on squares keeps a square root and a division off the chain)
+			const double ab = al * be, g2 = ga * ga;
+			if (ab == 0.0 || g2 <= 1e-32 * ab) continue;
+			off2 = fmax(off2, g2 / ab);
 			const double zeta = (be - al) / (2.0 * ga);
 			const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
 			const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
@@ -54,7 +56,7 @@ __device__ void svd3(const double *a, double *u, double *s, double *v) {
 				vw[r + 3 * q] = sn * vp + cs * vq;
 			}
 		}
-		if (off <= 1e-15) break;
+		if (off2 <= 1e-30) break;
 	}
 	double sv[3];
 	for (int c = 0; c < 3; c++) sv[c] = sqrt(w[3 * c] * w[3 * c] + w[1 + 3 * c] * w[1 + 3 * c] + w[2 + 3 * c] * w[2 + 3 * c]);

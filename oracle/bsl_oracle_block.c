@@ -111,7 +111,7 @@ static void svd3_jacobi(const double *a, double *s, double *u, double *vt) {
 		vw[k] = (k % 4) == 0 ? 1.0 : 0.0;
 	}
 	for (int sweep = 0; sweep < 30; sweep++) {
-		double off = 0.0;
+		double off2 = 0.0; /* largest ga^2 / (al be) of the sweep */
 		for (int pq = 0; pq < 3; pq++) {
 			const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
 			double al = 0.0, be = 0.0, ga = 0.0;
@@ -120,9 +120,9 @@ static void svd3_jacobi(const double *a, double *s, double *u, double *vt) {
 				be += w[r + 3 * q] * w[r + 3 * q];
 				ga += w[r + 3 * p] * w[r + 3 * q];
 			}
-			const double nrm = sqrt(al * be);
-			if (nrm == 0.0 || fabs(ga) <= 1e-16 * nrm) continue;
-			if (fabs(ga) / nrm > off) off = fabs(ga) / nrm;
+			const double ab = al * be, g2 = ga * ga;
+			if (ab == 0.0 || g2 <= 1e-32 * ab) continue;
+			if (g2 / ab > off2) off2 = g2 / ab;
 			const double zeta = (be - al) / (2.0 * ga);
 			const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
 			const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
@@ -135,7 +135,7 @@ static void svd3_jacobi(const double *a, double *s, double *u, double *vt) {
 				vw[r + 3 * q] = sn * vp + cs * vq;
 			}
 		}
-		if (off <= 1e-15) break;
+		if (off2 <= 1e-30) break;
 	}
 	double sv[3];
 	for (int c = 0; c < 3; c++) sv[c] = sqrt(w[3 * c] * w[3 * c] + w[1 + 3 * c] * w[1 + 3 * c] + w[2 + 3 * c] * w[2 + 3 * c]);
