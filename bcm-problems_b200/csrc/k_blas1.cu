@@ -77,30 +77,58 @@ __global__ void __launch_bounds__(RED_THREADS) k_mdot(int n, const double *V, lo
 	double v[K];
 #pragma unroll
 	for (int j = 0; j < K; j++) v[j] = 0.0;
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-		double wi = w[i];
+	// U grid-stride steps a round (more for fewer vectors), all their loads
+	// issued before the products, which keep the order of the plain loop
+	constexpr int U = K <= 2 ? 4 : 2;
+	const int T = gridDim.x * blockDim.x;
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	for (; (long long)i + (U - 1) * T < n; i += U * T) {
+		double a[U][K], wu[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			wu[u] = w[i + u * T];
+#pragma unroll
+			for (int j = 0; j < K; j++) a[u][j] = V[j * ld + i + u * T];
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++)
+#pragma unroll
+			for (int j = 0; j < K; j++) v[j] = fma(a[u][j], wu[u], v[j]);
+	}
+	for (; i < n; i += T) {
+		const double wi = w[i];
 #pragma unroll
 		for (int j = 0; j < K; j++) v[j] = fma(V[j * ld + i], wi, v[j]);
 	}
 	finish_reduction<K>(v, partials, counter, out, sh);
 }
 
+// s + sum_j c_j V_j[i] (c_j = -h_j when SUB), in the order j = 0, 1, ..;
+// four vectors' loads are issued before their products
+template <bool SUB>
+__device__ __forceinline__ double comb(double s, const double *V, long long ld, int k, const double *h, int i) {
+	int j = 0;
+	for (; j + 4 <= k; j += 4) {
+		double a[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++) a[q] = V[(j + q) * ld + i];
+#pragma unroll
+		for (int q = 0; q < 4; q++) s = fma(SUB ? -h[j + q] : h[j + q], a[q], s);
+	}
+	for (; j < k; j++) s = fma(SUB ? -h[j] : h[j], V[j * ld + i], s);
+	return s;
+}
+
 // w -= V h  (h on the device, k vectors)
 __global__ void k_gemv_sub(int n, const double *V, long long ld, int k, const double *h, double *w) {
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-		double s = w[i];
-		for (int j = 0; j < k; j++) s = fma(-h[j], V[j * ld + i], s);
-		w[i] = s;
-	}
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		w[i] = comb<true>(w[i], V, ld, k, h, i);
 }
 
 // x += V y (y on device)
 __global__ void k_gemv_add(int n, const double *V, long long ld, int k, const double *y, double *x) {
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-		double s = x[i];
-		for (int j = 0; j < k; j++) s = fma(y[j], V[j * ld + i], s);
-		x[i] = s;
-	}
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		x[i] = comb<false>(x[i], V, ld, k, y, i);
 }
 
 // y = x * scale, scale = num / den with num/den on the device (den <= 0 -> 0)
