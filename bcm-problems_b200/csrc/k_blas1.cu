@@ -61,7 +61,28 @@ __global__ void __launch_bounds__(RED_THREADS) k_dots(int n, const double *x0, c
                                                       double *partials, unsigned int *counter, double *out) {
 	__shared__ double sh[32];
 	double v[3] = {0.0, 0.0, 0.0};
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+	// four grid-stride steps a round, their loads issued before the products
+	// (which keep the order of the plain loop)
+	constexpr int U = 4;
+	const int T = gridDim.x * blockDim.x;
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	for (; (long long)i + (U - 1) * T < n; i += U * T) {
+		double a[3][U], b[3][U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			a[0][u] = x0[i + u * T];
+			b[0][u] = y0[i + u * T];
+			if (Q > 1) a[1][u] = x1[i + u * T], b[1][u] = y1[i + u * T];
+			if (Q > 2) a[2][u] = x2[i + u * T], b[2][u] = y2[i + u * T];
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			v[0] = fma(a[0][u], b[0][u], v[0]);
+			if (Q > 1) v[1] = fma(a[1][u], b[1][u], v[1]);
+			if (Q > 2) v[2] = fma(a[2][u], b[2][u], v[2]);
+		}
+	}
+	for (; i < n; i += T) {
 		v[0] = fma(x0[i], y0[i], v[0]);
 		if (Q > 1) v[1] = fma(x1[i], y1[i], v[1]);
 		if (Q > 2) v[2] = fma(x2[i], y2[i], v[2]);
@@ -152,7 +173,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_maxabs(int n, const double *x, 
 	__shared__ double sh[32];
 	__shared__ bool last;
 	double v = 0.0;
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v = fmax(v, fabs(x[i]));
+	{
+		const int T = gridDim.x * blockDim.x;
+		int i = blockIdx.x * blockDim.x + threadIdx.x;
+		for (; (long long)i + 3 * T < n; i += 4 * T) {
+			const double a0 = x[i], a1 = x[i + T], a2 = x[i + 2 * T], a3 = x[i + 3 * T];
+			v = fmax(fmax(fmax(fmax(v, fabs(a0)), fabs(a1)), fabs(a2)), fabs(a3));
+		}
+		for (; i < n; i += T) v = fmax(v, fabs(x[i]));
+	}
 	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
 	const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 	if (l == 0) sh[w] = v;

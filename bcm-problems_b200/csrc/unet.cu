@@ -385,7 +385,20 @@ __global__ void k_correct(long long n, const double *yd, const double *s, double
 __global__ void k_red2(long long n, const double *r, const double *yd, const double *ay, double *part) {
 	__shared__ double sh[2][8];
 	double a = 0, b = 0;
-	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+	// four grid-stride steps a round, loads first, products in loop order
+	const long long T = (long long)gridDim.x * blockDim.x;
+	long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	for (; v + 3 * T < n; v += 4 * T) {
+		double rr[4], yy[4], aa[4];
+#pragma unroll
+		for (int u = 0; u < 4; u++) rr[u] = r[v + u * T], yy[u] = yd[v + u * T], aa[u] = ay[v + u * T];
+#pragma unroll
+		for (int u = 0; u < 4; u++) {
+			a = fma(rr[u], yy[u], a);
+			b = fma(yy[u], aa[u], b);
+		}
+	}
+	for (; v < n; v += T) {
 		a = fma(r[v], yd[v], a);
 		b = fma(yd[v], ay[v], b);
 	}
@@ -439,8 +452,17 @@ __global__ void k_sub(long long n, const double *v, const double *t, double *r) 
 __global__ void k_sumsq_part(long long n, const double *x, double *part) {
 	__shared__ double sh[8];
 	double s = 0;
-	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-		s = fma(x[i], x[i], s);
+	// four grid-stride steps a round, loads first, products in loop order
+	const long long T = (long long)gridDim.x * blockDim.x;
+	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	for (; i + 3 * T < n; i += 4 * T) {
+		double xx[4];
+#pragma unroll
+		for (int u = 0; u < 4; u++) xx[u] = x[i + u * T];
+#pragma unroll
+		for (int u = 0; u < 4; u++) s = fma(xx[u], xx[u], s);
+	}
+	for (; i < n; i += T) s = fma(x[i], x[i], s);
 	s = warp_sum(s);
 	if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
 	__syncthreads();
