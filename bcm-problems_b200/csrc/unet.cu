@@ -319,20 +319,34 @@ __global__ void __launch_bounds__(256) k_conv3t(ConvArgs a) {
 }
 
 // 2x2x2 mean, bf16 in / out (dims of the input).
+// A thread takes 8 channels of one output voxel (16-byte loads and store; C
+// is a multiple of 8); each channel sums its 8 inputs in the order k = 0..7.
 __global__ void k_pool(int nz, int ny, int nx, int C, const bf16 *in, bf16 *out) {
-	const int oz = nz / 2, oy = ny / 2, ox = nx / 2;
-	const long long n = (long long)oz * oy * ox * C;
+	const int oz = nz / 2, oy = ny / 2, ox = nx / 2, G = C / 8;
+	const long long n = (long long)oz * oy * ox * G;
 	for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-		const int c = (int)(e % C);
-		const long long v = e / C;
+		const int c0 = 8 * (int)(e % G);
+		const long long v = e / G;
 		const int x = (int)(v % ox), y = (int)((v / ox) % oy), z = (int)(v / ((long long)ox * oy));
-		float s = 0.f;
+		uint4 q[8];
 #pragma unroll
 		for (int k = 0; k < 8; k++) {
 			const long long u = ((long long)(2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
-			s += __bfloat162float(in[u * C + c]);
+			q[k] = __ldg(reinterpret_cast<const uint4 *>(in + u * C + c0));
 		}
-		out[e] = __float2bfloat16_rn(s * 0.125f);
+		float s[8];
+#pragma unroll
+		for (int c = 0; c < 8; c++) s[c] = 0.f;
+#pragma unroll
+		for (int k = 0; k < 8; k++) {
+			const bf16 *h = reinterpret_cast<const bf16 *>(&q[k]);
+#pragma unroll
+			for (int c = 0; c < 8; c++) s[c] += __bfloat162float(h[c]);
+		}
+		__align__(16) bf16 o[8];
+#pragma unroll
+		for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(s[c] * 0.125f);
+		*reinterpret_cast<uint4 *>(out + v * C + c0) = *reinterpret_cast<const uint4 *>(o);
 	}
 }
 
@@ -355,9 +369,12 @@ __global__ void k_input(long long n, const double *r, const double *nrm2, const 
 // y = w7 . d0 per voxel (FP32).
 __global__ void k_head(long long n, const bf16 *d0, const float *w7, float *y) {
 	for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+		const uint4 *p = reinterpret_cast<const uint4 *>(d0 + v * 16);
+		const uint4 q[2] = {__ldg(p), __ldg(p + 1)};
+		const bf16 *h = reinterpret_cast<const bf16 *>(q);
 		float s = 0.f;
 #pragma unroll
-		for (int c = 0; c < 16; c++) s = fmaf(w7[c], __bfloat162float(d0[v * 16 + c]), s);
+		for (int c = 0; c < 16; c++) s = fmaf(w7[c], __bfloat162float(h[c]), s);
 		y[v] = s;
 	}
 }
@@ -1280,7 +1297,7 @@ int wgrad_launch(bsg_unet *u, int lvl, const bf16 *A, int Ca, int upA, const bf1
 
 int pool_launch(bsg_unet *u, int lvl, int C, const bf16 *in, bf16 *out) {
 	BSG_COUNT(1);
-	k_pool<<<ew(u->nv[lvl + 1] * C), 256, 0, u->ctx->stream>>>(u->nz >> lvl, u->ny >> lvl, u->nx >> lvl, C, in, out);
+	k_pool<<<ew(u->nv[lvl + 1] * (C / 8)), 256, 0, u->ctx->stream>>>(u->nz >> lvl, u->ny >> lvl, u->nx >> lvl, C, in, out);
 	BSG_CUDA(cudaGetLastError());
 	return BSG_OK;
 }
