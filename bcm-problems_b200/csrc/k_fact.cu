@@ -439,14 +439,27 @@ __device__ int promote(const FactArgs &A, int m) {
 	}
 }
 
+// Rows queued and not yet taken by a warp (negative: warps wait for rows).
+__device__ __forceinline__ long long q_backlog(const FactArgs &A) {
+	return (long long)(*(volatile unsigned long long *)A.qtail - *(volatile unsigned long long *)A.qhead);
+}
+
 // Hold row i (lane 0) for member m that no warp computes right now (m is
 // queued, or parked on a member of its own): spin until m is finished, for
 // at most HOLD_NS, instead of parking, which would recompute row i from the
 // start once m finishes.  At most hold_max warps hold at once, so the other
-// half keep serving the queue and m is computed without this warp.  1: m
-// finished; 0: the caller parks; -1: another warp failed.
+// half keep serving the queue and m is computed without this warp.  A warp
+// holds only while no more than HOLD_BACKLOG queued rows wait for a warp:
+// with rows waiting, m is taken late and this warp does better on one of
+// them (many independent problems keep the queue long; a chain-limited front
+// keeps it empty).  1: m finished; 0: the caller parks; -1: another warp
+// failed.
 #define HOLD_NS 1000000ull
+#ifndef HOLD_BACKLOG
+#define HOLD_BACKLOG 0
+#endif
 __device__ int hold_for(const FactArgs &A, int m) {
+	if (q_backlog(A) > HOLD_BACKLOG) return 0;
 	if (atomicAdd(A.nhold, 1) >= A.hold_max) {
 		atomicSub(A.nhold, 1);
 		return 0;
@@ -457,7 +470,7 @@ __device__ int hold_for(const FactArgs &A, int m) {
 		if (ld_acquire_u64(A.rec + m) & REC_DONE) { res = 1; break; }
 		if ((it & 15) == 15) {
 			if (*(volatile int *)&A.st->code != 0) { res = -1; break; }
-			if (globaltimer_ns() - t0 > HOLD_NS) break;
+			if (globaltimer_ns() - t0 > HOLD_NS || q_backlog(A) > HOLD_BACKLOG) break;
 		}
 		__nanosleep(128);
 	}
