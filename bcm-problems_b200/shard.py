@@ -66,13 +66,18 @@ def local_system(system, segs):
                     np.concatenate(rhs, axis=1), np.asarray(offs, dtype=np.int64), system.info)
 
 
-def gpu_batch_solver(ctx, param_kw):
-    """The solver of a rank's share on its GPU: IC2 + batched PCG."""
+def gpu_batch_solver(ctx, param_kw, upper_input=False):
+    """The solver of a rank's share on its GPU: IC2 + batched PCG.  With
+    upper_input the share is already stored as its upper triangle (the
+    symmetric solve's input format), else it is taken from full storage."""
     def solve(sysm):
         import torch
         import bsg
         p = bsg.default_param(**param_kw)
-        m = bsg.Matrix.from_system(ctx, sysm, symm_upper=True)
+        if upper_input:
+            m = bsg.Matrix(ctx, sysm.n, sysm.ia, sysm.ja, sysm.a, sysm.bs, symm_upper=True)
+        else:
+            m = bsg.Matrix.from_system(ctx, sysm, symm_upper=True)
         f = bsg.Factor(ctx, m, "ich2", p)
         B = torch.as_tensor(np.ascontiguousarray(sysm.rhs[:1]), device="cuda")
         X = torch.zeros_like(B)
