@@ -480,3 +480,29 @@ def test_transposed_solves_are_adjoint(ctx, oracle, heat, precision, mode):
         f.solve_lt(_t(x), out, mode=0)
         ref = oracle.solve_u(iu, ju, l, x)
         assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_time_kernel_kinds(ctx):
+    """bsg_time_kernel, the benchmark's event timer: the point and block
+    products (kind 0), the product of several vectors (kind 3, 1..64 of them)
+    and a sweep of a factor (kind 2); bad kinds and vector counts are refused."""
+    import ctypes as C
+    import bsg
+    L = bsg.lib()
+    tk = L.bsg_time_kernel
+    tk.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    s = P.lame3d(5, 0.3, 1.0, 7)
+    mb = bsg.Matrix.from_system(ctx, s)
+    h = P.heat3d(10, 9, 8, sigma=1.0, seed=13)
+    mp = bsg.Matrix.from_system(ctx, h, symm_upper=True)
+    f = bsg.Factor(ctx, mp, "ich2", bsg.default_param(ordtype=0, fcttyp=2, tau1=1e-3, tau2=1e-3, precision=1))
+    t = C.c_double()
+    for m in (mb, mp):
+        assert tk(ctx.h, 0, m.h, None, 0, 0, 3, C.byref(t)) == bsg.OK and t.value > 0
+        for nv in (1, 6, 64):
+            assert tk(ctx.h, 3, m.h, None, 0, nv, 3, C.byref(t)) == bsg.OK and t.value > 0
+        for nv in (0, 65):
+            assert tk(ctx.h, 3, m.h, None, 0, nv, 3, C.byref(t)) == bsg.ERR_ARG
+    assert tk(ctx.h, 2, None, f.h, 1, 1, 3, C.byref(t)) == bsg.OK and t.value > 0
+    assert tk(ctx.h, 4, mb.h, None, 0, 1, 3, C.byref(t)) == bsg.ERR_ARG
+    assert tk(ctx.h, 3, None, None, 0, 1, 3, C.byref(t)) == bsg.ERR_ARG
